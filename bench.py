@@ -1,0 +1,384 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 cull + meshlet-DAG LOD cut: views/s of the batched launch on the ruins-like scene.
+
+One step = one pass of the hot path over one batch of synthetic input: the 32 poses of the ruins-like scene's
+camera spline (113,106 instances of 40 meshes, 1920 x 1080, errorThreshold 1 px, HZB occlusion from each pose's
+1920 x 1080 occluder depth image): 32 HZB builds plus one batched cut (CUDA graph) of the 32 views.
+
+Printed (one JSON line on rank 0): views/s with inputs resident in HBM (`value`), the same metric end to end
+through the public C ABI with host buffers (`e2e`: depth images + views in, draw lists + counters out), the plain
+per-view launch beside it, per-view latency percentiles, the roofline of the dominant kernel, the CPU baseline
+(the oracle's double restatement of the reference path on the host cores) and sampled SM clocks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config ruins|plain_small]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "three-virtual-geometry_b200"))
+
+METRIC = "views/sec & p99 ms: served batched cull+LOD cut vs plain per-view, same B200"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="ruins", choices=["ruins", "plain_small"])
+    ap.add_argument("--poses", type=int, default=32, help="views per step (the spline's pose count)")
+    ap.add_argument("--profile-case", action="store_true", help="small case for an ncu capture (not a bench line)")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bound of the CPU-baseline sample")
+    return ap.parse_args()
+
+
+def read_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def read_traffic(kernel: str):
+    """dram read+write bytes per launch from the committed ncu summary of `kernel`, scaled to the full launch."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}.md")
+    try:
+        text = open(path).read()
+    except OSError:
+        return None
+    m = re.search(r"dram_bytes_per_full_launch\s*=\s*([0-9.eE+]+)", text)
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, n in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def build_scene(config: str, poses: int):
+    from vgcut import scenes
+    threads = os.cpu_count() or 8
+    if config == "plain_small":
+        return scenes.plain_small(threads=threads), dict(workload="plain_small: 1,048,820-triangle icosphere x 64 instances, 1080p, 1 view, t=1px")
+    spec = scenes.ruins(poses=poses, threads=threads)
+    return spec, dict(workload=f"ruins-like: {spec.instance_count} instances of {len(spec.meshes)} meshes "
+                               f"({spec.notes['meshlets']} meshlets, {spec.full_detail_triangles / 1e9:.2f}B full-detail "
+                               f"triangles), 1920x1080, {len(spec.cameras)} spline poses per step, t=1px, HZB 1920x1080")
+
+
+# ------------------------------------------------------------------ CPU baseline (the oracle, double precision)
+def cpu_baseline(spec, seconds: float, occlusion: bool):
+    """Times the oracle's double restatement of the reference path (cells, instances, meshlets, prefix, HZB) on
+    the host cores over a bounded sample of the step's views; returns (views/s, cores, sample description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from vgcut import engine
+    flags = [dict(occlusion=occlusion) for _ in spec.meshes]
+    scene, _, _ = O.scene_from_spec(spec.meshes, spec.instances, flags)
+    cores = os.cpu_count() or 1
+    done, t0 = 0, time.perf_counter()
+    selected = 0
+    while True:
+        k = done % len(spec.cameras)
+        hzb = O.hzb_build(spec.depth_images[k]) if (occlusion and spec.depth_images) else None
+        v = O.make_view(spec.cameras[k], engine.ViewParams(error_threshold=1.0), 1 << 20, (30_000_000, 12_000_000), hzb=hzb)
+        r = O.cull_pass(scene, v, "f64", threads=cores, capacity=1 << 18)
+        selected += r["counters"][2]
+        done += 1
+        if time.perf_counter() - t0 >= seconds or done >= 4 * len(spec.cameras):
+            break
+    dt = time.perf_counter() - t0
+    return done / dt, cores, f"{done} views of the same workload (oracle f64 full pass incl. HZB build, {cores} threads, {dt:.1f} s)"
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    spec, cfg = build_scene(args.config, args.poses)
+    occl = args.config == "ruins"
+    per_step = []
+    for _ in range(args.warmup):
+        cpu_baseline(spec, 0.0, occl)
+    views = 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        vps, cores, sample = cpu_baseline(spec, 0.0, occl)  # one view per step (bounded sample)
+        views += 1
+    dt = time.perf_counter() - t0
+    value = views / dt
+    cfg.update(dict(flush="n/a (host)", sample="1 view per step"))
+    line = dict(metric=METRIC, value=value, unit="views/s", n_gpus=args.gpus, steps=args.steps, warmup=args.warmup,
+                ms_per_step=dt / args.steps * 1e3, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
+                data="synthetic", config=cfg, impl="reference",
+                cpu_baseline=dict(value=value, unit="views/s", cores=cores, kind="port",
+                                  sample=f"1 view per step, {args.steps} steps: oracle f64 restatement of the reference "
+                                         f"passes (the TypeScript reference cannot run here)"),
+                e2e=dict(value=value, unit="views/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+    from vgcut import engine, scenes
+
+    torch.cuda.set_device(local)
+    spec, cfg = build_scene(args.config, args.poses)
+    P = len(spec.cameras)
+    occl = args.config == "ruins" and len(spec.depth_images) > 0
+    vg = engine.VirtualGeometry(max_triangles=10_000_000, max_shadow_triangles=4_000_000, max_meshlets=1 << 18,
+                                output_slots=P, device=local)
+    scenes.load_into(vg, spec, occlusion_culling=occl)
+    stream = torch.cuda.Stream()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    L = engine.lib()
+    d_depth = [torch.from_numpy(d).cuda() for d in spec.depth_images] if occl else []
+    h_depth = [torch.from_numpy(d).pin_memory() for d in spec.depth_images] if occl else []
+    views = [engine.make_view(c, engine.ViewParams(error_threshold=1.0, hzb=(k if occl else -1), state_slot=k))
+             for k, c in enumerate(spec.cameras)]
+    H, W = (spec.depth_images[0].shape if occl else (0, 0))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    def hzb_step(host: bool):
+        for k in range(P if occl else 0):
+            src = h_depth[k] if host else d_depth[k]
+            engine.check(L.vgc_hzb_build(vg.handle, k, src.data_ptr(), W, H, 0 if host else 1, sp))
+
+    def step_resident():
+        hzb_step(False)
+        vg.cut(views, first_slot=0, stream=sp, graph=True)
+
+    def timed(fn, steps):
+        out = []
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            out.append(a.elapsed_time(b))
+        return out
+
+    # warm-up (graph capture happens in the first step)
+    for _ in range(max(3, args.warmup)):
+        step_resident()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        t_wall = time.perf_counter()
+        step_ms = timed(step_resident, args.steps)
+        t_wall = time.perf_counter() - t_wall
+    torch.cuda.synchronize()
+    barrier(world)
+    total_ms = max_over_ranks(sum(step_ms), world)
+    value = world * P * args.steps / (total_ms / 1e3)
+
+    # per-view work counters of the last step (algorithmic bytes of the dominant kernel)
+    st = [vg.read_stats(k) for k in range(P)]
+    b_select = 0.0
+    for s in st:
+        sel = s["selected"][0] + s["selected"][1]
+        b_select += (8 * s["visible_cells"] + 32 * s["levels_read"] + 64 * s["instances_tested"] +
+                     64 * s["meshlets_tested"] + 16 * s["fast_emitted"] + 16 * sel)
+    b_hzb = (4 * W * H + 4 * W * H * 4 / 3) * (P if occl else 0)  # read mip 0, write the whole chain
+
+    # plain per-view launches, timed per kernel kind on the launching stream
+    vg.set_profiling(True)
+    vg.kernel_times(reset=True)
+    plain_ms = []
+    for i in range(max(1, args.steps // 2)):
+        for k in range(P):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            if occl:
+                engine.check(L.vgc_hzb_build(vg.handle, k, d_depth[k].data_ptr(), W, H, 1, sp))
+            arr = (engine.View * 1)(views[k])
+            engine.check(L.vgc_cut(vg.handle, arr, 1, k, sp))
+            b.record(stream)
+            b.synchronize()
+            plain_ms.append(a.elapsed_time(b))
+    kt = vg.kernel_times(reset=True)
+    vg.set_profiling(False)
+    plain_vps = 1e3 / statistics.mean(plain_ms)
+    sel_ms, sel_n = kt["select0"]
+    select_avg_ms = sel_ms / max(1, sel_n)
+    # the plain path launches k_select once per view: bytes per launch = the per-view average
+    achieved_select = (b_select / P) / (select_avg_ms / 1e3) / 1e9
+    hzb_ms, hzb_n = kt["hzb"]
+    peak, peak_kind = read_peaks()
+    traffic = read_traffic("k_select")
+
+    # end to end through the C ABI with host buffers: depth images + views in, draw lists + counters out
+    rt = ctypes.CDLL("libcudart.so.12")
+    rt.cudaMemcpyAsync.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_void_p]
+    out0 = vg.output(0)
+    cw = engine.COUNTER_HEADER + out0.mesh_slots * 8
+    h_counters = torch.empty(P * cw, dtype=torch.int32).pin_memory()
+    cap = 1 << 18
+    h_lists = torch.empty((P, cap, 4), dtype=torch.int32).pin_memory()
+    outs = [vg.output(k) for k in range(P)]
+    d2h_bytes = [0]
+
+    def step_e2e():
+        hzb_step(True)
+        vg.cut(views, first_slot=0, stream=sp, graph=True)
+        rt.cudaMemcpyAsync(h_counters.data_ptr(), out0.counters, P * cw * 4, 2, sp)
+        stream.synchronize()
+        c = h_counters.numpy().reshape(P, cw)
+        nbytes = P * cw * 4
+        for k in range(P):
+            n = min(int(c[k, 2]), cap)
+            if n:
+                rt.cudaMemcpyAsync(h_lists[k].data_ptr(), outs[k].draw_list[0], n * 16, 2, sp)
+                nbytes += n * 16
+        d2h_bytes[0] = nbytes
+
+    for _ in range(2):
+        step_e2e()
+    torch.cuda.synchronize()
+    e2e_ms = timed(step_e2e, args.steps)
+    e2e_total = max_over_ranks(sum(e2e_ms), world)
+    e2e_vps = world * P * args.steps / (e2e_total / 1e3)
+    h2d_bytes = (P * W * H * 4 if occl else 0) + P * ctypes.sizeof(engine.View)
+
+    clk = clocks.summary()
+    cfg.update(dict(views_per_step=P, flush="256 MB L2 flush before every timed step (outside the events)",
+                    max_meshlets_per_cut=1 << 18, threshold_px=1.0, occlusion=occl))
+    lat = sorted(plain_ms)
+    line = dict(
+        metric=METRIC, value=value, unit="views/s", n_gpus=world, steps=args.steps, warmup=max(3, args.warmup),
+        ms_per_step=statistics.mean(step_ms), higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
+        data="synthetic (seeded ruins-like scene; the reference's WebGPU scenes cannot run here)", config=cfg,
+        batched_ms_per_view=statistics.mean(step_ms) / P,
+        plain_views_per_sec=plain_vps, batched_over_plain=value / world / plain_vps,
+        p50_ms=lat[len(lat) // 2], p99_ms=lat[min(len(lat) - 1, int(math.ceil(0.99 * len(lat))) - 1)],
+        latency_note="p50/p99: one view through the plain launch (HZB build + cut), CUDA events",
+        e2e=dict(value=e2e_vps, unit="views/s", h2d_bytes_per_step=int(h2d_bytes), d2h_bytes_per_step=int(d2h_bytes[0])),
+        roofline=dict(bound="hbm", achieved=achieved_select, peak=peak, unit="GB/s", frac=achieved_select / peak,
+                      traffic=traffic, kernel="k_select", peak_source=f"{peak_kind} hbm_gbs",
+                      algorithmic_bytes_per_launch=b_select / P, avg_launch_ms=select_avg_ms,
+                      note="algorithmic bytes = 8 Cvis + 32 L Cvis + 64 I + 64 M + 16 F + 16 S per view; the scene's "
+                           "bounds sit in L2, so algorithmic GB/s can exceed DRAM GB/s"),
+        kernels={k: dict(ms=v[0], launches=v[1]) for k, v in kt.items() if v[1]},
+        hzb_achieved_gbs=(b_hzb / P) / (hzb_ms / max(1, hzb_n) / 1e3) / 1e9 if (occl and hzb_n) else None,
+        gpu_launches=args.steps * ((2 if (occl and H * W > 0) else 0) * P + 8),
+        clocks=clk,
+    )
+    if rank == 0:
+        vps, cores, sample = cpu_baseline(spec, args.cpu_seconds, occl)
+        line["cpu_baseline"] = dict(value=vps, unit="views/s", cores=cores, kind="port", sample=sample)
+        print(json.dumps(line), flush=True)
+    for b in list(vg._batches.values()):
+        pass
+    vg.dispose()
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            barrier(world)
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,229 @@
+/*
+ * vgcut.h - C ABI of the sm_100a instance-culling + meshlet-DAG LOD-cut engine.
+ *
+ * Drop-in for the per-frame compute path of three-virtual-geometry: the passes GeometryPool.build() emits
+ * (src/core/runtime/GeometryPool.ts:568-1092, dispatched by VirtualGeometry.update() at
+ * src/core/runtime/VirtualGeometry.ts:484) and the HZB occlusion test (src/core/runtime/OcclusionCulling.ts:119-170).
+ * Inputs keep the reference's layout (VirtualMeshData, 16-float column-major instance matrices, the same levers);
+ * outputs are the same visible-cluster list (uvec4 per drawn meshlet) and drawIndexedIndirect args (5 u32 per
+ * cut, mesh slot and part), left in device memory like the reference's storage buffers.
+ *
+ * Conventions
+ *   - Every function returns vgc_status (0 = OK). On error, vgc_last_error() returns a message for this thread.
+ *   - Caller memory is copied at the call; nothing is retained. Device output pointers stay valid until the next
+ *     cut that writes the same output slot, or until the context is destroyed.
+ *   - One context per host thread for the plain API (a context is not thread-safe). `stream` may be 0 (the
+ *     context's own stream).
+ */
+#ifndef VGCUT_H
+#define VGCUT_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum vgc_status {
+  VGC_OK = 0,
+  VGC_INVALID_ARG = -1,
+  VGC_OOM = -2,
+  VGC_OVER_BUDGET = -3,  /* admission refused: the request would exceed the context's HBM budget */
+  VGC_TIMEOUT = -4,      /* a bounded wait ran out (host deadline or a device-side iteration limit) */
+  VGC_DEVICE_ERROR = -5,
+  VGC_NOT_FOUND = -6,
+} vgc_status;
+
+typedef struct vgc_context vgc_context;
+typedef struct vgc_batch vgc_batch;
+typedef void *vgc_stream; /* cudaStream_t */
+
+/* Per-context capacities. Reference: VirtualGeometryOptions (VirtualGeometry.ts:62-75) and PoolCapacity
+   (GeometryPool.ts:142-149); the 120 MB WebGPU binding cap does not exist here (one resident buffer set). */
+typedef struct vgc_options {
+  uint32_t max_triangles;        /* camera-cut index capacity per view, in triangles (reference default 10M) */
+  uint32_t max_shadow_triangles; /* shadow-cut index capacity per view (reference default 4M) */
+  uint32_t max_meshlets;         /* draw-list capacity per cut per view (reference default 1 << 20) */
+  uint32_t output_slots;         /* views whose outputs can be resident at once (batch width), default 1 */
+  int32_t device;                /* CUDA device ordinal */
+  uint64_t hbm_budget_bytes;     /* admission limit for this context's allocations; 0 = no limit */
+} vgc_options;
+
+/* The part of VirtualMeshData (buildVirtualMesh.ts:75-138) that the cut reads. */
+typedef struct vgc_mesh_data {
+  uint32_t meshlet_count;
+  const float *meshlet_bounds;       /* 16 floats per meshlet */
+  const uint32_t *meshlet_info;      /* 4 u32 per meshlet: triangleCount, firstIndex, lodLevel, vertexOffset */
+  uint32_t meshlet_triangle_count;
+  const uint32_t *meshlet_triangles; /* packed local triangles (for vgc_expand); may be NULL */
+  uint32_t level_count;
+  const uint32_t *level_ranges;      /* 2 per level */
+  const float *level_errors;         /* 2 per level */
+  const float *level_guard_errors;   /* 2 per level */
+  float lod_bounds_sphere[4];
+  float cull_bounds_sphere[4];
+  float bounding_sphere[4];
+} vgc_mesh_data;
+
+/* Per-mesh levers: VirtualMeshOptions (VirtualMesh.ts:39-62) and the mesh-table flags (GeometryPool.ts:449-477). */
+typedef struct vgc_mesh_opts {
+  float max_draw_distance;  /* world units; <= 0 or >= 1e30 = never culled by distance */
+  float min_pixel_radius;   /* combined with the view's (the larger wins) */
+  uint32_t enabled;         /* mesh.visible */
+  uint32_t shadow;          /* the shadow cut includes this mesh */
+  uint32_t occlusion;       /* occlusion culling may remove this mesh's instances and meshlets */
+} vgc_mesh_opts;
+
+/* One cut request: the uniforms VirtualGeometry.update() writes (VirtualGeometry.ts:414-442) and the levers
+   (:78-183). Matrices are column-major like three.js Matrix4.elements. */
+typedef struct vgc_view {
+  double view[16];              /* camera.matrixWorldInverse (rigid) */
+  double proj[16];              /* camera.projectionMatrix, [0, 1] depth (WebGPU coordinate system) */
+  double near_;                 /* camera.near */
+  double viewport_height;       /* drawing-buffer height in CSS pixels: projScale = proj[5] * height / 2 */
+  double error_threshold;       /* errorThreshold, pixels */
+  double lod_blend;             /* lodBlend (<= 1: off) */
+  double min_pixel_radius;      /* minPixelRadius */
+  double shadow_error_scale;    /* shadowErrorScale */
+  double max_error_threshold;   /* maxErrorThreshold (capacity controller limit) */
+  double shadow_sweep[3];       /* shadowSweep */
+  double triangle_budget;       /* triangleBudget: > 0 selects the threshold by device histogram search */
+  double threshold_range[2];    /* thresholdRange searched by the budget (reference default [0.5, 3]) */
+  uint32_t frustum_culling;     /* frustumCulling */
+  int32_t hzb;                  /* HZB slot for occlusion culling of the camera cut; -1 = off */
+  uint32_t state_slot;          /* capacity-controller state carried between frames of one camera */
+  uint32_t flags;               /* reserved, 0 */
+} vgc_view;
+
+/* Device pointers of one output slot. */
+typedef struct vgc_output {
+  const uint32_t *draw_list[2]; /* per cut: uvec4 (instance, meshlet, firstIndex in region, triCount|lo<<8|hi<<16) */
+  const uint32_t *draw_args;    /* ((cut * mesh_slots + slot) * 2 + part) * 5 u32: drawIndexedIndirect args */
+  const uint32_t *counters;     /* VGC_COUNTER_* words, then per (cut, slot, part) requested indices and region start */
+  uint32_t max_drawn;
+  uint32_t mesh_slots;
+} vgc_output;
+
+/* Counter words of an output slot (GeometryPool.ts:112-119, plus this engine's round bookkeeping). */
+enum {
+  VGC_COUNTER_CELLS = 0,
+  VGC_COUNTER_OCCLUDED = 1,
+  VGC_COUNTER_CUT0 = 2, /* + VGC_CUT_SELECTED.. for the camera cut */
+  VGC_COUNTER_CUT1 = 7, /* + VGC_CUT_SELECTED.. for the shadow cut */
+  VGC_COUNTER_REDO0 = 12,
+  VGC_COUNTER_REDO1 = 13,
+  VGC_COUNTER_ROUNDS = 14,
+  VGC_COUNTER_ERROR = 15,
+  VGC_COUNTER_INSTANCES_TESTED = 16, /* instances of visible cells (all rounds) */
+  VGC_COUNTER_MESHLETS_TESTED = 17,  /* meshlets run through the per-meshlet test (all rounds) */
+  VGC_COUNTER_FAST_EMITTED = 18,     /* meshlets emitted by the instance fast path (all rounds) */
+  VGC_COUNTER_LEVELS_READ = 19,      /* level-table entries read (sum over visible cells, all rounds) */
+  VGC_COUNTER_HEADER = 24,
+};
+enum { VGC_CUT_SELECTED = 0, VGC_CUT_DRAWN = 1, VGC_CUT_SURVIVED = 2, VGC_CUT_WORK = 3, VGC_CUT_REQUESTED = 4 };
+
+/* Stats of one output slot: VirtualGeometryStats (VirtualGeometry.ts:24-47) per view. */
+typedef struct vgc_stats {
+  uint32_t visible_cells;
+  uint32_t occluded_instances;
+  uint32_t selected[2], drawn[2], survived[2], work[2], requested_indices[2];
+  uint32_t rounds;
+  uint32_t overflow;            /* a cut exceeded its draw buffers after the last retry round */
+  float threshold_scale[2];     /* capacity controller scale per cut */
+  float fill[2];
+  float effective_threshold;    /* errorThreshold used (after a budget search) */
+  uint32_t instances_tested, meshlets_tested, fast_emitted, levels_read; /* work done, all rounds */
+} vgc_stats;
+
+const char *vgc_last_error(void);
+const char *vgc_version(void);
+
+/* ---------------------------------------------------------------- context and scene residency */
+void vgc_default_options(vgc_options *opts);
+/* new VirtualGeometry(options) (VirtualGeometry.ts:191-198) */
+int vgc_context_create(const vgc_options *opts, vgc_context **out);
+/* VirtualGeometry.dispose() */
+int vgc_context_destroy(vgc_context *ctx);
+/* Bytes of device memory this context holds. */
+int vgc_context_footprint(const vgc_context *ctx, uint64_t *bytes);
+
+/* vg.createMesh(data, material, {matrices}, options) (VirtualGeometry.ts:231, VirtualMesh.ts:159-233,
+   GeometryPool.add :302-355): copies the DAG and the instances (Morton-ordered on the host, GeometryPool.ts:1263)
+   into device memory and returns the mesh slot. gpu_to_input (optional, n entries) receives the Morton order. */
+int vgc_mesh_add(vgc_context *ctx, const vgc_mesh_data *data, const float *matrices, uint32_t instance_count,
+                 const vgc_mesh_opts *opts, uint32_t *slot, uint32_t *gpu_to_input);
+/* mesh.maxDrawDistance / minPixelRadius / visible / castShadow / occlusionCulling (GeometryPool.writeFlags :463-477) */
+int vgc_mesh_set_flags(vgc_context *ctx, uint32_t slot, const vgc_mesh_opts *opts);
+/* mesh.setMatrixAt + commitInstances (VirtualMesh.ts:305-314, GeometryPool.ts:499-512): `count` matrices for GPU
+   (Morton) indices [first, first + count) of the mesh; the cells they touch are recomputed. */
+int vgc_instances_update(vgc_context *ctx, uint32_t slot, uint32_t first, uint32_t count, const float *matrices);
+/* mesh.dispose() (GeometryPool.remove :358-363) */
+int vgc_mesh_remove(vgc_context *ctx, uint32_t slot);
+/* Highest used mesh slot + 1 and the slot capacity (mesh table size). */
+int vgc_mesh_slots(const vgc_context *ctx, uint32_t *used, uint32_t *capacity);
+
+/* ---------------------------------------------------------------- HZB (OcclusionCulling.ts:284-350) */
+/* Builds the max-reduced mip chain of a depth image (NDC depth, row 0 at the top) into HZB slot `hzb`.
+   depth_is_device: the pointer is device memory (else host memory, copied). The view's proj[] is used by the
+   test, so the image must come from the same projection. */
+int vgc_hzb_build(vgc_context *ctx, int32_t hzb, const float *depth, uint32_t width, uint32_t height,
+                  int depth_is_device, vgc_stream stream);
+
+/* ---------------------------------------------------------------- the cut */
+/* Plain per-view launch (the drop-in for renderer.compute(pool.computeNodes)): runs the cut for `count` views into
+   output slots [first_slot, first_slot + count) as a sequence of kernel launches on `stream`. Asynchronous. */
+int vgc_cut(vgc_context *ctx, const vgc_view *views, uint32_t count, uint32_t first_slot, vgc_stream stream);
+
+/* Batched launch: the same kernels for up to `max_views` views captured once into a CUDA graph, replayed with the
+   new views' constants. Output slots are [first_slot, first_slot + count). */
+int vgc_batch_create(vgc_context *ctx, uint32_t max_views, vgc_batch **out);
+int vgc_batch_run(vgc_batch *batch, const vgc_view *views, uint32_t count, uint32_t first_slot, vgc_stream stream);
+int vgc_batch_destroy(vgc_batch *batch);
+
+/* Layout of HZB slot `hzb`: levels, per-level offset (floats) / width / height (16 entries each), and the device
+   pointer of the mip chain (level i at data + offset[i], row-major). */
+int vgc_hzb_info(const vgc_context *ctx, int32_t hzb, uint32_t *levels, uint32_t *offset, uint32_t *width,
+                 uint32_t *height, const float **data);
+
+/* Device pointers of an output slot (valid after the cut's stream work completes). */
+int vgc_get_output(const vgc_context *ctx, uint32_t slot, vgc_output *out);
+/* vg.readStats (VirtualGeometry.ts:591-632) for one output slot; synchronises with `stream`. */
+int vgc_read_stats(vgc_context *ctx, uint32_t slot, vgc_stats *stats, vgc_stream stream);
+/* Copies an output slot's draw list of `cut` into host memory: up to `capacity` entries (4 u32 each); *count
+   receives the number of drawn entries. Synchronises with `stream`. */
+int vgc_read_draw_list(vgc_context *ctx, uint32_t slot, uint32_t cut, uint32_t *entries, uint32_t capacity,
+                       uint32_t *count, vgc_stream stream);
+/* Capacity-controller state words of a state slot (8 u32, fixed point x 10000): read or overwrite. */
+int vgc_state_access(vgc_context *ctx, uint32_t state_slot, uint32_t *words, int write, vgc_stream stream);
+
+/* Index expansion (GeometryPool.ts:998-1021): writes 3 indices per drawn triangle, (drawSlot << 7) | localVertex,
+   into `index_buffer` (device, capacity of the cut in indices) for output slot `slot` and cut `cut`. */
+int vgc_expand(vgc_context *ctx, uint32_t slot, uint32_t cut, uint32_t *index_buffer, uint64_t capacity,
+               vgc_stream stream);
+
+/* ---------------------------------------------------------------- CPU-API equivalents on the GPU */
+/* selectCut / selectBlendCut (cut.ts:26-77) for mesh `slot` under `count` view-model matrices, in one launch:
+   per view i, viewmodel16[i*16..], proj_scale[i], near_[i], scale[i]; lo/hi receive count * meshlet_count bytes
+   (hi == 0: not drawn; blend <= 1 gives the plain cut with lo = 0, hi = 255). Synchronous. */
+int vgc_select_cut(vgc_context *ctx, uint32_t slot, uint32_t count, const double *viewmodel16, const double *proj_scale,
+                   const double *near_, const double *scale, double threshold, double blend, uint8_t *lo, uint8_t *hi);
+
+/* ---------------------------------------------------------------- profiling (no counterpart in the reference) */
+enum { VGC_KERNEL_RESET = 0, VGC_KERNEL_CELLS = 1, VGC_KERNEL_SELECT0 = 2, VGC_KERNEL_SELECT_RETRY = 3,
+       VGC_KERNEL_FINISH = 4, VGC_KERNEL_HZB = 5, VGC_KERNEL_KINDS = 8 };
+/* With `enable`, the plain path (vgc_cut, vgc_hzb_build) records CUDA events around each of its kernel launches
+   on the launching stream. vgc_kernel_times synchronises and returns, per VGC_KERNEL_* kind, the summed device
+   milliseconds and the launch count since the last reset (reset = 1 clears them). */
+int vgc_set_profiling(vgc_context *ctx, int enable);
+int vgc_kernel_times(vgc_context *ctx, double *ms, uint32_t *launches, int reset);
+
+/* ---------------------------------------------------------------- test support (no counterpart in the reference) */
+/* Host copies of the resident cell records (8 floats: centre xyz, radius, max instance radius, slot, first instance,
+   count; GeometryPool.ts:544 layout) and of the Morton-ordered instance matrices (16 floats each). */
+int vgc_debug_scene(const vgc_context *ctx, float *cells, uint32_t cell_capacity, float *matrices,
+                    uint32_t matrix_capacity, uint32_t *cell_count, uint32_t *instance_count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,113 @@
+"""Shared helpers for comparing the GPU cut with the oracle (test infrastructure)."""
+from __future__ import annotations
+
+import numpy as np
+
+import oracle as O
+from vgcut import engine, scenes
+
+MARGIN = 1e-5  # relative margin of the parity contract: decisions closer than this to a threshold are reported
+
+
+def small_ruins(seed=3, meshes=6, instances=3000, extent=220.0, poses=6, tri_lo=2_000, tri_hi=30_000, quads=24,
+                width=960, height=540):
+    return scenes.ruins(seed=seed, mesh_count=meshes, tri_lo=tri_lo, tri_hi=tri_hi, instances=instances, extent=extent,
+                        poses=poses, width=width, height=height, target_full_detail=instances * 8_000, quads=quads)
+
+
+def d2h(ptr, count: int, dtype=np.uint32) -> np.ndarray:
+    """Copies `count` elements from a device pointer (cudaMemcpy through the CUDA runtime the engine loaded)."""
+    import ctypes
+    rt = ctypes.CDLL("libcudart.so.12")
+    out = np.zeros(count, dtype)
+    rc = rt.cudaMemcpy(out.ctypes.data_as(ctypes.c_void_p), ctypes.c_void_p(ptr), ctypes.c_size_t(out.nbytes), 2)
+    assert rc == 0, f"cudaMemcpy failed ({rc})"
+    return out
+
+
+def key_set(entries: np.ndarray, cols=(0, 1, 2)) -> set:
+    e = np.asarray(entries)
+    return set(map(tuple, e[:, list(cols)].tolist())) if len(e) else set()
+
+
+def check_index_tiling(entries: np.ndarray, inst_slot: np.ndarray, mesh_counts: np.ndarray, cut: int) -> None:
+    """firstIndex values of each (slot, part) tile [0, requested) exactly (atomic order is free, the packing is not)."""
+    e = np.asarray(entries)
+    if len(e) == 0:
+        return
+    part = np.where((e[:, 3] & 0xFFFF00) == (255 << 16), 0, 1)
+    slot = inst_slot[e[:, 0]]
+    tris = e[:, 3] & 255
+    for s in np.unique(slot):
+        for p in (0, 1):
+            m = (slot == s) & (part == p)
+            if not m.any():
+                continue
+            order = np.argsort(e[m, 2], kind="stable")
+            first = e[m, 2][order].astype(np.int64)
+            size = 3 * tris[m][order].astype(np.int64)
+            assert first[0] == 0
+            assert np.all(first[1:] == first[:-1] + size[:-1]), "index regions overlap or leave gaps"
+            assert first[-1] + size[-1] == mesh_counts[cut, s, p]
+
+
+class Harness:
+    """One scene resident on the GPU and in the oracle."""
+
+    def __init__(self, spec, flags=None, max_meshlets=1 << 16, max_triangles=2_000_000, max_shadow=1_000_000):
+        self.spec = spec
+        self.flags = flags or [{} for _ in spec.meshes]
+        self.vg = engine.VirtualGeometry(max_triangles=max_triangles, max_shadow_triangles=max_shadow,
+                                         max_meshlets=max_meshlets, output_slots=8)
+        for d, m, f in zip(spec.meshes, spec.instances, self.flags):
+            self.vg.create_mesh(d, m, max_draw_distance=f.get("max_draw_distance", float("inf")),
+                                min_pixel_radius=f.get("min_pixel_radius", 0.0), cast_shadow=f.get("shadow", False),
+                                occlusion_culling=f.get("occlusion", False))
+        self.scene, self.mats, self.orders = O.scene_from_spec(spec.meshes, spec.instances, self.flags)
+        self.inst_slot = np.concatenate([np.full(len(m), i, np.uint32) for i, m in enumerate(spec.instances)])
+        self.max_meshlets, self.caps = max_meshlets, (max_triangles * 3, max_shadow * 3)
+
+    def check_layout(self):
+        cells, mats = self.vg.debug_scene()
+        assert np.array_equal(mats, self.mats), "instance order (Morton) differs from the oracle's"
+        ocells = np.asarray(self.scene.keep[-1]).reshape(-1, 8)
+        assert np.array_equal(cells, ocells), "cell records differ from the oracle's computeCell"
+
+    def oracle(self, cam, params, hzb=None, precision="f32", state=None):
+        v = O.make_view(cam, params, self.max_meshlets, self.caps, hzb=hzb, state=state)
+        return O.cull_pass(self.scene, v, precision), v
+
+    def gpu(self, cam, params, slot=0, graph=False):
+        v = engine.make_view(cam, params)
+        self.vg.cut([v], first_slot=slot, graph=graph)
+        stats = self.vg.read_stats(slot)
+        lists = [self.vg.draw_list(slot, c) for c in (0, 1)]
+        return stats, lists
+
+    def compare(self, cam, params, hzb_oracle=None, slot=0, graph=False):
+        """GPU result == float mirror (sets, counters, args); returns (gpu lists, oracle result)."""
+        state = list(self.vg.state(params.state_slot))  # the controller state both start from
+        res, _ = self.oracle(cam, params, hzb_oracle, "f32", state)
+        stats, lists = self.gpu(cam, params, slot, graph)
+        c = res["counters"]
+        assert stats["visible_cells"] == c[0]
+        assert stats["occluded_instances"] == c[1]
+        for cut in (0, 1):
+            k = c[2 + cut * 5: 7 + cut * 5]
+            got = [stats["selected"][cut], stats["drawn"][cut], stats["survived"][cut], stats["work"][cut],
+                   stats["requested_indices"][cut]]
+            assert got == k, f"cut {cut} counters gpu {got} oracle {k}"
+            overflow = k[0] > self.max_meshlets
+            if not overflow:
+                g = key_set(lists[cut], (0, 1, 3))
+                o = key_set(res["entries"][cut], (0, 1, 2))
+                assert g == o, f"cut {cut}: {len(g - o)} only on GPU, {len(o - g)} only in the oracle"
+                check_index_tiling(lists[cut], self.inst_slot, res["mesh_counts"], cut)
+        assert stats["rounds"] == res["rounds"]
+        out = self.vg.output(slot)
+        args = d2h(out.draw_args, 2 * out.mesh_slots * 2 * 5).reshape(2, out.mesh_slots, 2, 5)
+        n = len(self.spec.meshes)
+        assert np.array_equal(args[:, :n], res["draw_args"]), "drawIndexedIndirect args differ"
+        st = self.vg.state(params.state_slot)
+        assert list(st) == res["state"], f"controller state gpu {list(st)} oracle {res['state']}"
+        return lists, res

@@ -1,0 +1,208 @@
+"""GPU cut vs the oracle, through the C ABI: bit-exact against the float mirror (same arithmetic order) on sets,
+counters, draw args and controller state; against the double restatement of the reference outside the 1e-5
+relative margin."""
+import math
+
+import numpy as np
+import pytest
+
+import oracle as O
+from vgcut import engine, scenes
+from vgcut.camera import Camera
+from parity_util import Harness, MARGIN, key_set, small_ruins, d2h
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def plain():
+    spec = scenes.plain_small(n=60, seed=1)
+    h = Harness(spec)
+    h.check_layout()
+    return h
+
+
+def cameras_around(n, radius, height, seed=5):
+    r = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        a = r.uniform(0, 2 * math.pi)
+        d = radius * r.uniform(0.3, 1.6)
+        out.append(Camera.perspective_look_at((math.cos(a) * d, height * r.uniform(0.05, 1.5), math.sin(a) * d),
+                                              (r.uniform(-3, 3), 0, r.uniform(-3, 3)), 60, 1920, 1080, 0.1, 1000))
+    return out
+
+
+@pytest.mark.parametrize("threshold", [0.5, 1.0, 2.0, 3.0])
+def test_plain_small_bit_exact(plain, threshold):
+    p = engine.ViewParams(error_threshold=threshold)
+    for cam in plain.spec.cameras + cameras_around(6, 30, 10):
+        plain.compare(cam, p)
+
+
+def test_plain_small_levers(plain):
+    cam = cameras_around(1, 25, 8, seed=9)[0]
+    for p in [engine.ViewParams(frustum_culling=False), engine.ViewParams(min_pixel_radius=40.0),
+              engine.ViewParams(lod_blend=1.0, error_threshold=2.0), engine.ViewParams(lod_blend=3.0, error_threshold=2.5)]:
+        plain.compare(cam, p)
+
+
+def test_gpu_vs_reference_semantics(plain):
+    """Differences between the GPU selection and the double restatement are all decisions within the margin."""
+    total = near = 0
+    for cam in cameras_around(8, 30, 10, seed=21):
+        p = engine.ViewParams(error_threshold=1.0)
+        lists, _ = plain.compare(cam, p)
+        res, v = plain.oracle(cam, p, precision="f64")
+        g = key_set(lists[0], (0, 1, 3))
+        o = key_set(res["entries"][0], (0, 1, 2))
+        total += len(o)
+        for inst, m, _ in g ^ o:
+            slack = O.explain(plain.scene, v, 0, inst, m)
+            assert slack <= MARGIN, f"({inst}, {m}) differs with slack {slack}"
+            near += 1
+    assert total > 0
+    print(f"margin decisions: {near} of {total}")
+
+
+@pytest.fixture(scope="module")
+def ruins_small():
+    spec = small_ruins()
+    flags = [dict(shadow=(i % 2 == 0), occlusion=True, max_draw_distance=(80.0 if i == 1 else float("inf")),
+                  min_pixel_radius=(1.0 if i == 2 else 0.0)) for i in range(len(spec.meshes))]
+    h = Harness(spec, flags)
+    h.check_layout()
+    return h
+
+
+def test_ruins_small_with_shadow_and_occlusion(ruins_small):
+    h = ruins_small
+    vg = h.vg
+    for k, cam in enumerate(h.spec.cameras):
+        vg.build_hzb(k, h.spec.depth_images[k])
+        hzb = O.hzb_build(h.spec.depth_images[k])
+        p = engine.ViewParams(error_threshold=1.0, hzb=k, shadow_sweep=(30.0, -60.0, 10.0))
+        lists, res = h.compare(cam, p, hzb_oracle=hzb)
+        assert res["counters"][1] > 0 or k > 0  # occlusion is exercised
+        assert len(lists[1]) > 0  # the shadow cut is exercised
+
+
+def test_hzb_mips_bit_exact(ruins_small):
+    h = ruins_small
+    img = h.spec.depth_images[0]
+    h.vg.build_hzb(7, img)
+    mips, levels, off, w, hh = O.hzb_build(img)
+    info = h.vg.hzb_info(7)
+    assert info["levels"] == levels and info["offset"][:levels] == off[:levels] and info["width"][:levels] == w[:levels]
+    got = d2h(info["data"], len(mips), np.float32)
+    assert np.array_equal(got, mips), "HZB mips differ from the oracle's max reduction"
+    # from device memory too
+    import torch
+    d = torch.from_numpy(img).cuda()
+    engine.check(engine.lib().vgc_hzb_build(h.vg.handle, 8, d.data_ptr(), img.shape[1], img.shape[0], 1, None))
+    info = h.vg.hzb_info(8)
+    assert np.array_equal(d2h(info["data"], len(mips), np.float32), mips)
+
+
+def test_capacity_retry_rounds():
+    """A draw list too small for the cut triggers the same-frame redo at a coarser threshold (GeometryPool.ts:1032)
+    and the steer between frames; counters and controller state match the oracle round for round."""
+    spec = scenes.plain_small(n=60, seed=2)
+    h = Harness(spec, max_meshlets=300, max_triangles=40_000)
+    cam = cameras_around(1, 12, 4, seed=3)[0]
+    p = engine.ViewParams(error_threshold=0.5, state_slot=3)
+    for _ in range(3):  # state carries from frame to frame
+        h.compare(cam, p)
+
+
+def test_batch_graph_equals_plain(plain):
+    cams = cameras_around(5, 30, 10, seed=33)
+    views = [engine.make_view(c, engine.ViewParams(error_threshold=t, state_slot=10 + i))
+             for i, (c, t) in enumerate(zip(cams, [0.5, 1, 2, 3, 1]))]
+    plain.vg.cut(views, first_slot=0, graph=False)
+    a = [[plain.vg.draw_list(i, c) for c in (0, 1)] for i in range(5)]
+    for _ in range(2):
+        plain.vg.cut(views, first_slot=0, graph=True)
+        b = [[plain.vg.draw_list(i, c) for c in (0, 1)] for i in range(5)]
+        for i in range(5):
+            for c in (0, 1):
+                assert key_set(a[i][c], (0, 1, 3)) == key_set(b[i][c], (0, 1, 3))
+
+
+def test_select_cut_matches_reference(terrain, park_miller):
+    """GPU selectCut / selectBlendCut (cut.ts:26-77) vs the double oracle, margin decisions excepted."""
+    vg = engine.VirtualGeometry()
+    vg.create_mesh(terrain, np.eye(4, dtype=np.float32).reshape(1, 16))
+    rand = park_miller(7)
+    vms, cams = [], []
+    for _ in range(12):
+        eye = ((rand() - 0.5) * 300, 2 + rand() * 80, (rand() - 0.5) * 300)
+        tgt = ((rand() - 0.5) * 200, 0, (rand() - 0.5) * 200)
+        cams.append(Camera.perspective_look_at(eye, tgt, 60, 16, 9, 0.1, 5000))
+    vm = np.array([c.view for c in cams])
+    ps = np.array([c.proj[5] * 540 for c in cams])
+    b = terrain.meshlet_bounds.reshape(-1, 16).astype(np.float64)
+    for t, blend in [(0.5, 1), (1, 1), (3, 1), (1, 2), (2, 3)]:
+        lo, hi = vg.select_cut(0, vm, ps, 0.1, 1.0, t, blend)
+        for i, c in enumerate(cams):
+            olo, ohi = O.select_blend_cut(terrain, c.view, ps[i], 0.1, t, blend)
+            diff = np.nonzero((lo[i] != olo) | (hi[i] != ohi))[0]
+            for m in diff:  # every difference sits within the margin of a threshold or a fade-step boundary
+                V = np.asarray(c.view).reshape(4, 4).T
+                def pe(cc, r, e):
+                    p = V @ np.append(cc, 1.0)
+                    return e * ps[i] / max(np.linalg.norm(p[:3]) - r, 0.1)
+                own, par = pe(b[m, :3], b[m, 3], b[m, 8]), pe(b[m, 4:7], b[m, 7], b[m, 9])
+                high = t * blend if blend > 1 else t
+                close = [abs(own - high) / high, abs(par - t) / t]
+                if blend > 1:
+                    for e in (own, par):
+                        x = math.log(max(e, 1e-30) / t) * 255 / math.log(blend)
+                        close.append(abs(x - math.floor(x) - 0.5) / (255 / math.log(blend)))
+                assert min(close) <= MARGIN, f"meshlet {m} differs beyond the margin"
+            if blend == 1:
+                sel = (hi[i] > 0).astype(np.uint8)
+                assert len(O.verify_cut_coverage(terrain, sel)) == 0
+                assert len(O.verify_cut_overlap(terrain, sel)) == 0
+    vg.dispose()
+
+
+def test_expand_writes_draw_slots(plain):
+    cam = plain.spec.cameras[0]
+    p = engine.ViewParams()
+    lists, res = plain.compare(cam, p)
+    import torch
+    cap = 2_000_000 * 3
+    buf = torch.full((cap,), 0xFFFFFFFF, dtype=torch.int64).to(torch.int32).cuda()
+    engine.check(engine.lib().vgc_expand(plain.vg.handle, 0, 0, buf.data_ptr(), cap, None))
+    torch.cuda.synchronize()
+    idx = buf.cpu().numpy().view(np.uint32)
+    e = lists[0]
+    data = plain.spec.meshes[0]
+    info = data.meshlet_info.reshape(-1, 4)
+    counts = res["mesh_counts"]
+    region = {0: 0, 1: int(counts[0, 0, 0])}
+    for slot_in_list, (inst, m, first, packed) in enumerate(e[:200]):
+        part = 0 if (packed & 0xFFFF00) == (255 << 16) else 1
+        start = region[part] + first
+        tri = packed & 255
+        got = idx[start:start + 3 * tri]
+        fi = info[m, 1] // 3
+        tris = data.meshlet_triangles[fi:fi + tri]
+        want = np.stack([tris & 255, (tris >> 8) & 255, (tris >> 16) & 255], 1).reshape(-1)
+        assert np.array_equal(got & 127, want)
+        assert np.all((got >> 7) == got[0] >> 7)
+
+
+def test_instance_update_and_flags(plain):
+    h = plain
+    cam = h.spec.cameras[0]
+    p = engine.ViewParams()
+    before, _ = h.compare(cam, p)
+    mesh = h.vg.meshes[0]
+    mesh.visible = False
+    stats, lists = h.gpu(cam, p)
+    assert stats["visible_cells"] == 0 and len(lists[0]) == 0
+    mesh.visible = True
+    stats, lists = h.gpu(cam, p)
+    assert key_set(lists[0], (0, 1, 3)) == key_set(before[0], (0, 1, 3))

@@ -1,0 +1,1057 @@
+// Host side of the cut engine behind the C ABI of include/vgcut.h: scene residency in HBM, view constants,
+// the plain launch sequence, the CUDA-graph batch, HZB slots, stats and the CPU-API equivalents.
+//
+// The reference keeps a GeometryPool per 120 MB of WebGPU bindings (VirtualGeometry.ts:314-331) and grows its
+// buffers by reallocation (GeometryPool.ts:169-208). Here one context holds one resident buffer set per array;
+// growth re-uploads the host mirror into a larger allocation. Output slots (one per view of a batch) hold the
+// per-view results: counters, draw list, draw args.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "vgcut.h"
+#include "vgcut_internal.h"
+#include "vgcut_kernels.h"
+
+using namespace vgc;
+
+namespace {
+thread_local std::string g_error;
+
+int fail(int code, const std::string &msg) {
+  g_error = msg;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                                              \
+  do {                                                                                              \
+    cudaError_t _e = (expr);                                                                        \
+    if (_e != cudaSuccess) return fail(VGC_DEVICE_ERROR, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
+
+constexpr double kNoDrawDistance = 1e30;  // GeometryPool.ts:111
+
+struct DevBuf {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+};
+
+struct MeshHost {
+  bool used = false;
+  uint32_t meshlet_base = 0, meshlet_count = 0;
+  uint32_t level_base = 0, level_count = 0;
+  uint32_t triangle_base = 0, triangle_count = 0;
+  uint32_t instance_base = 0, instance_count = 0;
+  uint32_t cell_base = 0, cell_count = 0;
+  float sphere[4];
+};
+
+struct HzbSlot {
+  DevBuf data;
+  HzbDesc desc{};
+  bool valid = false;
+};
+
+uint32_t pad32(uint32_t x) { return (x + 31u) & ~31u; }
+
+}  // namespace
+
+// Launch scratch: view constants and the (view, cell) unit list of one launch sequence.
+struct LaunchScratch {
+  ViewConst *h_views = nullptr;  // pinned
+  ViewConst *d_views = nullptr;
+  uint2 *d_units = nullptr;
+  uint32_t *d_unit_count = nullptr;
+  uint32_t view_capacity = 0;
+  size_t unit_capacity = 0;
+  cudaEvent_t done = nullptr;
+  bool pending = false;
+};
+
+struct vgc_context {
+  vgc_options opts{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int sm_count = 0;
+  uint32_t select_grid = 0;
+  uint64_t bytes = 0;
+  std::mutex mu;
+  // host mirrors of the resident scene
+  std::vector<MeshHost> mesh_host;
+  std::vector<MeshRec> meshes;
+  std::vector<LevelRec> levels;
+  std::vector<float4> m_lod, m_parent, m_err, m_cull;
+  std::vector<uint4> m_info;
+  std::vector<uint32_t> m_tris;
+  std::vector<float4> inst;
+  std::vector<uint32_t> inst_slot;
+  std::vector<CellRec> cells;
+  uint32_t slot_capacity = 64;
+  uint32_t slots_used = 0;
+  bool dirty = true;
+  // device copies
+  DevBuf d_meshes, d_levels, d_m_lod, d_m_parent, d_m_err, d_m_cull, d_m_info, d_m_tris, d_inst, d_inst_slot, d_cells;
+  // output slots
+  uint32_t out_slots = 0;
+  uint32_t out_slot_capacity = 0;  // slot_capacity the output buffers were sized for
+  uint32_t counter_words = 0;
+  DevBuf d_counters, d_draw, d_args, d_dyn, d_hist;
+  // controller state slots
+  DevBuf d_state;
+  uint32_t state_slots = 0;
+  // HZB slots
+  std::vector<HzbSlot> hzb;
+  DevBuf d_hzb_desc;
+  static constexpr uint32_t kHzbSlots = 256;
+  LaunchScratch scratch;
+  // profiling: events around plain-path launches, resolved lazily
+  bool profiling = false;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_pending;
+  std::vector<cudaEvent_t> prof_free;
+  double prof_ms[VGC_KERNEL_KINDS] = {0};
+  uint32_t prof_count[VGC_KERNEL_KINDS] = {0};
+};
+
+struct vgc_batch {
+  vgc_context *ctx = nullptr;
+  uint32_t max_views = 0;
+  LaunchScratch scratch;
+  cudaStream_t capture_stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint32_t graph_views = 0;
+  uint32_t graph_cells = 0;
+  uint32_t graph_slots = 0;
+};
+
+namespace {
+
+int dev_alloc(vgc_context *ctx, DevBuf &b, size_t bytes) {
+  if (b.bytes >= bytes && b.ptr) return VGC_OK;
+  size_t want = std::max<size_t>(bytes, 256);
+  if (ctx->opts.hbm_budget_bytes && ctx->bytes - b.bytes + want > ctx->opts.hbm_budget_bytes)
+    return fail(VGC_OVER_BUDGET, "allocation of " + std::to_string(want) + " bytes exceeds the context's HBM budget");
+  void *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, want);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(VGC_OOM, "cudaMalloc(" + std::to_string(want) + "): " + cudaGetErrorString(e));
+  }
+  if (b.ptr) {
+    cudaFree(b.ptr);
+    ctx->bytes -= b.bytes;
+  }
+  b.ptr = p;
+  b.bytes = want;
+  ctx->bytes += want;
+  return VGC_OK;
+}
+
+void dev_free(vgc_context *ctx, DevBuf &b) {
+  if (b.ptr) {
+    cudaFree(b.ptr);
+    ctx->bytes -= b.bytes;
+  }
+  b.ptr = nullptr;
+  b.bytes = 0;
+}
+
+template <class T>
+int upload(vgc_context *ctx, DevBuf &b, const std::vector<T> &v) {
+  size_t bytes = v.size() * sizeof(T);
+  if (bytes == 0) bytes = sizeof(T);
+  int rc = dev_alloc(ctx, b, bytes + bytes / 2);  // grow ahead
+  if (rc) return rc;
+  if (!v.empty()) CUDA_TRY(cudaMemcpy(b.ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return VGC_OK;
+}
+
+int sync_scene(vgc_context *ctx) {
+  if (!ctx->dirty) return VGC_OK;
+  // buffers may be reallocated: no launch of any stream may still read the old ones
+  CUDA_TRY(cudaDeviceSynchronize());
+  int rc;
+  if ((rc = upload(ctx, ctx->d_meshes, ctx->meshes))) return rc;
+  if ((rc = upload(ctx, ctx->d_levels, ctx->levels))) return rc;
+  if ((rc = upload(ctx, ctx->d_m_lod, ctx->m_lod))) return rc;
+  if ((rc = upload(ctx, ctx->d_m_parent, ctx->m_parent))) return rc;
+  if ((rc = upload(ctx, ctx->d_m_err, ctx->m_err))) return rc;
+  if ((rc = upload(ctx, ctx->d_m_cull, ctx->m_cull))) return rc;
+  if ((rc = upload(ctx, ctx->d_m_info, ctx->m_info))) return rc;
+  if ((rc = upload(ctx, ctx->d_m_tris, ctx->m_tris))) return rc;
+  if ((rc = upload(ctx, ctx->d_inst, ctx->inst))) return rc;
+  if ((rc = upload(ctx, ctx->d_inst_slot, ctx->inst_slot))) return rc;
+  if ((rc = upload(ctx, ctx->d_cells, ctx->cells))) return rc;
+  ctx->dirty = false;
+  return VGC_OK;
+}
+
+Scene scene_of(const vgc_context *ctx) {
+  Scene S;
+  S.meshes = (const MeshRec *)ctx->d_meshes.ptr;
+  S.levels = (const LevelRec *)ctx->d_levels.ptr;
+  S.m_lod = (const float4 *)ctx->d_m_lod.ptr;
+  S.m_parent = (const float4 *)ctx->d_m_parent.ptr;
+  S.m_err = (const float4 *)ctx->d_m_err.ptr;
+  S.m_cull = (const float4 *)ctx->d_m_cull.ptr;
+  S.m_info = (const uint4 *)ctx->d_m_info.ptr;
+  S.m_tris = (const uint32_t *)ctx->d_m_tris.ptr;
+  S.inst = (const float4 *)ctx->d_inst.ptr;
+  S.inst_slot = (const uint32_t *)ctx->d_inst_slot.ptr;
+  S.cells = (const CellRec *)ctx->d_cells.ptr;
+  S.cell_count = (uint32_t)ctx->cells.size();
+  S.instance_count = (uint32_t)ctx->inst_slot.size();
+  S.meshlet_count = (uint32_t)ctx->m_lod.size();
+  S.slot_capacity = ctx->slot_capacity;
+  S.slots_used = ctx->slots_used;
+  return S;
+}
+
+// Output buffers for `slots` views, sized for the current mesh-slot capacity.
+int ensure_outputs(vgc_context *ctx, uint32_t slots) {
+  if (slots <= ctx->out_slots && ctx->out_slot_capacity == ctx->slot_capacity) return VGC_OK;
+  CUDA_TRY(cudaDeviceSynchronize());
+  uint32_t n = std::max(slots, ctx->out_slots);
+  ctx->counter_words = VGC_COUNTER_HEADER + ctx->slot_capacity * 8;
+  const size_t md = ctx->opts.max_meshlets;
+  int rc;
+  if ((rc = dev_alloc(ctx, ctx->d_counters, (size_t)n * ctx->counter_words * 4))) return rc;
+  if ((rc = dev_alloc(ctx, ctx->d_draw, (size_t)n * 2 * md * 16))) return rc;
+  if ((rc = dev_alloc(ctx, ctx->d_args, (size_t)n * 2 * ctx->slot_capacity * 2 * 5 * 4))) return rc;
+  if ((rc = dev_alloc(ctx, ctx->d_dyn, (size_t)n * 4 * 4))) return rc;
+  if ((rc = dev_alloc(ctx, ctx->d_hist, (size_t)n * 2 * kBudgetBins * 8))) return rc;
+  CUDA_TRY(cudaMemset(ctx->d_counters.ptr, 0, (size_t)n * ctx->counter_words * 4));
+  CUDA_TRY(cudaMemset(ctx->d_args.ptr, 0, (size_t)n * 2 * ctx->slot_capacity * 2 * 5 * 4));
+  ctx->out_slots = n;
+  ctx->out_slot_capacity = ctx->slot_capacity;
+  return VGC_OK;
+}
+
+int ensure_state(vgc_context *ctx, uint32_t slot) {
+  if (slot < ctx->state_slots) return VGC_OK;
+  uint32_t n = std::max<uint32_t>(slot + 1, ctx->state_slots * 2);
+  n = std::max<uint32_t>(n, 16);
+  std::vector<uint32_t> init((size_t)n * kStateWords, 0);
+  for (uint32_t i = 0; i < n; i++) init[(size_t)i * kStateWords] = init[(size_t)i * kStateWords + 1] = 10000u;
+  if (ctx->state_slots) {
+    CUDA_TRY(cudaDeviceSynchronize());
+    CUDA_TRY(cudaMemcpy(init.data(), ctx->d_state.ptr, (size_t)ctx->state_slots * kStateWords * 4, cudaMemcpyDeviceToHost));
+  }
+  DevBuf fresh;
+  std::swap(fresh, ctx->d_state);
+  ctx->bytes -= fresh.bytes;
+  int rc = dev_alloc(ctx, ctx->d_state, init.size() * 4);
+  if (fresh.ptr) cudaFree(fresh.ptr);
+  if (rc) return rc;
+  CUDA_TRY(cudaMemcpy(ctx->d_state.ptr, init.data(), init.size() * 4, cudaMemcpyHostToDevice));
+  ctx->state_slots = n;
+  return VGC_OK;
+}
+
+int ensure_scratch(vgc_context *ctx, LaunchScratch &s, uint32_t views, size_t units) {
+  if (views > s.view_capacity) {
+    if (s.h_views) cudaFreeHost(s.h_views);
+    if (s.d_views) {
+      cudaFree(s.d_views);
+      ctx->bytes -= sizeof(ViewConst) * s.view_capacity;
+    }
+    s.h_views = nullptr;
+    s.d_views = nullptr;
+    CUDA_TRY(cudaMallocHost(&s.h_views, sizeof(ViewConst) * views));
+    CUDA_TRY(cudaMalloc(&s.d_views, sizeof(ViewConst) * views));
+    ctx->bytes += sizeof(ViewConst) * views;
+    s.view_capacity = views;
+  }
+  if (units > s.unit_capacity || !s.d_units) {
+    if (s.d_units) {
+      cudaFree(s.d_units);
+      ctx->bytes -= s.unit_capacity * sizeof(uint2);
+    }
+    s.d_units = nullptr;
+    size_t n = std::max<size_t>(units, 32);
+    CUDA_TRY(cudaMalloc(&s.d_units, n * sizeof(uint2)));
+    ctx->bytes += n * sizeof(uint2);
+    s.unit_capacity = n;
+  }
+  if (!s.d_unit_count) CUDA_TRY(cudaMalloc(&s.d_unit_count, 16));
+  if (!s.done) CUDA_TRY(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
+  return VGC_OK;
+}
+
+void free_scratch(LaunchScratch &s) {
+  if (s.pending && s.done) cudaEventSynchronize(s.done);
+  if (s.h_views) cudaFreeHost(s.h_views);
+  if (s.d_views) cudaFree(s.d_views);
+  if (s.d_units) cudaFree(s.d_units);
+  if (s.d_unit_count) cudaFree(s.d_unit_count);
+  if (s.done) cudaEventDestroy(s.done);
+  s = LaunchScratch();
+}
+
+// Frustum planes of a column-major clip matrix, [0, 1] depth, normalised (Gribb & Hartmann plane extraction;
+// three.js Frustum.setFromProjectionMatrix with WebGPUCoordinateSystem, VirtualGeometry.ts:429-437).
+void planes_of(const double *me, double out[6][4]) {
+  double p[6][4] = {
+      {me[3] - me[0], me[7] - me[4], me[11] - me[8], me[15] - me[12]},
+      {me[3] + me[0], me[7] + me[4], me[11] + me[8], me[15] + me[12]},
+      {me[3] + me[1], me[7] + me[5], me[11] + me[9], me[15] + me[13]},
+      {me[3] - me[1], me[7] - me[5], me[11] - me[9], me[15] - me[13]},
+      {me[3] - me[2], me[7] - me[6], me[11] - me[10], me[15] - me[14]},
+      {me[2], me[6], me[10], me[14]},
+  };
+  for (int i = 0; i < 6; i++) {
+    double l = std::sqrt(p[i][0] * p[i][0] + p[i][1] * p[i][1] + p[i][2] * p[i][2]);
+    double inv = l > 0 ? 1.0 / l : 0;
+    for (int k = 0; k < 4; k++) out[i][k] = p[i][k] * inv;
+  }
+}
+
+int view_constants(vgc_context *ctx, const vgc_view &in, uint32_t out_slot, uint32_t unit_offset, ViewConst &k) {
+  if (!(in.viewport_height > 0) || !(in.error_threshold > 0) || !(in.near_ > 0))
+    return fail(VGC_INVALID_ARG, "view: viewport_height, error_threshold and near must be > 0");
+  if (in.hzb >= (int32_t)vgc_context::kHzbSlots || (in.hzb >= 0 && !ctx->hzb[in.hzb].valid))
+    return fail(VGC_INVALID_ARG, "view: hzb slot " + std::to_string(in.hzb) + " has no HZB");
+  int rc = ensure_state(ctx, in.state_slot);
+  if (rc) return rc;
+  std::memset(&k, 0, sizeof k);
+  double pvm[16];
+  for (int c = 0; c < 4; c++)
+    for (int r = 0; r < 4; r++) {
+      double s = 0;
+      for (int i = 0; i < 4; i++) s += in.proj[i * 4 + r] * in.view[c * 4 + i];
+      pvm[c * 4 + r] = s;
+    }
+  double pv[6][4], pw[6][4];
+  planes_of(in.proj, pv);
+  planes_of(pvm, pw);
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 4; c++) k.V[r * 4 + c] = (float)in.view[c * 4 + r];
+  for (int p = 0; p < 6; p++) {
+    for (int i = 0; i < 4; i++) k.plane[p * 4 + i] = (float)pv[p][i];
+    double d = pw[p][0] * in.shadow_sweep[0] + pw[p][1] * in.shadow_sweep[1] + pw[p][2] * in.shadow_sweep[2];
+    k.sweep[p] = (float)(d > 0 ? d : 0);
+  }
+  k.proj_scale = (float)(in.proj[5] * in.viewport_height * 0.5);
+  k.near_ = (float)in.near_;
+  k.P0 = (float)in.proj[0];
+  k.P5 = (float)in.proj[5];
+  k.P8 = (float)in.proj[8];
+  k.P9 = (float)in.proj[9];
+  k.P10 = (float)in.proj[10];
+  k.P14 = (float)in.proj[14];
+  k.error_threshold = (float)in.error_threshold;
+  k.lod_blend_max = (float)(in.lod_blend > 1 ? in.lod_blend : 1);
+  double limit = in.max_error_threshold / in.error_threshold;
+  k.lod_scale_limit = (float)(limit > 1 ? limit : 1);
+  k.min_pixel_radius = (float)in.min_pixel_radius;
+  k.shadow_error_scale = (float)in.shadow_error_scale;
+  k.budget = (float)(in.triangle_budget > 0 ? in.triangle_budget : 0);
+  k.budget_lo = (float)in.threshold_range[0];
+  k.budget_hi = (float)in.threshold_range[1];
+  k.frustum = in.frustum_culling ? 1u : 0u;
+  k.occl_active = in.hzb >= 0 ? 1u : 0u;
+  k.hzb = in.hzb;
+  k.unit_offset = unit_offset;
+  k.max_drawn = ctx->opts.max_meshlets;
+  k.index_capacity[0] = ctx->opts.max_triangles * 3;
+  k.index_capacity[1] = ctx->opts.max_shadow_triangles * 3;
+  k.counters = (uint32_t *)ctx->d_counters.ptr + (size_t)out_slot * ctx->counter_words;
+  k.state = (uint32_t *)ctx->d_state.ptr + (size_t)in.state_slot * kStateWords;
+  k.draw_list = (uint4 *)ctx->d_draw.ptr + (size_t)out_slot * 2 * ctx->opts.max_meshlets;
+  k.draw_args = (uint32_t *)ctx->d_args.ptr + (size_t)out_slot * 2 * ctx->slot_capacity * 2 * 5;
+  k.dyn = (float *)ctx->d_dyn.ptr + (size_t)out_slot * 4;
+  k.hist = (unsigned long long *)ctx->d_hist.ptr + (size_t)out_slot * 2 * kBudgetBins;
+  return VGC_OK;
+}
+
+// Prepares scene, outputs and the views' constants in `s.h_views` (pinned).
+int prepare(vgc_context *ctx, LaunchScratch &s, const vgc_view *views, uint32_t count, uint32_t first_slot) {
+  if (!views || count == 0) return fail(VGC_INVALID_ARG, "no views");
+  int rc = sync_scene(ctx);
+  if (rc) return rc;
+  if ((rc = ensure_outputs(ctx, first_slot + count))) return rc;
+  const uint32_t cells = pad32((uint32_t)ctx->cells.size());
+  if ((rc = ensure_scratch(ctx, s, count, (size_t)count * cells))) return rc;
+  if (s.pending) CUDA_TRY(cudaEventSynchronize(s.done));
+  for (uint32_t i = 0; i < count; i++)
+    if ((rc = view_constants(ctx, views[i], first_slot + i, i * cells, s.h_views[i]))) return rc;
+  return VGC_OK;
+}
+
+cudaEvent_t prof_event(vgc_context *ctx) {
+  if (!ctx->prof_free.empty()) {
+    cudaEvent_t e = ctx->prof_free.back();
+    ctx->prof_free.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Runs `launch` between two events on `st` when profiling is on (never inside a graph capture).
+template <class F>
+cudaError_t timed(vgc_context *ctx, bool capture, int kind, cudaStream_t st, F &&launch) {
+  if (!ctx->profiling || capture) return launch();
+  cudaEvent_t a = prof_event(ctx), b = prof_event(ctx);
+  cudaEventRecord(a, st);
+  cudaError_t e = launch();
+  cudaEventRecord(b, st);
+  ctx->prof_pending.push_back({kind, {a, b}});
+  return e;
+}
+
+// The launch sequence of one frame: reset, cells, then select + finish for the first round and two retry rounds
+// (GeometryPool.ts:1081-1092 without the dispatch-argument kernels, which persistent launches do not need).
+int enqueue(vgc_context *ctx, LaunchScratch &s, uint32_t count, cudaStream_t st, bool capture) {
+  const Scene S = scene_of(ctx);
+  const uint32_t cells = pad32(S.cell_count);
+  const HzbDesc *hzbs = (const HzbDesc *)ctx->d_hzb_desc.ptr;
+  CUDA_TRY(cudaMemcpyAsync(s.d_views, s.h_views, sizeof(ViewConst) * count, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(timed(ctx, capture, VGC_KERNEL_RESET, st,
+                 [&] { return launch_reset(s.d_views, count, ctx->counter_words, s.d_unit_count, st); }));
+  CUDA_TRY(timed(ctx, capture, VGC_KERNEL_CELLS, st,
+                 [&] { return launch_cells(S, s.d_views, count, count * cells, s.d_units, s.d_unit_count, st); }));
+  for (int round = 0; round < 3; round++) {
+    CUDA_TRY(timed(ctx, capture, round == 0 ? VGC_KERNEL_SELECT0 : VGC_KERNEL_SELECT_RETRY, st, [&] {
+      return launch_select(S, s.d_views, hzbs, s.d_units, s.d_unit_count, round, ctx->select_grid, st);
+    }));
+    CUDA_TRY(timed(ctx, capture, VGC_KERNEL_FINISH, st,
+                   [&] { return launch_finish(s.d_views, count, S.slot_capacity, S.slots_used, round, st); }));
+  }
+  return VGC_OK;
+}
+
+void compute_cell(vgc_context *ctx, uint32_t slot, uint32_t cell) {
+  // Bounding sphere of one cell's instances (GeometryPool.ts:519-545): the box of the instances' world spheres
+  // gives the centre, the radius reaches every instance sphere, and both radii are inflated so float rounding on
+  // the GPU cannot make the cell test stricter than the per-instance test.
+  const MeshHost &m = ctx->mesh_host[slot];
+  const uint32_t first = cell * kCellSize, end = std::min(first + kCellSize, m.instance_count);
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  double max_radius = 0;
+  std::vector<double> sph((size_t)(end - first) * 4);
+  for (uint32_t g = first; g < end; g++) {
+    const float4 *c = &ctx->inst[(size_t)(m.instance_base + g) * 4];
+    const double sx = m.sphere[0], sy = m.sphere[1], sz = m.sphere[2], sr = m.sphere[3];
+    double *s = &sph[(size_t)(g - first) * 4];
+    s[0] = c[0].x * sx + c[1].x * sy + c[2].x * sz + c[3].x;
+    s[1] = c[0].y * sx + c[1].y * sy + c[2].y * sz + c[3].y;
+    s[2] = c[0].z * sx + c[1].z * sy + c[2].z * sz + c[3].z;
+    const double c0 = std::sqrt((double)c[0].x * c[0].x + (double)c[0].y * c[0].y + (double)c[0].z * c[0].z);
+    const double c1 = std::sqrt((double)c[1].x * c[1].x + (double)c[1].y * c[1].y + (double)c[1].z * c[1].z);
+    const double c2 = std::sqrt((double)c[2].x * c[2].x + (double)c[2].y * c[2].y + (double)c[2].z * c[2].z);
+    s[3] = sr * std::max(c0, std::max(c1, c2));
+    for (int a = 0; a < 3; a++) {
+      lo[a] = std::min(lo[a], s[a] - s[3]);
+      hi[a] = std::max(hi[a], s[a] + s[3]);
+    }
+    max_radius = std::max(max_radius, s[3]);
+  }
+  const double cx = (lo[0] + hi[0]) / 2, cy = (lo[1] + hi[1]) / 2, cz = (lo[2] + hi[2]) / 2;
+  double radius = 0;
+  for (uint32_t g = first; g < end; g++) {
+    const double *s = &sph[(size_t)(g - first) * 4];
+    radius = std::max(radius, std::sqrt((s[0] - cx) * (s[0] - cx) + (s[1] - cy) * (s[1] - cy) + (s[2] - cz) * (s[2] - cz)) + s[3]);
+  }
+  CellRec &r = ctx->cells[m.cell_base + cell];
+  r.sphere = make_float4((float)cx, (float)cy, (float)cz, (float)(radius * (1 + 1e-4) + 1e-3));
+  r.max_radius = (float)(max_radius * (1 + 1e-4) + 1e-4);
+  r.slot = slot;
+  r.first = m.instance_base + first;
+  r.count = end - first;
+}
+
+uint32_t spread10(uint32_t v) {
+  v &= 0x3ff;
+  uint32_t r = 0;
+  for (int b = 0; b < 10; b++) r |= ((v >> b) & 1u) << (3 * b);
+  return r;
+}
+
+// 30-bit Morton order of the instance sphere centres, stable (GeometryPool.ts:1263-1311).
+void morton_order(const float *m, uint32_t n, const float *sphere, std::vector<uint32_t> &order) {
+  std::vector<double> c((size_t)n * 3);
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (uint32_t i = 0; i < n; i++) {
+    const float *e = m + (size_t)i * 16;
+    const double sx = sphere[0], sy = sphere[1], sz = sphere[2];
+    const double p[3] = {e[0] * sx + e[4] * sy + e[8] * sz + e[12], e[1] * sx + e[5] * sy + e[9] * sz + e[13],
+                         e[2] * sx + e[6] * sy + e[10] * sz + e[14]};
+    for (int a = 0; a < 3; a++) {
+      c[(size_t)i * 3 + a] = p[a];
+      lo[a] = std::min(lo[a], p[a]);
+      hi[a] = std::max(hi[a], p[a]);
+    }
+  }
+  const double extent = std::max({hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2], 1e-9});
+  std::vector<std::pair<uint32_t, uint32_t>> keys(n);
+  for (uint32_t i = 0; i < n; i++) {
+    uint32_t q[3];
+    for (int a = 0; a < 3; a++) {
+      double f = std::floor((c[(size_t)i * 3 + a] - lo[a]) / extent * 1024.0);
+      q[a] = (uint32_t)std::min(1023.0, std::max(0.0, f));
+    }
+    keys[i] = {spread10(q[0]) | (spread10(q[1]) << 1) | (spread10(q[2]) << 2), i};
+  }
+  std::stable_sort(keys.begin(), keys.end(), [](const auto &a, const auto &b) { return a.first < b.first; });
+  order.resize(n);
+  for (uint32_t i = 0; i < n; i++) order[i] = keys[i].second;
+}
+
+void write_flags(vgc_context *ctx, uint32_t slot, const vgc_mesh_opts *o) {
+  MeshRec &r = ctx->meshes[slot];
+  double dd = o ? o->max_draw_distance : 0;
+  r.max_draw_distance = (float)((dd > 0 && dd < kNoDrawDistance) ? dd : kNoDrawDistance);
+  r.min_pixel_radius = o ? std::max(0.0f, o->min_pixel_radius) : 0.0f;
+  r.enabled = o ? (o->enabled ? 1u : 0u) : 1u;
+  r.shadow = o ? (o->shadow ? 1u : 0u) : 0u;
+  r.occlusion = o ? (o->occlusion ? 1u : 0u) : 0u;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *vgc_last_error(void) { return g_error.c_str(); }
+const char *vgc_version(void) { return "vgcut 0.1.0 (sm_100a)"; }
+
+void vgc_default_options(vgc_options *o) {
+  o->max_triangles = 10000000;
+  o->max_shadow_triangles = 4000000;
+  o->max_meshlets = 1u << 20;
+  o->output_slots = 1;
+  o->device = 0;
+  o->hbm_budget_bytes = 0;
+}
+
+int vgc_context_create(const vgc_options *opts, vgc_context **out) {
+  if (!out) return fail(VGC_INVALID_ARG, "out is null");
+  *out = nullptr;
+  vgc_options o;
+  vgc_default_options(&o);
+  if (opts) o = *opts;
+  if (o.max_meshlets == 0 || o.max_meshlets > (1u << 24)) return fail(VGC_INVALID_ARG, "max_meshlets must be in [1, 2^24]");
+  if (o.max_triangles == 0 || o.max_shadow_triangles == 0) return fail(VGC_INVALID_ARG, "triangle capacities must be > 0");
+  if (o.max_triangles > 0x55555555u || o.max_shadow_triangles > 0x55555555u)
+    return fail(VGC_INVALID_ARG, "triangle capacities must fit 32-bit index counts");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(VGC_DEVICE_ERROR, "no CUDA device: the cut engine has no CPU fallback");
+  }
+  if (o.device < 0 || o.device >= ndev) return fail(VGC_INVALID_ARG, "device ordinal out of range");
+  vgc_context *ctx = new vgc_context();
+  ctx->opts = o;
+  ctx->device = o.device;
+  cudaSetDevice(o.device);
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, o.device);
+  ctx->sm_count = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return fail(VGC_DEVICE_ERROR, "cudaStreamCreate failed");
+  }
+  int per_sm = 0;
+  if (configure_select(&per_sm) != cudaSuccess) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  ctx->select_grid = (uint32_t)std::max(1, per_sm) * ctx->sm_count;
+  ctx->meshes.resize(ctx->slot_capacity);
+  ctx->mesh_host.resize(ctx->slot_capacity);
+  ctx->hzb.resize(vgc_context::kHzbSlots);
+  int rc = dev_alloc(ctx, ctx->d_hzb_desc, sizeof(HzbDesc) * vgc_context::kHzbSlots);
+  if (!rc) rc = ensure_outputs(ctx, std::max<uint32_t>(1, o.output_slots));
+  if (!rc) rc = ensure_state(ctx, 0);
+  if (rc) {
+    vgc_context_destroy(ctx);
+    return rc;
+  }
+  cudaMemset(ctx->d_hzb_desc.ptr, 0, sizeof(HzbDesc) * vgc_context::kHzbSlots);
+  *out = ctx;
+  return VGC_OK;
+}
+
+int vgc_context_destroy(vgc_context *ctx) {
+  if (!ctx) return VGC_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  free_scratch(ctx->scratch);
+  for (DevBuf *b : {&ctx->d_meshes, &ctx->d_levels, &ctx->d_m_lod, &ctx->d_m_parent, &ctx->d_m_err, &ctx->d_m_cull,
+                    &ctx->d_m_info, &ctx->d_m_tris, &ctx->d_inst, &ctx->d_inst_slot, &ctx->d_cells, &ctx->d_counters,
+                    &ctx->d_draw, &ctx->d_args, &ctx->d_dyn, &ctx->d_hist, &ctx->d_state, &ctx->d_hzb_desc})
+    dev_free(ctx, *b);
+  for (auto &h : ctx->hzb) dev_free(ctx, h.data);
+  for (auto &p : ctx->prof_pending) {
+    cudaEventDestroy(p.second.first);
+    cudaEventDestroy(p.second.second);
+  }
+  for (cudaEvent_t e : ctx->prof_free) cudaEventDestroy(e);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return VGC_OK;
+}
+
+int vgc_context_footprint(const vgc_context *ctx, uint64_t *bytes) {
+  if (!ctx || !bytes) return fail(VGC_INVALID_ARG, "null argument");
+  *bytes = ctx->bytes;
+  return VGC_OK;
+}
+
+int vgc_mesh_add(vgc_context *ctx, const vgc_mesh_data *d, const float *matrices, uint32_t n, const vgc_mesh_opts *opts,
+                 uint32_t *slot_out, uint32_t *gpu_to_input) {
+  if (!ctx || !d || !slot_out) return fail(VGC_INVALID_ARG, "null argument");
+  if (n && !matrices) return fail(VGC_INVALID_ARG, "matrices is null");
+  if (!d->meshlet_bounds || !d->meshlet_info || !d->level_ranges || !d->level_errors || !d->level_guard_errors)
+    return fail(VGC_INVALID_ARG, "mesh data arrays missing");
+  if (d->meshlet_count == 0 || d->level_count == 0) return fail(VGC_INVALID_ARG, "mesh has no meshlets or levels");
+  if (d->level_count > kMaxLevels) return fail(VGC_INVALID_ARG, "mesh has more than 48 LOD levels");
+  // validate the level table against the meshlets (meshlets sorted by level, levels contiguous)
+  uint32_t expect = 0;
+  for (uint32_t l = 0; l < d->level_count; l++) {
+    if (d->level_ranges[l * 2] != expect) return fail(VGC_INVALID_ARG, "level_ranges are not contiguous from 0");
+    expect += d->level_ranges[l * 2 + 1];
+  }
+  if (expect != d->meshlet_count) return fail(VGC_INVALID_ARG, "level_ranges do not cover meshlet_count");
+  uint64_t tri_total = 0;
+  for (uint32_t i = 0; i < d->meshlet_count; i++) {
+    const uint32_t tc = d->meshlet_info[(size_t)i * 4];
+    if (tc == 0 || tc > 128) return fail(VGC_INVALID_ARG, "meshlet triangle count outside 1..128");
+    tri_total += tc;
+  }
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  uint32_t slot = 0;
+  while (slot < ctx->slots_used && ctx->mesh_host[slot].used) slot++;
+  if (slot >= ctx->slot_capacity) {
+    uint32_t cap = ctx->slot_capacity * 2;
+    ctx->meshes.resize(cap);
+    ctx->mesh_host.resize(cap);
+    ctx->slot_capacity = cap;
+  }
+  MeshHost &m = ctx->mesh_host[slot];
+  m = MeshHost();
+  m.used = true;
+  m.meshlet_base = (uint32_t)ctx->m_lod.size();
+  m.meshlet_count = d->meshlet_count;
+  m.level_base = (uint32_t)ctx->levels.size();
+  m.level_count = d->level_count;
+  m.triangle_base = (uint32_t)ctx->m_tris.size();
+  m.triangle_count = d->meshlet_triangles ? d->meshlet_triangle_count : 0;
+  m.instance_base = (uint32_t)ctx->inst_slot.size();
+  m.instance_count = n;
+  m.cell_base = (uint32_t)ctx->cells.size();
+  m.cell_count = (n + kCellSize - 1) / kCellSize;
+  std::memcpy(m.sphere, d->bounding_sphere, sizeof m.sphere);
+  for (uint32_t i = 0; i < d->meshlet_count; i++) {
+    const float *b = d->meshlet_bounds + (size_t)i * 16;
+    const uint32_t *info = d->meshlet_info + (size_t)i * 4;
+    ctx->m_lod.push_back(make_float4(b[0], b[1], b[2], b[3]));
+    ctx->m_parent.push_back(make_float4(b[4], b[5], b[6], b[7]));
+    float tc;
+    std::memcpy(&tc, &info[0], 4);
+    ctx->m_err.push_back(make_float4(b[8], b[9], tc, 0.0f));
+    ctx->m_cull.push_back(make_float4(b[12], b[13], b[14], b[15]));
+    // rebased to pool-global index / vertex ranges (GeometryPool.ts:417-426)
+    ctx->m_info.push_back(make_uint4(info[0], info[1] + m.triangle_base * 3, info[2], info[3]));
+  }
+  if (d->meshlet_triangles) ctx->m_tris.insert(ctx->m_tris.end(), d->meshlet_triangles, d->meshlet_triangles + d->meshlet_triangle_count);
+  for (uint32_t l = 0; l < d->level_count; l++) {
+    LevelRec L;
+    L.first = d->level_ranges[l * 2] + m.meshlet_base;
+    L.count = d->level_ranges[l * 2 + 1];
+    L.min_own = d->level_errors[l * 2];
+    L.max_parent = d->level_errors[l * 2 + 1];
+    L.max_own = d->level_guard_errors[l * 2];
+    L.min_parent = d->level_guard_errors[l * 2 + 1];
+    L.pad0 = L.pad1 = 0;
+    ctx->levels.push_back(L);
+  }
+  std::vector<uint32_t> order;
+  morton_order(matrices, n, d->bounding_sphere, order);
+  for (uint32_t g = 0; g < n; g++) {
+    const float *e = matrices + (size_t)order[g] * 16;
+    for (int c = 0; c < 4; c++) ctx->inst.push_back(make_float4(e[c * 4], e[c * 4 + 1], e[c * 4 + 2], e[c * 4 + 3]));
+    ctx->inst_slot.push_back(slot);
+    if (gpu_to_input) gpu_to_input[g] = order[g];
+  }
+  ctx->cells.resize(ctx->cells.size() + m.cell_count);
+  for (uint32_t c = 0; c < m.cell_count; c++) compute_cell(ctx, slot, c);
+  MeshRec &r = ctx->meshes[slot];
+  r.sphere = make_float4(d->bounding_sphere[0], d->bounding_sphere[1], d->bounding_sphere[2], d->bounding_sphere[3]);
+  r.lod = make_float4(d->lod_bounds_sphere[0], d->lod_bounds_sphere[1], d->lod_bounds_sphere[2], d->lod_bounds_sphere[3]);
+  r.cull = make_float4(d->cull_bounds_sphere[0], d->cull_bounds_sphere[1], d->cull_bounds_sphere[2], d->cull_bounds_sphere[3]);
+  r.level_count = d->level_count;
+  r.level_base = m.level_base;
+  r.meshlet_base = m.meshlet_base;
+  vgc_mesh_opts def = {0.0f, 0.0f, 1u, 0u, 0u};
+  write_flags(ctx, slot, opts ? opts : &def);
+  ctx->slots_used = std::max(ctx->slots_used, slot + 1);
+  ctx->dirty = true;
+  (void)tri_total;
+  *slot_out = slot;
+  return VGC_OK;
+}
+
+int vgc_mesh_set_flags(vgc_context *ctx, uint32_t slot, const vgc_mesh_opts *opts) {
+  if (!ctx || !opts) return fail(VGC_INVALID_ARG, "null argument");
+  if (slot >= ctx->slots_used || !ctx->mesh_host[slot].used) return fail(VGC_NOT_FOUND, "no mesh in slot");
+  write_flags(ctx, slot, opts);
+  ctx->dirty = true;
+  return VGC_OK;
+}
+
+int vgc_instances_update(vgc_context *ctx, uint32_t slot, uint32_t first, uint32_t count, const float *matrices) {
+  if (!ctx || (count && !matrices)) return fail(VGC_INVALID_ARG, "null argument");
+  if (slot >= ctx->slots_used || !ctx->mesh_host[slot].used) return fail(VGC_NOT_FOUND, "no mesh in slot");
+  MeshHost &m = ctx->mesh_host[slot];
+  if ((uint64_t)first + count > m.instance_count) return fail(VGC_INVALID_ARG, "instance range out of bounds");
+  for (uint32_t g = 0; g < count; g++) {
+    const float *e = matrices + (size_t)g * 16;
+    for (int c = 0; c < 4; c++) ctx->inst[(size_t)(m.instance_base + first + g) * 4 + c] = make_float4(e[c * 4], e[c * 4 + 1], e[c * 4 + 2], e[c * 4 + 3]);
+  }
+  if (count)
+    for (uint32_t c = first / kCellSize; c <= (first + count - 1) / kCellSize; c++) compute_cell(ctx, slot, c);
+  ctx->dirty = true;
+  return VGC_OK;
+}
+
+int vgc_mesh_remove(vgc_context *ctx, uint32_t slot) {
+  if (!ctx) return fail(VGC_INVALID_ARG, "null argument");
+  if (slot >= ctx->slots_used || !ctx->mesh_host[slot].used) return fail(VGC_NOT_FOUND, "no mesh in slot");
+  // its cells stay in the cell buffer but point at a disabled slot (GeometryPool.ts:358-363)
+  ctx->meshes[slot].enabled = 0;
+  ctx->mesh_host[slot].used = false;
+  ctx->dirty = true;
+  return VGC_OK;
+}
+
+int vgc_mesh_slots(const vgc_context *ctx, uint32_t *used, uint32_t *capacity) {
+  if (!ctx) return fail(VGC_INVALID_ARG, "null argument");
+  if (used) *used = ctx->slots_used;
+  if (capacity) *capacity = ctx->slot_capacity;
+  return VGC_OK;
+}
+
+int vgc_hzb_build(vgc_context *ctx, int32_t hzb, const float *depth, uint32_t width, uint32_t height, int on_device,
+                  vgc_stream stream) {
+  if (!ctx || !depth) return fail(VGC_INVALID_ARG, "null argument");
+  if (hzb < 0 || hzb >= (int32_t)vgc_context::kHzbSlots) return fail(VGC_INVALID_ARG, "hzb slot out of range");
+  if (width == 0 || height == 0 || width > 32768 || height > 32768) return fail(VGC_INVALID_ARG, "HZB size out of range");
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  HzbSlot &h = ctx->hzb[hzb];
+  HzbDesc desc{};
+  uint32_t lw = width, lh = height, n = 0;
+  size_t total = 0;
+  for (;;) {
+    desc.off[n] = (uint32_t)total;
+    desc.w[n] = lw;
+    desc.h[n] = lh;
+    total += (size_t)lw * lh;
+    n++;
+    if ((lw == 1 && lh == 1) || n == kMaxHzbLevels) break;
+    lw = lw > 1 ? (lw + 1) / 2 : 1;
+    lh = lh > 1 ? (lh + 1) / 2 : 1;
+  }
+  desc.levels = n;
+  if (h.data.bytes < total * 4) {
+    CUDA_TRY(cudaStreamSynchronize(st));
+    int rc = dev_alloc(ctx, h.data, total * 4);
+    if (rc) return rc;
+  }
+  desc.data = (const float *)h.data.ptr;
+  float *out = (float *)h.data.ptr;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(st, &cs);
+  const bool capture = cs != cudaStreamCaptureStatusNone;
+  if (!on_device) {
+    CUDA_TRY(cudaMemcpyAsync(out, depth, (size_t)width * height * 4, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(timed(ctx, capture, VGC_KERNEL_HZB, st, [&] { return launch_hzb(out, desc, out, 0, st); }));
+  } else {
+    CUDA_TRY(timed(ctx, capture, VGC_KERNEL_HZB, st, [&] { return launch_hzb(depth, desc, out, 1, st); }));
+  }
+  h.desc = desc;
+  h.valid = true;
+  CUDA_TRY(cudaMemcpyAsync((HzbDesc *)ctx->d_hzb_desc.ptr + hzb, &h.desc, sizeof(HzbDesc), cudaMemcpyHostToDevice, st));
+  return VGC_OK;
+}
+
+int vgc_hzb_info(const vgc_context *ctx, int32_t hzb, uint32_t *levels, uint32_t *offset, uint32_t *width,
+                 uint32_t *height, const float **data) {
+  if (!ctx) return fail(VGC_INVALID_ARG, "null context");
+  if (hzb < 0 || hzb >= (int32_t)vgc_context::kHzbSlots || !ctx->hzb[hzb].valid) return fail(VGC_NOT_FOUND, "no HZB in slot");
+  const HzbDesc &d = ctx->hzb[hzb].desc;
+  if (levels) *levels = d.levels;
+  for (uint32_t i = 0; i < kMaxHzbLevels; i++) {
+    if (offset) offset[i] = d.off[i];
+    if (width) width[i] = d.w[i];
+    if (height) height[i] = d.h[i];
+  }
+  if (data) *data = d.data;
+  return VGC_OK;
+}
+
+int vgc_cut(vgc_context *ctx, const vgc_view *views, uint32_t count, uint32_t first_slot, vgc_stream stream) {
+  if (!ctx) return fail(VGC_INVALID_ARG, "null context");
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  int rc = prepare(ctx, ctx->scratch, views, count, first_slot);
+  if (rc) return rc;
+  if ((rc = enqueue(ctx, ctx->scratch, count, st, false))) return rc;
+  CUDA_TRY(cudaEventRecord(ctx->scratch.done, st));
+  ctx->scratch.pending = true;
+  return VGC_OK;
+}
+
+int vgc_batch_create(vgc_context *ctx, uint32_t max_views, vgc_batch **out) {
+  if (!ctx || !out || max_views == 0) return fail(VGC_INVALID_ARG, "bad arguments");
+  vgc_batch *b = new vgc_batch();
+  b->ctx = ctx;
+  b->max_views = max_views;
+  if (cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete b;
+    return fail(VGC_DEVICE_ERROR, "cudaStreamCreate failed");
+  }
+  *out = b;
+  return VGC_OK;
+}
+
+int vgc_batch_run(vgc_batch *b, const vgc_view *views, uint32_t count, uint32_t first_slot, vgc_stream stream) {
+  if (!b) return fail(VGC_INVALID_ARG, "null batch");
+  if (count > b->max_views) return fail(VGC_INVALID_ARG, "more views than the batch was created for");
+  vgc_context *ctx = b->ctx;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  int rc = prepare(ctx, b->scratch, views, count, first_slot);
+  if (rc) return rc;
+  const uint32_t cells = (uint32_t)ctx->cells.size();
+  if (!b->exec || b->graph_views != count || b->graph_cells != cells || b->graph_slots != ctx->slot_capacity) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    CUDA_TRY(cudaStreamBeginCapture(b->capture_stream, cudaStreamCaptureModeThreadLocal));
+    rc = enqueue(ctx, b->scratch, count, b->capture_stream, true);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(b->capture_stream, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return fail(VGC_DEVICE_ERROR, std::string("graph capture: ") + cudaGetErrorString(e));
+    b->graph = g;
+    CUDA_TRY(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    b->graph_views = count;
+    b->graph_cells = cells;
+    b->graph_slots = ctx->slot_capacity;
+  }
+  CUDA_TRY(cudaGraphLaunch(b->exec, st));
+  CUDA_TRY(cudaEventRecord(b->scratch.done, st));
+  b->scratch.pending = true;
+  return VGC_OK;
+}
+
+int vgc_batch_destroy(vgc_batch *b) {
+  if (!b) return VGC_OK;
+  cudaSetDevice(b->ctx->device);
+  if (b->scratch.pending) cudaEventSynchronize(b->scratch.done);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
+  if (b->scratch.d_views) b->ctx->bytes -= sizeof(ViewConst) * b->scratch.view_capacity;
+  if (b->scratch.d_units) b->ctx->bytes -= b->scratch.unit_capacity * sizeof(uint2);
+  free_scratch(b->scratch);
+  delete b;
+  return VGC_OK;
+}
+
+int vgc_get_output(const vgc_context *ctx, uint32_t slot, vgc_output *out) {
+  if (!ctx || !out) return fail(VGC_INVALID_ARG, "null argument");
+  if (slot >= ctx->out_slots) return fail(VGC_NOT_FOUND, "output slot not allocated");
+  const size_t md = ctx->opts.max_meshlets;
+  const uint4 *draw = (const uint4 *)ctx->d_draw.ptr + (size_t)slot * 2 * md;
+  out->draw_list[0] = (const uint32_t *)draw;
+  out->draw_list[1] = (const uint32_t *)(draw + md);
+  out->draw_args = (const uint32_t *)ctx->d_args.ptr + (size_t)slot * 2 * ctx->slot_capacity * 2 * 5;
+  out->counters = (const uint32_t *)ctx->d_counters.ptr + (size_t)slot * ctx->counter_words;
+  out->max_drawn = (uint32_t)md;
+  out->mesh_slots = ctx->slot_capacity;
+  return VGC_OK;
+}
+
+int vgc_read_stats(vgc_context *ctx, uint32_t slot, vgc_stats *s, vgc_stream stream) {
+  if (!ctx || !s) return fail(VGC_INVALID_ARG, "null argument");
+  if (slot >= ctx->out_slots) return fail(VGC_NOT_FOUND, "output slot not allocated");
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  CUDA_TRY(cudaStreamSynchronize(st));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  uint32_t c[VGC_COUNTER_HEADER];
+  CUDA_TRY(cudaMemcpy(c, (const uint32_t *)ctx->d_counters.ptr + (size_t)slot * ctx->counter_words, sizeof c, cudaMemcpyDeviceToHost));
+  std::memset(s, 0, sizeof *s);
+  s->visible_cells = c[VGC_COUNTER_CELLS];
+  s->occluded_instances = c[VGC_COUNTER_OCCLUDED];
+  for (int cut = 0; cut < 2; cut++) {
+    const uint32_t *k = c + VGC_COUNTER_CUT0 + cut * 5;
+    s->selected[cut] = k[VGC_CUT_SELECTED];
+    s->drawn[cut] = k[VGC_CUT_DRAWN];
+    s->survived[cut] = k[VGC_CUT_SURVIVED];
+    s->work[cut] = k[VGC_CUT_WORK];
+    s->requested_indices[cut] = k[VGC_CUT_REQUESTED];
+    const uint32_t cap = cut == 0 ? ctx->opts.max_triangles * 3 : ctx->opts.max_shadow_triangles * 3;
+    if (k[VGC_CUT_SELECTED] > ctx->opts.max_meshlets || k[VGC_CUT_REQUESTED] > cap) s->overflow = 1;
+  }
+  s->rounds = c[VGC_COUNTER_ROUNDS];
+  s->instances_tested = c[VGC_COUNTER_INSTANCES_TESTED];
+  s->meshlets_tested = c[VGC_COUNTER_MESHLETS_TESTED];
+  s->fast_emitted = c[VGC_COUNTER_FAST_EMITTED];
+  s->levels_read = c[VGC_COUNTER_LEVELS_READ];
+  float dyn = 0;
+  CUDA_TRY(cudaMemcpy(&dyn, (const float *)ctx->d_dyn.ptr + (size_t)slot * 4, 4, cudaMemcpyDeviceToHost));
+  s->effective_threshold = dyn;
+  return VGC_OK;
+}
+
+int vgc_read_draw_list(vgc_context *ctx, uint32_t slot, uint32_t cut, uint32_t *entries, uint32_t capacity,
+                       uint32_t *count, vgc_stream stream) {
+  if (!ctx || !count || cut > 1 || (capacity && !entries)) return fail(VGC_INVALID_ARG, "bad arguments");
+  if (slot >= ctx->out_slots) return fail(VGC_NOT_FOUND, "output slot not allocated");
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  CUDA_TRY(cudaStreamSynchronize(st));
+  uint32_t sel = 0;
+  CUDA_TRY(cudaMemcpy(&sel, (const uint32_t *)ctx->d_counters.ptr + (size_t)slot * ctx->counter_words + VGC_COUNTER_CUT0 + cut * 5 + VGC_CUT_SELECTED, 4, cudaMemcpyDeviceToHost));
+  const uint32_t n = std::min(sel, ctx->opts.max_meshlets);
+  *count = n;
+  const uint32_t copy = std::min(n, capacity);
+  if (copy) {
+    const uint4 *src = (const uint4 *)ctx->d_draw.ptr + ((size_t)slot * 2 + cut) * ctx->opts.max_meshlets;
+    CUDA_TRY(cudaMemcpy(entries, src, (size_t)copy * 16, cudaMemcpyDeviceToHost));
+  }
+  return VGC_OK;
+}
+
+int vgc_state_access(vgc_context *ctx, uint32_t state_slot, uint32_t *words, int write, vgc_stream stream) {
+  if (!ctx || !words) return fail(VGC_INVALID_ARG, "null argument");
+  int rc = ensure_state(ctx, state_slot);
+  if (rc) return rc;
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  CUDA_TRY(cudaStreamSynchronize(st));
+  uint32_t *dst = (uint32_t *)ctx->d_state.ptr + (size_t)state_slot * kStateWords;
+  if (write) CUDA_TRY(cudaMemcpy(dst, words, kStateWords * 4, cudaMemcpyHostToDevice));
+  else CUDA_TRY(cudaMemcpy(words, dst, kStateWords * 4, cudaMemcpyDeviceToHost));
+  return VGC_OK;
+}
+
+int vgc_expand(vgc_context *ctx, uint32_t slot, uint32_t cut, uint32_t *index_buffer, uint64_t capacity, vgc_stream stream) {
+  if (!ctx || !index_buffer || cut > 1) return fail(VGC_INVALID_ARG, "bad arguments");
+  if (slot >= ctx->out_slots) return fail(VGC_NOT_FOUND, "output slot not allocated");
+  for (uint32_t m = 0; m < ctx->slots_used; m++)
+    if (ctx->mesh_host[m].used && ctx->mesh_host[m].triangle_count == 0)
+      return fail(VGC_INVALID_ARG, "vgc_expand needs meshlet_triangles for every mesh (slot " + std::to_string(m) + ")");
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  // the view constants of this slot, rebuilt from the output pointers (only the pointers and sizes are read)
+  ViewConst k{};
+  k.max_drawn = ctx->opts.max_meshlets;
+  k.counters = (uint32_t *)ctx->d_counters.ptr + (size_t)slot * ctx->counter_words;
+  k.draw_list = (uint4 *)ctx->d_draw.ptr + (size_t)slot * 2 * ctx->opts.max_meshlets;
+  int rc = ensure_scratch(ctx, ctx->scratch, 1, 32);
+  if (rc) return rc;
+  if (ctx->scratch.pending) CUDA_TRY(cudaEventSynchronize(ctx->scratch.done));
+  ctx->scratch.h_views[0] = k;
+  CUDA_TRY(cudaMemcpyAsync(ctx->scratch.d_views, ctx->scratch.h_views, sizeof(ViewConst), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(launch_expand(scene_of(ctx), ctx->scratch.d_views, cut, index_buffer, capacity, ctx->sm_count * 8, st));
+  CUDA_TRY(cudaEventRecord(ctx->scratch.done, st));
+  ctx->scratch.pending = true;
+  return VGC_OK;
+}
+
+int vgc_select_cut(vgc_context *ctx, uint32_t slot, uint32_t count, const double *vm16, const double *proj_scale,
+                   const double *near_, const double *scale, double threshold, double blend, uint8_t *lo, uint8_t *hi) {
+  if (!ctx || !vm16 || !proj_scale || !near_ || !scale || !lo || !hi) return fail(VGC_INVALID_ARG, "null argument");
+  if (slot >= ctx->slots_used || !ctx->mesh_host[slot].used) return fail(VGC_NOT_FOUND, "no mesh in slot");
+  if (count == 0) return VGC_OK;
+  cudaSetDevice(ctx->device);
+  int rc = sync_scene(ctx);
+  if (rc) return rc;
+  const uint32_t mcount = ctx->mesh_host[slot].meshlet_count;
+  std::vector<float> m((size_t)count * 16), p((size_t)count * 3);
+  for (size_t i = 0; i < m.size(); i++) m[i] = (float)vm16[i];
+  for (uint32_t i = 0; i < count; i++) {
+    p[i * 3] = (float)proj_scale[i];
+    p[i * 3 + 1] = (float)near_[i];
+    p[i * 3 + 2] = (float)scale[i];
+  }
+  const size_t outn = (size_t)count * mcount;
+  void *d = nullptr;
+  CUDA_TRY(cudaMalloc(&d, m.size() * 4 + p.size() * 4 + outn * 2 + 64));
+  float *dm = (float *)d, *dp = dm + m.size();
+  uint8_t *dlo = (uint8_t *)(dp + p.size()), *dhi = dlo + outn;
+  cudaStream_t st = ctx->stream;
+  cudaError_t e = cudaMemcpyAsync(dm, m.data(), m.size() * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dp, p.data(), p.size() * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = launch_select_cut(scene_of(ctx), slot, mcount, count, dm, dp, (float)threshold, (float)blend, dlo, dhi,
+                          ctx->sm_count * 8, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(lo, dlo, outn, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(hi, dhi, outn, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(VGC_DEVICE_ERROR, std::string("select_cut: ") + cudaGetErrorString(e));
+  return VGC_OK;
+}
+
+int vgc_set_profiling(vgc_context *ctx, int enable) {
+  if (!ctx) return fail(VGC_INVALID_ARG, "null context");
+  ctx->profiling = enable != 0;
+  return VGC_OK;
+}
+
+int vgc_kernel_times(vgc_context *ctx, double *ms, uint32_t *launches, int reset) {
+  if (!ctx) return fail(VGC_INVALID_ARG, "null context");
+  for (auto &p : ctx->prof_pending) {
+    CUDA_TRY(cudaEventSynchronize(p.second.second));
+    float t = 0;
+    CUDA_TRY(cudaEventElapsedTime(&t, p.second.first, p.second.second));
+    ctx->prof_ms[p.first] += t;
+    ctx->prof_count[p.first] += 1;
+    ctx->prof_free.push_back(p.second.first);
+    ctx->prof_free.push_back(p.second.second);
+  }
+  ctx->prof_pending.clear();
+  for (int k = 0; k < VGC_KERNEL_KINDS; k++) {
+    if (ms) ms[k] = ctx->prof_ms[k];
+    if (launches) launches[k] = ctx->prof_count[k];
+    if (reset) {
+      ctx->prof_ms[k] = 0;
+      ctx->prof_count[k] = 0;
+    }
+  }
+  return VGC_OK;
+}
+
+// Test support: the scene's cell records (8 floats each: centre, radius, max radius, slot, first, count as float
+// values, the reference's cell layout GeometryPool.ts:544) and the Morton-ordered instance matrices.
+int vgc_debug_scene(const vgc_context *ctx, float *cells, uint32_t cell_capacity, float *matrices,
+                    uint32_t matrix_capacity, uint32_t *cell_count, uint32_t *instance_count) {
+  if (!ctx) return fail(VGC_INVALID_ARG, "null context");
+  if (cell_count) *cell_count = (uint32_t)ctx->cells.size();
+  if (instance_count) *instance_count = (uint32_t)ctx->inst_slot.size();
+  if (cells)
+    for (uint32_t i = 0; i < std::min<uint32_t>(cell_capacity, (uint32_t)ctx->cells.size()); i++) {
+      const CellRec &c = ctx->cells[i];
+      float *o = cells + (size_t)i * 8;
+      o[0] = c.sphere.x; o[1] = c.sphere.y; o[2] = c.sphere.z; o[3] = c.sphere.w;
+      o[4] = c.max_radius; o[5] = (float)c.slot; o[6] = (float)c.first; o[7] = (float)c.count;
+    }
+  if (matrices)
+    for (uint32_t i = 0; i < std::min<uint32_t>(matrix_capacity, (uint32_t)ctx->inst_slot.size()); i++)
+      std::memcpy(matrices + (size_t)i * 16, &ctx->inst[(size_t)i * 4], 64);
+  return VGC_OK;
+}
+
+}  // extern "C"

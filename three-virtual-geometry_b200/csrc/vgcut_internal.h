@@ -1,0 +1,95 @@
+// Device data layout shared by the kernels and the host context of the cut engine.
+//
+// HBM layout of a resident scene (one context):
+//   meshes      MeshRec[slot_capacity]            mesh table (GeometryPool.ts:449-460: spheres, levers, flags)
+//   levels      LevelRec[]                        level tables (GeometryPool.ts:432-445), 32 B per level
+//   m_lod       float4[M]  LOD sphere             \
+//   m_parent    float4[M]  parent LOD sphere       | meshletBounds (buildVirtualMesh.ts:85-91) split into
+//   m_err       float4[M]  (error, parentError,    | structure-of-arrays so each pass reads only the 16-byte
+//                           triCount bits, 0)      | columns it needs, coalesced (one float4 per lane)
+//   m_cull      float4[M]  culling sphere         /
+//   m_info      uint4[M]   triangleCount, firstIndex (pool-global), lodLevel, vertexOffset
+//   m_tris      u32[]      packed local triangles (meshletTriangles), pool-global
+//   inst        float4[4 I] instance matrix columns, Morton order per mesh (GeometryPool.ts:484-497)
+//   inst_slot   u32[I]     mesh slot of each instance
+//   cells       CellRec[C] 128 consecutive instances of one mesh (GeometryPool.ts:519-545)
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "vgcut.h"
+
+namespace vgc {
+
+constexpr uint32_t kCellSize = 128;        // GeometryPool.ts:96
+constexpr uint32_t kMaxLevels = 48;        // GeometryPool.ts:101
+constexpr uint32_t kFastPathMax = 4;       // constants.ts FAST_PATH_MAX_MESHLETS
+constexpr uint32_t kFullFadeBits = 255u << 16;
+constexpr uint32_t kLocalVertexBits = 7;   // ceil(log2(MAX_MESHLET_VERTICES = 128))
+constexpr uint32_t kMaxHzbLevels = 16;
+constexpr uint32_t kStateWords = 8;        // S_SCALE 0..1, S_FILL 2..3, S_RETRY 4..5
+constexpr uint32_t kBudgetBins = 256;
+
+struct MeshRec {  // 80 bytes
+  float4 sphere;
+  float4 lod;
+  float4 cull;
+  float max_draw_distance, min_pixel_radius;
+  uint32_t level_count, level_base;
+  uint32_t enabled, shadow, occlusion, meshlet_base;
+};
+
+struct LevelRec {  // 32 bytes
+  uint32_t first, count;
+  float min_own, max_parent, max_own, min_parent;
+  uint32_t pad0, pad1;
+};
+
+struct CellRec {  // 32 bytes
+  float4 sphere;
+  float max_radius;
+  uint32_t slot, first, count;
+};
+
+struct Scene {
+  const MeshRec *meshes;
+  const LevelRec *levels;
+  const float4 *m_lod, *m_parent, *m_err, *m_cull;
+  const uint4 *m_info;
+  const uint32_t *m_tris;
+  const float4 *inst;
+  const uint32_t *inst_slot;
+  const CellRec *cells;
+  uint32_t cell_count, instance_count, meshlet_count, slot_capacity, slots_used;
+};
+
+struct HzbDesc {
+  const float *data;
+  uint32_t levels;
+  uint32_t off[kMaxHzbLevels], w[kMaxHzbLevels], h[kMaxHzbLevels];
+};
+
+// Per-view constants derived on the host in double precision (VirtualGeometry.ts:414-442) and stored as float.
+struct ViewConst {
+  float V[12];        // rows 0..2 of world->view, row-major 3x4
+  float plane[24];    // 6 view-space frustum planes (xyz normal, w), normalised
+  float sweep[6];     // per-plane max(dot(world normal, shadowSweep), 0)
+  float proj_scale, near_, P0, P5, P8, P9, P10, P14;
+  float error_threshold, lod_blend_max, shadow_error_scale, lod_scale_limit, min_pixel_radius;
+  float budget, budget_lo, budget_hi;  // triangleBudget search (0 = off)
+  uint32_t frustum, occl_active;
+  uint32_t unit_offset;  // first padded (view, cell) unit of this view in the cell pass
+  uint32_t max_drawn;
+  uint32_t index_capacity[2];
+  int32_t hzb;          // HZB slot or -1
+  uint32_t pad;
+  uint32_t *counters;   // VGC_COUNTER_* header, then per (cut, slot, part): count, start
+  uint32_t *state;      // kStateWords, carried between frames
+  uint4 *draw_list;     // 2 * max_drawn
+  uint32_t *draw_args;  // 2 cuts * slot_capacity * 2 parts * 5
+  float *dyn;           // [0] effective error threshold (budget search result)
+  unsigned long long *hist;  // 2 * kBudgetBins: triangles entering / leaving the cut per threshold bin
+};
+
+}  // namespace vgc
