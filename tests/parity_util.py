@@ -96,8 +96,10 @@ class Harness:
             k = c[2 + cut * 5: 7 + cut * 5]
             got = [stats["selected"][cut], stats["drawn"][cut], stats["survived"][cut], stats["work"][cut],
                    stats["requested_indices"][cut]]
-            assert got == k, f"cut {cut} counters gpu {got} oracle {k}"
             overflow = k[0] > self.max_meshlets
+            if overflow:  # which entries are kept (and so the requested index count) depends on atomic order
+                got, k = got[:4], k[:4]
+            assert got == k, f"cut {cut} counters gpu {got} oracle {k}"
             if not overflow:
                 g = key_set(lists[cut], (0, 1, 3))
                 o = key_set(res["entries"][cut], (0, 1, 2))

@@ -78,13 +78,18 @@ def ruins_small():
 def test_ruins_small_with_shadow_and_occlusion(ruins_small):
     h = ruins_small
     vg = h.vg
+    with_hzb = without = shadow = 0
     for k, cam in enumerate(h.spec.cameras):
         vg.build_hzb(k, h.spec.depth_images[k])
         hzb = O.hzb_build(h.spec.depth_images[k])
         p = engine.ViewParams(error_threshold=1.0, hzb=k, shadow_sweep=(30.0, -60.0, 10.0))
         lists, res = h.compare(cam, p, hzb_oracle=hzb)
-        assert res["counters"][1] > 0 or k > 0  # occlusion is exercised
-        assert len(lists[1]) > 0  # the shadow cut is exercised
+        with_hzb += len(lists[0])
+        shadow += len(lists[1])
+        res_open, _ = h.oracle(cam, engine.ViewParams(error_threshold=1.0, shadow_sweep=(30.0, -60.0, 10.0)))
+        without += len(res_open["entries"][0])
+    assert shadow > 0, "the shadow cut is exercised"
+    assert with_hzb < without, "occlusion removes instances or meshlets"
 
 
 def test_hzb_mips_bit_exact(ruins_small):
