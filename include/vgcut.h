@@ -93,6 +93,11 @@ typedef struct vgc_view {
   int32_t hzb;                  /* HZB slot for occlusion culling of the camera cut; -1 = off */
   uint32_t state_slot;          /* capacity-controller state carried between frames of one camera */
   uint32_t flags;               /* reserved, 0 */
+  /* Optional occluder depth of this frame (device memory, NDC depth, row 0 at the top): when set with hzb >= 0,
+     the cut first builds HZB slot `hzb` from it in the same launch sequence, as the reference prepends its HZB
+     kernels to the frame's compute submission (VirtualGeometry.ts:482-484). NULL: use the slot as built. */
+  const float *depth;
+  uint32_t depth_width, depth_height;
 } vgc_view;
 
 /* Device pointers of one output slot. */
@@ -210,7 +215,7 @@ int vgc_select_cut(vgc_context *ctx, uint32_t slot, uint32_t count, const double
 
 /* ---------------------------------------------------------------- profiling (no counterpart in the reference) */
 enum { VGC_KERNEL_RESET = 0, VGC_KERNEL_CELLS = 1, VGC_KERNEL_SELECT0 = 2, VGC_KERNEL_SELECT_RETRY = 3,
-       VGC_KERNEL_FINISH = 4, VGC_KERNEL_HZB = 5, VGC_KERNEL_KINDS = 8 };
+       VGC_KERNEL_FINISH = 4, VGC_KERNEL_HZB = 5, VGC_KERNEL_CHUNKS0 = 6, VGC_KERNEL_KINDS = 8 };
 /* With `enable`, the plain path (vgc_cut, vgc_hzb_build) records CUDA events around each of its kernel launches
    on the launching stream. vgc_kernel_times synchronises and returns, per VGC_KERNEL_* kind, the summed device
    milliseconds and the launch count since the last reset (reset = 1 clears them). */

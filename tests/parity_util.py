@@ -109,7 +109,9 @@ class Harness:
         out = self.vg.output(slot)
         args = d2h(out.draw_args, 2 * out.mesh_slots * 2 * 5).reshape(2, out.mesh_slots, 2, 5)
         n = len(self.spec.meshes)
-        assert np.array_equal(args[:, :n], res["draw_args"]), "drawIndexedIndirect args differ"
+        for cut in (0, 1):
+            if c[2 + cut * 5] <= self.max_meshlets:  # under overflow the kept entries depend on atomic order
+                assert np.array_equal(args[cut, :n], res["draw_args"][cut]), "drawIndexedIndirect args differ"
         st = self.vg.state(params.state_slot)
         assert list(st) == res["state"], f"controller state gpu {list(st)} oracle {res['state']}"
         return lists, res

@@ -211,3 +211,23 @@ def test_instance_update_and_flags(plain):
     mesh.visible = True
     stats, lists = h.gpu(cam, p)
     assert key_set(lists[0], (0, 1, 3)) == key_set(before[0], (0, 1, 3))
+
+
+def test_hzb_built_in_cut_sequence(ruins_small):
+    """A view that carries its depth image builds the HZB inside the cut's launches (plain and graph) with the same
+    result as a separately built HZB."""
+    import torch
+    h = ruins_small
+    for graph in (False, True):
+        for k, cam in enumerate(h.spec.cameras[:3]):
+            img = h.spec.depth_images[k]
+            d = torch.from_numpy(img).cuda()
+            p = engine.ViewParams(error_threshold=1.0, hzb=20 + k)
+            v = engine.make_view(cam, p, depth=(d.data_ptr(), img.shape[1], img.shape[0]))
+            h.vg.cut([v], first_slot=0, graph=graph)
+            got = h.vg.draw_list(0, 0)
+            res, _ = h.oracle(cam, p, hzb=O.hzb_build(img))
+            assert key_set(got, (0, 1, 3)) == key_set(res["entries"][0], (0, 1, 2))
+            info = h.vg.hzb_info(20 + k)
+            mips = O.hzb_build(img)[0]
+            assert np.array_equal(d2h(info["data"], len(mips), np.float32), mips)

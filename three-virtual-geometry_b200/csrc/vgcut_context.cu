@@ -64,10 +64,14 @@ uint32_t pad32(uint32_t x) { return (x + 31u) & ~31u; }
 
 // Launch scratch: view constants and the (view, cell) unit list of one launch sequence.
 struct LaunchScratch {
+  uint32_t hzb_w = 0, hzb_h = 0;  // largest depth image the views of this launch build an HZB from (0: none)
+  bool hzb_tail = false;
   ViewConst *h_views = nullptr;  // pinned
   ViewConst *d_views = nullptr;
   uint2 *d_units = nullptr;
-  uint32_t *d_unit_count = nullptr;
+  uint32_t *d_unit_count = nullptr;  // control words (see launch_reset)
+  uint4 *d_chunks = nullptr;
+  uint32_t chunk_capacity = 0;
   uint32_t view_capacity = 0;
   size_t unit_capacity = 0;
   cudaEvent_t done = nullptr;
@@ -128,6 +132,8 @@ struct vgc_batch {
   uint32_t graph_views = 0;
   uint32_t graph_cells = 0;
   uint32_t graph_slots = 0;
+  uint32_t graph_hzb_w = 0, graph_hzb_h = 0;
+  bool graph_hzb_tail = false;
 };
 
 namespace {
@@ -224,7 +230,7 @@ int ensure_outputs(vgc_context *ctx, uint32_t slots) {
   if ((rc = dev_alloc(ctx, ctx->d_counters, (size_t)n * ctx->counter_words * 4))) return rc;
   if ((rc = dev_alloc(ctx, ctx->d_draw, (size_t)n * 2 * md * 16))) return rc;
   if ((rc = dev_alloc(ctx, ctx->d_args, (size_t)n * 2 * ctx->slot_capacity * 2 * 5 * 4))) return rc;
-  if ((rc = dev_alloc(ctx, ctx->d_dyn, (size_t)n * 4 * 4))) return rc;
+  if ((rc = dev_alloc(ctx, ctx->d_dyn, (size_t)n * 8 * 4))) return rc;
   if ((rc = dev_alloc(ctx, ctx->d_hist, (size_t)n * 2 * kBudgetBins * 8))) return rc;
   CUDA_TRY(cudaMemset(ctx->d_counters.ptr, 0, (size_t)n * ctx->counter_words * 4));
   CUDA_TRY(cudaMemset(ctx->d_args.ptr, 0, (size_t)n * 2 * ctx->slot_capacity * 2 * 5 * 4));
@@ -279,7 +285,20 @@ int ensure_scratch(vgc_context *ctx, LaunchScratch &s, uint32_t views, size_t un
     ctx->bytes += n * sizeof(uint2);
     s.unit_capacity = n;
   }
-  if (!s.d_unit_count) CUDA_TRY(cudaMalloc(&s.d_unit_count, 16));
+  if (!s.d_unit_count) CUDA_TRY(cudaMalloc(&s.d_unit_count, 64));
+  // chunk queue: every instance with a level range queues ceil(range / 256) chunks per cut. Sized for 64k chunks
+  // per view; a warp that cannot reserve tests its meshlets itself, so a full queue costs time, not correctness.
+  const uint32_t want_chunks = std::max<uint32_t>(65536, views * 65536u);
+  if (want_chunks > s.chunk_capacity) {
+    if (s.d_chunks) {
+      cudaFree(s.d_chunks);
+      ctx->bytes -= (size_t)s.chunk_capacity * sizeof(uint4);
+    }
+    s.d_chunks = nullptr;
+    CUDA_TRY(cudaMalloc(&s.d_chunks, (size_t)want_chunks * sizeof(uint4)));
+    ctx->bytes += (size_t)want_chunks * sizeof(uint4);
+    s.chunk_capacity = want_chunks;
+  }
   if (!s.done) CUDA_TRY(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
   return VGC_OK;
 }
@@ -290,6 +309,7 @@ void free_scratch(LaunchScratch &s) {
   if (s.d_views) cudaFree(s.d_views);
   if (s.d_units) cudaFree(s.d_units);
   if (s.d_unit_count) cudaFree(s.d_unit_count);
+  if (s.d_chunks) cudaFree(s.d_chunks);
   if (s.done) cudaEventDestroy(s.done);
   s = LaunchScratch();
 }
@@ -312,11 +332,50 @@ void planes_of(const double *me, double out[6][4]) {
   }
 }
 
+HzbDesc hzb_layout(uint32_t width, uint32_t height, size_t *total_floats) {
+  HzbDesc desc{};
+  uint32_t lw = width, lh = height, n = 0;
+  size_t total = 0;
+  for (;;) {
+    desc.off[n] = (uint32_t)total;
+    desc.w[n] = lw;
+    desc.h[n] = lh;
+    total += (size_t)lw * lh;
+    n++;
+    if ((lw == 1 && lh == 1) || n == kMaxHzbLevels) break;
+    lw = lw > 1 ? (lw + 1) / 2 : 1;
+    lh = lh > 1 ? (lh + 1) / 2 : 1;
+  }
+  desc.levels = n;
+  *total_floats = total;
+  return desc;
+}
+
+// Allocates / lays out HZB slot `hzb` for a width x height mip 0 and publishes its descriptor; returns whether the
+// device descriptor array changed (the caller uploads it).
+int hzb_prepare(vgc_context *ctx, int32_t hzb, uint32_t width, uint32_t height, bool *changed) {
+  if (width == 0 || height == 0 || width > 32768 || height > 32768) return fail(VGC_INVALID_ARG, "HZB size out of range");
+  size_t total = 0;
+  HzbDesc desc = hzb_layout(width, height, &total);
+  auto &h = ctx->hzb[hzb];
+  if (h.data.bytes < total * 4) {
+    CUDA_TRY(cudaDeviceSynchronize());
+    int rc = dev_alloc(ctx, h.data, total * 4);
+    if (rc) return rc;
+  }
+  desc.data = (const float *)h.data.ptr;
+  *changed = !h.valid || std::memcmp(&desc, &h.desc, sizeof desc) != 0;
+  h.desc = desc;
+  h.valid = true;
+  return VGC_OK;
+}
+
 int view_constants(vgc_context *ctx, const vgc_view &in, uint32_t out_slot, uint32_t unit_offset, ViewConst &k) {
   if (!(in.viewport_height > 0) || !(in.error_threshold > 0) || !(in.near_ > 0))
     return fail(VGC_INVALID_ARG, "view: viewport_height, error_threshold and near must be > 0");
-  if (in.hzb >= (int32_t)vgc_context::kHzbSlots || (in.hzb >= 0 && !ctx->hzb[in.hzb].valid))
-    return fail(VGC_INVALID_ARG, "view: hzb slot " + std::to_string(in.hzb) + " has no HZB");
+  if (in.hzb >= (int32_t)vgc_context::kHzbSlots) return fail(VGC_INVALID_ARG, "view: hzb slot out of range");
+  if (in.hzb >= 0 && !in.depth && !ctx->hzb[in.hzb].valid)
+    return fail(VGC_INVALID_ARG, "view: hzb slot " + std::to_string(in.hzb) + " has no HZB and the view brings no depth");
   int rc = ensure_state(ctx, in.state_slot);
   if (rc) return rc;
   std::memset(&k, 0, sizeof k);
@@ -357,6 +416,8 @@ int view_constants(vgc_context *ctx, const vgc_view &in, uint32_t out_slot, uint
   k.frustum = in.frustum_culling ? 1u : 0u;
   k.occl_active = in.hzb >= 0 ? 1u : 0u;
   k.hzb = in.hzb;
+  k.build_hzb = (in.hzb >= 0 && in.depth) ? 1u : 0u;
+  k.depth = in.depth;
   k.unit_offset = unit_offset;
   k.max_drawn = ctx->opts.max_meshlets;
   k.index_capacity[0] = ctx->opts.max_triangles * 3;
@@ -365,7 +426,7 @@ int view_constants(vgc_context *ctx, const vgc_view &in, uint32_t out_slot, uint
   k.state = (uint32_t *)ctx->d_state.ptr + (size_t)in.state_slot * kStateWords;
   k.draw_list = (uint4 *)ctx->d_draw.ptr + (size_t)out_slot * 2 * ctx->opts.max_meshlets;
   k.draw_args = (uint32_t *)ctx->d_args.ptr + (size_t)out_slot * 2 * ctx->slot_capacity * 2 * 5;
-  k.dyn = (float *)ctx->d_dyn.ptr + (size_t)out_slot * 4;
+  k.dyn = (float *)ctx->d_dyn.ptr + (size_t)out_slot * 8;
   k.hist = (unsigned long long *)ctx->d_hist.ptr + (size_t)out_slot * 2 * kBudgetBins;
   return VGC_OK;
 }
@@ -379,6 +440,27 @@ int prepare(vgc_context *ctx, LaunchScratch &s, const vgc_view *views, uint32_t 
   const uint32_t cells = pad32((uint32_t)ctx->cells.size());
   if ((rc = ensure_scratch(ctx, s, count, (size_t)count * cells))) return rc;
   if (s.pending) CUDA_TRY(cudaEventSynchronize(s.done));
+  bool changed = false;
+  s.hzb_w = s.hzb_h = 0;
+  s.hzb_tail = false;
+  for (uint32_t i = 0; i < count; i++) {
+    const vgc_view &v = views[i];
+    if (v.hzb >= 0 && v.depth) {
+      for (uint32_t j = 0; j < i; j++)
+        if (views[j].hzb == v.hzb && views[j].depth) return fail(VGC_INVALID_ARG, "two views build the same HZB slot");
+      bool c = false;
+      if ((rc = hzb_prepare(ctx, v.hzb, v.depth_width, v.depth_height, &c))) return rc;
+      changed = changed || c;
+      s.hzb_w = std::max(s.hzb_w, v.depth_width);
+      s.hzb_h = std::max(s.hzb_h, v.depth_height);
+      s.hzb_tail = s.hzb_tail || ctx->hzb[v.hzb].desc.levels > 6;
+    }
+  }
+  if (changed) {
+    std::vector<HzbDesc> all(vgc_context::kHzbSlots);
+    for (uint32_t i = 0; i < vgc_context::kHzbSlots; i++) all[i] = ctx->hzb[i].desc;
+    CUDA_TRY(cudaMemcpy(ctx->d_hzb_desc.ptr, all.data(), sizeof(HzbDesc) * all.size(), cudaMemcpyHostToDevice));
+  }
   for (uint32_t i = 0; i < count; i++)
     if ((rc = view_constants(ctx, views[i], first_slot + i, i * cells, s.h_views[i]))) return rc;
   return VGC_OK;
@@ -414,16 +496,25 @@ int enqueue(vgc_context *ctx, LaunchScratch &s, uint32_t count, cudaStream_t st,
   const uint32_t cells = pad32(S.cell_count);
   const HzbDesc *hzbs = (const HzbDesc *)ctx->d_hzb_desc.ptr;
   CUDA_TRY(cudaMemcpyAsync(s.d_views, s.h_views, sizeof(ViewConst) * count, cudaMemcpyHostToDevice, st));
+  if (s.hzb_w)
+    CUDA_TRY(timed(ctx, capture, VGC_KERNEL_HZB, st, [&] {
+      return launch_hzb_views(s.d_views, count, hzbs, s.hzb_w, s.hzb_h, s.hzb_tail, st);
+    }));
   CUDA_TRY(timed(ctx, capture, VGC_KERNEL_RESET, st,
                  [&] { return launch_reset(s.d_views, count, ctx->counter_words, s.d_unit_count, st); }));
   CUDA_TRY(timed(ctx, capture, VGC_KERNEL_CELLS, st,
                  [&] { return launch_cells(S, s.d_views, count, count * cells, s.d_units, s.d_unit_count, st); }));
   for (int round = 0; round < 3; round++) {
     CUDA_TRY(timed(ctx, capture, round == 0 ? VGC_KERNEL_SELECT0 : VGC_KERNEL_SELECT_RETRY, st, [&] {
-      return launch_select(S, s.d_views, hzbs, s.d_units, s.d_unit_count, round, ctx->select_grid, st);
+      return launch_instances(S, s.d_views, hzbs, s.d_units, s.d_unit_count, s.d_chunks, s.chunk_capacity, round,
+                              ctx->select_grid, st);
     }));
-    CUDA_TRY(timed(ctx, capture, VGC_KERNEL_FINISH, st,
-                   [&] { return launch_finish(s.d_views, count, S.slot_capacity, S.slots_used, round, st); }));
+    CUDA_TRY(timed(ctx, capture, round == 0 ? VGC_KERNEL_CHUNKS0 : VGC_KERNEL_SELECT_RETRY, st, [&] {
+      return launch_chunks(S, s.d_views, hzbs, s.d_chunks, s.d_unit_count, s.chunk_capacity, round, ctx->select_grid, st);
+    }));
+    CUDA_TRY(timed(ctx, capture, VGC_KERNEL_FINISH, st, [&] {
+      return launch_finish(s.d_views, count, S.slot_capacity, S.slots_used, s.d_unit_count, round, st);
+    }));
   }
   return VGC_OK;
 }
@@ -745,27 +836,11 @@ int vgc_hzb_build(vgc_context *ctx, int32_t hzb, const float *depth, uint32_t wi
   if (hzb < 0 || hzb >= (int32_t)vgc_context::kHzbSlots) return fail(VGC_INVALID_ARG, "hzb slot out of range");
   if (width == 0 || height == 0 || width > 32768 || height > 32768) return fail(VGC_INVALID_ARG, "HZB size out of range");
   cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  bool changed = false;
+  int rc = hzb_prepare(ctx, hzb, width, height, &changed);
+  if (rc) return rc;
   HzbSlot &h = ctx->hzb[hzb];
-  HzbDesc desc{};
-  uint32_t lw = width, lh = height, n = 0;
-  size_t total = 0;
-  for (;;) {
-    desc.off[n] = (uint32_t)total;
-    desc.w[n] = lw;
-    desc.h[n] = lh;
-    total += (size_t)lw * lh;
-    n++;
-    if ((lw == 1 && lh == 1) || n == kMaxHzbLevels) break;
-    lw = lw > 1 ? (lw + 1) / 2 : 1;
-    lh = lh > 1 ? (lh + 1) / 2 : 1;
-  }
-  desc.levels = n;
-  if (h.data.bytes < total * 4) {
-    CUDA_TRY(cudaStreamSynchronize(st));
-    int rc = dev_alloc(ctx, h.data, total * 4);
-    if (rc) return rc;
-  }
-  desc.data = (const float *)h.data.ptr;
+  const HzbDesc desc = h.desc;
   float *out = (float *)h.data.ptr;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   cudaStreamIsCapturing(st, &cs);
@@ -776,9 +851,8 @@ int vgc_hzb_build(vgc_context *ctx, int32_t hzb, const float *depth, uint32_t wi
   } else {
     CUDA_TRY(timed(ctx, capture, VGC_KERNEL_HZB, st, [&] { return launch_hzb(depth, desc, out, 1, st); }));
   }
-  h.desc = desc;
-  h.valid = true;
-  CUDA_TRY(cudaMemcpyAsync((HzbDesc *)ctx->d_hzb_desc.ptr + hzb, &h.desc, sizeof(HzbDesc), cudaMemcpyHostToDevice, st));
+  if (changed)
+    CUDA_TRY(cudaMemcpyAsync((HzbDesc *)ctx->d_hzb_desc.ptr + hzb, &h.desc, sizeof(HzbDesc), cudaMemcpyHostToDevice, st));
   return VGC_OK;
 }
 
@@ -831,7 +905,8 @@ int vgc_batch_run(vgc_batch *b, const vgc_view *views, uint32_t count, uint32_t 
   int rc = prepare(ctx, b->scratch, views, count, first_slot);
   if (rc) return rc;
   const uint32_t cells = (uint32_t)ctx->cells.size();
-  if (!b->exec || b->graph_views != count || b->graph_cells != cells || b->graph_slots != ctx->slot_capacity) {
+  if (!b->exec || b->graph_views != count || b->graph_cells != cells || b->graph_slots != ctx->slot_capacity ||
+      b->graph_hzb_w != b->scratch.hzb_w || b->graph_hzb_h != b->scratch.hzb_h || b->graph_hzb_tail != b->scratch.hzb_tail) {
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     b->exec = nullptr;
@@ -850,6 +925,9 @@ int vgc_batch_run(vgc_batch *b, const vgc_view *views, uint32_t count, uint32_t 
     b->graph_views = count;
     b->graph_cells = cells;
     b->graph_slots = ctx->slot_capacity;
+    b->graph_hzb_w = b->scratch.hzb_w;
+    b->graph_hzb_h = b->scratch.hzb_h;
+    b->graph_hzb_tail = b->scratch.hzb_tail;
   }
   CUDA_TRY(cudaGraphLaunch(b->exec, st));
   CUDA_TRY(cudaEventRecord(b->scratch.done, st));
@@ -912,7 +990,7 @@ int vgc_read_stats(vgc_context *ctx, uint32_t slot, vgc_stats *s, vgc_stream str
   s->fast_emitted = c[VGC_COUNTER_FAST_EMITTED];
   s->levels_read = c[VGC_COUNTER_LEVELS_READ];
   float dyn = 0;
-  CUDA_TRY(cudaMemcpy(&dyn, (const float *)ctx->d_dyn.ptr + (size_t)slot * 4, 4, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(&dyn, (const float *)ctx->d_dyn.ptr + (size_t)slot * 8, 4, cudaMemcpyDeviceToHost));
   s->effective_threshold = dyn;
   return VGC_OK;
 }

@@ -83,12 +83,14 @@ struct ViewConst {
   uint32_t max_drawn;
   uint32_t index_capacity[2];
   int32_t hzb;          // HZB slot or -1
-  uint32_t pad;
+  uint32_t build_hzb;   // 1: build HZB slot `hzb` from `depth` before the cut
+  const float *depth;   // occluder depth of this frame (build_hzb)
   uint32_t *counters;   // VGC_COUNTER_* header, then per (cut, slot, part): count, start
   uint32_t *state;      // kStateWords, carried between frames
   uint4 *draw_list;     // 2 * max_drawn
   uint32_t *draw_args;  // 2 cuts * slot_capacity * 2 parts * 5
-  float *dyn;           // [0] effective error threshold (budget search result)
+  float *dyn;           // [0] error threshold of this frame (errorThreshold or the budget search result),
+                        // [1..5] its bands: low (cut 0, 1), high (cut 0, 1), fade scale
   unsigned long long *hist;  // 2 * kBudgetBins: triangles entering / leaving the cut per threshold bin
 };
 

@@ -3,12 +3,11 @@
 // Pass structure for a batch of views (all views of one scene in each launch):
 //   k_cells    one thread per (view, cell): the cell tests of GeometryPool.ts:728-760; surviving (view, cell)
 //              units are compacted with one atomic per warp (__ballot_sync / __popc).
-//   k_select   persistent blocks of 128 threads, one visible unit at a time. Thread i tests instance i of the
-//              cell (GeometryPool.ts:846-913) and picks its LOD level range (selectLevels :771-843). Fast-path
-//              instances emit their meshlets directly; the others become work items kept in shared memory, whose
-//              meshlets the block then tests one per thread over a flattened (item, meshlet) index
-//              (GeometryPool.ts:916-970), reading the struct-of-arrays bounds coalesced. Drawn meshlets are staged
-//              in shared memory (one shared atomic per warp) and flushed with one global atomic per cut and part.
+//   k_instances one warp per 32 instances of a visible unit: the instance tests (GeometryPool.ts:846-913) and the
+//              LOD level range (selectLevels :771-843). Fast-path instances emit their meshlets with warp-aggregated
+//              atomics; the others queue their range as chunks of <= 256 meshlets (one warp-wide reservation).
+//   k_chunks   one warp per chunk: the meshlet tests (GeometryPool.ts:916-970), reading the struct-of-arrays
+//              bounds coalesced; drawn meshlets are staged per warp and placed with one atomic per cut and part.
 //   k_finish   one warp per view: the prefix pass (GeometryPool.ts:973-995) as a warp scan over mesh slots, the
 //              capacity check that schedules a retry round (:1032-1054), and after the last round the steer (:1056-1069).
 //   k_expand   one warp per drawn meshlet: index expansion (GeometryPool.ts:998-1021).
@@ -229,316 +228,390 @@ __global__ void __launch_bounds__(256) k_cells(Scene S, const ViewConst *__restr
   if (vis) units[base + __popc(mask & ((1u << lane) - 1u))] = make_uint2(v, cell);
 }
 
-// ------------------------------------------------------------------------------------------------ k_select
-constexpr int kSelThreads = 128;
-constexpr int kStage = 512;  // staged draw entries per cut (fast path: up to 4 per instance)
+// ------------------------------------------------------------------------------------------------ k_instances
+constexpr int kWarpStage = 96;   // staged draw entries per warp and cut (a step adds <= 32)
+constexpr uint32_t kChunk = 256;  // meshlets per chunk (one warp in k_chunks)
 
-struct SelectSmem {
-  ViewConst view;
-  LevelRec levels[kMaxLevels];
-  float vm[kCellSize][13];
-  uint4 items[2][kCellSize];       // per cut: (instance local | occl << 31, first, last, 0)
-  uint32_t prefix[2][kCellSize + 1];
-  uint4 stage[2][kStage];
-  uint32_t n_items[2];
-  uint32_t stage_n[2];
-  uint32_t idx_n[2][2];
-  uint32_t base_sel[2], base_idx[2][2], kept[2];
-  uint32_t survived[2], work[2], occluded, fast[2];
-  Bands bands;
-  float threshold;
-  uint32_t redo[2];
-  int skip;
+// Band values of a view for the current round, written by k_reset and by the capacity check (dyn[1..5]).
+struct ViewBands {
+  float low0, low1, high0, high1, fade_scale;
 };
 
-// Appends drawn entries of one warp to the block's staging area: one shared atomic for the slot count and one
-// for the two parts' index counts (packed 16 + 16 bits: a warp adds at most 32 * 384 indices per part).
-__device__ __forceinline__ void stage_entries(SelectSmem &sm, uint32_t cut, bool drawn, uint32_t instance,
-                                              uint32_t meshlet, uint32_t packed) {
+__device__ __forceinline__ ViewBands bands_of(const ViewConst &V) {
+  const float *d = V.dyn;
+  return ViewBands{d[1], d[2], d[3], d[4], d[5]};
+}
+
+__device__ __forceinline__ void store_bands(const ViewConst &V, float threshold) {
+  Bands b;
+  load_bands(V, threshold, b);
+  V.dyn[0] = threshold;
+  V.dyn[1] = b.low[0];
+  V.dyn[2] = b.low[1];
+  V.dyn[3] = b.high[0];
+  V.dyn[4] = b.high[1];
+  V.dyn[5] = b.fade_scale;
+}
+
+// Drawn entries of one warp waiting for their draw-list positions; the counts are warp-uniform registers.
+struct WarpStage {
+  uint4 e[2][kWarpStage];
+};
+
+struct WarpCount {
+  uint32_t n;     // staged entries of this cut
+  uint32_t idx0;  // index counts per part, relative to the warp's next region reservation
+  uint32_t idx1;
+};
+
+__device__ __forceinline__ uint32_t warp_scan_incl(uint32_t v) {
+  const uint32_t lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= (uint32_t)o) v += t;
+  }
+  return v;
+}
+
+// Writes one warp's staged entries of `cut` to the view's draw list: one global atomic for the list position and
+// one per part for the mesh's index region (GeometryPool.ts:959-965). Entries past max_drawn are dropped and only
+// the kept ones are counted in the index region, as the reference does.
+__device__ __forceinline__ void warp_flush(WarpStage &ws, WarpCount &wc, const ViewConst &V, uint32_t slot_capacity,
+                                           uint32_t slot, uint32_t cut) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t n = wc.n;
+  if (!n) return;
+  __syncwarp();
+  uint32_t base = 0, kept = 0, b0 = 0, b1 = 0;
+  if (lane == 0) {
+    base = atomicAdd(V.counters + C_CUT(cut) + VGC_CUT_SELECTED, n);
+    kept = base >= V.max_drawn ? 0u : min(n, V.max_drawn - base);
+    uint32_t add0 = wc.idx0, add1 = wc.idx1;
+    if (kept != n) {  // overflow: re-pack the kept prefix
+      add0 = add1 = 0;
+      for (uint32_t s = 0; s < kept; s++) {
+        uint4 &e = ws.e[cut][s];
+        const uint32_t tri3 = (e.w & 255u) * 3u;
+        if (part_of(e.w)) {
+          e.z = add1;
+          add1 += tri3;
+        } else {
+          e.z = add0;
+          add0 += tri3;
+        }
+      }
+    }
+    b0 = add0 ? atomicAdd(mesh_count(V, slot_capacity, cut, slot, 0), add0) : 0u;
+    b1 = add1 ? atomicAdd(mesh_count(V, slot_capacity, cut, slot, 1), add1) : 0u;
+  }
+  base = __shfl_sync(0xffffffffu, base, 0);
+  kept = __shfl_sync(0xffffffffu, kept, 0);
+  b0 = __shfl_sync(0xffffffffu, b0, 0);
+  b1 = __shfl_sync(0xffffffffu, b1, 0);
+  __syncwarp();
+  uint4 *dst = V.draw_list + (size_t)cut * V.max_drawn + base;
+  for (uint32_t s = lane; s < kept; s += 32) {
+    uint4 e = ws.e[cut][s];
+    e.z += part_of(e.w) ? b1 : b0;
+    dst[s] = e;
+  }
+  __syncwarp();
+  wc.n = 0;
+  wc.idx0 = wc.idx1 = 0;
+}
+
+// Stages the drawn entries of one warp-wide step (warp-aggregated: one ballot, one packed 16 + 16-bit scan of the
+// two parts' index counts), flushing when the next step might not fit.
+__device__ __forceinline__ void warp_stage(WarpStage &ws, WarpCount &wc, const ViewConst &V, uint32_t slot_capacity,
+                                           uint32_t slot, uint32_t cut, bool drawn, uint32_t instance, uint32_t meshlet,
+                                           uint32_t packed) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t mask = __ballot_sync(0xffffffffu, drawn);
   if (!mask) return;
   const uint32_t tri3 = drawn ? (packed & 255u) * 3u : 0u;
   const uint32_t part = part_of(packed);
   const uint32_t mine = part == 0 ? tri3 : (tri3 << 16);
-  uint32_t incl = mine;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    uint32_t n = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= (uint32_t)o) incl += n;
-  }
+  const uint32_t incl = warp_scan_incl(mine);
   const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-  uint32_t slot_base = 0, idx0 = 0, idx1 = 0;
-  if (lane == 0) {
-    slot_base = atomicAdd(&sm.stage_n[cut], __popc(mask));
-    idx0 = atomicAdd(&sm.idx_n[cut][0], total & 0xffffu);
-    idx1 = atomicAdd(&sm.idx_n[cut][1], total >> 16);
-  }
-  slot_base = __shfl_sync(0xffffffffu, slot_base, 0);
-  idx0 = __shfl_sync(0xffffffffu, idx0, 0);
-  idx1 = __shfl_sync(0xffffffffu, idx1, 0);
   if (drawn) {
     const uint32_t excl = incl - mine;
-    const uint32_t local = part == 0 ? idx0 + (excl & 0xffffu) : idx1 + (excl >> 16);
-    sm.stage[cut][slot_base + __popc(mask & ((1u << lane) - 1u))] = make_uint4(instance, meshlet, local, packed);
+    const uint32_t local = part == 0 ? wc.idx0 + (excl & 0xffffu) : wc.idx1 + (excl >> 16);
+    ws.e[cut][wc.n + __popc(mask & ((1u << lane) - 1u))] = make_uint4(instance, meshlet, local, packed);
   }
+  wc.n += __popc(mask);
+  wc.idx0 += total & 0xffffu;
+  wc.idx1 += total >> 16;
+  if (wc.n > kWarpStage - 32) warp_flush(ws, wc, V, slot_capacity, slot, cut);
 }
 
-// Writes the staged entries to the view's draw list: one global atomic per cut for the list position and one per
-// (cut, part) for the index region, then a coalesced copy. Entries past max_drawn are dropped, and only the kept
-// ones are counted in the index region, as the reference does (GeometryPool.ts:959-965).
-__device__ void flush_stage(SelectSmem &sm, uint32_t slot_capacity, uint32_t slot) {
-  __syncthreads();
-  const ViewConst &V = sm.view;
-  if (threadIdx.x == 0) {
-    for (uint32_t cut = 0; cut < 2; cut++) {
-      const uint32_t n = sm.stage_n[cut];
-      sm.kept[cut] = 0;
-      if (!n) continue;
-      const uint32_t base = atomicAdd(V.counters + C_CUT(cut) + VGC_CUT_SELECTED, n);
-      sm.base_sel[cut] = base;
-      const uint32_t kept = base >= V.max_drawn ? 0u : min(n, V.max_drawn - base);
-      sm.kept[cut] = kept;
-      uint32_t add[2] = {sm.idx_n[cut][0], sm.idx_n[cut][1]};
-      if (kept != n) {  // overflow: re-pack the kept prefix
-        add[0] = add[1] = 0;
-        for (uint32_t s = 0; s < kept; s++) {
-          uint4 &e = sm.stage[cut][s];
-          const uint32_t p = part_of(e.w);
-          e.z = add[p];
-          add[p] += (e.w & 255u) * 3u;
-        }
-      }
-      for (uint32_t p = 0; p < 2; p++)
-        sm.base_idx[cut][p] = add[p] ? atomicAdd(mesh_count(V, slot_capacity, cut, slot, p), add[p]) : 0u;
-    }
-  }
-  __syncthreads();
-  for (uint32_t cut = 0; cut < 2; cut++) {
-    const uint32_t kept = sm.kept[cut];
-    uint4 *dst = V.draw_list + (size_t)cut * V.max_drawn + sm.base_sel[cut];
-    for (uint32_t s = threadIdx.x; s < kept; s += blockDim.x) {
-      uint4 e = sm.stage[cut][s];
-      e.z += sm.base_idx[cut][part_of(e.w)];
-      dst[s] = e;
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    sm.stage_n[0] = sm.stage_n[1] = 0;
-    sm.idx_n[0][0] = sm.idx_n[0][1] = sm.idx_n[1][0] = sm.idx_n[1][1] = 0;
-  }
-  __syncthreads();
+// The per-meshlet test of GeometryPool.ts:938-957. The conditions are evaluated LOD band first (it rejects most
+// meshlets and needs no HZB samples), then the culling sphere against the frustum and, for the camera cut, the HZB;
+// `drawn` is their conjunction either way. `packed` receives triCount | lo << 8 | hi << 16.
+__device__ __forceinline__ bool test_meshlet(const Scene &S, const ViewConst &V, const HzbDesc *hzbs, float low,
+                                             float high, float fs, float high0, uint32_t cut, bool occl_on,
+                                             const float *VM, uint32_t meshlet, uint32_t &packed) {
+  const float scale = VM[12];
+  const float4 ls = __ldg(S.m_lod + meshlet), ps = __ldg(S.m_parent + meshlet), er = __ldg(S.m_err + meshlet);
+  const float own = proj_error(V, VM, scale, ls, er.x);
+  const float parent = proj_error(V, VM, scale, ps, er.y);
+  if (!(own <= high && parent > low)) return false;
+  const uint32_t lo = fs > 0.0f ? fade_step(own, low, fs) : 0u;
+  const uint32_t hi = fs > 0.0f ? fade_step(parent, low, fs) : 255u;
+  if (!(hi > lo)) return false;
+  packed = __float_as_uint(er.z) | (lo << 8) | (hi << 16);
+  const float4 cs = __ldg(S.m_cull + meshlet);
+  float c[3];
+  xform(VM, cs.x, cs.y, cs.z, c);
+  const float r = cs.w * scale;
+  if (V.frustum && !(frustum(V, c, cut == 1) >= -r)) return false;
+  if (cut == 0 && occluded(V, hzbs, high0, occl_on, c, r)) return false;
+  return true;
 }
 
-// selectLevels (GeometryPool.ts:771-843) for one instance and cut; returns true when the instance survives
-__device__ __forceinline__ void select_levels(SelectSmem &sm, const Scene &S, const MeshRec &mesh, uint32_t cut,
-                                              uint32_t il, uint32_t instance, bool occl_flag, const float *VM,
-                                              float scale, float px_min, float px_max, uint32_t levels,
-                                              uint32_t &fast_n, uint32_t &fast_first) {
-  const float low = sm.bands.low[cut], high = sm.bands.high[cut];
-  uint32_t first = 0xffffffffu, last = 0, possible_m = 0, guaranteed = 0;
+struct LevelRange {
+  uint32_t first, last, possible, guaranteed;
+};
+
+// selectLevels' level loop (GeometryPool.ts:788-812) over the mesh's level table (read through L1: every lane
+// of a warp reads the same entries)
+__device__ __forceinline__ LevelRange level_range(const LevelRec *L, uint32_t levels, float low, float high,
+                                                  float px_min, float px_max) {
+  LevelRange r{0xffffffffu, 0u, 0u, 0u};
   for (uint32_t l = 0; l < levels; l++) {
-    const LevelRec &L = sm.levels[l];
-    bool possible = L.min_own * px_max <= high && (L.max_parent >= float(1e30 * 0.5) || L.max_parent * px_min > low);
-    bool sure = L.max_own * px_min <= low * float(1 - 1e-3) &&
-                (L.min_parent >= float(1e30 * 0.5) || L.min_parent * px_max > high * float(1 + 1e-3));
+    const LevelRec e = L[l];
+    const bool possible = e.min_own * px_max <= high && (e.max_parent >= float(1e30 * 0.5) || e.max_parent * px_min > low);
+    const bool sure = e.max_own * px_min <= low * float(1 - 1e-3) &&
+                      (e.min_parent >= float(1e30 * 0.5) || e.min_parent * px_max > high * float(1 + 1e-3));
     if (possible) {
-      first = min(first, L.first);
-      last = max(last, L.first + L.count);
-      possible_m += L.count;
-      if (sure) guaranteed += L.count;
+      r.first = min(r.first, e.first);
+      r.last = max(r.last, e.first + e.count);
+      r.possible += e.count;
+      if (sure) r.guaranteed += e.count;
     }
   }
-  fast_n = 0;
-  if (!(last > first)) return;
-  float cc[3];
-  xform(VM, mesh.cull.x, mesh.cull.y, mesh.cull.z, cc);
-  const float cr = mesh.cull.w * scale;
-  const bool fast = possible_m > 0 && possible_m == last - first && guaranteed == possible_m &&
-                    possible_m <= kFastPathMax && (!sm.view.frustum || frustum(sm.view, cc, cut == 1) >= cr);
-  atomicAdd(&sm.survived[cut], 1u);
-  if (fast) {
-    fast_n = possible_m;
-    fast_first = first;
-    atomicAdd(&sm.fast[cut], possible_m);
-  } else {
-    const uint32_t k = atomicAdd(&sm.n_items[cut], 1u);
-    sm.items[cut][k] = make_uint4(il | (occl_flag ? 0x80000000u : 0u), first, last, 0);
-  }
+  return r;
 }
 
-__global__ void __launch_bounds__(kSelThreads) k_select(Scene S, const ViewConst *__restrict__ views,
-                                                        const HzbDesc *__restrict__ hzbs,
-                                                        const uint2 *__restrict__ units,
-                                                        const uint32_t *__restrict__ unit_count, int round) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  SelectSmem &sm = *reinterpret_cast<SelectSmem *>(smem_raw);
-  const uint32_t tid = threadIdx.x;
-  const uint32_t n_units = *unit_count;
-  for (uint32_t u = blockIdx.x; u < n_units; u += gridDim.x) {
-    __syncthreads();
-    const uint2 unit = units[u];
-    {  // view constants into shared memory
-      const uint32_t *src = reinterpret_cast<const uint32_t *>(views + unit.x);
-      uint32_t *dst = reinterpret_cast<uint32_t *>(&sm.view);
-      for (uint32_t i = tid; i < sizeof(ViewConst) / 4; i += blockDim.x) dst[i] = src[i];
+// Fast-path entries of one cut for a warp (GeometryPool.ts:827-836): up to 4 meshlets per lane, placed with one
+// atomic for the list position and one for the mesh's region (part 0: drawn over every pixel).
+__device__ __forceinline__ void emit_fast(const Scene &S, const ViewConst &V, uint32_t slot, uint32_t cut,
+                                          uint32_t n, uint32_t first, uint32_t instance) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t incl_n = warp_scan_incl(n);
+  const uint32_t total_n = __shfl_sync(0xffffffffu, incl_n, 31);
+  if (!total_n) return;
+  uint32_t base = 0;
+  if (lane == 0) base = atomicAdd(V.counters + C_CUT(cut) + VGC_CUT_SELECTED, total_n);
+  base = __shfl_sync(0xffffffffu, base, 0) + (incl_n - n);
+  uint32_t tri[kFastPathMax];
+  uint32_t kept_tri3 = 0;
+#pragma unroll
+  for (uint32_t k = 0; k < kFastPathMax; k++) {
+    tri[k] = k < n ? __float_as_uint(S.m_err[first + k].z) : 0u;
+    if (k < n && base + k < V.max_drawn) kept_tri3 += tri[k] * 3u;
+  }
+  const uint32_t incl_t = warp_scan_incl(kept_tri3);
+  const uint32_t total_t = __shfl_sync(0xffffffffu, incl_t, 31);
+  uint32_t ib = 0;
+  if (lane == 0 && total_t) ib = atomicAdd(mesh_count(V, S.slot_capacity, cut, slot, 0), total_t);
+  uint32_t acc = __shfl_sync(0xffffffffu, ib, 0) + (incl_t - kept_tri3);
+  uint4 *dst = V.draw_list + (size_t)cut * V.max_drawn;
+#pragma unroll
+  for (uint32_t k = 0; k < kFastPathMax; k++)
+    if (k < n && base + k < V.max_drawn) {
+      dst[base + k] = make_uint4(instance, first + k, acc, tri[k] | kFullFadeBits);
+      acc += tri[k] * 3u;
     }
-    __syncthreads();
-    const ViewConst &V = sm.view;
-    if (tid == 0) {
-      sm.redo[0] = round == 0 ? 1u : V.counters[VGC_COUNTER_REDO0];
-      sm.redo[1] = round == 0 ? 1u : V.counters[VGC_COUNTER_REDO1];
-      sm.skip = !(sm.redo[0] || sm.redo[1]);
-      sm.threshold = V.budget > 0.0f ? V.dyn[0] : V.error_threshold;
-      load_bands(V, sm.threshold, sm.bands);
-      sm.n_items[0] = sm.n_items[1] = 0;
-      sm.stage_n[0] = sm.stage_n[1] = 0;
-      sm.idx_n[0][0] = sm.idx_n[0][1] = sm.idx_n[1][0] = sm.idx_n[1][1] = 0;
-      sm.survived[0] = sm.survived[1] = sm.work[0] = sm.work[1] = sm.occluded = 0;
-      sm.fast[0] = sm.fast[1] = 0;
+}
+
+// Tests a whole item (one instance's meshlets [first, first + count) of one cut) with the warp: the fallback when
+// the chunk queue is full.
+__device__ void warp_item(const Scene &S, const ViewConst &V, const HzbDesc *hzbs, WarpStage &ws, uint32_t slot,
+                          uint32_t cut, bool occl_on, const float *VM, uint32_t instance, uint32_t first,
+                          uint32_t count) {
+  const ViewBands b = bands_of(V);
+  const float low = cut ? b.low1 : b.low0, high = cut ? b.high1 : b.high0;
+  WarpCount wc{0, 0, 0};
+  for (uint32_t base = 0; base < count; base += 32) {
+    const uint32_t t = base + (threadIdx.x & 31);
+    bool drawn = false;
+    uint32_t packed = 0;
+    if (t < count) drawn = test_meshlet(S, V, hzbs, low, high, b.fade_scale, b.high0, cut, occl_on, VM, first + t, packed);
+    warp_stage(ws, wc, V, S.slot_capacity, slot, cut, drawn, instance, first + t, packed);
+  }
+  warp_flush(ws, wc, V, S.slot_capacity, slot, cut);
+}
+
+// One warp per 32 instances of a visible (view, cell) unit: the instance pass of GeometryPool.ts:846-913. Fast-path
+// instances emit their meshlets; the others hand their level range to k_chunks as chunks of <= kChunk meshlets.
+__global__ void __launch_bounds__(128) k_instances(Scene S, const ViewConst *__restrict__ views,
+                                                   const HzbDesc *__restrict__ hzbs, const uint2 *__restrict__ units,
+                                                   uint32_t *__restrict__ ctl, uint4 *__restrict__ chunks,
+                                                   uint32_t chunk_capacity, int round) {
+  __shared__ WarpStage stage[4];
+  WarpStage &ws = stage[threadIdx.x >> 5];
+  if (round > 0 && ctl[round] == 0) return;  // no view redoes a cut in this round
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t work = ctl[0] * 4;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < work; w += nwarps) {
+    const uint2 unit = units[w >> 2];
+    const ViewConst &V = views[unit.x];
+    bool redo0 = true, redo1 = true;
+    if (round > 0) {
+      redo0 = V.counters[VGC_COUNTER_REDO0] != 0;
+      redo1 = V.counters[VGC_COUNTER_REDO1] != 0;
+      if (!redo0 && !redo1) continue;
     }
     const CellRec cell = S.cells[unit.y];
+    const uint32_t il = ((w & 3u) << 5) + lane;
+    if (((w & 3u) << 5) >= cell.count) continue;
     const MeshRec &mesh = S.meshes[cell.slot];
+    const ViewBands b = bands_of(V);
     const uint32_t levels = min(mesh.level_count, kMaxLevels);
-    {
-      const uint32_t *src = reinterpret_cast<const uint32_t *>(S.levels + mesh.level_base);
-      uint32_t *dst = reinterpret_cast<uint32_t *>(sm.levels);
-      for (uint32_t i = tid; i < levels * (sizeof(LevelRec) / 4); i += blockDim.x) dst[i] = src[i];
-    }
-    __syncthreads();
-    if (sm.skip) continue;
-
-    // ---- instance phase (GeometryPool.ts:874-912)
-    uint32_t fast_n[2] = {0, 0}, fast_first[2] = {0, 0};
-    const uint32_t instance = cell.first + tid;
-    if (tid < cell.count) {
-      float VM[12], scale;
-      model_view(V.V, S.inst + (size_t)instance * 4, VM, scale);
-#pragma unroll
-      for (int i = 0; i < 12; i++) sm.vm[tid][i] = VM[i];
-      sm.vm[tid][12] = scale;
+    const LevelRec *L = S.levels + mesh.level_base;
+    const uint32_t instance = cell.first + il;
+    const bool valid = il < cell.count;
+    const bool occl_on = mesh.occlusion != 0;
+    float VM[13];
+    bool occluded_now = false;
+    LevelRange r0{0xffffffffu, 0, 0, 0}, r1{0xffffffffu, 0, 0, 0};
+    bool fast0 = false, fast1 = false;
+    if (valid) {
+      model_view(V.V, S.inst + (size_t)instance * 4, VM, VM[12]);
+      const float scale = VM[12];
       float c[3];
       xform(VM, mesh.sphere.x, mesh.sphere.y, mesh.sphere.z, c);
       const float radius = mesh.sphere.w * scale;
       const bool no_frustum = !V.frustum;
       bool in_camera = no_frustum || frustum(V, c, false) >= -radius;
       bool in_shadow = mesh.shadow != 0 && (no_frustum || frustum(V, c, true) >= -radius);
-      if (round > 0) {
-        in_camera = in_camera && sm.redo[0];
-        in_shadow = in_shadow && sm.redo[1];
-      }
+      in_camera = in_camera && redo0;
+      in_shadow = in_shadow && redo1;
       const float min_pixels = fmx(V.min_pixel_radius, mesh.min_pixel_radius);
       const float view_distance = len3(c);
       const bool too_small = view_distance > radius && (radius * V.proj_scale) / view_distance < min_pixels;
       const bool too_far = view_distance - radius > mesh.max_draw_distance;
       if ((in_camera || in_shadow) && !too_small && !too_far) {
-        const bool occl_on = mesh.occlusion != 0;
-        if (in_camera && occluded(V, hzbs, sm.bands.high[0], occl_on, c, radius)) {
+        if (in_camera && occluded(V, hzbs, b.high0, occl_on, c, radius)) {
           in_camera = false;
-          atomicAdd(&sm.occluded, 1u);
+          occluded_now = true;
         }
         float lc[3];
         xform(VM, mesh.lod.x, mesh.lod.y, mesh.lod.z, lc);
         const float d = len3(lc), r = mesh.lod.w * scale;
         const float px_min = (scale * V.proj_scale) / fmx(d - r, V.near_);
         const float px_max = (scale * V.proj_scale) / fmx(d + r, V.near_);
-        if (in_camera)
-          select_levels(sm, S, mesh, 0, tid, instance, occl_on, VM, scale, px_min, px_max, levels, fast_n[0], fast_first[0]);
-        if (in_shadow)
-          select_levels(sm, S, mesh, 1, tid, instance, false, VM, scale, px_min, px_max, levels, fast_n[1], fast_first[1]);
-      }
-    }
-    // fast path entries (at most 4 per instance and cut), staged warp by warp
-#pragma unroll
-    for (uint32_t cut = 0; cut < 2; cut++)
-      for (uint32_t k = 0; k < kFastPathMax; k++) {
-        const bool emit = k < fast_n[cut];
-        uint32_t meshlet = fast_first[cut] + k, packed = 0;
-        if (emit) packed = __float_as_uint(S.m_err[meshlet].z) | kFullFadeBits;
-        stage_entries(sm, cut, emit, instance, meshlet, packed);
-      }
-    __syncthreads();
-    // flattened (item, meshlet) index: prefix over item sizes, per cut
-    if (tid < 64) {
-      const uint32_t cut = tid >> 5, lane = tid & 31;
-      const uint32_t n = sm.n_items[cut];
-      uint32_t carry = 0;
-      if (lane == 0) sm.prefix[cut][0] = 0;
-      for (uint32_t b = 0; b < n; b += 32) {
-        const uint32_t k = b + lane;
-        const uint32_t sz = k < n ? sm.items[cut][k].z - sm.items[cut][k].y : 0u;
-        uint32_t incl = sz;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-          if (lane >= (uint32_t)o) incl += t;
+        float cc[3];
+        xform(VM, mesh.cull.x, mesh.cull.y, mesh.cull.z, cc);
+        const float cr = mesh.cull.w * scale;
+        if (in_camera) {
+          r0 = level_range(L, levels, b.low0, b.high0, px_min, px_max);
+          fast0 = r0.last > r0.first && r0.possible == r0.last - r0.first && r0.guaranteed == r0.possible &&
+                  r0.possible <= kFastPathMax && (no_frustum || frustum(V, cc, false) >= cr);
         }
-        if (k < n) sm.prefix[cut][k + 1] = carry + incl;
-        carry += __shfl_sync(0xffffffffu, incl, 31);
+        if (in_shadow) {
+          r1 = level_range(L, levels, b.low1, b.high1, px_min, px_max);
+          fast1 = r1.last > r1.first && r1.possible == r1.last - r1.first && r1.guaranteed == r1.possible &&
+                  r1.possible <= kFastPathMax && (no_frustum || frustum(V, cc, true) >= cr);
+        }
       }
-      if (lane == 0) sm.work[cut] = n;
     }
-    __syncthreads();
-    if (sm.stage_n[0] + sm.stage_n[1]) flush_stage(sm, S.slot_capacity, cell.slot);
+    const bool surv0 = r0.last > r0.first, surv1 = r1.last > r1.first;
+    const bool item0 = surv0 && !fast0, item1 = surv1 && !fast1;
+    // warp totals for the view's counters (one atomic per counter and warp)
+    const uint32_t n_occl = __popc(__ballot_sync(0xffffffffu, occluded_now));
+    const uint32_t n_s0 = __popc(__ballot_sync(0xffffffffu, surv0)), n_s1 = __popc(__ballot_sync(0xffffffffu, surv1));
+    const uint32_t n_i0 = __popc(__ballot_sync(0xffffffffu, item0)), n_i1 = __popc(__ballot_sync(0xffffffffu, item1));
+    const uint32_t fast_m = __reduce_add_sync(0xffffffffu, (fast0 ? r0.possible : 0u) + (fast1 ? r1.possible : 0u));
+    const uint32_t tested = __reduce_add_sync(0xffffffffu, (item0 ? r0.last - r0.first : 0u) + (item1 ? r1.last - r1.first : 0u));
+    if (lane == 0) {
+      uint32_t *ctr = V.counters;
+      if (n_occl) atomicAdd(ctr + VGC_COUNTER_OCCLUDED, n_occl);
+      if (n_s0) atomicAdd(ctr + C_CUT(0) + VGC_CUT_SURVIVED, n_s0);
+      if (n_s1) atomicAdd(ctr + C_CUT(1) + VGC_CUT_SURVIVED, n_s1);
+      if (n_i0) atomicAdd(ctr + C_CUT(0) + VGC_CUT_WORK, n_i0);
+      if (n_i1) atomicAdd(ctr + C_CUT(1) + VGC_CUT_WORK, n_i1);
+      if (fast_m) atomicAdd(ctr + VGC_COUNTER_FAST_EMITTED, fast_m);
+      if (tested) atomicAdd(ctr + VGC_COUNTER_MESHLETS_TESTED, tested);
+      atomicAdd(ctr + VGC_COUNTER_INSTANCES_TESTED, min(32u, cell.count - ((w & 3u) << 5)));
+      if ((w & 3u) == 0) atomicAdd(ctr + VGC_COUNTER_LEVELS_READ, levels);
+    }
+    emit_fast(S, V, cell.slot, 0, fast0 ? r0.possible : 0u, r0.first, instance);
+    emit_fast(S, V, cell.slot, 1, fast1 ? r1.possible : 0u, r1.first, instance);
+    // items -> chunks of <= kChunk meshlets
+    const uint32_t c0 = item0 ? (r0.last - r0.first + kChunk - 1) / kChunk : 0u;
+    const uint32_t c1 = item1 ? (r1.last - r1.first + kChunk - 1) / kChunk : 0u;
+    const uint32_t incl = warp_scan_incl(c0 + c1);
+    const uint32_t want = __shfl_sync(0xffffffffu, incl, 31);
+    if (!want) continue;
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(&ctl[3], want);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    // slots below the capacity are written (k_chunks reads exactly those); chunks past it are tested here
+    const uint32_t at0 = base + incl - (c0 + c1);
+    const uint32_t tag = il | (occl_on ? 1u << 8 : 0u);
+    for (uint32_t k = 0; k < c0 + c1; k++) {
+      if (at0 + k >= chunk_capacity) break;
+      const uint32_t cut = k < c0 ? 0u : 1u, kk = k < c0 ? k : k - c0;
+      const uint32_t first = (cut ? r1.first : r0.first) + kk * kChunk;
+      const uint32_t cnt = min(kChunk, (cut ? r1.last - r1.first : r0.last - r0.first) - kk * kChunk);
+      chunks[at0 + k] = make_uint4(unit.x, unit.y, (cut ? (il | (1u << 7)) : tag) | (cnt << 16), first);
+    }
+    uint32_t over = __ballot_sync(0xffffffffu, at0 + c0 + c1 > chunk_capacity);
+    while (over) {
+      const uint32_t j = __ffs(over) - 1;
+      over &= over - 1;
+      float vmj[13];
+#pragma unroll
+      for (int i = 0; i < 13; i++) vmj[i] = __shfl_sync(0xffffffffu, VM[i], j);
+      const uint32_t jc0 = __shfl_sync(0xffffffffu, c0, j), jn = jc0 + __shfl_sync(0xffffffffu, c1, j);
+      const uint32_t jat = __shfl_sync(0xffffffffu, at0, j);
+      const uint32_t f0 = __shfl_sync(0xffffffffu, r0.first, j), e0 = __shfl_sync(0xffffffffu, r0.last, j);
+      const uint32_t f1 = __shfl_sync(0xffffffffu, r1.first, j), e1 = __shfl_sync(0xffffffffu, r1.last, j);
+      for (uint32_t k = 0; k < jn; k++) {
+        if (jat + k < chunk_capacity) continue;
+        const uint32_t cut = k < jc0 ? 0u : 1u, kk = k < jc0 ? k : k - jc0;
+        const uint32_t first = (cut ? f1 : f0) + kk * kChunk;
+        const uint32_t cnt = min(kChunk, (cut ? e1 - f1 : e0 - f0) - kk * kChunk);
+        warp_item(S, V, hzbs, ws, cell.slot, cut, cut == 0 && occl_on, vmj, cell.first + ((w & 3u) << 5) + j, first, cnt);
+      }
+    }
+  }
+}
 
-    // ---- meshlet phase (GeometryPool.ts:938-967)
-    for (uint32_t cut = 0; cut < 2; cut++) {
-      const uint32_t n = sm.n_items[cut];
-      const uint32_t total = n ? sm.prefix[cut][n] : 0u;
-      const float low = sm.bands.low[cut], high = sm.bands.high[cut], fs = sm.bands.fade_scale;
-      for (uint32_t base = 0; base < total; base += kSelThreads) {
-        const uint32_t t = base + tid;
-        bool drawn = false;
-        uint32_t inst = 0, meshlet = 0, packed = 0;
-        if (t < total) {
-          uint32_t a = 0, b = n;  // largest k with prefix[k] <= t
-          while (b - a > 1) {
-            const uint32_t mid = (a + b) >> 1;
-            if (sm.prefix[cut][mid] <= t) a = mid;
-            else b = mid;
-          }
-          const uint4 item = sm.items[cut][a];
-          const uint32_t il = item.x & 0xffffu;
-          const bool occl_on = (item.x >> 31) != 0;
-          meshlet = item.y + (t - sm.prefix[cut][a]);
-          inst = cell.first + il;
-          const float *VM = sm.vm[il];
-          const float scale = VM[12];
-          const float4 cs = __ldg(S.m_cull + meshlet);
-          float c[3];
-          xform(VM, cs.x, cs.y, cs.z, c);
-          const float r = cs.w * scale;
-          bool visible = !V.frustum || frustum(V, c, cut == 1) >= -r;
-          if (cut == 0 && visible) visible = !occluded(V, hzbs, sm.bands.high[0], occl_on, c, r);
-          if (visible) {
-            const float4 ls = __ldg(S.m_lod + meshlet), ps = __ldg(S.m_parent + meshlet), er = __ldg(S.m_err + meshlet);
-            const float own = proj_error(V, VM, scale, ls, er.x);
-            const float parent = proj_error(V, VM, scale, ps, er.y);
-            const uint32_t lo = fs > 0.0f ? fade_step(own, low, fs) : 0u;
-            const uint32_t hi = fs > 0.0f ? fade_step(parent, low, fs) : 255u;
-            drawn = own <= high && parent > low && hi > lo;
-            packed = __float_as_uint(er.z) | (lo << 8) | (hi << 16);
-          }
-        }
-        stage_entries(sm, cut, drawn, inst, meshlet, packed);
-        __syncthreads();
-        if (sm.stage_n[cut] > kStage - kSelThreads) flush_stage(sm, S.slot_capacity, cell.slot);
-      }
+// ------------------------------------------------------------------------------------------------ k_chunks
+// The meshlet pass (GeometryPool.ts:916-970) over the chunks k_instances queued, one chunk (<= kChunk meshlets of
+// one instance and cut) per warp: every lane derives the view-model matrix itself, so warps never wait on each other.
+__global__ void __launch_bounds__(128) k_chunks(Scene S, const ViewConst *__restrict__ views,
+                                                const HzbDesc *__restrict__ hzbs, const uint4 *__restrict__ chunks,
+                                                uint32_t *__restrict__ ctl, uint32_t chunk_capacity, int round) {
+  __shared__ WarpStage stage[4];
+  WarpStage &ws = stage[threadIdx.x >> 5];
+  if (round > 0 && ctl[round] == 0) return;  // no view redoes a cut in this round
+  const uint32_t n_chunks = min(ctl[3], chunk_capacity);
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < n_chunks; c += warps) {
+    const uint4 ch = chunks[c];
+    const ViewConst &V = views[ch.x];
+    const CellRec cell = S.cells[ch.y];
+    const uint32_t il = ch.z & 0x7fu, cut = (ch.z >> 7) & 1u, count = ch.z >> 16;
+    const bool occl_on = ((ch.z >> 8) & 1u) != 0;
+    const uint32_t instance = cell.first + il;
+    const ViewBands b = bands_of(V);
+    const float low = cut ? b.low1 : b.low0, high = cut ? b.high1 : b.high0;
+    float VM[13];
+    model_view(V.V, S.inst + (size_t)instance * 4, VM, VM[12]);
+    WarpCount wc{0, 0, 0};
+    for (uint32_t base = 0; base < count; base += 32) {
+      const uint32_t t = base + (threadIdx.x & 31);
+      bool drawn = false;
+      uint32_t packed = 0;
+      if (t < count) drawn = test_meshlet(S, V, hzbs, low, high, b.fade_scale, b.high0, cut, occl_on, VM, ch.w + t, packed);
+      warp_stage(ws, wc, V, S.slot_capacity, cell.slot, cut, drawn, instance, ch.w + t, packed);
     }
-    flush_stage(sm, S.slot_capacity, cell.slot);
-    if (tid == 0) {
-      for (uint32_t cut = 0; cut < 2; cut++) {
-        if (sm.survived[cut]) atomicAdd(V.counters + C_CUT(cut) + VGC_CUT_SURVIVED, sm.survived[cut]);
-        if (sm.work[cut]) atomicAdd(V.counters + C_CUT(cut) + VGC_CUT_WORK, sm.work[cut]);
-      }
-      if (sm.occluded) atomicAdd(V.counters + VGC_COUNTER_OCCLUDED, sm.occluded);
-      const uint32_t tested = (sm.n_items[0] ? sm.prefix[0][sm.n_items[0]] : 0u) + (sm.n_items[1] ? sm.prefix[1][sm.n_items[1]] : 0u);
-      atomicAdd(V.counters + VGC_COUNTER_INSTANCES_TESTED, cell.count);
-      if (tested) atomicAdd(V.counters + VGC_COUNTER_MESHLETS_TESTED, tested);
-      if (sm.fast[0] + sm.fast[1]) atomicAdd(V.counters + VGC_COUNTER_FAST_EMITTED, sm.fast[0] + sm.fast[1]);
-      atomicAdd(V.counters + VGC_COUNTER_LEVELS_READ, levels);
-    }
+    warp_flush(ws, wc, V, S.slot_capacity, cell.slot, cut);
   }
 }
 
@@ -550,9 +623,11 @@ __device__ __forceinline__ float fill_of(const ViewConst &V, uint32_t cut) {
 }
 
 __global__ void __launch_bounds__(128) k_finish(const ViewConst *__restrict__ views, uint32_t nviews,
-                                                uint32_t slot_capacity, uint32_t slots_used, int round) {
+                                                uint32_t slot_capacity, uint32_t slots_used, uint32_t *__restrict__ ctl,
+                                                int round) {
   const uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t lane = threadIdx.x & 31;
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctl[3] = 0;  // chunk queue of the next round starts empty
   if (v >= nviews) return;
   const ViewConst &V = views[v];
   uint32_t *ctr = V.counters;
@@ -616,7 +691,11 @@ __global__ void __launch_bounds__(128) k_finish(const ViewConst *__restrict__ vi
         }
         ctr[VGC_COUNTER_REDO0 + cut] = (again >> cut) & 1u;
       }
-      if (again) ctr[VGC_COUNTER_ROUNDS] += 1;
+      if (again) store_bands(V, V.dyn[0]);  // the redone round selects with the new scale
+      if (again) {
+        ctr[VGC_COUNTER_ROUNDS] += 1;
+        atomicOr(&ctl[1 + round], 1u);
+      }
     }
     again = __shfl_sync(0xffffffffu, again, 0);
     for (uint32_t cut = 0; cut < 2; cut++)
@@ -711,6 +790,71 @@ __global__ void __launch_bounds__(256) k_hzb_tiles(const float *__restrict__ dep
   }
 }
 
+// The HZB builds of a batch in two launches: grid.z = view, views without a depth image skip.
+__global__ void __launch_bounds__(256) k_hzb_tiles_views(const ViewConst *__restrict__ views,
+                                                         const HzbDesc *__restrict__ hzbs) {
+  __shared__ float buf[2][32][33];
+  const ViewConst &V = views[blockIdx.z];
+  if (!V.build_hzb) return;
+  const HzbDesc &H = hzbs[V.hzb];
+  const uint32_t ox = blockIdx.x * 32, oy = blockIdx.y * 32;
+  if (ox >= H.w[0] || oy >= H.h[0]) return;
+  float *out = const_cast<float *>(H.data);
+  const float *depth = V.depth;
+  const uint32_t W = H.w[0], Hh = H.h[0];
+  for (uint32_t i = threadIdx.x; i < 1024; i += blockDim.x) {
+    const uint32_t lx = i & 31, ly = i >> 5, gx = ox + lx, gy = oy + ly;
+    float v = 0.0f;
+    if (gx < W && gy < Hh) {
+      v = depth[(size_t)gy * W + gx];
+      out[H.off[0] + (size_t)gy * W + gx] = v;
+    }
+    buf[0][ly][lx] = v;
+  }
+  __syncthreads();
+  const uint32_t top = min(H.levels, 6u);
+  for (uint32_t l = 1; l < top; l++) {
+    const uint32_t s = 32u >> l;
+    const uint32_t px = ox >> (l - 1), py = oy >> (l - 1);
+    const uint32_t qx = ox >> l, qy = oy >> l;
+    const float(*src)[33] = buf[(l - 1) & 1];
+    float(*dst)[33] = buf[l & 1];
+    for (uint32_t i = threadIdx.x; i < s * s; i += blockDim.x) {
+      const uint32_t lx = i % s, ly = i / s, gx = qx + lx, gy = qy + ly;
+      if (gx < H.w[l] && gy < H.h[l]) {
+        const uint32_t x0 = 2 * gx, y0 = 2 * gy;
+        const uint32_t x1 = min(x0 + 1, H.w[l - 1] - 1), y1 = min(y0 + 1, H.h[l - 1] - 1);
+        const float a = fmaxf(src[y0 - py][x0 - px], src[y0 - py][x1 - px]);
+        const float b = fmaxf(src[y1 - py][x0 - px], src[y1 - py][x1 - px]);
+        const float v = fmaxf(a, b);
+        dst[ly][lx] = v;
+        out[H.off[l] + (size_t)gy * H.w[l] + gx] = v;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_hzb_tail_views(const ViewConst *__restrict__ views,
+                                                         const HzbDesc *__restrict__ hzbs) {
+  const ViewConst &V = views[blockIdx.x];
+  if (!V.build_hzb) return;
+  const HzbDesc &H = hzbs[V.hzb];
+  float *out = const_cast<float *>(H.data);
+  for (uint32_t l = 6; l < H.levels; l++) {
+    const float *src = out + H.off[l - 1];
+    const uint32_t sw = H.w[l - 1], sh = H.h[l - 1];
+    for (uint32_t i = threadIdx.x; i < H.w[l] * H.h[l]; i += blockDim.x) {
+      const uint32_t x = i % H.w[l], y = i / H.w[l];
+      const uint32_t x0 = 2 * x, y0 = 2 * y, x1 = min(x0 + 1, sw - 1), y1 = min(y0 + 1, sh - 1);
+      const float a = fmaxf(src[y0 * sw + x0], src[y0 * sw + x1]);
+      const float b = fmaxf(src[y1 * sw + x0], src[y1 * sw + x1]);
+      out[H.off[l] + i] = fmaxf(a, b);
+    }
+    __syncthreads();
+  }
+}
+
 // Levels 6 and up (at most 60 x 34 texels for a 1080p mip 0) by one block.
 __global__ void __launch_bounds__(1024) k_hzb_tail(HzbDesc H, float *__restrict__ out) {
   for (uint32_t l = 6; l < H.levels; l++) {
@@ -784,22 +928,22 @@ __global__ void __launch_bounds__(256) k_select_cut(Scene S, uint32_t slot, uint
 // Zeroes each view's counter block (reset pass, GeometryPool.ts:714-725) and the batch's unit count; reads the
 // output pointers from the view constants, so a captured graph serves any output slots.
 __global__ void __launch_bounds__(256) k_reset(const ViewConst *__restrict__ views, uint32_t nviews, uint32_t words,
-                                               uint32_t *__restrict__ unit_count) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) *unit_count = 0;
+                                               uint32_t *__restrict__ ctl) {
+  if (blockIdx.x == 0 && threadIdx.x < 16) ctl[threadIdx.x] = 0;
   for (uint32_t v = blockIdx.x; v < nviews; v += gridDim.x) {
     uint32_t *c = views[v].counters;
     for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) c[i] = 0;
+    if (threadIdx.x == 0 && !(views[v].budget > 0.0f)) store_bands(views[v], views[v].error_threshold);
   }
 }
 
 // ------------------------------------------------------------------------------------------------ launchers
-cudaError_t launch_reset(const ViewConst *views, uint32_t nviews, uint32_t words, uint32_t *unit_count, cudaStream_t st) {
+cudaError_t launch_reset(const ViewConst *views, uint32_t nviews, uint32_t words, uint32_t *ctl, cudaStream_t st) {
   const uint32_t blocks = nviews < 1024 ? (nviews ? nviews : 1) : 1024;
-  k_reset<<<blocks, 256, 0, st>>>(views, nviews, words, unit_count);
+  k_reset<<<blocks, 256, 0, st>>>(views, nviews, words, ctl);
   return cudaGetLastError();
 }
 
-size_t select_smem_bytes() { return sizeof(SelectSmem); }
 
 cudaError_t launch_cells(const Scene &S, const ViewConst *views, uint32_t nviews, uint32_t total_units, uint2 *units,
                          uint32_t *unit_count, cudaStream_t st) {
@@ -810,21 +954,26 @@ cudaError_t launch_cells(const Scene &S, const ViewConst *views, uint32_t nviews
 }
 
 cudaError_t configure_select(int *blocks_per_sm) {
-  cudaError_t e = cudaFuncSetAttribute(k_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SelectSmem));
-  if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_select, kSelThreads, sizeof(SelectSmem));
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_instances, 128, 0);
 }
 
-cudaError_t launch_select(const Scene &S, const ViewConst *views, const HzbDesc *hzbs, const uint2 *units,
-                          const uint32_t *unit_count, int round, uint32_t grid, cudaStream_t st) {
-  k_select<<<grid, kSelThreads, sizeof(SelectSmem), st>>>(S, views, hzbs, units, unit_count, round);
+cudaError_t launch_instances(const Scene &S, const ViewConst *views, const HzbDesc *hzbs, const uint2 *units,
+                             uint32_t *ctl, uint4 *chunks, uint32_t chunk_capacity, int round, uint32_t grid,
+                             cudaStream_t st) {
+  k_instances<<<grid, 128, 0, st>>>(S, views, hzbs, units, ctl, chunks, chunk_capacity, round);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_chunks(const Scene &S, const ViewConst *views, const HzbDesc *hzbs, const uint4 *chunks,
+                          uint32_t *ctl, uint32_t chunk_capacity, int round, uint32_t grid, cudaStream_t st) {
+  k_chunks<<<grid, 128, 0, st>>>(S, views, hzbs, chunks, ctl, chunk_capacity, round);
   return cudaGetLastError();
 }
 
 cudaError_t launch_finish(const ViewConst *views, uint32_t nviews, uint32_t slot_capacity, uint32_t slots_used,
-                          int round, cudaStream_t st) {
+                          uint32_t *ctl, int round, cudaStream_t st) {
   const uint32_t blocks = (nviews * 32 + 127) / 128;
-  k_finish<<<blocks, 128, 0, st>>>(views, nviews, slot_capacity, slots_used, round);
+  k_finish<<<blocks, 128, 0, st>>>(views, nviews, slot_capacity, slots_used, ctl, round);
   return cudaGetLastError();
 }
 
@@ -840,6 +989,16 @@ cudaError_t launch_hzb(const float *depth, const HzbDesc &H, float *out, int cop
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || H.levels <= 6) return e;
   k_hzb_tail<<<1, 1024, 0, st>>>(H, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_hzb_views(const ViewConst *views, uint32_t nviews, const HzbDesc *hzbs, uint32_t max_w,
+                             uint32_t max_h, bool tail, cudaStream_t st) {
+  dim3 grid((max_w + 31) / 32, (max_h + 31) / 32, nviews);
+  k_hzb_tiles_views<<<grid, 256, 0, st>>>(views, hzbs);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !tail) return e;
+  k_hzb_tail_views<<<nviews, 1024, 0, st>>>(views, hzbs);
   return cudaGetLastError();
 }
 

@@ -7,19 +7,25 @@
 
 namespace vgc {
 
-size_t select_smem_bytes();
-// Sets k_select's shared-memory limit and returns its resident blocks per SM.
+// Resident 128-thread blocks per SM of the instance / chunk kernels (their persistent grid size).
 cudaError_t configure_select(int *blocks_per_sm);
-cudaError_t launch_reset(const ViewConst *views, uint32_t nviews, uint32_t words, uint32_t *unit_count, cudaStream_t st);
+// ctl: per-batch control words: [0] visible units, [1..2] a view redoes a cut in round 1..2, [3] chunks queued
+cudaError_t launch_reset(const ViewConst *views, uint32_t nviews, uint32_t words, uint32_t *ctl, cudaStream_t st);
 cudaError_t launch_cells(const Scene &S, const ViewConst *views, uint32_t nviews, uint32_t total_units, uint2 *units,
                          uint32_t *unit_count, cudaStream_t st);
-cudaError_t launch_select(const Scene &S, const ViewConst *views, const HzbDesc *hzbs, const uint2 *units,
-                          const uint32_t *unit_count, int round, uint32_t grid, cudaStream_t st);
+cudaError_t launch_instances(const Scene &S, const ViewConst *views, const HzbDesc *hzbs, const uint2 *units,
+                             uint32_t *ctl, uint4 *chunks, uint32_t chunk_capacity, int round, uint32_t grid,
+                             cudaStream_t st);
+cudaError_t launch_chunks(const Scene &S, const ViewConst *views, const HzbDesc *hzbs, const uint4 *chunks,
+                          uint32_t *ctl, uint32_t chunk_capacity, int round, uint32_t grid, cudaStream_t st);
 cudaError_t launch_finish(const ViewConst *views, uint32_t nviews, uint32_t slot_capacity, uint32_t slots_used,
-                          int round, cudaStream_t st);
+                          uint32_t *ctl, int round, cudaStream_t st);
 cudaError_t launch_expand(const Scene &S, const ViewConst *view, uint32_t cut, uint32_t *out, uint64_t capacity,
                           uint32_t grid, cudaStream_t st);
 cudaError_t launch_hzb(const float *depth, const HzbDesc &H, float *out, int copy_mip0, cudaStream_t st);
+// HZB builds of the views whose constants carry build_hzb (grid covers the largest depth image).
+cudaError_t launch_hzb_views(const ViewConst *views, uint32_t nviews, const HzbDesc *hzbs, uint32_t max_w,
+                             uint32_t max_h, bool tail, cudaStream_t st);
 cudaError_t launch_select_cut(const Scene &S, uint32_t slot, uint32_t mcount, uint32_t count, const float *vm16,
                               const float *params, float threshold, float blend, uint8_t *lo, uint8_t *hi, uint32_t grid,
                               cudaStream_t st);

@@ -56,7 +56,8 @@ class View(C.Structure):
                 ("max_error_threshold", C.c_double), ("shadow_sweep", C.c_double * 3),
                 ("triangle_budget", C.c_double), ("threshold_range", C.c_double * 2),
                 ("frustum_culling", C.c_uint32), ("hzb", C.c_int32), ("state_slot", C.c_uint32),
-                ("flags", C.c_uint32)]
+                ("flags", C.c_uint32), ("depth", C.c_void_p), ("depth_width", C.c_uint32),
+                ("depth_height", C.c_uint32)]
 
 
 class Output(C.Structure):
@@ -179,7 +180,9 @@ class ViewParams:
     state_slot: int = 0
 
 
-def make_view(camera: Camera, p: ViewParams | None = None) -> View:
+def make_view(camera: Camera, p: ViewParams | None = None, depth=None) -> View:
+    """View struct for a camera. `depth`: optional (device pointer, width, height) of this frame's occluder depth,
+    from which the cut builds HZB slot `p.hzb` first."""
     p = p or ViewParams()
     v = View()
     for k in range(16):
@@ -200,6 +203,8 @@ def make_view(camera: Camera, p: ViewParams | None = None) -> View:
     v.hzb = p.hzb
     v.state_slot = p.state_slot
     v.flags = 0
+    if depth is not None:
+        v.depth, v.depth_width, v.depth_height = depth
     return v
 
 
@@ -361,7 +366,7 @@ class VirtualGeometry:
         check(lib().vgc_state_access(self.handle, state_slot, _up(w), 0 if words is None else 1, None))
         return w
 
-    KERNEL_KINDS = ("reset", "cells", "select0", "select_retry", "finish", "hzb")
+    KERNEL_KINDS = ("reset", "cells", "select0", "retry", "finish", "hzb", "chunks0")
 
     def set_profiling(self, enable: bool) -> None:
         check(lib().vgc_set_profiling(self.handle, 1 if enable else 0))
