@@ -83,7 +83,8 @@ struct vgc_context {
   int device = 0;
   cudaStream_t stream = nullptr;
   int sm_count = 0;
-  uint32_t select_grid = 0;
+  uint32_t select_grid = 0;  // persistent grid of k_instances
+  uint32_t chunk_grid = 0;   // persistent grid of k_chunks
   uint64_t bytes = 0;
   std::mutex mu;
   // host mirrors of the resident scene
@@ -510,7 +511,7 @@ int enqueue(vgc_context *ctx, LaunchScratch &s, uint32_t count, cudaStream_t st,
                               ctx->select_grid, st);
     }));
     CUDA_TRY(timed(ctx, capture, round == 0 ? VGC_KERNEL_CHUNKS0 : VGC_KERNEL_SELECT_RETRY, st, [&] {
-      return launch_chunks(S, s.d_views, hzbs, s.d_chunks, s.d_unit_count, s.chunk_capacity, round, ctx->select_grid, st);
+      return launch_chunks(S, s.d_views, hzbs, s.d_chunks, s.d_unit_count, s.chunk_capacity, round, ctx->chunk_grid, st);
     }));
     CUDA_TRY(timed(ctx, capture, VGC_KERNEL_FINISH, st, [&] {
       return launch_finish(s.d_views, count, S.slot_capacity, S.slots_used, s.d_unit_count, round, st);
@@ -649,12 +650,13 @@ int vgc_context_create(const vgc_options *opts, vgc_context **out) {
     delete ctx;
     return fail(VGC_DEVICE_ERROR, "cudaStreamCreate failed");
   }
-  int per_sm = 0;
-  if (configure_select(&per_sm) != cudaSuccess) {
+  int per_sm = 0, chunks_per_sm = 0;
+  if (configure_select(&per_sm, &chunks_per_sm) != cudaSuccess) {
     cudaGetLastError();
-    per_sm = 1;
+    per_sm = chunks_per_sm = 1;
   }
   ctx->select_grid = (uint32_t)std::max(1, per_sm) * ctx->sm_count;
+  ctx->chunk_grid = (uint32_t)std::max(1, chunks_per_sm) * ctx->sm_count;
   ctx->meshes.resize(ctx->slot_capacity);
   ctx->mesh_host.resize(ctx->slot_capacity);
   ctx->hzb.resize(vgc_context::kHzbSlots);

@@ -124,11 +124,13 @@ __device__ bool hzb_occluded(const ViewConst &V, const HzbDesc &H, const float c
   if (!(near_depth > V.near_)) return false;
   float far_depth = depth + radius;
   float xlo = c[0] - radius, xhi = c[0] + radius, ylo = c[1] - radius, yhi = c[1] + radius;
-  float min_x = fmn(xlo / near_depth, xlo / far_depth) * V.P0 - V.P8;
-  float max_x = fmx(xhi / near_depth, xhi / far_depth) * V.P0 - V.P8;
-  float min_y = fmn(ylo / near_depth, ylo / far_depth) * V.P5 - V.P9;
-  float max_y = fmx(yhi / near_depth, yhi / far_depth) * V.P5 - V.P9;
-  float min_z = V.P14 / near_depth - V.P10;
+  // x / depth as x * (1 / depth): two divisions instead of nine
+  const float inv_near = 1.0f / near_depth, inv_far = 1.0f / far_depth;
+  float min_x = fmn(xlo * inv_near, xlo * inv_far) * V.P0 - V.P8;
+  float max_x = fmx(xhi * inv_near, xhi * inv_far) * V.P0 - V.P8;
+  float min_y = fmn(ylo * inv_near, ylo * inv_far) * V.P5 - V.P9;
+  float max_y = fmx(yhi * inv_near, yhi * inv_far) * V.P5 - V.P9;
+  float min_z = V.P14 * inv_near - V.P10;
   if (!(min_z < 1.0f)) return false;
   float W = float(H.w[0]), Hh = float(H.h[0]);
   float fx0 = floorf((min_x * 0.5f + 0.5f) * W);
@@ -350,7 +352,7 @@ __device__ __forceinline__ void warp_stage(WarpStage &ws, WarpCount &wc, const V
 // `drawn` is their conjunction either way. `packed` receives triCount | lo << 8 | hi << 16.
 __device__ __forceinline__ bool test_meshlet(const Scene &S, const ViewConst &V, const HzbDesc *hzbs, float low,
                                              float high, float fs, float high0, uint32_t cut, bool occl_on,
-                                             const float *VM, uint32_t meshlet, uint32_t &packed) {
+                                             bool inside, const float *VM, uint32_t meshlet, uint32_t &packed) {
   const float scale = VM[12];
   const float4 ls = __ldg(S.m_lod + meshlet), ps = __ldg(S.m_parent + meshlet), er = __ldg(S.m_err + meshlet);
   const float own = proj_error(V, VM, scale, ls, er.x);
@@ -364,7 +366,8 @@ __device__ __forceinline__ bool test_meshlet(const Scene &S, const ViewConst &V,
   float c[3];
   xform(VM, cs.x, cs.y, cs.z, c);
   const float r = cs.w * scale;
-  if (V.frustum && !(frustum(V, c, cut == 1) >= -r)) return false;
+  // `inside`: the instance's cullBoundsSphere, which encloses every meshlet's culling sphere, is inside the frustum
+  if (V.frustum && !inside && !(frustum(V, c, cut == 1) >= -r)) return false;
   if (cut == 0 && occluded(V, hzbs, high0, occl_on, c, r)) return false;
   return true;
 }
@@ -428,7 +431,7 @@ __device__ __forceinline__ void emit_fast(const Scene &S, const ViewConst &V, ui
 // Tests a whole item (one instance's meshlets [first, first + count) of one cut) with the warp: the fallback when
 // the chunk queue is full.
 __device__ void warp_item(const Scene &S, const ViewConst &V, const HzbDesc *hzbs, WarpStage &ws, uint32_t slot,
-                          uint32_t cut, bool occl_on, const float *VM, uint32_t instance, uint32_t first,
+                          uint32_t cut, bool occl_on, bool inside, const float *VM, uint32_t instance, uint32_t first,
                           uint32_t count) {
   const ViewBands b = bands_of(V);
   const float low = cut ? b.low1 : b.low0, high = cut ? b.high1 : b.high0;
@@ -437,7 +440,8 @@ __device__ void warp_item(const Scene &S, const ViewConst &V, const HzbDesc *hzb
     const uint32_t t = base + (threadIdx.x & 31);
     bool drawn = false;
     uint32_t packed = 0;
-    if (t < count) drawn = test_meshlet(S, V, hzbs, low, high, b.fade_scale, b.high0, cut, occl_on, VM, first + t, packed);
+    if (t < count)
+      drawn = test_meshlet(S, V, hzbs, low, high, b.fade_scale, b.high0, cut, occl_on, inside, VM, first + t, packed);
     warp_stage(ws, wc, V, S.slot_capacity, slot, cut, drawn, instance, first + t, packed);
   }
   warp_flush(ws, wc, V, S.slot_capacity, slot, cut);
@@ -477,7 +481,7 @@ __global__ void __launch_bounds__(128) k_instances(Scene S, const ViewConst *__r
     float VM[13];
     bool occluded_now = false;
     LevelRange r0{0xffffffffu, 0, 0, 0}, r1{0xffffffffu, 0, 0, 0};
-    bool fast0 = false, fast1 = false;
+    bool fast0 = false, fast1 = false, inside0 = true, inside1 = true;
     if (valid) {
       model_view(V.V, S.inst + (size_t)instance * 4, VM, VM[12]);
       const float scale = VM[12];
@@ -506,15 +510,18 @@ __global__ void __launch_bounds__(128) k_instances(Scene S, const ViewConst *__r
         float cc[3];
         xform(VM, mesh.cull.x, mesh.cull.y, mesh.cull.z, cc);
         const float cr = mesh.cull.w * scale;
+        // inside: the cullBoundsSphere lies in the frustum, so every meshlet passes its frustum test
         if (in_camera) {
           r0 = level_range(L, levels, b.low0, b.high0, px_min, px_max);
+          inside0 = no_frustum || frustum(V, cc, false) >= cr;
           fast0 = r0.last > r0.first && r0.possible == r0.last - r0.first && r0.guaranteed == r0.possible &&
-                  r0.possible <= kFastPathMax && (no_frustum || frustum(V, cc, false) >= cr);
+                  r0.possible <= kFastPathMax && inside0;
         }
         if (in_shadow) {
           r1 = level_range(L, levels, b.low1, b.high1, px_min, px_max);
+          inside1 = no_frustum || frustum(V, cc, true) >= cr;
           fast1 = r1.last > r1.first && r1.possible == r1.last - r1.first && r1.guaranteed == r1.possible &&
-                  r1.possible <= kFastPathMax && (no_frustum || frustum(V, cc, true) >= cr);
+                  r1.possible <= kFastPathMax && inside1;
         }
       }
     }
@@ -551,13 +558,15 @@ __global__ void __launch_bounds__(128) k_instances(Scene S, const ViewConst *__r
     base = __shfl_sync(0xffffffffu, base, 0);
     // slots below the capacity are written (k_chunks reads exactly those); chunks past it are tested here
     const uint32_t at0 = base + incl - (c0 + c1);
-    const uint32_t tag = il | (occl_on ? 1u << 8 : 0u);
+    // tag: instance local (bits 0-6), cut (7), occlusion (8), inside the frustum (9), meshlet count (16-31)
+    const uint32_t tag0 = il | (occl_on ? 1u << 8 : 0u) | (inside0 ? 1u << 9 : 0u);
+    const uint32_t tag1 = il | (1u << 7) | (inside1 ? 1u << 9 : 0u);
     for (uint32_t k = 0; k < c0 + c1; k++) {
       if (at0 + k >= chunk_capacity) break;
       const uint32_t cut = k < c0 ? 0u : 1u, kk = k < c0 ? k : k - c0;
       const uint32_t first = (cut ? r1.first : r0.first) + kk * kChunk;
       const uint32_t cnt = min(kChunk, (cut ? r1.last - r1.first : r0.last - r0.first) - kk * kChunk);
-      chunks[at0 + k] = make_uint4(unit.x, unit.y, (cut ? (il | (1u << 7)) : tag) | (cnt << 16), first);
+      chunks[at0 + k] = make_uint4(unit.x, unit.y, (cut ? tag1 : tag0) | (cnt << 16), first);
     }
     uint32_t over = __ballot_sync(0xffffffffu, at0 + c0 + c1 > chunk_capacity);
     while (over) {
@@ -568,6 +577,7 @@ __global__ void __launch_bounds__(128) k_instances(Scene S, const ViewConst *__r
       for (int i = 0; i < 13; i++) vmj[i] = __shfl_sync(0xffffffffu, VM[i], j);
       const uint32_t jc0 = __shfl_sync(0xffffffffu, c0, j), jn = jc0 + __shfl_sync(0xffffffffu, c1, j);
       const uint32_t jat = __shfl_sync(0xffffffffu, at0, j);
+      const bool jin0 = __shfl_sync(0xffffffffu, inside0 ? 1 : 0, j) != 0, jin1 = __shfl_sync(0xffffffffu, inside1 ? 1 : 0, j) != 0;
       const uint32_t f0 = __shfl_sync(0xffffffffu, r0.first, j), e0 = __shfl_sync(0xffffffffu, r0.last, j);
       const uint32_t f1 = __shfl_sync(0xffffffffu, r1.first, j), e1 = __shfl_sync(0xffffffffu, r1.last, j);
       for (uint32_t k = 0; k < jn; k++) {
@@ -575,7 +585,8 @@ __global__ void __launch_bounds__(128) k_instances(Scene S, const ViewConst *__r
         const uint32_t cut = k < jc0 ? 0u : 1u, kk = k < jc0 ? k : k - jc0;
         const uint32_t first = (cut ? f1 : f0) + kk * kChunk;
         const uint32_t cnt = min(kChunk, (cut ? e1 - f1 : e0 - f0) - kk * kChunk);
-        warp_item(S, V, hzbs, ws, cell.slot, cut, cut == 0 && occl_on, vmj, cell.first + ((w & 3u) << 5) + j, first, cnt);
+        warp_item(S, V, hzbs, ws, cell.slot, cut, cut == 0 && occl_on, cut ? jin1 : jin0, vmj,
+                  cell.first + ((w & 3u) << 5) + j, first, cnt);
       }
     }
   }
@@ -597,7 +608,7 @@ __global__ void __launch_bounds__(128) k_chunks(Scene S, const ViewConst *__rest
     const ViewConst &V = views[ch.x];
     const CellRec cell = S.cells[ch.y];
     const uint32_t il = ch.z & 0x7fu, cut = (ch.z >> 7) & 1u, count = ch.z >> 16;
-    const bool occl_on = ((ch.z >> 8) & 1u) != 0;
+    const bool occl_on = ((ch.z >> 8) & 1u) != 0, inside = ((ch.z >> 9) & 1u) != 0;
     const uint32_t instance = cell.first + il;
     const ViewBands b = bands_of(V);
     const float low = cut ? b.low1 : b.low0, high = cut ? b.high1 : b.high0;
@@ -608,7 +619,8 @@ __global__ void __launch_bounds__(128) k_chunks(Scene S, const ViewConst *__rest
       const uint32_t t = base + (threadIdx.x & 31);
       bool drawn = false;
       uint32_t packed = 0;
-      if (t < count) drawn = test_meshlet(S, V, hzbs, low, high, b.fade_scale, b.high0, cut, occl_on, VM, ch.w + t, packed);
+      if (t < count)
+        drawn = test_meshlet(S, V, hzbs, low, high, b.fade_scale, b.high0, cut, occl_on, inside, VM, ch.w + t, packed);
       warp_stage(ws, wc, V, S.slot_capacity, cell.slot, cut, drawn, instance, ch.w + t, packed);
     }
     warp_flush(ws, wc, V, S.slot_capacity, cell.slot, cut);
@@ -953,8 +965,10 @@ cudaError_t launch_cells(const Scene &S, const ViewConst *views, uint32_t nviews
   return cudaGetLastError();
 }
 
-cudaError_t configure_select(int *blocks_per_sm) {
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_instances, 128, 0);
+cudaError_t configure_select(int *instances_per_sm, int *chunks_per_sm) {
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(instances_per_sm, k_instances, 128, 0);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(chunks_per_sm, k_chunks, 128, 0);
 }
 
 cudaError_t launch_instances(const Scene &S, const ViewConst *views, const HzbDesc *hzbs, const uint2 *units,

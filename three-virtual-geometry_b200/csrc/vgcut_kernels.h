@@ -8,7 +8,7 @@
 namespace vgc {
 
 // Resident 128-thread blocks per SM of the instance / chunk kernels (their persistent grid size).
-cudaError_t configure_select(int *blocks_per_sm);
+cudaError_t configure_select(int *instances_per_sm, int *chunks_per_sm);
 // ctl: per-batch control words: [0] visible units, [1..2] a view redoes a cut in round 1..2, [3] chunks queued
 cudaError_t launch_reset(const ViewConst *views, uint32_t nviews, uint32_t words, uint32_t *ctl, cudaStream_t st);
 cudaError_t launch_cells(const Scene &S, const ViewConst *views, uint32_t nviews, uint32_t total_units, uint2 *units,
