@@ -179,6 +179,19 @@ int vgc_hzb_build(vgc_context *ctx, int32_t hzb, const float *depth, uint32_t wi
    output slots [first_slot, first_slot + count) as a sequence of kernel launches on `stream`. Asynchronous. */
 int vgc_cut(vgc_context *ctx, const vgc_view *views, uint32_t count, uint32_t first_slot, vgc_stream stream);
 
+/* The plain single-view cut with no device allocation on the call. It has no counterpart in the reference. For
+   callers that cannot call cudaMalloc while they run - a renderer's frame loop that records into a CUDA graph or
+   runs on a real-time thread, or a host that reserves all of its GPU memory up front - it keeps its per-call
+   scratch in a fixed 1.5 MiB device array inside the library (held by every GPU that loads it until the process
+   exits) rather than in context allocations. Limits: a scene of at most 65,536 cells (8,388,608 instances); the
+   output slot, the view's state slot and (for a view with `depth`) its HZB slot at that size must already exist
+   (create the context with enough output_slots; build the HZB once with vgc_hzb_build); the scene must have been
+   published by an earlier vgc_cut after the last mesh change. Meshlet chunks past the fixed queue are tested in
+   place, so the result is the same as vgc_cut's. The first call on a device looks the array's device address up
+   (make that call before any stream capture). Every call shares the one array: calls whose GPU work overlaps -
+   on two streams, or two contexts on one device - race; order them on one stream. Asynchronous on `stream`. */
+int vgc_cut_noalloc(vgc_context *ctx, const vgc_view *view, uint32_t slot, vgc_stream stream);
+
 /* Batched launch: the same kernels for up to `max_views` views captured once into a CUDA graph, replayed with the
    new views' constants. Output slots are [first_slot, first_slot + count). */
 int vgc_batch_create(vgc_context *ctx, uint32_t max_views, vgc_batch **out);

@@ -1135,3 +1135,101 @@ int vgc_debug_scene(const vgc_context *ctx, float *cells, uint32_t cell_capacity
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------------ no-alloc cut
+// vgc_cut_noalloc: the single-view cut for callers that must not allocate device memory on the call (a renderer's
+// frame loop running inside a CUDA graph capture or a real-time thread that forbids cudaMalloc, a host that
+// pre-reserves all of its GPU memory). Its per-call scratch - the batch control words, the view constants, the
+// (view, cell) unit list and the meshlet chunk queue - lives in this fixed file-scope device array instead of the
+// context's launch scratch. Every GPU that loads the library holds the array until the process exits.
+namespace {
+constexpr size_t kNoAllocCtl = 0;                                   // 16 control words
+constexpr size_t kNoAllocView = 256;                                // one ViewConst
+constexpr uint32_t kNoAllocMaxUnits = 65536;                        // visible (view, cell) units: cells of the scene
+constexpr uint32_t kNoAllocMaxChunks = 65536;                       // queued meshlet chunks (beyond: tested in place)
+constexpr size_t kNoAllocUnits = 1024;
+constexpr size_t kNoAllocChunks = kNoAllocUnits + (size_t)kNoAllocMaxUnits * sizeof(uint2);
+constexpr size_t kNoAllocBytes = kNoAllocChunks + (size_t)kNoAllocMaxChunks * sizeof(uint4);  // 1.5 MiB
+static_assert(sizeof(ViewConst) <= kNoAllocUnits - kNoAllocView, "view constants must fit their scratch slot");
+static_assert(kNoAllocChunks % 256 == 0, "chunk queue must stay 256-byte aligned");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mu;
+unsigned char *g_noalloc_ptr[64] = {nullptr};  // device address of g_noalloc_scratch per device ordinal
+
+// Device address of the scratch array on `device` (current), looked up once per device: in host code the array's
+// name only stands in for the symbol, so kernels must receive this address instead.
+int noalloc_scratch(int device, unsigned char **out) {
+  if (device < 0 || device >= 64) return fail(VGC_INVALID_ARG, "device ordinal out of range for the no-alloc scratch");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[device]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return fail(VGC_DEVICE_ERROR, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    g_noalloc_ptr[device] = (unsigned char *)p;
+  }
+  *out = g_noalloc_ptr[device];
+  return VGC_OK;
+}
+}  // namespace
+
+extern "C" int vgc_cut_noalloc(vgc_context *ctx, const vgc_view *view, uint32_t slot, vgc_stream stream) {
+  if (!ctx || !view) return fail(VGC_INVALID_ARG, "null argument");
+  cudaSetDevice(ctx->device);
+  // everything this call writes must exist already: it allocates nothing
+  if (ctx->dirty)
+    return fail(VGC_INVALID_ARG, "vgc_cut_noalloc: the scene changed since the last upload; one allocating call "
+                                 "(vgc_cut) must publish it first");
+  if (slot >= ctx->out_slots || ctx->out_slot_capacity != ctx->slot_capacity)
+    return fail(VGC_INVALID_ARG, "vgc_cut_noalloc: output slot " + std::to_string(slot) +
+                                     " is not allocated (create the context with enough output_slots)");
+  if (view->state_slot >= ctx->state_slots)
+    return fail(VGC_INVALID_ARG, "vgc_cut_noalloc: state slot " + std::to_string(view->state_slot) + " is not allocated");
+  const uint32_t cells = pad32((uint32_t)ctx->cells.size());
+  if (cells > kNoAllocMaxUnits)
+    return fail(VGC_INVALID_ARG, "vgc_cut_noalloc: the scene has " + std::to_string(ctx->cells.size()) +
+                                     " cells; the fixed scratch holds at most " + std::to_string(kNoAllocMaxUnits));
+  bool build_hzb = false;
+  if (view->hzb >= 0) {
+    if (view->hzb >= (int32_t)vgc_context::kHzbSlots) return fail(VGC_INVALID_ARG, "view: hzb slot out of range");
+    const HzbSlot &h = ctx->hzb[view->hzb];
+    if (view->depth) {
+      size_t total = 0;
+      HzbDesc want = hzb_layout(view->depth_width, view->depth_height, &total);
+      if (!h.valid || h.data.bytes < total * 4 || h.desc.levels != want.levels || h.desc.w[0] != want.w[0] ||
+          h.desc.h[0] != want.h[0])
+        return fail(VGC_INVALID_ARG, "vgc_cut_noalloc: HZB slot " + std::to_string(view->hzb) +
+                                         " is not laid out for this depth size (build it once with vgc_hzb_build)");
+      build_hzb = true;
+    } else if (!h.valid) {
+      return fail(VGC_INVALID_ARG, "view: hzb slot " + std::to_string(view->hzb) + " has no HZB");
+    }
+  }
+  unsigned char *scratch = nullptr;
+  int rc = noalloc_scratch(ctx->device, &scratch);
+  if (rc) return rc;
+  ViewConst k;
+  if ((rc = view_constants(ctx, *view, slot, 0, k))) return rc;
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  uint32_t *ctl = (uint32_t *)(scratch + kNoAllocCtl);
+  ViewConst *d_view = (ViewConst *)(scratch + kNoAllocView);
+  uint2 *units = (uint2 *)(scratch + kNoAllocUnits);
+  uint4 *chunks = (uint4 *)(scratch + kNoAllocChunks);
+  // `k` is pageable: the copy has read it when cudaMemcpyAsync returns. k_reset clears the control words.
+  CUDA_TRY(cudaMemcpyAsync(d_view, &k, sizeof(ViewConst), cudaMemcpyHostToDevice, st));
+  const Scene S = scene_of(ctx);
+  const HzbDesc *hzbs = (const HzbDesc *)ctx->d_hzb_desc.ptr;
+  if (build_hzb) {
+    const HzbDesc &d = ctx->hzb[view->hzb].desc;
+    CUDA_TRY(launch_hzb_views(d_view, 1, hzbs, d.w[0], d.h[0], d.levels > 6, st));
+  }
+  CUDA_TRY(launch_reset(d_view, 1, ctx->counter_words, ctl, st));
+  CUDA_TRY(launch_cells(S, d_view, 1, cells, units, ctl, st));
+  for (int round = 0; round < 3; round++) {
+    CUDA_TRY(launch_instances(S, d_view, hzbs, units, ctl, chunks, kNoAllocMaxChunks, round, ctx->select_grid, st));
+    CUDA_TRY(launch_chunks(S, d_view, hzbs, chunks, ctl, kNoAllocMaxChunks, round, ctx->chunk_grid, st));
+    CUDA_TRY(launch_finish(d_view, 1, S.slot_capacity, S.slots_used, ctl, round, st));
+  }
+  return VGC_OK;
+}

@@ -105,6 +105,7 @@ def lib() -> C.CDLL:
         "vgc_mesh_slots": ([vp, P(C.c_uint32), P(C.c_uint32)], C.c_int),
         "vgc_hzb_build": ([vp, C.c_int32, vp, C.c_uint32, C.c_uint32, C.c_int, vp], C.c_int),
         "vgc_cut": ([vp, P(View), C.c_uint32, C.c_uint32, vp], C.c_int),
+        "vgc_cut_noalloc": ([vp, P(View), C.c_uint32, vp], C.c_int),
         "vgc_batch_create": ([vp, C.c_uint32, P(vp)], C.c_int),
         "vgc_batch_run": ([vp, P(View), C.c_uint32, C.c_uint32, vp], C.c_int),
         "vgc_batch_destroy": ([vp], C.c_int),
@@ -340,6 +341,10 @@ class VirtualGeometry:
             check(lib().vgc_batch_create(self.handle, len(views), C.byref(b)))
             self._batches[len(views)] = b
         check(lib().vgc_batch_run(b, arr, len(views), first_slot, stream))
+
+    def cut_noalloc(self, view: View, slot: int = 0, stream=None) -> None:
+        """The single-view cut that allocates nothing on the call (see vgc_cut_noalloc in include/vgcut.h)."""
+        check(lib().vgc_cut_noalloc(self.handle, C.byref(view), slot, stream))
 
     def read_stats(self, slot: int = 0) -> dict:
         s = Stats()
