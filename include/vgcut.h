@@ -123,6 +123,9 @@ enum {
   VGC_COUNTER_MESHLETS_TESTED = 17,  /* meshlets run through the per-meshlet test (all rounds) */
   VGC_COUNTER_FAST_EMITTED = 18,     /* meshlets emitted by the instance fast path (all rounds) */
   VGC_COUNTER_LEVELS_READ = 19,      /* level-table entries read (sum over visible cells, all rounds) */
+  VGC_COUNTER_PREDICTED_LO = 20,     /* triangleBudget search: plain camera-cut triangles predicted at the */
+  VGC_COUNTER_PREDICTED_HI = 21,     /*   chosen threshold (64-bit, low and high words) */
+  VGC_COUNTER_BUDGET_BIN = 22,       /* the chosen threshold bin k: t = lo + (hi - lo) k / 255 */
   VGC_COUNTER_HEADER = 24,
 };
 enum { VGC_CUT_SELECTED = 0, VGC_CUT_DRAWN = 1, VGC_CUT_SURVIVED = 2, VGC_CUT_WORK = 3, VGC_CUT_REQUESTED = 4 };
@@ -138,6 +141,7 @@ typedef struct vgc_stats {
   float fill[2];
   float effective_threshold;    /* errorThreshold used (after a budget search) */
   uint32_t instances_tested, meshlets_tested, fast_emitted, levels_read; /* work done, all rounds */
+  uint64_t predicted_triangles; /* triangleBudget search: predicted plain camera-cut triangles */
 } vgc_stats;
 
 const char *vgc_last_error(void);
@@ -228,7 +232,7 @@ int vgc_select_cut(vgc_context *ctx, uint32_t slot, uint32_t count, const double
 
 /* ---------------------------------------------------------------- profiling (no counterpart in the reference) */
 enum { VGC_KERNEL_RESET = 0, VGC_KERNEL_CELLS = 1, VGC_KERNEL_SELECT0 = 2, VGC_KERNEL_SELECT_RETRY = 3,
-       VGC_KERNEL_FINISH = 4, VGC_KERNEL_HZB = 5, VGC_KERNEL_CHUNKS0 = 6, VGC_KERNEL_KINDS = 8 };
+       VGC_KERNEL_FINISH = 4, VGC_KERNEL_HZB = 5, VGC_KERNEL_CHUNKS0 = 6, VGC_KERNEL_BUDGET = 7, VGC_KERNEL_KINDS = 8 };
 /* With `enable`, the plain path (vgc_cut, vgc_hzb_build) records CUDA events around each of its kernel launches
    on the launching stream. vgc_kernel_times synchronises and returns, per VGC_KERNEL_* kind, the summed device
    milliseconds and the launch count since the last reset (reset = 1 clears them). */

@@ -162,7 +162,9 @@ class _View(C.Structure):
                 ("max_error_threshold", C.c_double), ("shadow_sweep", C.c_double * 3), ("frustum_culling", C.c_uint32),
                 ("occlusion_active", C.c_uint32), ("hzb", C.POINTER(C.c_float)), ("hzb_levels", C.c_uint32),
                 ("hzb_offset", C.c_uint32 * 16), ("hzb_width", C.c_uint32 * 16), ("hzb_height", C.c_uint32 * 16),
-                ("max_drawn", C.c_uint32), ("index_capacity", C.c_uint32 * 2), ("state", C.c_uint32 * 8)]
+                ("max_drawn", C.c_uint32), ("index_capacity", C.c_uint32 * 2), ("state", C.c_uint32 * 8),
+                ("triangle_budget", C.c_double), ("threshold_range", C.c_double * 2),
+                ("chosen_threshold", C.c_double), ("predicted_triangles", C.c_uint64)]
 
 
 class _Result(C.Structure):
@@ -264,6 +266,9 @@ def make_view(camera, params, max_drawn=1 << 20, index_capacity=(30_000_000, 12_
     st = state if state is not None else [10000, 10000, 0, 0, 0, 0, 0, 0]
     for i in range(8):
         v.state[i] = int(st[i])
+    v.triangle_budget = float(getattr(params, "triangle_budget", 0.0))
+    tr = getattr(params, "threshold_range", (0.5, 3.0))
+    v.threshold_range[0], v.threshold_range[1] = float(tr[0]), float(tr[1])
     v.occlusion_active = 0
     if hzb is not None:
         mips, levels, off, ww, hh = hzb
@@ -291,7 +296,8 @@ def cull_pass(scene: OracleScene, view: _View, precision: str = "f32", threads: 
     fn(C.addressof(scene.struct), C.addressof(view), C.addressof(r), threads)
     return dict(entries=[e0[:r.entry_count[0]].copy(), e1[:r.entry_count[1]].copy()], counters=list(r.counters),
                 mesh_counts=mc.reshape(2, scene.mesh_count, 2), draw_args=args.reshape(2, scene.mesh_count, 2, 5),
-                rounds=r.rounds, state=list(view.state))
+                rounds=r.rounds, state=list(view.state), threshold=view.chosen_threshold,
+                predicted=view.predicted_triangles)
 
 
 def explain(scene: OracleScene, view: _View, cut: int, instance: int, meshlet: int) -> float:

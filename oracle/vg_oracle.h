@@ -99,6 +99,10 @@ typedef struct vgo_view {
   uint32_t max_drawn;         /* draw-list capacity per cut (maxMeshlets) */
   uint32_t index_capacity[2]; /* index-buffer capacity per cut (3 x maxTriangles, 3 x maxShadowTriangles) */
   uint32_t state[8];          /* capacity controller state words (fixed point x 10000), carried between frames */
+  double triangle_budget;     /* > 0: pick errorThreshold by the histogram search over threshold_range */
+  double threshold_range[2];
+  double chosen_threshold;    /* out: errorThreshold the budget search picked */
+  uint64_t predicted_triangles; /* out: plain camera-cut triangles the histogram predicts at that threshold */
 } vgo_view;
 
 typedef struct vgo_result {

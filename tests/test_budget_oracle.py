@@ -1,0 +1,43 @@
+"""triangleBudget histogram search in the oracle: the predicted plain-cut triangles equal the cut's drawn triangles
+at the chosen threshold (blend off, no occlusion), and one bin finer the cut exceeds the budget."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+import oracle as O
+from vgcut import engine, scenes
+from vgcut.camera import Camera
+
+
+@pytest.fixture(scope="module")
+def small():
+    spec = scenes.plain_small(n=40, seed=1)
+    scene, _, _ = O.scene_from_spec(spec.meshes, spec.instances)
+    return spec, scene
+
+
+def drawn_triangles(scene, cam, p, precision):
+    r = O.cull_pass(scene, O.make_view(cam, p), precision)
+    return r["counters"][2 + 4] // 3, r
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_budget_prediction_is_exact_without_blend(small, precision):
+    spec, scene = small
+    cams = [spec.cameras[0], Camera.perspective_look_at((14, 6, -9), (0, 0, 0), 60, 1920, 1080, 0.1, 1000)]
+    for cam in cams:
+        full, _ = drawn_triangles(scene, cam, engine.ViewParams(error_threshold=0.5, lod_blend=1.0), precision)
+        for frac in (0.2, 0.5, 0.9):
+            budget = full * frac
+            p = engine.ViewParams(lod_blend=1.0, triangle_budget=budget, threshold_range=(0.5, 3.0))
+            got, r = drawn_triangles(scene, cam, p, precision)
+            t = r["threshold"]
+            assert 0.5 <= t <= 3.0
+            assert got == r["predicted"], "histogram prediction equals the cut at the chosen threshold"
+            if t < 3.0:
+                assert got <= budget
+            if t > 0.5:  # one bin finer would not fit
+                finer = 0.5 + (3.0 - 0.5) * (round((t - 0.5) / 2.5 * 255) - 1) / 255
+                over, _ = drawn_triangles(scene, cam, engine.ViewParams(error_threshold=finer, lod_blend=1.0), precision)
+                assert over > budget

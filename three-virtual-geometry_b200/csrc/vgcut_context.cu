@@ -66,6 +66,7 @@ uint32_t pad32(uint32_t x) { return (x + 31u) & ~31u; }
 struct LaunchScratch {
   uint32_t hzb_w = 0, hzb_h = 0;  // largest depth image the views of this launch build an HZB from (0: none)
   bool hzb_tail = false;
+  bool any_budget = false;        // a view of this launch searches its threshold for a triangleBudget
   ViewConst *h_views = nullptr;  // pinned
   ViewConst *d_views = nullptr;
   uint2 *d_units = nullptr;
@@ -135,6 +136,7 @@ struct vgc_batch {
   uint32_t graph_slots = 0;
   uint32_t graph_hzb_w = 0, graph_hzb_h = 0;
   bool graph_hzb_tail = false;
+  bool graph_budget = false;
 };
 
 namespace {
@@ -412,6 +414,9 @@ int view_constants(vgc_context *ctx, const vgc_view &in, uint32_t out_slot, uint
   k.min_pixel_radius = (float)in.min_pixel_radius;
   k.shadow_error_scale = (float)in.shadow_error_scale;
   k.budget = (float)(in.triangle_budget > 0 ? in.triangle_budget : 0);
+  k.budget_tris = in.triangle_budget > 0 ? (unsigned long long)in.triangle_budget : 0ull;
+  if (in.triangle_budget > 0 && !(in.threshold_range[0] > 0 && in.threshold_range[1] > in.threshold_range[0]))
+    return fail(VGC_INVALID_ARG, "view: triangle_budget needs 0 < threshold_range[0] < threshold_range[1]");
   k.budget_lo = (float)in.threshold_range[0];
   k.budget_hi = (float)in.threshold_range[1];
   k.frustum = in.frustum_culling ? 1u : 0u;
@@ -444,6 +449,8 @@ int prepare(vgc_context *ctx, LaunchScratch &s, const vgc_view *views, uint32_t 
   bool changed = false;
   s.hzb_w = s.hzb_h = 0;
   s.hzb_tail = false;
+  s.any_budget = false;
+  for (uint32_t i = 0; i < count; i++) s.any_budget = s.any_budget || views[i].triangle_budget > 0;
   for (uint32_t i = 0; i < count; i++) {
     const vgc_view &v = views[i];
     if (v.hzb >= 0 && v.depth) {
@@ -505,6 +512,16 @@ int enqueue(vgc_context *ctx, LaunchScratch &s, uint32_t count, cudaStream_t st,
                  [&] { return launch_reset(s.d_views, count, ctx->counter_words, s.d_unit_count, st); }));
   CUDA_TRY(timed(ctx, capture, VGC_KERNEL_CELLS, st,
                  [&] { return launch_cells(S, s.d_views, count, count * cells, s.d_units, s.d_unit_count, st); }));
+  if (s.any_budget) {  // the triangleBudget search: histogram pass, then the threshold of each budget view
+    CUDA_TRY(timed(ctx, capture, VGC_KERNEL_BUDGET, st, [&] {
+      cudaError_t e = launch_instances(S, s.d_views, hzbs, s.d_units, s.d_unit_count, s.d_chunks, s.chunk_capacity, -1,
+                                       ctx->select_grid, st);
+      if (e == cudaSuccess)
+        e = launch_chunks(S, s.d_views, hzbs, s.d_chunks, s.d_unit_count, s.chunk_capacity, -1, ctx->chunk_grid, st);
+      if (e == cudaSuccess) e = launch_budget(s.d_views, count, s.d_unit_count, st);
+      return e;
+    }));
+  }
   for (int round = 0; round < 3; round++) {
     CUDA_TRY(timed(ctx, capture, round == 0 ? VGC_KERNEL_SELECT0 : VGC_KERNEL_SELECT_RETRY, st, [&] {
       return launch_instances(S, s.d_views, hzbs, s.d_units, s.d_unit_count, s.d_chunks, s.chunk_capacity, round,
@@ -908,7 +925,8 @@ int vgc_batch_run(vgc_batch *b, const vgc_view *views, uint32_t count, uint32_t 
   if (rc) return rc;
   const uint32_t cells = (uint32_t)ctx->cells.size();
   if (!b->exec || b->graph_views != count || b->graph_cells != cells || b->graph_slots != ctx->slot_capacity ||
-      b->graph_hzb_w != b->scratch.hzb_w || b->graph_hzb_h != b->scratch.hzb_h || b->graph_hzb_tail != b->scratch.hzb_tail) {
+      b->graph_hzb_w != b->scratch.hzb_w || b->graph_hzb_h != b->scratch.hzb_h || b->graph_hzb_tail != b->scratch.hzb_tail ||
+      b->graph_budget != b->scratch.any_budget) {
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     b->exec = nullptr;
@@ -930,6 +948,7 @@ int vgc_batch_run(vgc_batch *b, const vgc_view *views, uint32_t count, uint32_t 
     b->graph_hzb_w = b->scratch.hzb_w;
     b->graph_hzb_h = b->scratch.hzb_h;
     b->graph_hzb_tail = b->scratch.hzb_tail;
+    b->graph_budget = b->scratch.any_budget;
   }
   CUDA_TRY(cudaGraphLaunch(b->exec, st));
   CUDA_TRY(cudaEventRecord(b->scratch.done, st));
@@ -991,6 +1010,7 @@ int vgc_read_stats(vgc_context *ctx, uint32_t slot, vgc_stats *s, vgc_stream str
   s->meshlets_tested = c[VGC_COUNTER_MESHLETS_TESTED];
   s->fast_emitted = c[VGC_COUNTER_FAST_EMITTED];
   s->levels_read = c[VGC_COUNTER_LEVELS_READ];
+  s->predicted_triangles = (uint64_t)c[VGC_COUNTER_PREDICTED_LO] | ((uint64_t)c[VGC_COUNTER_PREDICTED_HI] << 32);
   float dyn = 0;
   CUDA_TRY(cudaMemcpy(&dyn, (const float *)ctx->d_dyn.ptr + (size_t)slot * 8, 4, cudaMemcpyDeviceToHost));
   s->effective_threshold = dyn;
@@ -1226,6 +1246,11 @@ extern "C" int vgc_cut_noalloc(vgc_context *ctx, const vgc_view *view, uint32_t 
   }
   CUDA_TRY(launch_reset(d_view, 1, ctx->counter_words, ctl, st));
   CUDA_TRY(launch_cells(S, d_view, 1, cells, units, ctl, st));
+  if (view->triangle_budget > 0) {
+    CUDA_TRY(launch_instances(S, d_view, hzbs, units, ctl, chunks, kNoAllocMaxChunks, -1, ctx->select_grid, st));
+    CUDA_TRY(launch_chunks(S, d_view, hzbs, chunks, ctl, kNoAllocMaxChunks, -1, ctx->chunk_grid, st));
+    CUDA_TRY(launch_budget(d_view, 1, ctl, st));
+  }
   for (int round = 0; round < 3; round++) {
     CUDA_TRY(launch_instances(S, d_view, hzbs, units, ctl, chunks, kNoAllocMaxChunks, round, ctx->select_grid, st));
     CUDA_TRY(launch_chunks(S, d_view, hzbs, chunks, ctl, kNoAllocMaxChunks, round, ctx->chunk_grid, st));

@@ -92,6 +92,7 @@ struct ViewConst {
   float *dyn;           // [0] error threshold of this frame (errorThreshold or the budget search result),
                         // [1..5] its bands: low (cut 0, 1), high (cut 0, 1), fade scale
   unsigned long long *hist;  // 2 * kBudgetBins: triangles entering / leaving the cut per threshold bin
+  unsigned long long budget_tris;  // triangleBudget as an integer (the search compares T(t) <= budget_tris)
 };
 
 }  // namespace vgc

@@ -428,12 +428,71 @@ __device__ __forceinline__ void emit_fast(const Scene &S, const ViewConst &V, ui
     }
 }
 
+// ---- triangleBudget search. Thresholds t_k = lo + (hi - lo) * (k / 255) over thresholdRange, effective
+// e_k = t_k * cameraScale; a meshlet of a visible instance is in the plain camera cut at t_k iff b_own <= k < b_par
+// with b_x = the first k such that x <= e_k. Its triangles enter the histogram at b_own and leave at b_par.
+__device__ __forceinline__ float budget_e(const ViewConst &V, float s, uint32_t k) {
+  return (V.budget_lo + (V.budget_hi - V.budget_lo) * (float(k) / 255.0f)) * s;
+}
+
+__device__ __forceinline__ uint32_t budget_bin(const ViewConst &V, float s, float x) {
+  // estimate, then exact comparisons with e_k (bounded: the estimate is off by a few bins at most)
+  const float guess = ((x / s - V.budget_lo) / (V.budget_hi - V.budget_lo)) * 255.0f;
+  int k = guess != guess ? 0 : (guess < 0.0f ? 0 : (guess > 256.0f ? 256 : int(guess)));
+  for (int i = 0; i < 600 && k > 0 && x <= budget_e(V, s, uint32_t(k - 1)); i++) k--;
+  for (int i = 0; i < 600 && k < int(kBudgetBins) && !(x <= budget_e(V, s, uint32_t(k))); i++) k++;
+  return uint32_t(k);
+}
+
+// Histogram bins of one meshlet (camera cut): false when it is in no cut of the range or culled.
+__device__ __forceinline__ bool hist_meshlet(const Scene &S, const ViewConst &V, const HzbDesc *hzbs, float s,
+                                             float high0, bool occl_on, bool inside, const float *VM, uint32_t meshlet,
+                                             uint32_t &bo, uint32_t &bp, uint32_t &tris) {
+  const float scale = VM[12];
+  const float4 ls = __ldg(S.m_lod + meshlet), ps = __ldg(S.m_parent + meshlet), er = __ldg(S.m_err + meshlet);
+  bo = budget_bin(V, s, proj_error(V, VM, scale, ls, er.x));
+  bp = budget_bin(V, s, proj_error(V, VM, scale, ps, er.y));
+  if (!(bo < bp)) return false;
+  tris = __float_as_uint(er.z);
+  const float4 cs = __ldg(S.m_cull + meshlet);
+  float c[3];
+  xform(VM, cs.x, cs.y, cs.z, c);
+  const float r = cs.w * scale;
+  if (V.frustum && !inside && !(frustum(V, c, false) >= -r)) return false;
+  if (occluded(V, hzbs, high0, occl_on, c, r)) return false;
+  return true;
+}
+
+// Adds one warp step's triangles to the view's histogram: one atomic per distinct bin in the warp.
+__device__ __forceinline__ void warp_hist_add(unsigned long long *hist, bool add, uint32_t bin, uint32_t tris) {
+  uint32_t pending = __ballot_sync(0xffffffffu, add && bin < kBudgetBins);
+  while (pending) {
+    const uint32_t key = __shfl_sync(0xffffffffu, bin, __ffs(pending) - 1);
+    const uint32_t group = __ballot_sync(0xffffffffu, add && bin == key);
+    const uint32_t sum = __reduce_add_sync(0xffffffffu, (group >> (threadIdx.x & 31)) & 1u ? tris : 0u);
+    if ((threadIdx.x & 31) == __ffs(group) - 1) atomicAdd(hist + key, (unsigned long long)sum);
+    pending &= ~group;
+  }
+}
+
 // Tests a whole item (one instance's meshlets [first, first + count) of one cut) with the warp: the fallback when
-// the chunk queue is full.
+// the chunk queue is full. HIST: the budget histogram instead of the draw list.
+template <bool HIST>
 __device__ void warp_item(const Scene &S, const ViewConst &V, const HzbDesc *hzbs, WarpStage &ws, uint32_t slot,
                           uint32_t cut, bool occl_on, bool inside, const float *VM, uint32_t instance, uint32_t first,
                           uint32_t count) {
   const ViewBands b = bands_of(V);
+  if (HIST) {
+    const float s = get_state(V.state, 0);
+    for (uint32_t base = 0; base < count; base += 32) {
+      const uint32_t t = base + (threadIdx.x & 31);
+      uint32_t bo = 0, bp = 0, tris = 0;
+      const bool add = t < count && hist_meshlet(S, V, hzbs, s, b.high0, occl_on, inside, VM, first + t, bo, bp, tris);
+      warp_hist_add(V.hist, add, bo, tris);
+      warp_hist_add(V.hist + kBudgetBins, add, bp, tris);
+    }
+    return;
+  }
   const float low = cut ? b.low1 : b.low0, high = cut ? b.high1 : b.high0;
   WarpCount wc{0, 0, 0};
   for (uint32_t base = 0; base < count; base += 32) {
@@ -449,6 +508,9 @@ __device__ void warp_item(const Scene &S, const ViewConst &V, const HzbDesc *hzb
 
 // One warp per 32 instances of a visible (view, cell) unit: the instance pass of GeometryPool.ts:846-913. Fast-path
 // instances emit their meshlets; the others hand their level range to k_chunks as chunks of <= kChunk meshlets.
+// HIST: the budget search's pass (views with a triangleBudget only): the camera cut's level range over the whole
+// threshold range, no fast path, no counters.
+template <bool HIST>
 __global__ void __launch_bounds__(128) k_instances(Scene S, const ViewConst *__restrict__ views,
                                                    const HzbDesc *__restrict__ hzbs, const uint2 *__restrict__ units,
                                                    uint32_t *__restrict__ ctl, uint4 *__restrict__ chunks,
@@ -462,7 +524,8 @@ __global__ void __launch_bounds__(128) k_instances(Scene S, const ViewConst *__r
   for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < work; w += nwarps) {
     const uint2 unit = units[w >> 2];
     const ViewConst &V = views[unit.x];
-    bool redo0 = true, redo1 = true;
+    if (HIST && !(V.budget > 0.0f)) continue;
+    bool redo0 = true, redo1 = !HIST;
     if (round > 0) {
       redo0 = V.counters[VGC_COUNTER_REDO0] != 0;
       redo1 = V.counters[VGC_COUNTER_REDO1] != 0;
@@ -511,7 +574,11 @@ __global__ void __launch_bounds__(128) k_instances(Scene S, const ViewConst *__r
         xform(VM, mesh.cull.x, mesh.cull.y, mesh.cull.z, cc);
         const float cr = mesh.cull.w * scale;
         // inside: the cullBoundsSphere lies in the frustum, so every meshlet passes its frustum test
-        if (in_camera) {
+        if (HIST && in_camera) {
+          const float sc = get_state(V.state, 0);
+          r0 = level_range(L, levels, budget_e(V, sc, 0), budget_e(V, sc, 255), px_min, px_max);
+          inside0 = no_frustum || frustum(V, cc, false) >= cr;
+        } else if (in_camera) {
           r0 = level_range(L, levels, b.low0, b.high0, px_min, px_max);
           inside0 = no_frustum || frustum(V, cc, false) >= cr;
           fast0 = r0.last > r0.first && r0.possible == r0.last - r0.first && r0.guaranteed == r0.possible &&
@@ -527,6 +594,7 @@ __global__ void __launch_bounds__(128) k_instances(Scene S, const ViewConst *__r
     }
     const bool surv0 = r0.last > r0.first, surv1 = r1.last > r1.first;
     const bool item0 = surv0 && !fast0, item1 = surv1 && !fast1;
+    if (!HIST) {
     // warp totals for the view's counters (one atomic per counter and warp)
     const uint32_t n_occl = __popc(__ballot_sync(0xffffffffu, occluded_now));
     const uint32_t n_s0 = __popc(__ballot_sync(0xffffffffu, surv0)), n_s1 = __popc(__ballot_sync(0xffffffffu, surv1));
@@ -547,6 +615,7 @@ __global__ void __launch_bounds__(128) k_instances(Scene S, const ViewConst *__r
     }
     emit_fast(S, V, cell.slot, 0, fast0 ? r0.possible : 0u, r0.first, instance);
     emit_fast(S, V, cell.slot, 1, fast1 ? r1.possible : 0u, r1.first, instance);
+    }
     // items -> chunks of <= kChunk meshlets
     const uint32_t c0 = item0 ? (r0.last - r0.first + kChunk - 1) / kChunk : 0u;
     const uint32_t c1 = item1 ? (r1.last - r1.first + kChunk - 1) / kChunk : 0u;
@@ -585,8 +654,8 @@ __global__ void __launch_bounds__(128) k_instances(Scene S, const ViewConst *__r
         const uint32_t cut = k < jc0 ? 0u : 1u, kk = k < jc0 ? k : k - jc0;
         const uint32_t first = (cut ? f1 : f0) + kk * kChunk;
         const uint32_t cnt = min(kChunk, (cut ? e1 - f1 : e0 - f0) - kk * kChunk);
-        warp_item(S, V, hzbs, ws, cell.slot, cut, cut == 0 && occl_on, cut ? jin1 : jin0, vmj,
-                  cell.first + ((w & 3u) << 5) + j, first, cnt);
+        warp_item<HIST>(S, V, hzbs, ws, cell.slot, cut, cut == 0 && occl_on, cut ? jin1 : jin0, vmj,
+                        cell.first + ((w & 3u) << 5) + j, first, cnt);
       }
     }
   }
@@ -595,6 +664,8 @@ __global__ void __launch_bounds__(128) k_instances(Scene S, const ViewConst *__r
 // ------------------------------------------------------------------------------------------------ k_chunks
 // The meshlet pass (GeometryPool.ts:916-970) over the chunks k_instances queued, one chunk (<= kChunk meshlets of
 // one instance and cut) per warp: every lane derives the view-model matrix itself, so warps never wait on each other.
+// HIST: the budget histogram of the chunks the budget pass queued.
+template <bool HIST>
 __global__ void __launch_bounds__(128) k_chunks(Scene S, const ViewConst *__restrict__ views,
                                                 const HzbDesc *__restrict__ hzbs, const uint4 *__restrict__ chunks,
                                                 uint32_t *__restrict__ ctl, uint32_t chunk_capacity, int round) {
@@ -614,6 +685,17 @@ __global__ void __launch_bounds__(128) k_chunks(Scene S, const ViewConst *__rest
     const float low = cut ? b.low1 : b.low0, high = cut ? b.high1 : b.high0;
     float VM[13];
     model_view(V.V, S.inst + (size_t)instance * 4, VM, VM[12]);
+    if (HIST) {
+      const float sc = get_state(V.state, 0);
+      for (uint32_t base = 0; base < count; base += 32) {
+        const uint32_t t = base + (threadIdx.x & 31);
+        uint32_t bo = 0, bp = 0, tris = 0;
+        const bool add = t < count && hist_meshlet(S, V, hzbs, sc, b.high0, occl_on, inside, VM, ch.w + t, bo, bp, tris);
+        warp_hist_add(V.hist, add, bo, tris);
+        warp_hist_add(V.hist + kBudgetBins, add, bp, tris);
+      }
+      continue;
+    }
     WarpCount wc{0, 0, 0};
     for (uint32_t base = 0; base < count; base += 32) {
       const uint32_t t = base + (threadIdx.x & 31);
@@ -624,6 +706,50 @@ __global__ void __launch_bounds__(128) k_chunks(Scene S, const ViewConst *__rest
       warp_stage(ws, wc, V, S.slot_capacity, cell.slot, cut, drawn, instance, ch.w + t, packed);
     }
     warp_flush(ws, wc, V, S.slot_capacity, cell.slot, cut);
+  }
+}
+
+// ------------------------------------------------------------------------------------------------ k_budget
+// One warp per view with a triangleBudget: T(t_k) = prefix sum of (entering - leaving) triangles; the smallest k with
+// T(t_k) <= budget (255 when none) sets this frame's errorThreshold and bands. Also empties the chunk queue for the
+// frame's first selection round.
+__global__ void __launch_bounds__(128) k_budget(const ViewConst *__restrict__ views, uint32_t nviews,
+                                                uint32_t *__restrict__ ctl) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctl[3] = 0;
+  const uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31;
+  if (v >= nviews) return;
+  const ViewConst &V = views[v];
+  if (!(V.budget > 0.0f)) return;
+  long long carry = 0;
+  uint32_t pick = kBudgetBins - 1;
+  long long predicted = 0;
+  bool found = false;
+  for (uint32_t base = 0; base < kBudgetBins && !found; base += 32) {
+    const uint32_t k = base + lane;
+    long long d = (long long)V.hist[k] - (long long)V.hist[kBudgetBins + k];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long t = __shfl_up_sync(0xffffffffu, d, o);
+      if (lane >= (uint32_t)o) d += t;
+    }
+    const long long T = carry + d;
+    const uint32_t ok = __ballot_sync(0xffffffffu, T <= (long long)V.budget_tris);
+    if (ok) {
+      const uint32_t j = __ffs(ok) - 1;
+      pick = base + j;
+      predicted = __shfl_sync(0xffffffffu, T, j);
+      found = true;
+    }
+    carry += __shfl_sync(0xffffffffu, d, 31);
+  }
+  if (!found) predicted = carry;
+  if (lane == 0) {
+    const float t = V.budget_lo + (V.budget_hi - V.budget_lo) * (float(pick) / 255.0f);
+    store_bands(V, t);
+    V.counters[VGC_COUNTER_PREDICTED_LO] = (uint32_t)((unsigned long long)predicted & 0xffffffffull);
+    V.counters[VGC_COUNTER_PREDICTED_HI] = (uint32_t)((unsigned long long)predicted >> 32);
+    V.counters[VGC_COUNTER_BUDGET_BIN] = pick;
   }
 }
 
@@ -945,7 +1071,10 @@ __global__ void __launch_bounds__(256) k_reset(const ViewConst *__restrict__ vie
   for (uint32_t v = blockIdx.x; v < nviews; v += gridDim.x) {
     uint32_t *c = views[v].counters;
     for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) c[i] = 0;
-    if (threadIdx.x == 0 && !(views[v].budget > 0.0f)) store_bands(views[v], views[v].error_threshold);
+    if (threadIdx.x == 0)  // budget views: the search's pass uses the band at the top of the threshold range
+      store_bands(views[v], views[v].budget > 0.0f ? views[v].budget_hi : views[v].error_threshold);
+    if (views[v].budget > 0.0f)
+      for (uint32_t i = threadIdx.x; i < 2 * kBudgetBins; i += blockDim.x) views[v].hist[i] = 0;
   }
 }
 
@@ -966,21 +1095,33 @@ cudaError_t launch_cells(const Scene &S, const ViewConst *views, uint32_t nviews
 }
 
 cudaError_t configure_select(int *instances_per_sm, int *chunks_per_sm) {
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(instances_per_sm, k_instances, 128, 0);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(instances_per_sm, k_instances<false>, 128, 0);
   if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(chunks_per_sm, k_chunks, 128, 0);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(chunks_per_sm, k_chunks<false>, 128, 0);
 }
 
 cudaError_t launch_instances(const Scene &S, const ViewConst *views, const HzbDesc *hzbs, const uint2 *units,
                              uint32_t *ctl, uint4 *chunks, uint32_t chunk_capacity, int round, uint32_t grid,
                              cudaStream_t st) {
-  k_instances<<<grid, 128, 0, st>>>(S, views, hzbs, units, ctl, chunks, chunk_capacity, round);
+  if (round < 0)  // the budget search's pass
+    k_instances<true><<<grid, 128, 0, st>>>(S, views, hzbs, units, ctl, chunks, chunk_capacity, 0);
+  else
+    k_instances<false><<<grid, 128, 0, st>>>(S, views, hzbs, units, ctl, chunks, chunk_capacity, round);
   return cudaGetLastError();
 }
 
 cudaError_t launch_chunks(const Scene &S, const ViewConst *views, const HzbDesc *hzbs, const uint4 *chunks,
                           uint32_t *ctl, uint32_t chunk_capacity, int round, uint32_t grid, cudaStream_t st) {
-  k_chunks<<<grid, 128, 0, st>>>(S, views, hzbs, chunks, ctl, chunk_capacity, round);
+  if (round < 0)
+    k_chunks<true><<<grid, 128, 0, st>>>(S, views, hzbs, chunks, ctl, chunk_capacity, 0);
+  else
+    k_chunks<false><<<grid, 128, 0, st>>>(S, views, hzbs, chunks, ctl, chunk_capacity, round);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_budget(const ViewConst *views, uint32_t nviews, uint32_t *ctl, cudaStream_t st) {
+  const uint32_t blocks = (nviews * 32 + 127) / 128;
+  k_budget<<<blocks, 128, 0, st>>>(views, nviews, ctl);
   return cudaGetLastError();
 }
 

@@ -13,6 +13,9 @@ cudaError_t configure_select(int *instances_per_sm, int *chunks_per_sm);
 cudaError_t launch_reset(const ViewConst *views, uint32_t nviews, uint32_t words, uint32_t *ctl, cudaStream_t st);
 cudaError_t launch_cells(const Scene &S, const ViewConst *views, uint32_t nviews, uint32_t total_units, uint2 *units,
                          uint32_t *unit_count, cudaStream_t st);
+// round < 0: the triangleBudget search's histogram pass (k_instances / k_chunks), then launch_budget picks the
+// threshold of each budget view.
+cudaError_t launch_budget(const ViewConst *views, uint32_t nviews, uint32_t *ctl, cudaStream_t st);
 cudaError_t launch_instances(const Scene &S, const ViewConst *views, const HzbDesc *hzbs, const uint2 *units,
                              uint32_t *ctl, uint4 *chunks, uint32_t chunk_capacity, int round, uint32_t grid,
                              cudaStream_t st);

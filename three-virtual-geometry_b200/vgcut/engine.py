@@ -71,7 +71,7 @@ class Stats(C.Structure):
                 ("requested_indices", C.c_uint32 * 2), ("rounds", C.c_uint32), ("overflow", C.c_uint32),
                 ("threshold_scale", C.c_float * 2), ("fill", C.c_float * 2), ("effective_threshold", C.c_float),
                 ("instances_tested", C.c_uint32), ("meshlets_tested", C.c_uint32), ("fast_emitted", C.c_uint32),
-                ("levels_read", C.c_uint32)]
+                ("levels_read", C.c_uint32), ("predicted_triangles", C.c_uint64)]
 
     def as_dict(self) -> dict:
         out = {}
@@ -371,7 +371,7 @@ class VirtualGeometry:
         check(lib().vgc_state_access(self.handle, state_slot, _up(w), 0 if words is None else 1, None))
         return w
 
-    KERNEL_KINDS = ("reset", "cells", "select0", "retry", "finish", "hzb", "chunks0")
+    KERNEL_KINDS = ("reset", "cells", "select0", "retry", "finish", "hzb", "chunks0", "budget")
 
     def set_profiling(self, enable: bool) -> None:
         check(lib().vgc_set_profiling(self.handle, 1 if enable else 0))
