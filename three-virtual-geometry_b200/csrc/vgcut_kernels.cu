@@ -233,6 +233,8 @@ __global__ void __launch_bounds__(256) k_cells(Scene S, const ViewConst *__restr
 // ------------------------------------------------------------------------------------------------ k_instances
 constexpr int kWarpStage = 96;   // staged draw entries per warp and cut (a step adds <= 32)
 constexpr uint32_t kChunk = 256;  // meshlets per chunk (one warp in k_chunks)
+static_assert(kChunk % kBlock == 0 && kChunk / kBlock + 1 <= 32, "a chunk's blocks are tested one per lane");
+constexpr uint32_t kBlockTestMin = 128;  // chunks of at least this many meshlets test their blocks' bounds first
 
 // Band values of a view for the current round, written by k_reset and by the capacity check (dyn[1..5]).
 struct ViewBands {
@@ -352,12 +354,14 @@ __device__ __forceinline__ void warp_stage(WarpStage &ws, WarpCount &wc, const V
 // `drawn` is their conjunction either way. `packed` receives triCount | lo << 8 | hi << 16.
 __device__ __forceinline__ bool test_meshlet(const Scene &S, const ViewConst &V, const HzbDesc *hzbs, float low,
                                              float high, float fs, float high0, uint32_t cut, bool occl_on,
-                                             bool inside, const float *VM, uint32_t meshlet, uint32_t &packed) {
+                                             bool inside, const float *VM, uint32_t meshlet, uint32_t &packed,
+                                             uint32_t &id) {
   const float scale = VM[12];
   const float4 ls = __ldg(S.m_lod + meshlet), ps = __ldg(S.m_parent + meshlet), er = __ldg(S.m_err + meshlet);
   const float own = proj_error(V, VM, scale, ls, er.x);
   const float parent = proj_error(V, VM, scale, ps, er.y);
   if (!(own <= high && parent > low)) return false;
+  id = __float_as_uint(er.w);  // pool-global meshlet id (the columns are in test order)
   const uint32_t lo = fs > 0.0f ? fade_step(own, low, fs) : 0u;
   const uint32_t hi = fs > 0.0f ? fade_step(parent, low, fs) : 255u;
   if (!(hi > lo)) return false;
@@ -370,6 +374,111 @@ __device__ __forceinline__ bool test_meshlet(const Scene &S, const ViewConst &V,
   if (V.frustum && !inside && !(frustum(V, c, cut == 1) >= -r)) return false;
   if (cut == 0 && occluded(V, hzbs, high0, occl_on, c, r)) return false;
   return true;
+}
+
+// ---- Bounds blocks: kBlock pool-consecutive meshlets with spheres enclosing their LOD, parent-LOD and culling
+// spheres and the extreme errors. block_may_pass is false only when no meshlet of the block can pass the LOD band
+// (own <= high && parent > low) or the frustum test in the float arithmetic test_meshlet uses, so skipping such a
+// block never changes a decision:
+//  * |VM (c_m - C)| <= sigma |c_m - C| <= sigma (R - r_m), sigma = sqrt(max row sum of |VM3^T VM3|) bounding the
+//    spectral norm of the instance's linear part (= the largest axis scale for rotation x scale matrices);
+//  * so every meshlet distance max(|VM c_m| - r_m s, near) lies in [D - sigma R, D + sigma R] around the block's D;
+//  * proj_error's rounding is monotone in the error and the distance, so the bound's float result orders the same
+//    way as each meshlet's, and `slack` (1e-5 of the magnitudes involved, hundreds of float ulps) absorbs the
+//    rounding of the transforms, lengths and plane dot products on both sides.
+struct BlockFrame {
+  float sigma, tmag;  // spectral-norm bound of VM's 3x3 part; length of VM's translation
+};
+
+__device__ __forceinline__ BlockFrame block_frame(const float *VM) {
+  float g[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) g[i][j] = (VM[i] * VM[j] + VM[4 + i] * VM[4 + j]) + VM[8 + i] * VM[8 + j];
+  float row = 0.0f;
+#pragma unroll
+  for (int i = 0; i < 3; i++) row = fmx(row, (fabsf(g[i][0]) + fabsf(g[i][1])) + fabsf(g[i][2]));
+  BlockFrame f;
+  f.sigma = sqrtf(row) * 1.00001f;
+  const float t[3] = {VM[3], VM[7], VM[11]};
+  f.tmag = len3(t);
+  return f;
+}
+
+__device__ __forceinline__ bool block_may_pass(const Scene &S, const ViewConst &V, const float *VM, const BlockFrame &F,
+                                               uint32_t block, float low, float high, bool test_frustum, bool swept) {
+  const float scale = VM[12];
+  const float4 *B = S.blocks + (size_t)block * 4;
+  const float4 bo = __ldg(B), bp = __ldg(B + 1), be = __ldg(B + 3);
+  float c[3];
+  // own error: every meshlet's >= err_min * s / (D + sigma R) * P
+  xform(VM, bo.x, bo.y, bo.z, c);
+  float d = len3(c);
+  float cm[3] = {bo.x, bo.y, bo.z};
+  float slack = 1e-5f * ((d + F.tmag) + F.sigma * (len3(cm) + bo.w));
+  const float own_lo = ((be.x * scale) / fmx((d + F.sigma * bo.w) + slack, V.near_)) * V.proj_scale;
+  if (own_lo > high) return false;
+  // parent error: every meshlet's <= err_max * s / max(D - sigma R, near) * P (roots: 1e30, always above low)
+  if (be.y < float(1e30 * 0.5)) {
+    xform(VM, bp.x, bp.y, bp.z, c);
+    d = len3(c);
+    cm[0] = bp.x, cm[1] = bp.y, cm[2] = bp.z;
+    slack = 1e-5f * ((d + F.tmag) + F.sigma * (len3(cm) + bp.w));
+    const float par_hi = ((be.y * scale) / fmx((d - F.sigma * bp.w) - slack, V.near_)) * V.proj_scale;
+    if (!(par_hi > low)) return false;
+  }
+  if (test_frustum) {  // a plane with the whole enclosing culling sphere behind it
+    const float4 bc = __ldg(B + 2);
+    xform(VM, bc.x, bc.y, bc.z, c);
+    d = len3(c);
+    cm[0] = bc.x, cm[1] = bc.y, cm[2] = bc.z;
+    const float reach = F.sigma * bc.w;
+    const float base = (d + F.tmag) + F.sigma * (len3(cm) + bc.w);
+#pragma unroll
+    for (int p = 0; p < 6; p++) {
+      float dp = ((V.plane[p * 4] * c[0] + V.plane[p * 4 + 1] * c[1]) + V.plane[p * 4 + 2] * c[2]) + V.plane[p * 4 + 3];
+      float sw = swept ? V.sweep[p] : 0.0f;
+      dp = dp + sw;
+      const float sl = 1e-5f * ((base + fabsf(V.plane[p * 4 + 3])) + sw);
+      if (dp < -(reach + sl)) return false;
+    }
+  }
+  return true;
+}
+
+// Meshlets of one chunk that passed the LOD band, waiting for the rest of their test with all 32 lanes busy
+// (about a third of the tested meshlets pass; testing them in place would leave most lanes idle).
+struct LodQueue {
+  uint32_t pos[64];
+  float own[64], parent[64];
+};
+
+// The rest of test_meshlet for queue entries [0, n): fade steps, culling sphere against the frustum, HZB.
+__device__ __forceinline__ void drain_queue(const Scene &S, const ViewConst &V, const HzbDesc *hzbs, LodQueue &q,
+                                            uint32_t n, WarpStage &ws, WarpCount &wc, float low, float fs, float high0,
+                                            uint32_t cut, bool occl_on, bool inside, const float *VM, uint32_t slot,
+                                            uint32_t instance) {
+  const uint32_t lane = threadIdx.x & 31;
+  bool drawn = false;
+  uint32_t packed = 0, id = 0;
+  if (lane < n) {
+    const uint32_t pos = q.pos[lane];
+    const float own = q.own[lane], parent = q.parent[lane];
+    const uint32_t lo = fs > 0.0f ? fade_step(own, low, fs) : 0u;
+    const uint32_t hi = fs > 0.0f ? fade_step(parent, low, fs) : 255u;
+    if (hi > lo) {
+      const float4 er = __ldg(S.m_err + pos), cs = __ldg(S.m_cull + pos);
+      id = __float_as_uint(er.w);
+      packed = __float_as_uint(er.z) | (lo << 8) | (hi << 16);
+      float c[3];
+      xform(VM, cs.x, cs.y, cs.z, c);
+      const float r = cs.w * VM[12];
+      drawn = !(V.frustum && !inside && !(frustum(V, c, cut == 1) >= -r)) &&
+              !(cut == 0 && occluded(V, hzbs, high0, occl_on, c, r));
+    }
+  }
+  warp_stage(ws, wc, V, S.slot_capacity, slot, cut, drawn, instance, id, packed);
 }
 
 struct LevelRange {
@@ -407,11 +516,13 @@ __device__ __forceinline__ void emit_fast(const Scene &S, const ViewConst &V, ui
   uint32_t base = 0;
   if (lane == 0) base = atomicAdd(V.counters + C_CUT(cut) + VGC_CUT_SELECTED, total_n);
   base = __shfl_sync(0xffffffffu, base, 0) + (incl_n - n);
-  uint32_t tri[kFastPathMax];
+  uint32_t tri[kFastPathMax], id[kFastPathMax];
   uint32_t kept_tri3 = 0;
 #pragma unroll
   for (uint32_t k = 0; k < kFastPathMax; k++) {
-    tri[k] = k < n ? __float_as_uint(S.m_err[first + k].z) : 0u;
+    const float4 er = k < n ? S.m_err[first + k] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    tri[k] = __float_as_uint(er.z);
+    id[k] = __float_as_uint(er.w);
     if (k < n && base + k < V.max_drawn) kept_tri3 += tri[k] * 3u;
   }
   const uint32_t incl_t = warp_scan_incl(kept_tri3);
@@ -423,7 +534,7 @@ __device__ __forceinline__ void emit_fast(const Scene &S, const ViewConst &V, ui
 #pragma unroll
   for (uint32_t k = 0; k < kFastPathMax; k++)
     if (k < n && base + k < V.max_drawn) {
-      dst[base + k] = make_uint4(instance, first + k, acc, tri[k] | kFullFadeBits);
+      dst[base + k] = make_uint4(instance, id[k], acc, tri[k] | kFullFadeBits);
       acc += tri[k] * 3u;
     }
 }
@@ -482,6 +593,7 @@ __device__ void warp_item(const Scene &S, const ViewConst &V, const HzbDesc *hzb
                           uint32_t cut, bool occl_on, bool inside, const float *VM, uint32_t instance, uint32_t first,
                           uint32_t count) {
   const ViewBands b = bands_of(V);
+  if ((threadIdx.x & 31) == 0) atomicAdd(V.counters + VGC_COUNTER_MESHLETS_EVALUATED, count);
   if (HIST) {
     const float s = get_state(V.state, 0);
     for (uint32_t base = 0; base < count; base += 32) {
@@ -498,10 +610,10 @@ __device__ void warp_item(const Scene &S, const ViewConst &V, const HzbDesc *hzb
   for (uint32_t base = 0; base < count; base += 32) {
     const uint32_t t = base + (threadIdx.x & 31);
     bool drawn = false;
-    uint32_t packed = 0;
+    uint32_t packed = 0, id = 0;
     if (t < count)
-      drawn = test_meshlet(S, V, hzbs, low, high, b.fade_scale, b.high0, cut, occl_on, inside, VM, first + t, packed);
-    warp_stage(ws, wc, V, S.slot_capacity, slot, cut, drawn, instance, first + t, packed);
+      drawn = test_meshlet(S, V, hzbs, low, high, b.fade_scale, b.high0, cut, occl_on, inside, VM, first + t, packed, id);
+    warp_stage(ws, wc, V, S.slot_capacity, slot, cut, drawn, instance, id, packed);
   }
   warp_flush(ws, wc, V, S.slot_capacity, slot, cut);
 }
@@ -616,7 +728,7 @@ __global__ void __launch_bounds__(128) k_instances(Scene S, const ViewConst *__r
     emit_fast(S, V, cell.slot, 0, fast0 ? r0.possible : 0u, r0.first, instance);
     emit_fast(S, V, cell.slot, 1, fast1 ? r1.possible : 0u, r1.first, instance);
     }
-    // items -> chunks of <= kChunk meshlets
+    // items -> chunks of <= kChunk meshlets (each touches <= kChunk / kBlock + 1 bounds blocks)
     const uint32_t c0 = item0 ? (r0.last - r0.first + kChunk - 1) / kChunk : 0u;
     const uint32_t c1 = item1 ? (r1.last - r1.first + kChunk - 1) / kChunk : 0u;
     const uint32_t incl = warp_scan_incl(c0 + c1);
@@ -670,7 +782,9 @@ __global__ void __launch_bounds__(128) k_chunks(Scene S, const ViewConst *__rest
                                                 const HzbDesc *__restrict__ hzbs, const uint4 *__restrict__ chunks,
                                                 uint32_t *__restrict__ ctl, uint32_t chunk_capacity, int round) {
   __shared__ WarpStage stage[4];
+  __shared__ LodQueue queues[4];
   WarpStage &ws = stage[threadIdx.x >> 5];
+  LodQueue &q = queues[threadIdx.x >> 5];
   if (round > 0 && ctl[round] == 0) return;  // no view redoes a cut in this round
   const uint32_t n_chunks = min(ctl[3], chunk_capacity);
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
@@ -685,26 +799,76 @@ __global__ void __launch_bounds__(128) k_chunks(Scene S, const ViewConst *__rest
     const float low = cut ? b.low1 : b.low0, high = cut ? b.high1 : b.high0;
     float VM[13];
     model_view(V.V, S.inst + (size_t)instance * 4, VM, VM[12]);
+    // bounds blocks the chunk touches (<= kChunk / kBlock + 1): one lane each tests the block's conservative bounds
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t b0 = ch.w / kBlock, nb = (ch.w + count - 1) / kBlock - b0 + 1;
+    const float sc = HIST ? get_state(V.state, 0) : 0.0f;
+    uint32_t live = nb >= 32 ? 0xffffffffu : (1u << nb) - 1u;
+    if (count >= kBlockTestMin) {  // the block test costs about one meshlet step: worth it on long chunks only
+      const BlockFrame F = block_frame(VM);
+      const float blo = HIST ? budget_e(V, sc, 0) : low, bhi = HIST ? budget_e(V, sc, kBudgetBins - 1) : high;
+      const bool may = lane < nb && block_may_pass(S, V, VM, F, b0 + lane, blo, bhi, V.frustum && !inside, cut == 1);
+      live = __ballot_sync(0xffffffffu, may);
+    }
+    if (lane == 0) {  // meshlets of the chunk that run the per-meshlet test
+      uint32_t n = 0;
+      for (uint32_t k = 0; k < nb; k++)
+        if ((live >> k) & 1u) n += min(ch.w + count, (b0 + k + 1) * kBlock) - max(ch.w, (b0 + k) * kBlock);
+      if (n) atomicAdd(V.counters + VGC_COUNTER_MESHLETS_EVALUATED, n);
+    }
     if (HIST) {
-      const float sc = get_state(V.state, 0);
-      for (uint32_t base = 0; base < count; base += 32) {
-        const uint32_t t = base + (threadIdx.x & 31);
+      while (live) {
+        const uint32_t k = __ffs(live) - 1;
+        live &= live - 1;
+        const uint32_t m = (b0 + k) * kBlock + lane;
         uint32_t bo = 0, bp = 0, tris = 0;
-        const bool add = t < count && hist_meshlet(S, V, hzbs, sc, b.high0, occl_on, inside, VM, ch.w + t, bo, bp, tris);
+        const bool add = m >= ch.w && m < ch.w + count &&
+                         hist_meshlet(S, V, hzbs, sc, b.high0, occl_on, inside, VM, m, bo, bp, tris);
         warp_hist_add(V.hist, add, bo, tris);
         warp_hist_add(V.hist + kBudgetBins, add, bp, tris);
       }
       continue;
     }
+    // LOD band first on every meshlet of the live blocks; the survivors queue up and finish 32 at a time
     WarpCount wc{0, 0, 0};
-    for (uint32_t base = 0; base < count; base += 32) {
-      const uint32_t t = base + (threadIdx.x & 31);
-      bool drawn = false;
-      uint32_t packed = 0;
-      if (t < count)
-        drawn = test_meshlet(S, V, hzbs, low, high, b.fade_scale, b.high0, cut, occl_on, inside, VM, ch.w + t, packed);
-      warp_stage(ws, wc, V, S.slot_capacity, cell.slot, cut, drawn, instance, ch.w + t, packed);
+    uint32_t qn = 0;  // warp-uniform
+    const float scale = VM[12];
+    while (live) {
+      const uint32_t k = __ffs(live) - 1;
+      live &= live - 1;
+      const uint32_t m = (b0 + k) * kBlock + lane;
+      bool pass = false;
+      float own = 0.0f, parent = 0.0f;
+      if (m >= ch.w && m < ch.w + count) {
+        const float4 ls = __ldg(S.m_lod + m), ps = __ldg(S.m_parent + m);
+        const float2 er = __ldg(reinterpret_cast<const float2 *>(S.m_err + m));
+        own = proj_error(V, VM, scale, ls, er.x);
+        parent = proj_error(V, VM, scale, ps, er.y);
+        pass = own <= high && parent > low;
+      }
+      const uint32_t mask = __ballot_sync(0xffffffffu, pass);
+      if (pass) {
+        const uint32_t at = qn + __popc(mask & ((1u << lane) - 1u));
+        q.pos[at] = m;
+        q.own[at] = own;
+        q.parent[at] = parent;
+      }
+      qn += __popc(mask);
+      __syncwarp();
+      if (qn >= 32) {
+        drain_queue(S, V, hzbs, q, 32, ws, wc, low, b.fade_scale, b.high0, cut, occl_on, inside, VM, cell.slot, instance);
+        qn -= 32;
+        __syncwarp();
+        if (lane < qn) {
+          q.pos[lane] = q.pos[32 + lane];
+          q.own[lane] = q.own[32 + lane];
+          q.parent[lane] = q.parent[32 + lane];
+        }
+        __syncwarp();
+      }
     }
+    if (qn) drain_queue(S, V, hzbs, q, qn, ws, wc, low, b.fade_scale, b.high0, cut, occl_on, inside, VM, cell.slot, instance);
+    __syncwarp();
     warp_flush(ws, wc, V, S.slot_capacity, cell.slot, cut);
   }
 }
@@ -1057,8 +1221,9 @@ __global__ void __launch_bounds__(256) k_select_cut(Scene S, uint32_t slot, uint
         }
       }
     }
-    lo[i] = l;
-    hi[i] = h;
+    const size_t out = (size_t)v * mcount + (__float_as_uint(er.w) - base);  // the caller's meshlet order
+    lo[out] = l;
+    hi[out] = h;
   }
 }
 
