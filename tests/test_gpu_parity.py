@@ -109,6 +109,30 @@ def test_hzb_mips_bit_exact(ruins_small):
     assert np.array_equal(d2h(info["data"], len(mips), np.float32), mips)
 
 
+@pytest.mark.parametrize("shape", [(611, 997), (1, 7), (9, 1), (130, 64), (1080, 1920), (67, 129)])
+def test_hzb_mips_odd_sizes(ruins_small, shape):
+    """Edge clamping at every level: odd and tiny sizes through the host-copy, device and in-sequence builds."""
+    import torch
+    h = ruins_small
+    rng = np.random.default_rng(shape[0] * 7919 + shape[1])
+    img = rng.random(shape, dtype=np.float32)
+    mips = O.hzb_build(img)[0]
+    h.vg.build_hzb(9, img)
+    info = h.vg.hzb_info(9)
+    assert np.array_equal(d2h(info["data"], len(mips), np.float32), mips)
+    d = torch.from_numpy(img).cuda()
+    # an unaligned device pointer takes the scalar-load path
+    dd = torch.zeros(img.size + 1, dtype=torch.float32, device="cuda")
+    dd[1:] = d.flatten()
+    for ptr in (d.data_ptr(), dd.data_ptr() + 4):
+        engine.check(engine.lib().vgc_hzb_build(h.vg.handle, 10, ptr, img.shape[1], img.shape[0], 1, None))
+        assert np.array_equal(d2h(h.vg.hzb_info(10)["data"], len(mips), np.float32), mips)
+    cam = h.spec.cameras[0]
+    v = engine.make_view(cam, engine.ViewParams(error_threshold=1.0, hzb=11), depth=(d.data_ptr(), img.shape[1], img.shape[0]))
+    h.vg.cut([v], first_slot=0)
+    assert np.array_equal(d2h(h.vg.hzb_info(11)["data"], len(mips), np.float32), mips)
+
+
 def test_capacity_retry_rounds():
     """A draw list too small for the cut triggers the same-frame redo at a coarser threshold (GeometryPool.ts:1032)
     and the steer between frames; counters and controller state match the oracle round for round."""

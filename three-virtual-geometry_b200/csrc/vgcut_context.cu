@@ -527,7 +527,7 @@ int prepare(vgc_context *ctx, LaunchScratch &s, const vgc_view *views, uint32_t 
       changed = changed || c;
       s.hzb_w = std::max(s.hzb_w, v.depth_width);
       s.hzb_h = std::max(s.hzb_h, v.depth_height);
-      s.hzb_tail = s.hzb_tail || ctx->hzb[v.hzb].desc.levels > 6;
+      s.hzb_tail = s.hzb_tail || ctx->hzb[v.hzb].desc.levels > 7;  // levels 7+ by the tail kernel
     }
   }
   if (changed) {
@@ -1323,7 +1323,7 @@ extern "C" int vgc_cut_noalloc(vgc_context *ctx, const vgc_view *view, uint32_t 
   const HzbDesc *hzbs = (const HzbDesc *)ctx->d_hzb_desc.ptr;
   if (build_hzb) {
     const HzbDesc &d = ctx->hzb[view->hzb].desc;
-    CUDA_TRY(launch_hzb_views(d_view, 1, hzbs, d.w[0], d.h[0], d.levels > 6, st));
+    CUDA_TRY(launch_hzb_views(d_view, 1, hzbs, d.w[0], d.h[0], d.levels > 7, st));
   }
   CUDA_TRY(launch_reset(d_view, 1, ctx->counter_words, ctl, st));
   CUDA_TRY(launch_cells(S, d_view, 1, cells, units, ctl, st));

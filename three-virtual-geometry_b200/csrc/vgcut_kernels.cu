@@ -1051,90 +1051,108 @@ __global__ void __launch_bounds__(256) k_expand(Scene S, const ViewConst *__rest
 }
 
 // ------------------------------------------------------------------------------------------------ HZB
-// 32x32 tile of mip 0 per block; levels 1..5 of the tile are reduced in shared memory. Mip i texel (x, y) is the
-// max of texels (2x, 2y), (min(2x+1, w-1), 2y), ... of mip i-1: tile borders fall on even coordinates at every
-// level, so the clamped neighbour is always inside the tile.
-__global__ void __launch_bounds__(256) k_hzb_tiles(const float *__restrict__ depth, HzbDesc H, float *__restrict__ out,
-                                                   int copy_mip0) {
-  __shared__ float buf[2][32][33];
-  const uint32_t ox = blockIdx.x * 32, oy = blockIdx.y * 32;
+// Max-reduced mip chain (OcclusionCulling.ts:320-350): mip i texel (x, y) = max of mip i-1 texels (2x, 2y),
+// (min(2x+1, w-1), 2y), (2x, min(2y+1, h-1)), (min(2x+1, w-1), min(2y+1, h-1)), sizes halved rounding up. By
+// induction every texel of mip i is the max over its mip-0 footprint [2^i x, 2^i (x+1)) x [2^i y, 2^i (y+1)) inside
+// the image, so a reduction whose loads clamp to the image edge gives the same values.
+//
+// One 64x64 tile of mip 0 per block of 256 threads: each thread reduces a 4x4 patch (float4 rows when the image
+// allows) to its 2x2 texels of mip 1 and its texel of mip 2 in registers; mips 3..6 of the tile come from shared
+// memory (tiles are aligned to 64, so every clamped neighbour lies inside the tile); mips 7+ by the tail kernel.
+constexpr uint32_t kHzbTile = 64, kHzbTileLevels = 7;
+
+__device__ __forceinline__ void hzb_tile64(const float *__restrict__ depth, const HzbDesc &H, float *__restrict__ out,
+                                           bool copy_mip0, uint32_t ox, uint32_t oy, float (*sm)[16][17]) {
+  const uint32_t t = threadIdx.x, tx = t & 15u, ty = t >> 4;
   const uint32_t W = H.w[0], Hh = H.h[0];
-  for (uint32_t i = threadIdx.x; i < 1024; i += blockDim.x) {
-    const uint32_t lx = i & 31, ly = i >> 5, gx = ox + lx, gy = oy + ly;
-    float v = 0.0f;
-    if (gx < W && gy < Hh) {
-      v = depth[(size_t)gy * W + gx];
-      if (copy_mip0) out[H.off[0] + (size_t)gy * W + gx] = v;
+  const uint32_t gx = ox + 4 * tx, gy = oy + 4 * ty;
+  const bool vec = (W & 3u) == 0 && (reinterpret_cast<uintptr_t>(depth) & 15u) == 0 && gx + 3 < W;
+  float v[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const uint32_t y = min(gy + r, Hh - 1);
+    const float *row = depth + (size_t)y * W;
+    if (vec) {
+      const float4 q = __ldg(reinterpret_cast<const float4 *>(row + gx));
+      v[r][0] = q.x, v[r][1] = q.y, v[r][2] = q.z, v[r][3] = q.w;
+    } else {
+#pragma unroll
+      for (int c = 0; c < 4; c++) v[r][c] = __ldg(row + min(gx + c, W - 1));
     }
-    buf[0][ly][lx] = v;
   }
+  if (copy_mip0) {
+    float *o0 = out + H.off[0];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      if (gy + r >= Hh) continue;
+      float *row = o0 + (size_t)(gy + r) * W;
+      if (vec && (reinterpret_cast<uintptr_t>(o0) & 15u) == 0) {
+        *reinterpret_cast<float4 *>(row + gx) = make_float4(v[r][0], v[r][1], v[r][2], v[r][3]);
+      } else {
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+          if (gx + c < W) row[gx + c] = v[r][c];
+      }
+    }
+  }
+  float a[2][2];
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+      a[i][j] = fmaxf(fmaxf(v[2 * i][2 * j], v[2 * i][2 * j + 1]), fmaxf(v[2 * i + 1][2 * j], v[2 * i + 1][2 * j + 1]));
+  if (H.levels > 1) {
+    float *o1 = out + H.off[1];
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        const uint32_t x = gx / 2 + j, y = gy / 2 + i;
+        if (x < H.w[1] && y < H.h[1]) o1[(size_t)y * H.w[1] + x] = a[i][j];
+      }
+  }
+  const float b = fmaxf(fmaxf(a[0][0], a[0][1]), fmaxf(a[1][0], a[1][1]));
+  if (H.levels > 2 && gx / 4 < H.w[2] && gy / 4 < H.h[2]) out[H.off[2] + (size_t)(gy / 4) * H.w[2] + gx / 4] = b;
+  sm[0][ty][tx] = b;
   __syncthreads();
-  const uint32_t top = min(H.levels, 6u);
-  for (uint32_t l = 1; l < top; l++) {
-    const uint32_t s = 32u >> l;
+  const uint32_t top = min(H.levels, kHzbTileLevels);
+  for (uint32_t l = 3; l < top; l++) {
+    const uint32_t n = kHzbTile >> l;                     // tile texels per side at level l
     const uint32_t px = ox >> (l - 1), py = oy >> (l - 1);  // tile origin at level l-1
     const uint32_t qx = ox >> l, qy = oy >> l;              // tile origin at level l
-    const float(*src)[33] = buf[(l - 1) & 1];
-    float(*dst)[33] = buf[l & 1];
-    for (uint32_t i = threadIdx.x; i < s * s; i += blockDim.x) {
-      const uint32_t lx = i % s, ly = i / s, gx = qx + lx, gy = qy + ly;
-      if (gx < H.w[l] && gy < H.h[l]) {
-        const uint32_t x0 = 2 * gx, y0 = 2 * gy;
+    const float(*src)[17] = sm[(l - 1) & 1];
+    float(*dst)[17] = sm[l & 1];
+    if (t < n * n) {
+      const uint32_t lx = t % n, ly = t / n, x = qx + lx, y = qy + ly;
+      if (x < H.w[l] && y < H.h[l]) {
+        const uint32_t x0 = 2 * x, y0 = 2 * y;
         const uint32_t x1 = min(x0 + 1, H.w[l - 1] - 1), y1 = min(y0 + 1, H.h[l - 1] - 1);
-        const float a = fmaxf(src[y0 - py][x0 - px], src[y0 - py][x1 - px]);
-        const float b = fmaxf(src[y1 - py][x0 - px], src[y1 - py][x1 - px]);
-        const float v = fmaxf(a, b);
-        dst[ly][lx] = v;
-        out[H.off[l] + (size_t)gy * H.w[l] + gx] = v;
+        const float m = fmaxf(fmaxf(src[y0 - py][x0 - px], src[y0 - py][x1 - px]),
+                              fmaxf(src[y1 - py][x0 - px], src[y1 - py][x1 - px]));
+        dst[ly][lx] = m;
+        out[H.off[l] + (size_t)y * H.w[l] + x] = m;
       }
     }
     __syncthreads();
   }
 }
 
-// The HZB builds of a batch in two launches: grid.z = view, views without a depth image skip.
+__global__ void __launch_bounds__(256) k_hzb_tiles(const float *__restrict__ depth, HzbDesc H, float *__restrict__ out,
+                                                   int copy_mip0) {
+  __shared__ float sm[2][16][17];
+  hzb_tile64(depth, H, out, copy_mip0 != 0, blockIdx.x * kHzbTile, blockIdx.y * kHzbTile, sm);
+}
+
+// The HZB builds of a batch: grid.z = view, views without a depth image skip.
 __global__ void __launch_bounds__(256) k_hzb_tiles_views(const ViewConst *__restrict__ views,
                                                          const HzbDesc *__restrict__ hzbs) {
-  __shared__ float buf[2][32][33];
+  __shared__ float sm[2][16][17];
   const ViewConst &V = views[blockIdx.z];
   if (!V.build_hzb) return;
   const HzbDesc &H = hzbs[V.hzb];
-  const uint32_t ox = blockIdx.x * 32, oy = blockIdx.y * 32;
+  const uint32_t ox = blockIdx.x * kHzbTile, oy = blockIdx.y * kHzbTile;
   if (ox >= H.w[0] || oy >= H.h[0]) return;
-  float *out = const_cast<float *>(H.data);
-  const float *depth = V.depth;
-  const uint32_t W = H.w[0], Hh = H.h[0];
-  for (uint32_t i = threadIdx.x; i < 1024; i += blockDim.x) {
-    const uint32_t lx = i & 31, ly = i >> 5, gx = ox + lx, gy = oy + ly;
-    float v = 0.0f;
-    if (gx < W && gy < Hh) {
-      v = depth[(size_t)gy * W + gx];
-      out[H.off[0] + (size_t)gy * W + gx] = v;
-    }
-    buf[0][ly][lx] = v;
-  }
-  __syncthreads();
-  const uint32_t top = min(H.levels, 6u);
-  for (uint32_t l = 1; l < top; l++) {
-    const uint32_t s = 32u >> l;
-    const uint32_t px = ox >> (l - 1), py = oy >> (l - 1);
-    const uint32_t qx = ox >> l, qy = oy >> l;
-    const float(*src)[33] = buf[(l - 1) & 1];
-    float(*dst)[33] = buf[l & 1];
-    for (uint32_t i = threadIdx.x; i < s * s; i += blockDim.x) {
-      const uint32_t lx = i % s, ly = i / s, gx = qx + lx, gy = qy + ly;
-      if (gx < H.w[l] && gy < H.h[l]) {
-        const uint32_t x0 = 2 * gx, y0 = 2 * gy;
-        const uint32_t x1 = min(x0 + 1, H.w[l - 1] - 1), y1 = min(y0 + 1, H.h[l - 1] - 1);
-        const float a = fmaxf(src[y0 - py][x0 - px], src[y0 - py][x1 - px]);
-        const float b = fmaxf(src[y1 - py][x0 - px], src[y1 - py][x1 - px]);
-        const float v = fmaxf(a, b);
-        dst[ly][lx] = v;
-        out[H.off[l] + (size_t)gy * H.w[l] + gx] = v;
-      }
-    }
-    __syncthreads();
-  }
+  hzb_tile64(V.depth, H, const_cast<float *>(H.data), true, ox, oy, sm);
 }
 
 __global__ void __launch_bounds__(1024) k_hzb_tail_views(const ViewConst *__restrict__ views,
@@ -1143,7 +1161,7 @@ __global__ void __launch_bounds__(1024) k_hzb_tail_views(const ViewConst *__rest
   if (!V.build_hzb) return;
   const HzbDesc &H = hzbs[V.hzb];
   float *out = const_cast<float *>(H.data);
-  for (uint32_t l = 6; l < H.levels; l++) {
+  for (uint32_t l = kHzbTileLevels; l < H.levels; l++) {
     const float *src = out + H.off[l - 1];
     const uint32_t sw = H.w[l - 1], sh = H.h[l - 1];
     for (uint32_t i = threadIdx.x; i < H.w[l] * H.h[l]; i += blockDim.x) {
@@ -1157,9 +1175,9 @@ __global__ void __launch_bounds__(1024) k_hzb_tail_views(const ViewConst *__rest
   }
 }
 
-// Levels 6 and up (at most 60 x 34 texels for a 1080p mip 0) by one block.
+// Levels 7 and up (at most 15 x 9 texels for a 1080p mip 0) by one block.
 __global__ void __launch_bounds__(1024) k_hzb_tail(HzbDesc H, float *__restrict__ out) {
-  for (uint32_t l = 6; l < H.levels; l++) {
+  for (uint32_t l = kHzbTileLevels; l < H.levels; l++) {
     const float *src = out + H.off[l - 1];
     const uint32_t sw = H.w[l - 1], sh = H.h[l - 1];
     for (uint32_t i = threadIdx.x; i < H.w[l] * H.h[l]; i += blockDim.x) {
@@ -1304,17 +1322,17 @@ cudaError_t launch_expand(const Scene &S, const ViewConst *view, uint32_t cut, u
 }
 
 cudaError_t launch_hzb(const float *depth, const HzbDesc &H, float *out, int copy_mip0, cudaStream_t st) {
-  dim3 grid((H.w[0] + 31) / 32, (H.h[0] + 31) / 32);
+  dim3 grid((H.w[0] + kHzbTile - 1) / kHzbTile, (H.h[0] + kHzbTile - 1) / kHzbTile);
   k_hzb_tiles<<<grid, 256, 0, st>>>(depth, H, out, copy_mip0);
   cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess || H.levels <= 6) return e;
+  if (e != cudaSuccess || H.levels <= kHzbTileLevels) return e;
   k_hzb_tail<<<1, 1024, 0, st>>>(H, out);
   return cudaGetLastError();
 }
 
 cudaError_t launch_hzb_views(const ViewConst *views, uint32_t nviews, const HzbDesc *hzbs, uint32_t max_w,
                              uint32_t max_h, bool tail, cudaStream_t st) {
-  dim3 grid((max_w + 31) / 32, (max_h + 31) / 32, nviews);
+  dim3 grid((max_w + kHzbTile - 1) / kHzbTile, (max_h + kHzbTile - 1) / kHzbTile, nviews);
   k_hzb_tiles_views<<<grid, 256, 0, st>>>(views, hzbs);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || !tail) return e;
