@@ -93,7 +93,6 @@ struct vgc_context {
   std::vector<MeshRec> meshes;
   std::vector<LevelRec> levels;
   std::vector<float4> m_lod, m_parent, m_err, m_cull;
-  std::vector<float4> blocks;  // 4 per kBlock pool-consecutive meshlets
   std::vector<uint4> m_info;
   std::vector<uint32_t> m_tris;
   std::vector<float4> inst;
@@ -104,7 +103,6 @@ struct vgc_context {
   bool dirty = true;
   // device copies
   DevBuf d_meshes, d_levels, d_m_lod, d_m_parent, d_m_err, d_m_cull, d_m_info, d_m_tris, d_inst, d_inst_slot, d_cells;
-  DevBuf d_blocks;
   // output slots
   uint32_t out_slots = 0;
   uint32_t out_slot_capacity = 0;  // slot_capacity the output buffers were sized for
@@ -184,8 +182,8 @@ int upload(vgc_context *ctx, DevBuf &b, const std::vector<T> &v) {
 }
 
 // Local meshlet ids in test order: each level's meshlets sorted by parent error (ties by id), levels in place. The
-// meshlets of one DAG group share their parent error, so groups stay together, and a block of kBlock consecutive
-// meshlets spans a narrow error range: its LOD bounds then reject it whole wherever the band lies elsewhere.
+// meshlets of one DAG group share their parent error and parent sphere, so a group's meshlets are tested side by side
+// (their parent-sphere reads hit the same lines).
 void test_order(const vgc_mesh_data *d, std::vector<uint32_t> &order) {
   order.resize(d->meshlet_count);
   std::vector<std::pair<uint32_t, uint32_t>> keyed;
@@ -204,47 +202,6 @@ void test_order(const vgc_mesh_data *d, std::vector<uint32_t> &order) {
   }
 }
 
-// Sphere (centre stored as float, radius rounded up) enclosing the spheres s[0..n) exactly in double precision.
-float4 enclosing_sphere(const float4 *s, uint32_t n) {
-  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-  for (uint32_t i = 0; i < n; i++) {
-    const double c[3] = {s[i].x, s[i].y, s[i].z};
-    for (int a = 0; a < 3; a++) {
-      lo[a] = std::min(lo[a], c[a] - (double)s[i].w);
-      hi[a] = std::max(hi[a], c[a] + (double)s[i].w);
-    }
-  }
-  const float C[3] = {(float)(0.5 * (lo[0] + hi[0])), (float)(0.5 * (lo[1] + hi[1])), (float)(0.5 * (lo[2] + hi[2]))};
-  double R = 0;
-  for (uint32_t i = 0; i < n; i++) {
-    const double dx = (double)s[i].x - C[0], dy = (double)s[i].y - C[1], dz = (double)s[i].z - C[2];
-    R = std::max(R, std::sqrt(dx * dx + dy * dy + dz * dz) + (double)s[i].w);
-  }
-  float Rf = (float)R;
-  if ((double)Rf < R) Rf = std::nextafter(Rf, INFINITY);
-  return make_float4(C[0], C[1], C[2], Rf);
-}
-
-// Recomputes the bounds blocks that hold meshlets from `first_meshlet` on (a block may span two meshes: its bounds
-// then cover both, which stays conservative for each).
-void update_blocks(vgc_context *ctx, uint32_t first_meshlet) {
-  const uint32_t M = (uint32_t)ctx->m_lod.size();
-  const uint32_t nb = (M + kBlock - 1) / kBlock;
-  ctx->blocks.resize((size_t)nb * 4);
-  for (uint32_t b = first_meshlet / kBlock; b < nb; b++) {
-    const uint32_t f = b * kBlock, n = std::min(kBlock, M - f);
-    float e_own = INFINITY, e_par = 0;
-    for (uint32_t i = f; i < f + n; i++) {
-      e_own = std::min(e_own, ctx->m_err[i].x);
-      e_par = std::max(e_par, ctx->m_err[i].y);
-    }
-    ctx->blocks[(size_t)b * 4 + 0] = enclosing_sphere(&ctx->m_lod[f], n);
-    ctx->blocks[(size_t)b * 4 + 1] = enclosing_sphere(&ctx->m_parent[f], n);
-    ctx->blocks[(size_t)b * 4 + 2] = enclosing_sphere(&ctx->m_cull[f], n);
-    ctx->blocks[(size_t)b * 4 + 3] = make_float4(e_own, e_par, 0.0f, 0.0f);
-  }
-}
-
 int sync_scene(vgc_context *ctx) {
   if (!ctx->dirty) return VGC_OK;
   // buffers may be reallocated: no launch of any stream may still read the old ones
@@ -258,7 +215,6 @@ int sync_scene(vgc_context *ctx) {
   if ((rc = upload(ctx, ctx->d_m_cull, ctx->m_cull))) return rc;
   if ((rc = upload(ctx, ctx->d_m_info, ctx->m_info))) return rc;
   if ((rc = upload(ctx, ctx->d_m_tris, ctx->m_tris))) return rc;
-  if ((rc = upload(ctx, ctx->d_blocks, ctx->blocks))) return rc;
   if ((rc = upload(ctx, ctx->d_inst, ctx->inst))) return rc;
   if ((rc = upload(ctx, ctx->d_inst_slot, ctx->inst_slot))) return rc;
   if ((rc = upload(ctx, ctx->d_cells, ctx->cells))) return rc;
@@ -276,7 +232,6 @@ Scene scene_of(const vgc_context *ctx) {
   S.m_cull = (const float4 *)ctx->d_m_cull.ptr;
   S.m_info = (const uint4 *)ctx->d_m_info.ptr;
   S.m_tris = (const uint32_t *)ctx->d_m_tris.ptr;
-  S.blocks = (const float4 *)ctx->d_blocks.ptr;
   S.inst = (const float4 *)ctx->d_inst.ptr;
   S.inst_slot = (const uint32_t *)ctx->d_inst_slot.ptr;
   S.cells = (const CellRec *)ctx->d_cells.ptr;
@@ -761,7 +716,6 @@ int vgc_context_destroy(vgc_context *ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   free_scratch(ctx->scratch);
   for (DevBuf *b : {&ctx->d_meshes, &ctx->d_levels, &ctx->d_m_lod, &ctx->d_m_parent, &ctx->d_m_err, &ctx->d_m_cull,
-                    &ctx->d_blocks,
                     &ctx->d_m_info, &ctx->d_m_tris, &ctx->d_inst, &ctx->d_inst_slot, &ctx->d_cells, &ctx->d_counters,
                     &ctx->d_draw, &ctx->d_args, &ctx->d_dyn, &ctx->d_hist, &ctx->d_state, &ctx->d_hzb_desc})
     dev_free(ctx, *b);
@@ -826,8 +780,8 @@ int vgc_mesh_add(vgc_context *ctx, const vgc_mesh_data *d, const float *matrices
   m.cell_base = (uint32_t)ctx->cells.size();
   m.cell_count = (n + kCellSize - 1) / kCellSize;
   std::memcpy(m.sphere, d->bounding_sphere, sizeof m.sphere);
-  // Test order of the meshlets: within each level (levels stay the same contiguous ranges) by parent error, so each
-  // bounds block of kBlock consecutive meshlets has tight LOD bounds. The test columns
+  // Test order of the meshlets: within each level (levels stay the same contiguous ranges) by parent error. The test
+  // columns
   // (m_lod, m_parent, m_err, m_cull) follow the test order and m_err.w carries the meshlet's pool-global id, which is
   // what every output (draw list, selectCut) reports; m_info and the triangles stay in the caller's order.
   std::vector<uint32_t> order_of_test;
@@ -851,7 +805,6 @@ int vgc_mesh_add(vgc_context *ctx, const vgc_mesh_data *d, const float *matrices
     ctx->m_info.push_back(make_uint4(info[0], info[1] + m.triangle_base * 3, info[2], info[3]));
   }
   if (d->meshlet_triangles) ctx->m_tris.insert(ctx->m_tris.end(), d->meshlet_triangles, d->meshlet_triangles + d->meshlet_triangle_count);
-  update_blocks(ctx, m.meshlet_base);
   for (uint32_t l = 0; l < d->level_count; l++) {
     LevelRec L;
     L.first = d->level_ranges[l * 2] + m.meshlet_base;
@@ -1091,7 +1044,6 @@ int vgc_read_stats(vgc_context *ctx, uint32_t slot, vgc_stats *s, vgc_stream str
   s->fast_emitted = c[VGC_COUNTER_FAST_EMITTED];
   s->levels_read = c[VGC_COUNTER_LEVELS_READ];
   s->predicted_triangles = (uint64_t)c[VGC_COUNTER_PREDICTED_LO] | ((uint64_t)c[VGC_COUNTER_PREDICTED_HI] << 32);
-  s->meshlets_evaluated = c[VGC_COUNTER_MESHLETS_EVALUATED];
   float dyn = 0;
   CUDA_TRY(cudaMemcpy(&dyn, (const float *)ctx->d_dyn.ptr + (size_t)slot * 8, 4, cudaMemcpyDeviceToHost));
   s->effective_threshold = dyn;
@@ -1247,7 +1199,7 @@ namespace {
 constexpr size_t kNoAllocCtl = 0;                                   // 16 control words
 constexpr size_t kNoAllocView = 256;                                // one ViewConst
 constexpr uint32_t kNoAllocMaxUnits = 65536;                        // visible (view, cell) units: cells of the scene
-constexpr uint32_t kNoAllocMaxChunks = 65536;                       // queued meshlet chunks (beyond: tested in place)
+constexpr uint32_t kNoAllocMaxChunks = 65536;                       // meshlet work queue entries (beyond: tested in place)
 constexpr size_t kNoAllocUnits = 1024;
 constexpr size_t kNoAllocChunks = kNoAllocUnits + (size_t)kNoAllocMaxUnits * sizeof(uint2);
 constexpr size_t kNoAllocBytes = kNoAllocChunks + (size_t)kNoAllocMaxChunks * sizeof(uint4);  // 1.5 MiB

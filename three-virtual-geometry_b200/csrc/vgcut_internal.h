@@ -10,8 +10,6 @@
 //   m_cull      float4[M]  culling sphere         /
 //   m_info      uint4[M]   triangleCount, firstIndex (pool-global), lodLevel, vertexOffset
 //   m_tris      u32[]      packed local triangles (meshletTriangles), pool-global
-//   blocks      float4[4 * ceil(M / 32)]  conservative bounds of each 32 pool-consecutive meshlets: spheres enclosing
-//                          their LOD, parent-LOD and culling spheres, (min own error, max parent error, 0, 0)
 //   inst        float4[4 I] instance matrix columns, Morton order per mesh (GeometryPool.ts:484-497)
 //   inst_slot   u32[I]     mesh slot of each instance
 //   cells       CellRec[C] 128 consecutive instances of one mesh (GeometryPool.ts:519-545)
@@ -32,7 +30,6 @@ constexpr uint32_t kLocalVertexBits = 7;   // ceil(log2(MAX_MESHLET_VERTICES = 1
 constexpr uint32_t kMaxHzbLevels = 16;
 constexpr uint32_t kStateWords = 8;        // S_SCALE 0..1, S_FILL 2..3, S_RETRY 4..5
 constexpr uint32_t kBudgetBins = 256;
-constexpr uint32_t kBlock = 32;            // meshlets per bounds block (one warp step)
 
 struct MeshRec {  // 80 bytes
   float4 sphere;
@@ -61,7 +58,6 @@ struct Scene {
   const float4 *m_lod, *m_parent, *m_err, *m_cull;
   const uint4 *m_info;
   const uint32_t *m_tris;
-  const float4 *blocks;  // 4 per block of kBlock meshlets: own sphere, parent sphere, cull sphere, errors
   const float4 *inst;
   const uint32_t *inst_slot;
   const CellRec *cells;

@@ -232,9 +232,28 @@ __global__ void __launch_bounds__(256) k_cells(Scene S, const ViewConst *__restr
 
 // ------------------------------------------------------------------------------------------------ k_instances
 constexpr int kWarpStage = 96;   // staged draw entries per warp and cut (a step adds <= 32)
-constexpr uint32_t kChunk = 256;  // meshlets per chunk (one warp in k_chunks)
-static_assert(kChunk % kBlock == 0 && kChunk / kBlock + 1 <= 32, "a chunk's blocks are tested one per lane");
-constexpr uint32_t kBlockTestMin = 128;  // chunks of at least this many meshlets test their blocks' bounds first
+constexpr uint32_t kChunk = 512;  // meshlets per chunk (one warp in k_chunks)
+
+// The meshlet work queue between k_instances and k_chunks, in one buffer of `capacity` uint4: spans (one item's
+// meshlets inside one kChunk window of its warp's items laid end to end) and chunks (the <= 32 spans of one
+// window: one (view, cell, cut)). ctl[4..5] is the 64-bit reservation counter: spans low, chunks high.
+struct WorkQueue {
+  uint4 *spans, *chunks;
+  uint32_t span_cap, chunk_cap;
+};
+
+__device__ __forceinline__ WorkQueue work_queue(uint4 *buf, uint32_t capacity) {
+  WorkQueue q;
+  q.chunk_cap = capacity / 4;
+  q.span_cap = capacity - q.chunk_cap;
+  q.spans = buf;
+  q.chunks = buf + q.span_cap;
+  return q;
+}
+
+__device__ __forceinline__ unsigned long long *queue_counter(uint32_t *ctl) {
+  return reinterpret_cast<unsigned long long *>(ctl + 4);
+}
 
 // Band values of a view for the current round, written by k_reset and by the capacity check (dyn[1..5]).
 struct ViewBands {
@@ -376,111 +395,6 @@ __device__ __forceinline__ bool test_meshlet(const Scene &S, const ViewConst &V,
   return true;
 }
 
-// ---- Bounds blocks: kBlock pool-consecutive meshlets with spheres enclosing their LOD, parent-LOD and culling
-// spheres and the extreme errors. block_may_pass is false only when no meshlet of the block can pass the LOD band
-// (own <= high && parent > low) or the frustum test in the float arithmetic test_meshlet uses, so skipping such a
-// block never changes a decision:
-//  * |VM (c_m - C)| <= sigma |c_m - C| <= sigma (R - r_m), sigma = sqrt(max row sum of |VM3^T VM3|) bounding the
-//    spectral norm of the instance's linear part (= the largest axis scale for rotation x scale matrices);
-//  * so every meshlet distance max(|VM c_m| - r_m s, near) lies in [D - sigma R, D + sigma R] around the block's D;
-//  * proj_error's rounding is monotone in the error and the distance, so the bound's float result orders the same
-//    way as each meshlet's, and `slack` (1e-5 of the magnitudes involved, hundreds of float ulps) absorbs the
-//    rounding of the transforms, lengths and plane dot products on both sides.
-struct BlockFrame {
-  float sigma, tmag;  // spectral-norm bound of VM's 3x3 part; length of VM's translation
-};
-
-__device__ __forceinline__ BlockFrame block_frame(const float *VM) {
-  float g[3][3];
-#pragma unroll
-  for (int i = 0; i < 3; i++)
-#pragma unroll
-    for (int j = 0; j < 3; j++) g[i][j] = (VM[i] * VM[j] + VM[4 + i] * VM[4 + j]) + VM[8 + i] * VM[8 + j];
-  float row = 0.0f;
-#pragma unroll
-  for (int i = 0; i < 3; i++) row = fmx(row, (fabsf(g[i][0]) + fabsf(g[i][1])) + fabsf(g[i][2]));
-  BlockFrame f;
-  f.sigma = sqrtf(row) * 1.00001f;
-  const float t[3] = {VM[3], VM[7], VM[11]};
-  f.tmag = len3(t);
-  return f;
-}
-
-__device__ __forceinline__ bool block_may_pass(const Scene &S, const ViewConst &V, const float *VM, const BlockFrame &F,
-                                               uint32_t block, float low, float high, bool test_frustum, bool swept) {
-  const float scale = VM[12];
-  const float4 *B = S.blocks + (size_t)block * 4;
-  const float4 bo = __ldg(B), bp = __ldg(B + 1), be = __ldg(B + 3);
-  float c[3];
-  // own error: every meshlet's >= err_min * s / (D + sigma R) * P
-  xform(VM, bo.x, bo.y, bo.z, c);
-  float d = len3(c);
-  float cm[3] = {bo.x, bo.y, bo.z};
-  float slack = 1e-5f * ((d + F.tmag) + F.sigma * (len3(cm) + bo.w));
-  const float own_lo = ((be.x * scale) / fmx((d + F.sigma * bo.w) + slack, V.near_)) * V.proj_scale;
-  if (own_lo > high) return false;
-  // parent error: every meshlet's <= err_max * s / max(D - sigma R, near) * P (roots: 1e30, always above low)
-  if (be.y < float(1e30 * 0.5)) {
-    xform(VM, bp.x, bp.y, bp.z, c);
-    d = len3(c);
-    cm[0] = bp.x, cm[1] = bp.y, cm[2] = bp.z;
-    slack = 1e-5f * ((d + F.tmag) + F.sigma * (len3(cm) + bp.w));
-    const float par_hi = ((be.y * scale) / fmx((d - F.sigma * bp.w) - slack, V.near_)) * V.proj_scale;
-    if (!(par_hi > low)) return false;
-  }
-  if (test_frustum) {  // a plane with the whole enclosing culling sphere behind it
-    const float4 bc = __ldg(B + 2);
-    xform(VM, bc.x, bc.y, bc.z, c);
-    d = len3(c);
-    cm[0] = bc.x, cm[1] = bc.y, cm[2] = bc.z;
-    const float reach = F.sigma * bc.w;
-    const float base = (d + F.tmag) + F.sigma * (len3(cm) + bc.w);
-#pragma unroll
-    for (int p = 0; p < 6; p++) {
-      float dp = ((V.plane[p * 4] * c[0] + V.plane[p * 4 + 1] * c[1]) + V.plane[p * 4 + 2] * c[2]) + V.plane[p * 4 + 3];
-      float sw = swept ? V.sweep[p] : 0.0f;
-      dp = dp + sw;
-      const float sl = 1e-5f * ((base + fabsf(V.plane[p * 4 + 3])) + sw);
-      if (dp < -(reach + sl)) return false;
-    }
-  }
-  return true;
-}
-
-// Meshlets of one chunk that passed the LOD band, waiting for the rest of their test with all 32 lanes busy
-// (about a third of the tested meshlets pass; testing them in place would leave most lanes idle).
-struct LodQueue {
-  uint32_t pos[64];
-  float own[64], parent[64];
-};
-
-// The rest of test_meshlet for queue entries [0, n): fade steps, culling sphere against the frustum, HZB.
-__device__ __forceinline__ void drain_queue(const Scene &S, const ViewConst &V, const HzbDesc *hzbs, LodQueue &q,
-                                            uint32_t n, WarpStage &ws, WarpCount &wc, float low, float fs, float high0,
-                                            uint32_t cut, bool occl_on, bool inside, const float *VM, uint32_t slot,
-                                            uint32_t instance) {
-  const uint32_t lane = threadIdx.x & 31;
-  bool drawn = false;
-  uint32_t packed = 0, id = 0;
-  if (lane < n) {
-    const uint32_t pos = q.pos[lane];
-    const float own = q.own[lane], parent = q.parent[lane];
-    const uint32_t lo = fs > 0.0f ? fade_step(own, low, fs) : 0u;
-    const uint32_t hi = fs > 0.0f ? fade_step(parent, low, fs) : 255u;
-    if (hi > lo) {
-      const float4 er = __ldg(S.m_err + pos), cs = __ldg(S.m_cull + pos);
-      id = __float_as_uint(er.w);
-      packed = __float_as_uint(er.z) | (lo << 8) | (hi << 16);
-      float c[3];
-      xform(VM, cs.x, cs.y, cs.z, c);
-      const float r = cs.w * VM[12];
-      drawn = !(V.frustum && !inside && !(frustum(V, c, cut == 1) >= -r)) &&
-              !(cut == 0 && occluded(V, hzbs, high0, occl_on, c, r));
-    }
-  }
-  warp_stage(ws, wc, V, S.slot_capacity, slot, cut, drawn, instance, id, packed);
-}
-
 struct LevelRange {
   uint32_t first, last, possible, guaranteed;
 };
@@ -593,7 +507,6 @@ __device__ void warp_item(const Scene &S, const ViewConst &V, const HzbDesc *hzb
                           uint32_t cut, bool occl_on, bool inside, const float *VM, uint32_t instance, uint32_t first,
                           uint32_t count) {
   const ViewBands b = bands_of(V);
-  if ((threadIdx.x & 31) == 0) atomicAdd(V.counters + VGC_COUNTER_MESHLETS_EVALUATED, count);
   if (HIST) {
     const float s = get_state(V.state, 0);
     for (uint32_t base = 0; base < count; base += 32) {
@@ -618,6 +531,69 @@ __device__ void warp_item(const Scene &S, const ViewConst &V, const HzbDesc *hzb
   warp_flush(ws, wc, V, S.slot_capacity, slot, cut);
 }
 
+// Meshlets of one chunk that passed the LOD band (HIST: that enter the cut somewhere in the threshold range),
+// waiting for the rest of their test with all 32 lanes busy: about a third of the tested meshlets pass, and testing
+// them in place would leave most lanes idle.
+struct LodQueue {
+  uint32_t pos[64], span[64];
+  float own[64], parent[64];  // HIST: the bins b_own, b_par as integers
+};
+
+// Per warp: the view-model matrix of each span's instance (rows 0..2, scale), its instance and inside flag.
+struct SpanFrame {
+  float4 vm[32][4];  // [3] = (VM[12] scale, instance as bits, inside as bits, 0)
+};
+
+__device__ __forceinline__ void frame_vm(const SpanFrame &F, uint32_t j, float *VM, uint32_t &instance, bool &inside) {
+  const float4 a = F.vm[j][0], b = F.vm[j][1], c = F.vm[j][2], d = F.vm[j][3];
+  VM[0] = a.x, VM[1] = a.y, VM[2] = a.z, VM[3] = a.w;
+  VM[4] = b.x, VM[5] = b.y, VM[6] = b.z, VM[7] = b.w;
+  VM[8] = c.x, VM[9] = c.y, VM[10] = c.z, VM[11] = c.w;
+  VM[12] = d.x;
+  instance = __float_as_uint(d.y);
+  inside = __float_as_uint(d.z) != 0;
+}
+
+// The rest of the meshlet test for queue entries [0, n): fade steps, culling sphere against the frustum, HZB; then
+// staging (draw list) or the histogram (HIST).
+template <bool HIST>
+__device__ __forceinline__ void drain_queue(const Scene &S, const ViewConst &V, const HzbDesc *hzbs, const LodQueue &q,
+                                            const SpanFrame &F, uint32_t n, WarpStage &ws, WarpCount &wc, float low,
+                                            float fs, float high0, uint32_t cut, bool occl_on, uint32_t slot) {
+  const uint32_t lane = threadIdx.x & 31;
+  bool drawn = false;
+  uint32_t packed = 0, id = 0, instance = 0, lo = 0, hi = 255;
+  if (lane < n) {
+    const uint32_t pos = q.pos[lane];
+    float VM[13];
+    bool inside;
+    frame_vm(F, q.span[lane], VM, instance, inside);
+    if (HIST) {
+      lo = __float_as_uint(q.own[lane]);
+      hi = __float_as_uint(q.parent[lane]);
+    } else if (fs > 0.0f) {
+      lo = fade_step(q.own[lane], low, fs);
+      hi = fade_step(q.parent[lane], low, fs);
+    }
+    if (HIST || hi > lo) {
+      const float4 er = __ldg(S.m_err + pos), cs = __ldg(S.m_cull + pos);
+      id = __float_as_uint(er.w);
+      packed = HIST ? __float_as_uint(er.z) : (__float_as_uint(er.z) | (lo << 8) | (hi << 16));
+      float c[3];
+      xform(VM, cs.x, cs.y, cs.z, c);
+      const float r = cs.w * VM[12];
+      drawn = !(V.frustum && !inside && !(frustum(V, c, cut == 1) >= -r)) &&
+              !(cut == 0 && occluded(V, hzbs, high0, occl_on, c, r));
+    }
+  }
+  if (HIST) {
+    warp_hist_add(V.hist, drawn, lo, packed);
+    warp_hist_add(V.hist + kBudgetBins, drawn, hi, packed);
+  } else {
+    warp_stage(ws, wc, V, S.slot_capacity, slot, cut, drawn, instance, id, packed);
+  }
+}
+
 // One warp per 32 instances of a visible (view, cell) unit: the instance pass of GeometryPool.ts:846-913. Fast-path
 // instances emit their meshlets; the others hand their level range to k_chunks as chunks of <= kChunk meshlets.
 // HIST: the budget search's pass (views with a triangleBudget only): the camera cut's level range over the whole
@@ -625,8 +601,8 @@ __device__ void warp_item(const Scene &S, const ViewConst &V, const HzbDesc *hzb
 template <bool HIST>
 __global__ void __launch_bounds__(128) k_instances(Scene S, const ViewConst *__restrict__ views,
                                                    const HzbDesc *__restrict__ hzbs, const uint2 *__restrict__ units,
-                                                   uint32_t *__restrict__ ctl, uint4 *__restrict__ chunks,
-                                                   uint32_t chunk_capacity, int round) {
+                                                   uint32_t *__restrict__ ctl, uint4 *__restrict__ queue,
+                                                   uint32_t capacity, int round) {
   __shared__ WarpStage stage[4];
   WarpStage &ws = stage[threadIdx.x >> 5];
   if (round > 0 && ctl[round] == 0) return;  // no view redoes a cut in this round
@@ -728,148 +704,181 @@ __global__ void __launch_bounds__(128) k_instances(Scene S, const ViewConst *__r
     emit_fast(S, V, cell.slot, 0, fast0 ? r0.possible : 0u, r0.first, instance);
     emit_fast(S, V, cell.slot, 1, fast1 ? r1.possible : 0u, r1.first, instance);
     }
-    // items -> chunks of <= kChunk meshlets (each touches <= kChunk / kBlock + 1 bounds blocks)
-    const uint32_t c0 = item0 ? (r0.last - r0.first + kChunk - 1) / kChunk : 0u;
-    const uint32_t c1 = item1 ? (r1.last - r1.first + kChunk - 1) / kChunk : 0u;
-    const uint32_t incl = warp_scan_incl(c0 + c1);
-    const uint32_t want = __shfl_sync(0xffffffffu, incl, 31);
-    if (!want) continue;
-    uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(&ctl[3], want);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    // slots below the capacity are written (k_chunks reads exactly those); chunks past it are tested here
-    const uint32_t at0 = base + incl - (c0 + c1);
-    // tag: instance local (bits 0-6), cut (7), occlusion (8), inside the frustum (9), meshlet count (16-31)
-    const uint32_t tag0 = il | (occl_on ? 1u << 8 : 0u) | (inside0 ? 1u << 9 : 0u);
-    const uint32_t tag1 = il | (1u << 7) | (inside1 ? 1u << 9 : 0u);
-    for (uint32_t k = 0; k < c0 + c1; k++) {
-      if (at0 + k >= chunk_capacity) break;
-      const uint32_t cut = k < c0 ? 0u : 1u, kk = k < c0 ? k : k - c0;
-      const uint32_t first = (cut ? r1.first : r0.first) + kk * kChunk;
-      const uint32_t cnt = min(kChunk, (cut ? r1.last - r1.first : r0.last - r0.first) - kk * kChunk);
-      chunks[at0 + k] = make_uint4(unit.x, unit.y, (cut ? tag1 : tag0) | (cnt << 16), first);
-    }
-    uint32_t over = __ballot_sync(0xffffffffu, at0 + c0 + c1 > chunk_capacity);
-    while (over) {
-      const uint32_t j = __ffs(over) - 1;
-      over &= over - 1;
-      float vmj[13];
+    // items -> spans -> chunks: per cut, the warp's items laid end to end in lane order and cut into kChunk windows;
+    // a window's spans (<= 32, one per item) form one chunk of one (view, cell, cut)
+    const uint32_t n0 = item0 ? r0.last - r0.first : 0u, n1 = item1 ? r1.last - r1.first : 0u;
+    const uint32_t s0 = warp_scan_incl(n0) - n0, s1 = warp_scan_incl(n1) - n1;  // starts in the laid-out items
+    const uint32_t T0 = __shfl_sync(0xffffffffu, s0 + n0, 31), T1 = __shfl_sync(0xffffffffu, s1 + n1, 31);
+    if (T0 + T1 == 0) continue;
+    const uint32_t p0 = n0 ? (s0 + n0 - 1) / kChunk - s0 / kChunk + 1 : 0u;  // spans of this lane's item
+    const uint32_t p1 = n1 ? (s1 + n1 - 1) / kChunk - s1 / kChunk + 1 : 0u;
+    const uint32_t q0 = warp_scan_incl(p0) - p0, q1 = warp_scan_incl(p1) - p1;
+    const uint32_t P0 = __shfl_sync(0xffffffffu, q0 + p0, 31), P1 = __shfl_sync(0xffffffffu, q1 + p1, 31);
+    const uint32_t N0 = (T0 + kChunk - 1) / kChunk, N1 = (T1 + kChunk - 1) / kChunk;
+    unsigned long long got = 0;
+    if (lane == 0)
+      got = atomicAdd(queue_counter(ctl), ((unsigned long long)(N0 + N1) << 32) | (unsigned long long)(P0 + P1));
+    got = __shfl_sync(0xffffffffu, got, 0);
+    const uint32_t span_at = uint32_t(got), chunk_at = uint32_t(got >> 32);
+    const WorkQueue Q = work_queue(queue, capacity);
+    if (span_at + P0 + P1 <= Q.span_cap && chunk_at + N0 + N1 <= Q.chunk_cap) {
 #pragma unroll
-      for (int i = 0; i < 13; i++) vmj[i] = __shfl_sync(0xffffffffu, VM[i], j);
-      const uint32_t jc0 = __shfl_sync(0xffffffffu, c0, j), jn = jc0 + __shfl_sync(0xffffffffu, c1, j);
-      const uint32_t jat = __shfl_sync(0xffffffffu, at0, j);
-      const bool jin0 = __shfl_sync(0xffffffffu, inside0 ? 1 : 0, j) != 0, jin1 = __shfl_sync(0xffffffffu, inside1 ? 1 : 0, j) != 0;
-      const uint32_t f0 = __shfl_sync(0xffffffffu, r0.first, j), e0 = __shfl_sync(0xffffffffu, r0.last, j);
-      const uint32_t f1 = __shfl_sync(0xffffffffu, r1.first, j), e1 = __shfl_sync(0xffffffffu, r1.last, j);
-      for (uint32_t k = 0; k < jn; k++) {
-        if (jat + k < chunk_capacity) continue;
-        const uint32_t cut = k < jc0 ? 0u : 1u, kk = k < jc0 ? k : k - jc0;
-        const uint32_t first = (cut ? f1 : f0) + kk * kChunk;
-        const uint32_t cnt = min(kChunk, (cut ? e1 - f1 : e0 - f0) - kk * kChunk);
-        warp_item<HIST>(S, V, hzbs, ws, cell.slot, cut, cut == 0 && occl_on, cut ? jin1 : jin0, vmj,
-                        cell.first + ((w & 3u) << 5) + j, first, cnt);
+      for (uint32_t cut = 0; cut < 2; cut++) {
+        const uint32_t n = cut ? n1 : n0, st = cut ? s1 : s0, np = cut ? p1 : p0;
+        const uint32_t first = cut ? r1.first : r0.first;
+        const uint32_t flags = il | ((cut ? inside1 : inside0) ? 1u << 7 : 0u);
+        uint4 *dst = Q.spans + span_at + (cut ? P0 + q1 : q0);
+        for (uint32_t k = 0; k < np; k++) {
+          const uint32_t win = st / kChunk + k;
+          const uint32_t lo = max(st, win * kChunk), hi = min(st + n, (win + 1) * kChunk);
+          dst[k] = make_uint4(flags, first + (lo - st), hi - lo, 0u);
+        }
+        // chunk t starts at the span holding laid-out position t * kChunk: that of the last item starting at or
+        // before it, plus the windows that item crossed before t
+        const uint32_t N = cut ? N1 : N0;
+        for (uint32_t t = 0; t < N; t++) {
+          const uint32_t X = t * kChunk;
+          const uint32_t owner = 31 - __clz(__ballot_sync(0xffffffffu, st <= X));
+          const uint32_t first_span = __shfl_sync(0xffffffffu, cut ? q1 : q0, owner) + t -
+                                      __shfl_sync(0xffffffffu, st, owner) / kChunk;
+          const uint32_t spans = __popc(__ballot_sync(0xffffffffu, n > 0 && st < X + kChunk && st + n > X));
+          if (lane == 0)
+            Q.chunks[chunk_at + (cut ? N0 : 0u) + t] =
+                make_uint4(unit.x, unit.y, cut | ((cut == 0 && occl_on) ? 2u : 0u) | (spans << 8),
+                           span_at + (cut ? P0 : 0u) + first_span);
+        }
+      }
+    } else {
+      // the queue is full: chunk slots reserved below its capacity become empty records, the items are tested here
+      for (uint32_t t = lane; t < N0 + N1; t += 32)
+        if (chunk_at + t < Q.chunk_cap) Q.chunks[chunk_at + t] = make_uint4(0u, 0u, 0u, 0u);
+      uint32_t over = __ballot_sync(0xffffffffu, n0 + n1 > 0);
+      while (over) {
+        const uint32_t j = __ffs(over) - 1;
+        over &= over - 1;
+        float vmj[13];
+#pragma unroll
+        for (int i = 0; i < 13; i++) vmj[i] = __shfl_sync(0xffffffffu, VM[i], j);
+        const bool jin0 = __shfl_sync(0xffffffffu, inside0 ? 1 : 0, j) != 0;
+        const bool jin1 = __shfl_sync(0xffffffffu, inside1 ? 1 : 0, j) != 0;
+        const uint32_t f0 = __shfl_sync(0xffffffffu, r0.first, j), c0 = __shfl_sync(0xffffffffu, n0, j);
+        const uint32_t f1 = __shfl_sync(0xffffffffu, r1.first, j), c1 = __shfl_sync(0xffffffffu, n1, j);
+        const uint32_t inst = cell.first + ((w & 3u) << 5) + j;
+        if (c0) warp_item<HIST>(S, V, hzbs, ws, cell.slot, 0, occl_on, jin0, vmj, inst, f0, c0);
+        if (c1) warp_item<HIST>(S, V, hzbs, ws, cell.slot, 1, false, jin1, vmj, inst, f1, c1);
       }
     }
   }
 }
 
 // ------------------------------------------------------------------------------------------------ k_chunks
-// The meshlet pass (GeometryPool.ts:916-970) over the chunks k_instances queued, one chunk (<= kChunk meshlets of
-// one instance and cut) per warp: every lane derives the view-model matrix itself, so warps never wait on each other.
+// The meshlet pass (GeometryPool.ts:916-970) over the chunks k_instances queued, one chunk per warp: the chunk's
+// spans (instances of one cell) get their view-model matrices once, in parallel, into shared memory; then the lanes
+// walk the chunk's meshlets end to end, 32 per step whatever span they belong to. The LOD band comes first; the
+// meshlets that pass queue up and finish 32 at a time (drain_queue). One draw-list flush per chunk.
 // HIST: the budget histogram of the chunks the budget pass queued.
 template <bool HIST>
 __global__ void __launch_bounds__(128) k_chunks(Scene S, const ViewConst *__restrict__ views,
-                                                const HzbDesc *__restrict__ hzbs, const uint4 *__restrict__ chunks,
-                                                uint32_t *__restrict__ ctl, uint32_t chunk_capacity, int round) {
+                                                const HzbDesc *__restrict__ hzbs, uint4 *__restrict__ queue,
+                                                uint32_t *__restrict__ ctl, uint32_t capacity, int round) {
   __shared__ WarpStage stage[4];
   __shared__ LodQueue queues[4];
+  __shared__ SpanFrame frames[4];
   WarpStage &ws = stage[threadIdx.x >> 5];
   LodQueue &q = queues[threadIdx.x >> 5];
+  SpanFrame &F = frames[threadIdx.x >> 5];
   if (round > 0 && ctl[round] == 0) return;  // no view redoes a cut in this round
-  const uint32_t n_chunks = min(ctl[3], chunk_capacity);
+  const WorkQueue Q = work_queue(queue, capacity);
+  const uint32_t n_chunks = min(uint32_t(*queue_counter(ctl) >> 32), Q.chunk_cap);
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31;
   for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < n_chunks; c += warps) {
-    const uint4 ch = chunks[c];
+    const uint4 ch = Q.chunks[c];
+    const uint32_t ns = ch.z >> 8;
+    if (ns == 0) continue;
     const ViewConst &V = views[ch.x];
     const CellRec cell = S.cells[ch.y];
-    const uint32_t il = ch.z & 0x7fu, cut = (ch.z >> 7) & 1u, count = ch.z >> 16;
-    const bool occl_on = ((ch.z >> 8) & 1u) != 0, inside = ((ch.z >> 9) & 1u) != 0;
-    const uint32_t instance = cell.first + il;
+    const uint32_t cut = ch.z & 1u;
+    const bool occl_on = (ch.z & 2u) != 0;
     const ViewBands b = bands_of(V);
     const float low = cut ? b.low1 : b.low0, high = cut ? b.high1 : b.high0;
-    float VM[13];
-    model_view(V.V, S.inst + (size_t)instance * 4, VM, VM[12]);
-    // bounds blocks the chunk touches (<= kChunk / kBlock + 1): one lane each tests the block's conservative bounds
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t b0 = ch.w / kBlock, nb = (ch.w + count - 1) / kBlock - b0 + 1;
     const float sc = HIST ? get_state(V.state, 0) : 0.0f;
-    uint32_t live = nb >= 32 ? 0xffffffffu : (1u << nb) - 1u;
-    if (count >= kBlockTestMin) {  // the block test costs about one meshlet step: worth it on long chunks only
-      const BlockFrame F = block_frame(VM);
-      const float blo = HIST ? budget_e(V, sc, 0) : low, bhi = HIST ? budget_e(V, sc, kBudgetBins - 1) : high;
-      const bool may = lane < nb && block_may_pass(S, V, VM, F, b0 + lane, blo, bhi, V.frustum && !inside, cut == 1);
-      live = __ballot_sync(0xffffffffu, may);
+    // spans: one lane each
+    uint32_t sp_first = 0, sp_count = 0;
+    if (lane < ns) {
+      const uint4 sp = Q.spans[ch.w + lane];
+      sp_first = sp.y;
+      sp_count = sp.z;
+      const uint32_t instance = cell.first + (sp.x & 127u);
+      float VM[13];
+      model_view(V.V, S.inst + (size_t)instance * 4, VM, VM[12]);
+      F.vm[lane][0] = make_float4(VM[0], VM[1], VM[2], VM[3]);
+      F.vm[lane][1] = make_float4(VM[4], VM[5], VM[6], VM[7]);
+      F.vm[lane][2] = make_float4(VM[8], VM[9], VM[10], VM[11]);
+      F.vm[lane][3] = make_float4(VM[12], __uint_as_float(instance), __uint_as_float((sp.x >> 7) & 1u), 0.0f);
     }
-    if (lane == 0) {  // meshlets of the chunk that run the per-meshlet test
-      uint32_t n = 0;
-      for (uint32_t k = 0; k < nb; k++)
-        if ((live >> k) & 1u) n += min(ch.w + count, (b0 + k + 1) * kBlock) - max(ch.w, (b0 + k) * kBlock);
-      if (n) atomicAdd(V.counters + VGC_COUNTER_MESHLETS_EVALUATED, n);
-    }
-    if (HIST) {
-      while (live) {
-        const uint32_t k = __ffs(live) - 1;
-        live &= live - 1;
-        const uint32_t m = (b0 + k) * kBlock + lane;
-        uint32_t bo = 0, bp = 0, tris = 0;
-        const bool add = m >= ch.w && m < ch.w + count &&
-                         hist_meshlet(S, V, hzbs, sc, b.high0, occl_on, inside, VM, m, bo, bp, tris);
-        warp_hist_add(V.hist, add, bo, tris);
-        warp_hist_add(V.hist + kBudgetBins, add, bp, tris);
-      }
-      continue;
-    }
-    // LOD band first on every meshlet of the live blocks; the survivors queue up and finish 32 at a time
+    const uint32_t sp_off = warp_scan_incl(sp_count) - sp_count;
+    const uint32_t total = __shfl_sync(0xffffffffu, sp_off + sp_count, 31);
+    __syncwarp();
     WarpCount wc{0, 0, 0};
     uint32_t qn = 0;  // warp-uniform
-    const float scale = VM[12];
-    while (live) {
-      const uint32_t k = __ffs(live) - 1;
-      live &= live - 1;
-      const uint32_t m = (b0 + k) * kBlock + lane;
+    for (uint32_t base = 0; base < total; base += 32) {
+      const uint32_t p = base + lane;
+      // span of position p: the last span starting at or before it (spans are non-empty, in order)
+      uint32_t j = 0;
+#pragma unroll
+      for (uint32_t k = 16; k > 0; k >>= 1) {
+        const uint32_t o = __shfl_sync(0xffffffffu, sp_off, min(j + k, 31u));
+        if (j + k < ns && o <= p) j += k;
+      }
+      const uint32_t m = __shfl_sync(0xffffffffu, sp_first, j) + (p - __shfl_sync(0xffffffffu, sp_off, j));
       bool pass = false;
       float own = 0.0f, parent = 0.0f;
-      if (m >= ch.w && m < ch.w + count) {
+      if (p < total) {
+        float VM[13];
+        uint32_t inst;
+        bool inside;
+        frame_vm(F, j, VM, inst, inside);
         const float4 ls = __ldg(S.m_lod + m), ps = __ldg(S.m_parent + m);
         const float2 er = __ldg(reinterpret_cast<const float2 *>(S.m_err + m));
-        own = proj_error(V, VM, scale, ls, er.x);
-        parent = proj_error(V, VM, scale, ps, er.y);
-        pass = own <= high && parent > low;
+        own = proj_error(V, VM, VM[12], ls, er.x);
+        parent = proj_error(V, VM, VM[12], ps, er.y);
+        if (HIST) {
+          const uint32_t bo = budget_bin(V, sc, own), bp = budget_bin(V, sc, parent);
+          pass = bo < bp;
+          own = __uint_as_float(bo);
+          parent = __uint_as_float(bp);
+        } else {
+          pass = own <= high && parent > low;
+        }
       }
       const uint32_t mask = __ballot_sync(0xffffffffu, pass);
       if (pass) {
         const uint32_t at = qn + __popc(mask & ((1u << lane) - 1u));
         q.pos[at] = m;
+        q.span[at] = j;
         q.own[at] = own;
         q.parent[at] = parent;
       }
       qn += __popc(mask);
       __syncwarp();
       if (qn >= 32) {
-        drain_queue(S, V, hzbs, q, 32, ws, wc, low, b.fade_scale, b.high0, cut, occl_on, inside, VM, cell.slot, instance);
+        drain_queue<HIST>(S, V, hzbs, q, F, 32, ws, wc, low, b.fade_scale, b.high0, cut, occl_on, cell.slot);
         qn -= 32;
         __syncwarp();
         if (lane < qn) {
           q.pos[lane] = q.pos[32 + lane];
+          q.span[lane] = q.span[32 + lane];
           q.own[lane] = q.own[32 + lane];
           q.parent[lane] = q.parent[32 + lane];
         }
         __syncwarp();
       }
     }
-    if (qn) drain_queue(S, V, hzbs, q, qn, ws, wc, low, b.fade_scale, b.high0, cut, occl_on, inside, VM, cell.slot, instance);
+    if (qn) drain_queue<HIST>(S, V, hzbs, q, F, qn, ws, wc, low, b.fade_scale, b.high0, cut, occl_on, cell.slot);
     __syncwarp();
-    warp_flush(ws, wc, V, S.slot_capacity, cell.slot, cut);
+    if (!HIST) warp_flush(ws, wc, V, S.slot_capacity, cell.slot, cut);
+    __syncwarp();  // the frame and queue are rewritten by the next chunk
   }
 }
 
@@ -879,7 +888,7 @@ __global__ void __launch_bounds__(128) k_chunks(Scene S, const ViewConst *__rest
 // frame's first selection round.
 __global__ void __launch_bounds__(128) k_budget(const ViewConst *__restrict__ views, uint32_t nviews,
                                                 uint32_t *__restrict__ ctl) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) ctl[3] = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *queue_counter(ctl) = 0;
   const uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t lane = threadIdx.x & 31;
   if (v >= nviews) return;
@@ -929,7 +938,7 @@ __global__ void __launch_bounds__(128) k_finish(const ViewConst *__restrict__ vi
                                                 int round) {
   const uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t lane = threadIdx.x & 31;
-  if (blockIdx.x == 0 && threadIdx.x == 0) ctl[3] = 0;  // chunk queue of the next round starts empty
+  if (blockIdx.x == 0 && threadIdx.x == 0) *queue_counter(ctl) = 0;  // the next round's work queue starts empty
   if (v >= nviews) return;
   const ViewConst &V = views[v];
   uint32_t *ctr = V.counters;
@@ -1284,21 +1293,21 @@ cudaError_t configure_select(int *instances_per_sm, int *chunks_per_sm) {
 }
 
 cudaError_t launch_instances(const Scene &S, const ViewConst *views, const HzbDesc *hzbs, const uint2 *units,
-                             uint32_t *ctl, uint4 *chunks, uint32_t chunk_capacity, int round, uint32_t grid,
+                             uint32_t *ctl, uint4 *queue, uint32_t capacity, int round, uint32_t grid,
                              cudaStream_t st) {
   if (round < 0)  // the budget search's pass
-    k_instances<true><<<grid, 128, 0, st>>>(S, views, hzbs, units, ctl, chunks, chunk_capacity, 0);
+    k_instances<true><<<grid, 128, 0, st>>>(S, views, hzbs, units, ctl, queue, capacity, 0);
   else
-    k_instances<false><<<grid, 128, 0, st>>>(S, views, hzbs, units, ctl, chunks, chunk_capacity, round);
+    k_instances<false><<<grid, 128, 0, st>>>(S, views, hzbs, units, ctl, queue, capacity, round);
   return cudaGetLastError();
 }
 
-cudaError_t launch_chunks(const Scene &S, const ViewConst *views, const HzbDesc *hzbs, const uint4 *chunks,
-                          uint32_t *ctl, uint32_t chunk_capacity, int round, uint32_t grid, cudaStream_t st) {
+cudaError_t launch_chunks(const Scene &S, const ViewConst *views, const HzbDesc *hzbs, uint4 *queue,
+                          uint32_t *ctl, uint32_t capacity, int round, uint32_t grid, cudaStream_t st) {
   if (round < 0)
-    k_chunks<true><<<grid, 128, 0, st>>>(S, views, hzbs, chunks, ctl, chunk_capacity, 0);
+    k_chunks<true><<<grid, 128, 0, st>>>(S, views, hzbs, queue, ctl, capacity, 0);
   else
-    k_chunks<false><<<grid, 128, 0, st>>>(S, views, hzbs, chunks, ctl, chunk_capacity, round);
+    k_chunks<false><<<grid, 128, 0, st>>>(S, views, hzbs, queue, ctl, capacity, round);
   return cudaGetLastError();
 }
 
