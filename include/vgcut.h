@@ -74,6 +74,13 @@ typedef struct vgc_mesh_opts {
   uint32_t occlusion;       /* occlusion culling may remove this mesh's instances and meshlets */
 } vgc_mesh_opts;
 
+/* vgc_view.flags */
+enum {
+  VGC_VIEW_FRESH_STATE = 1 /* the capacity controller starts this cut from its initial state (threshold scale 1, no
+                              fill history) instead of the state slot's contents; the slot then holds this cut's
+                              state as usual */
+};
+
 /* One cut request: the uniforms VirtualGeometry.update() writes (VirtualGeometry.ts:414-442) and the levers
    (:78-183). Matrices are column-major like three.js Matrix4.elements. */
 typedef struct vgc_view {
@@ -92,7 +99,7 @@ typedef struct vgc_view {
   uint32_t frustum_culling;     /* frustumCulling */
   int32_t hzb;                  /* HZB slot for occlusion culling of the camera cut; -1 = off */
   uint32_t state_slot;          /* capacity-controller state carried between frames of one camera */
-  uint32_t flags;               /* reserved, 0 */
+  uint32_t flags;               /* VGC_VIEW_* bits */
   /* Optional occluder depth of this frame (device memory, NDC depth, row 0 at the top): when set with hzb >= 0,
      the cut first builds HZB slot `hzb` from it in the same launch sequence, as the reference prepends its HZB
      kernels to the frame's compute submission (VirtualGeometry.ts:482-484). NULL: use the slot as built. */
@@ -201,6 +208,52 @@ int vgc_cut_noalloc(vgc_context *ctx, const vgc_view *view, uint32_t slot, vgc_s
 int vgc_batch_create(vgc_context *ctx, uint32_t max_views, vgc_batch **out);
 int vgc_batch_run(vgc_batch *batch, const vgc_view *views, uint32_t count, uint32_t first_slot, vgc_stream stream);
 int vgc_batch_destroy(vgc_batch *batch);
+
+/* ---------------------------------------------------------------- serving (no counterpart in the reference) */
+/* A request loop over several resident scenes (one context each). The reference cuts once per rendered frame of
+   one camera; a server takes cut requests (scene, view) from any thread as they arrive. One worker thread admits a
+   request while an output slot of its scene is free and the output-slot bytes of the admitted, unreleased requests
+   stay within the HBM budget; it batches admitted requests of one scene into one launch sequence and keeps up to
+   `streams` batches in flight, so requests that arrive while others run start as soon as a stream and slots free
+   up (continuous batching). Each request runs as vgc_cut of its view alone would with VGC_VIEW_FRESH_STATE, its
+   output slot doubling as its state slot: the result is the same alone and in any mix. While a server runs, its
+   contexts take no other cut or scene change; completed requests' outputs are read with vgc_get_output /
+   vgc_read_draw_list on (scene context, result.slot) until vgc_server_release. */
+typedef struct vgc_server vgc_server;
+typedef struct {
+  uint32_t streams;          /* batches in flight at once (default 2) */
+  uint32_t max_batch;        /* views per launch (default 64) */
+  uint32_t slots_per_scene;  /* output slots reserved per scene (default streams * max_batch) */
+  uint64_t hbm_budget_bytes; /* admission limit on the output-slot bytes of admitted, unreleased requests (0: none) */
+  uint32_t linger_us;        /* a batch smaller than max_batch waits up to this long for more requests (default 0) */
+} vgc_server_options;
+typedef struct {
+  uint64_t ticket;
+  uint32_t scene, slot;       /* scene index and the output slot holding the result */
+  int32_t status;             /* VGC_OK, or the error of the launch that carried it */
+  uint32_t batch_views;       /* views in that launch */
+  double submit_us, start_us, done_us; /* host steady clock, microseconds: submitted, launched, seen complete */
+  float batch_gpu_ms;         /* device time of that launch (CUDA events on its stream) */
+  vgc_stats stats;            /* its counters, copied back with the launch */
+} vgc_serve_result;
+typedef struct {
+  uint64_t submitted, completed, batches, views_launched;
+  uint64_t bytes_in_use, max_bytes_in_use; /* admitted output-slot bytes now / at most */
+  uint32_t max_in_flight;                 /* most batches in flight at once */
+} vgc_server_stats;
+void vgc_server_default_options(vgc_server_options *opts);
+int vgc_server_create(vgc_context *const *scenes, uint32_t scene_count, const vgc_server_options *opts,
+                      vgc_server **out);
+/* Thread-safe. `view` is copied; its state_slot and VGC_VIEW_FRESH_STATE are set by the server. */
+int vgc_server_submit(vgc_server *server, uint32_t scene, const vgc_view *view, uint64_t *ticket);
+/* Waits up to timeout_ms for the request; VGC_TIMEOUT if it has not completed. */
+int vgc_server_wait(vgc_server *server, uint64_t ticket, uint32_t timeout_ms, vgc_serve_result *out);
+/* Frees the request's output slot (and its HBM share) for later requests; its outputs are no longer valid. */
+int vgc_server_release(vgc_server *server, uint64_t ticket);
+/* Waits until every submitted request has completed (VGC_TIMEOUT after timeout_ms). */
+int vgc_server_drain(vgc_server *server, uint32_t timeout_ms);
+int vgc_server_stats_get(vgc_server *server, vgc_server_stats *out);
+int vgc_server_destroy(vgc_server *server);
 
 /* Layout of HZB slot `hzb`: levels, per-level offset (floats) / width / height (16 entries each), and the device
    pointer of the mip chain (level i at data + offset[i], row-major). */

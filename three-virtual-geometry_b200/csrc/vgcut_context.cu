@@ -15,131 +15,49 @@
 #include <string>
 #include <vector>
 
-#include "vgcut.h"
-#include "vgcut_internal.h"
+#include "vgcut_host.h"
 #include "vgcut_kernels.h"
 
-using namespace vgc;
-
+namespace vgch {
 namespace {
 thread_local std::string g_error;
+}  // namespace
 
 int fail(int code, const std::string &msg) {
   g_error = msg;
   return code;
 }
 
-#define CUDA_TRY(expr)                                                                              \
-  do {                                                                                              \
-    cudaError_t _e = (expr);                                                                        \
-    if (_e != cudaSuccess) return fail(VGC_DEVICE_ERROR, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
-  } while (0)
+void decode_stats(const vgc_context *ctx, const uint32_t *c, float threshold, vgc_stats *s) {
+  std::memset(s, 0, sizeof *s);
+  s->visible_cells = c[VGC_COUNTER_CELLS];
+  s->occluded_instances = c[VGC_COUNTER_OCCLUDED];
+  for (int cut = 0; cut < 2; cut++) {
+    const uint32_t *k = c + VGC_COUNTER_CUT0 + cut * 5;
+    s->selected[cut] = k[VGC_CUT_SELECTED];
+    s->drawn[cut] = k[VGC_CUT_DRAWN];
+    s->survived[cut] = k[VGC_CUT_SURVIVED];
+    s->work[cut] = k[VGC_CUT_WORK];
+    s->requested_indices[cut] = k[VGC_CUT_REQUESTED];
+    const uint32_t cap = cut == 0 ? ctx->opts.max_triangles * 3 : ctx->opts.max_shadow_triangles * 3;
+    if (k[VGC_CUT_SELECTED] > ctx->opts.max_meshlets || k[VGC_CUT_REQUESTED] > cap) s->overflow = 1;
+  }
+  s->rounds = c[VGC_COUNTER_ROUNDS];
+  s->instances_tested = c[VGC_COUNTER_INSTANCES_TESTED];
+  s->meshlets_tested = c[VGC_COUNTER_MESHLETS_TESTED];
+  s->fast_emitted = c[VGC_COUNTER_FAST_EMITTED];
+  s->levels_read = c[VGC_COUNTER_LEVELS_READ];
+  s->predicted_triangles = (uint64_t)c[VGC_COUNTER_PREDICTED_LO] | ((uint64_t)c[VGC_COUNTER_PREDICTED_HI] << 32);
+  s->effective_threshold = threshold;
+}
 
-constexpr double kNoDrawDistance = 1e30;  // GeometryPool.ts:111
-
-struct DevBuf {
-  void *ptr = nullptr;
-  size_t bytes = 0;
-};
-
-struct MeshHost {
-  bool used = false;
-  uint32_t meshlet_base = 0, meshlet_count = 0;
-  uint32_t level_base = 0, level_count = 0;
-  uint32_t triangle_base = 0, triangle_count = 0;
-  uint32_t instance_base = 0, instance_count = 0;
-  uint32_t cell_base = 0, cell_count = 0;
-  float sphere[4];
-};
-
-struct HzbSlot {
-  DevBuf data;
-  HzbDesc desc{};
-  bool valid = false;
-};
-
-uint32_t pad32(uint32_t x) { return (x + 31u) & ~31u; }
-
-}  // namespace
-
-// Launch scratch: view constants and the (view, cell) unit list of one launch sequence.
-struct LaunchScratch {
-  uint32_t hzb_w = 0, hzb_h = 0;  // largest depth image the views of this launch build an HZB from (0: none)
-  bool hzb_tail = false;
-  bool any_budget = false;        // a view of this launch searches its threshold for a triangleBudget
-  ViewConst *h_views = nullptr;  // pinned
-  ViewConst *d_views = nullptr;
-  uint2 *d_units = nullptr;
-  uint32_t *d_unit_count = nullptr;  // control words (see launch_reset)
-  uint4 *d_chunks = nullptr;
-  uint32_t chunk_capacity = 0;
-  uint32_t view_capacity = 0;
-  size_t unit_capacity = 0;
-  cudaEvent_t done = nullptr;
-  bool pending = false;
-};
-
-struct vgc_context {
-  vgc_options opts{};
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  int sm_count = 0;
-  uint32_t select_grid = 0;  // persistent grid of k_instances
-  uint32_t chunk_grid = 0;   // persistent grid of k_chunks
-  uint64_t bytes = 0;
-  std::mutex mu;
-  // host mirrors of the resident scene
-  std::vector<MeshHost> mesh_host;
-  std::vector<MeshRec> meshes;
-  std::vector<LevelRec> levels;
-  std::vector<float4> m_lod, m_parent, m_err, m_cull;
-  std::vector<uint4> m_info;
-  std::vector<uint32_t> m_tris;
-  std::vector<float4> inst;
-  std::vector<uint32_t> inst_slot;
-  std::vector<CellRec> cells;
-  uint32_t slot_capacity = 64;
-  uint32_t slots_used = 0;
-  bool dirty = true;
-  // device copies
-  DevBuf d_meshes, d_levels, d_m_lod, d_m_parent, d_m_err, d_m_cull, d_m_info, d_m_tris, d_inst, d_inst_slot, d_cells;
-  // output slots
-  uint32_t out_slots = 0;
-  uint32_t out_slot_capacity = 0;  // slot_capacity the output buffers were sized for
-  uint32_t counter_words = 0;
-  DevBuf d_counters, d_draw, d_args, d_dyn, d_hist;
-  // controller state slots
-  DevBuf d_state;
-  uint32_t state_slots = 0;
-  // HZB slots
-  std::vector<HzbSlot> hzb;
-  DevBuf d_hzb_desc;
-  static constexpr uint32_t kHzbSlots = 256;
-  LaunchScratch scratch;
-  // profiling: events around plain-path launches, resolved lazily
-  bool profiling = false;
-  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_pending;
-  std::vector<cudaEvent_t> prof_free;
-  double prof_ms[VGC_KERNEL_KINDS] = {0};
-  uint32_t prof_count[VGC_KERNEL_KINDS] = {0};
-};
-
-struct vgc_batch {
-  vgc_context *ctx = nullptr;
-  uint32_t max_views = 0;
-  LaunchScratch scratch;
-  cudaStream_t capture_stream = nullptr;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  uint32_t graph_views = 0;
-  uint32_t graph_cells = 0;
-  uint32_t graph_slots = 0;
-  uint32_t graph_hzb_w = 0, graph_hzb_h = 0;
-  bool graph_hzb_tail = false;
-  bool graph_budget = false;
-};
+}  // namespace vgch
 
 namespace {
+constexpr double kNoDrawDistance = 1e30;  // GeometryPool.ts:111
+}  // namespace
+
+namespace vgch {
 
 int dev_alloc(vgc_context *ctx, DevBuf &b, size_t bytes) {
   if (b.bytes >= bytes && b.ptr) return VGC_OK;
@@ -263,6 +181,12 @@ int ensure_outputs(vgc_context *ctx, uint32_t slots) {
   return VGC_OK;
 }
 
+size_t output_slot_bytes(const vgc_context *ctx) {
+  const size_t words = VGC_COUNTER_HEADER + (size_t)ctx->slot_capacity * 8;
+  return words * 4 + 2 * (size_t)ctx->opts.max_meshlets * 16 + 2 * (size_t)ctx->slot_capacity * 2 * 5 * 4 + 8 * 4 +
+         2 * kBudgetBins * 8 + kStateWords * 4;
+}
+
 int ensure_state(vgc_context *ctx, uint32_t slot) {
   if (slot < ctx->state_slots) return VGC_OK;
   uint32_t n = std::max<uint32_t>(slot + 1, ctx->state_slots * 2);
@@ -310,8 +234,9 @@ int ensure_scratch(vgc_context *ctx, LaunchScratch &s, uint32_t views, size_t un
     s.unit_capacity = n;
   }
   if (!s.d_unit_count) CUDA_TRY(cudaMalloc(&s.d_unit_count, 64));
-  // chunk queue: every instance with a level range queues ceil(range / 256) chunks per cut. Sized for 64k chunks
-  // per view; a warp that cannot reserve tests its meshlets itself, so a full queue costs time, not correctness.
+  // meshlet work queue: about one span per instance with a level range and cut, one chunk per 512 meshlets of a
+  // warp's items. Sized for 64k entries per view; a warp that cannot reserve tests its items itself, so a full
+  // queue costs time, not correctness.
   const uint32_t want_chunks = std::max<uint32_t>(65536, views * 65536u);
   if (want_chunks > s.chunk_capacity) {
     if (s.d_chunks) {
@@ -444,6 +369,7 @@ int view_constants(vgc_context *ctx, const vgc_view &in, uint32_t out_slot, uint
   k.occl_active = in.hzb >= 0 ? 1u : 0u;
   k.hzb = in.hzb;
   k.build_hzb = (in.hzb >= 0 && in.depth) ? 1u : 0u;
+  k.fresh_state = (in.flags & VGC_VIEW_FRESH_STATE) ? 1u : 0u;
   k.depth = in.depth;
   k.unit_offset = unit_offset;
   k.max_drawn = ctx->opts.max_meshlets;
@@ -459,11 +385,17 @@ int view_constants(vgc_context *ctx, const vgc_view &in, uint32_t out_slot, uint
 }
 
 // Prepares scene, outputs and the views' constants in `s.h_views` (pinned).
-int prepare(vgc_context *ctx, LaunchScratch &s, const vgc_view *views, uint32_t count, uint32_t first_slot) {
+int prepare(vgc_context *ctx, LaunchScratch &s, const vgc_view *views, uint32_t count, uint32_t first_slot,
+            const uint32_t *slots) {
   if (!views || count == 0) return fail(VGC_INVALID_ARG, "no views");
   int rc = sync_scene(ctx);
   if (rc) return rc;
-  if ((rc = ensure_outputs(ctx, first_slot + count))) return rc;
+  uint32_t slot_end = first_slot + count;
+  if (slots) {
+    slot_end = 0;
+    for (uint32_t i = 0; i < count; i++) slot_end = std::max(slot_end, slots[i] + 1);
+  }
+  if ((rc = ensure_outputs(ctx, slot_end))) return rc;
   const uint32_t cells = pad32((uint32_t)ctx->cells.size());
   if ((rc = ensure_scratch(ctx, s, count, (size_t)count * cells))) return rc;
   if (s.pending) CUDA_TRY(cudaEventSynchronize(s.done));
@@ -491,7 +423,7 @@ int prepare(vgc_context *ctx, LaunchScratch &s, const vgc_view *views, uint32_t 
     CUDA_TRY(cudaMemcpy(ctx->d_hzb_desc.ptr, all.data(), sizeof(HzbDesc) * all.size(), cudaMemcpyHostToDevice));
   }
   for (uint32_t i = 0; i < count; i++)
-    if ((rc = view_constants(ctx, views[i], first_slot + i, i * cells, s.h_views[i]))) return rc;
+    if ((rc = view_constants(ctx, views[i], slots ? slots[i] : first_slot + i, i * cells, s.h_views[i]))) return rc;
   return VGC_OK;
 }
 
@@ -645,7 +577,7 @@ void write_flags(vgc_context *ctx, uint32_t slot, const vgc_mesh_opts *o) {
   r.occlusion = o ? (o->occlusion ? 1u : 0u) : 0u;
 }
 
-}  // namespace
+}  // namespace vgch
 
 extern "C" {
 
@@ -1025,28 +957,9 @@ int vgc_read_stats(vgc_context *ctx, uint32_t slot, vgc_stats *s, vgc_stream str
   CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   uint32_t c[VGC_COUNTER_HEADER];
   CUDA_TRY(cudaMemcpy(c, (const uint32_t *)ctx->d_counters.ptr + (size_t)slot * ctx->counter_words, sizeof c, cudaMemcpyDeviceToHost));
-  std::memset(s, 0, sizeof *s);
-  s->visible_cells = c[VGC_COUNTER_CELLS];
-  s->occluded_instances = c[VGC_COUNTER_OCCLUDED];
-  for (int cut = 0; cut < 2; cut++) {
-    const uint32_t *k = c + VGC_COUNTER_CUT0 + cut * 5;
-    s->selected[cut] = k[VGC_CUT_SELECTED];
-    s->drawn[cut] = k[VGC_CUT_DRAWN];
-    s->survived[cut] = k[VGC_CUT_SURVIVED];
-    s->work[cut] = k[VGC_CUT_WORK];
-    s->requested_indices[cut] = k[VGC_CUT_REQUESTED];
-    const uint32_t cap = cut == 0 ? ctx->opts.max_triangles * 3 : ctx->opts.max_shadow_triangles * 3;
-    if (k[VGC_CUT_SELECTED] > ctx->opts.max_meshlets || k[VGC_CUT_REQUESTED] > cap) s->overflow = 1;
-  }
-  s->rounds = c[VGC_COUNTER_ROUNDS];
-  s->instances_tested = c[VGC_COUNTER_INSTANCES_TESTED];
-  s->meshlets_tested = c[VGC_COUNTER_MESHLETS_TESTED];
-  s->fast_emitted = c[VGC_COUNTER_FAST_EMITTED];
-  s->levels_read = c[VGC_COUNTER_LEVELS_READ];
-  s->predicted_triangles = (uint64_t)c[VGC_COUNTER_PREDICTED_LO] | ((uint64_t)c[VGC_COUNTER_PREDICTED_HI] << 32);
   float dyn = 0;
   CUDA_TRY(cudaMemcpy(&dyn, (const float *)ctx->d_dyn.ptr + (size_t)slot * 8, 4, cudaMemcpyDeviceToHost));
-  s->effective_threshold = dyn;
+  decode_stats(ctx, c, dyn, s);
   return VGC_OK;
 }
 

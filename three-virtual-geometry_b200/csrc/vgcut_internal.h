@@ -84,6 +84,7 @@ struct ViewConst {
   uint32_t index_capacity[2];
   int32_t hzb;          // HZB slot or -1
   uint32_t build_hzb;   // 1: build HZB slot `hzb` from `depth` before the cut
+  uint32_t fresh_state; // 1: k_reset puts the controller state back to its initial words first
   const float *depth;   // occluder depth of this frame (build_hzb)
   uint32_t *counters;   // VGC_COUNTER_* header, then per (cut, slot, part): count, start
   uint32_t *state;      // kStateWords, carried between frames

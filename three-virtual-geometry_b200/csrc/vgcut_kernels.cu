@@ -1263,14 +1263,36 @@ __global__ void __launch_bounds__(256) k_reset(const ViewConst *__restrict__ vie
   for (uint32_t v = blockIdx.x; v < nviews; v += gridDim.x) {
     uint32_t *c = views[v].counters;
     for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) c[i] = 0;
-    if (threadIdx.x == 0)  // budget views: the search's pass uses the band at the top of the threshold range
+    if (threadIdx.x == 0) {
+      if (views[v].fresh_state) {  // initial controller state: scales 1.0 (fixed point x10000), no fill, no retry
+        uint32_t *st = views[v].state;
+        for (uint32_t i = 0; i < kStateWords; i++) st[i] = i < 2 ? 10000u : 0u;
+      }
+      // budget views: the search's pass uses the band at the top of the threshold range
       store_bands(views[v], views[v].budget > 0.0f ? views[v].budget_hi : views[v].error_threshold);
+    }
     if (views[v].budget > 0.0f)
       for (uint32_t i = threadIdx.x; i < 2 * kBudgetBins; i += blockDim.x) views[v].hist[i] = 0;
   }
 }
 
+// Each view's counter header and the threshold its cut used, 32 words per view, for one device-to-host copy.
+__global__ void __launch_bounds__(32) k_gather_stats(const ViewConst *__restrict__ views, uint32_t nviews,
+                                                     uint32_t *__restrict__ out) {
+  const uint32_t v = blockIdx.x, t = threadIdx.x;
+  if (v >= nviews) return;
+  uint32_t w = 0;
+  if (t < VGC_COUNTER_HEADER) w = views[v].counters[t];
+  else if (t == VGC_COUNTER_HEADER) w = __float_as_uint(views[v].dyn[0]);
+  out[v * 32 + t] = w;
+}
+
 // ------------------------------------------------------------------------------------------------ launchers
+cudaError_t launch_gather_stats(const ViewConst *views, uint32_t nviews, uint32_t *out, cudaStream_t st) {
+  k_gather_stats<<<nviews, 32, 0, st>>>(views, nviews, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_reset(const ViewConst *views, uint32_t nviews, uint32_t words, uint32_t *ctl, cudaStream_t st) {
   const uint32_t blocks = nviews < 1024 ? (nviews ? nviews : 1) : 1024;
   k_reset<<<blocks, 256, 0, st>>>(views, nviews, words, ctl);

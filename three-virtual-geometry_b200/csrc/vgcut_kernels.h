@@ -22,6 +22,8 @@ cudaError_t launch_instances(const Scene &S, const ViewConst *views, const HzbDe
 // The meshlet work queue (spans and chunks) lives in `queue`, `capacity` uint4 entries; ctl[4..5] counts it.
 cudaError_t launch_chunks(const Scene &S, const ViewConst *views, const HzbDesc *hzbs, uint4 *queue,
                           uint32_t *ctl, uint32_t capacity, int round, uint32_t grid, cudaStream_t st);
+// 32 words per view: the VGC_COUNTER_HEADER counter words, then the threshold the cut used (float bits).
+cudaError_t launch_gather_stats(const ViewConst *views, uint32_t nviews, uint32_t *out, cudaStream_t st);
 cudaError_t launch_finish(const ViewConst *views, uint32_t nviews, uint32_t slot_capacity, uint32_t slots_used,
                           uint32_t *ctl, int round, cudaStream_t st);
 cudaError_t launch_expand(const Scene &S, const ViewConst *view, uint32_t cut, uint32_t *out, uint64_t capacity,

@@ -60,6 +60,17 @@ class View(C.Structure):
                 ("depth_height", C.c_uint32)]
 
 
+class ServerOptions(C.Structure):
+    _fields_ = [("streams", C.c_uint32), ("max_batch", C.c_uint32), ("slots_per_scene", C.c_uint32),
+                ("hbm_budget_bytes", C.c_uint64), ("linger_us", C.c_uint32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("batches", C.c_uint64),
+                ("views_launched", C.c_uint64), ("bytes_in_use", C.c_uint64), ("max_bytes_in_use", C.c_uint64),
+                ("max_in_flight", C.c_uint32)]
+
+
 class Output(C.Structure):
     _fields_ = [("draw_list", C.c_void_p * 2), ("draw_args", C.c_void_p), ("counters", C.c_void_p),
                 ("max_drawn", C.c_uint32), ("mesh_slots", C.c_uint32)]
@@ -79,6 +90,12 @@ class Stats(C.Structure):
             v = getattr(self, name)
             out[name] = list(v) if hasattr(v, "__len__") else v
         return out
+
+
+class ServeResult(C.Structure):
+    _fields_ = [("ticket", C.c_uint64), ("scene", C.c_uint32), ("slot", C.c_uint32), ("status", C.c_int32),
+                ("batch_views", C.c_uint32), ("submit_us", C.c_double), ("start_us", C.c_double),
+                ("done_us", C.c_double), ("batch_gpu_ms", C.c_float), ("stats", Stats)]
 
 
 _configured = False
@@ -120,6 +137,14 @@ def lib() -> C.CDLL:
         "vgc_set_profiling": ([vp, C.c_int], C.c_int),
         "vgc_kernel_times": ([vp, P(C.c_double), P(C.c_uint32), C.c_int], C.c_int),
         "vgc_debug_scene": ([vp, P(C.c_float), C.c_uint32, P(C.c_float), C.c_uint32, P(C.c_uint32), P(C.c_uint32)], C.c_int),
+        "vgc_server_default_options": ([P(ServerOptions)], None),
+        "vgc_server_create": ([P(vp), C.c_uint32, P(ServerOptions), P(vp)], C.c_int),
+        "vgc_server_submit": ([vp, C.c_uint32, P(View), P(C.c_uint64)], C.c_int),
+        "vgc_server_wait": ([vp, C.c_uint64, C.c_uint32, P(ServeResult)], C.c_int),
+        "vgc_server_release": ([vp, C.c_uint64], C.c_int),
+        "vgc_server_drain": ([vp, C.c_uint32], C.c_int),
+        "vgc_server_stats_get": ([vp, P(ServerStats)], C.c_int),
+        "vgc_server_destroy": ([vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -179,6 +204,10 @@ class ViewParams:
     frustum_culling: bool = True
     hzb: int = -1
     state_slot: int = 0
+    fresh_state: bool = False  # VGC_VIEW_FRESH_STATE: the capacity controller starts from its initial state
+
+
+VGC_VIEW_FRESH_STATE = 1
 
 
 def make_view(camera: Camera, p: ViewParams | None = None, depth=None) -> View:
@@ -203,7 +232,7 @@ def make_view(camera: Camera, p: ViewParams | None = None, depth=None) -> View:
     v.frustum_culling = 1 if p.frustum_culling else 0
     v.hzb = p.hzb
     v.state_slot = p.state_slot
-    v.flags = 0
+    v.flags = VGC_VIEW_FRESH_STATE if p.fresh_state else 0
     if depth is not None:
         v.depth, v.depth_width, v.depth_height = depth
     return v
@@ -427,3 +456,48 @@ class VirtualGeometry:
             self.dispose()
         except Exception:
             pass
+
+
+class Server:
+    """The serving loop over several resident scenes (vgc_server_* in include/vgcut.h): requests (scene index, view)
+    are submitted from any thread, admitted by free output slots and HBM budget, batched per scene and run on
+    `streams` CUDA streams with continuous batching. Results stay in the scene's output slot until released."""
+
+    def __init__(self, scenes: list, streams: int = 2, max_batch: int = 64, slots_per_scene: int = 0,
+                 hbm_budget_bytes: int = 0, linger_us: int = 0):
+        self.scenes = list(scenes)
+        o = ServerOptions()
+        lib().vgc_server_default_options(C.byref(o))
+        o.streams, o.max_batch, o.slots_per_scene = streams, max_batch, slots_per_scene
+        o.hbm_budget_bytes, o.linger_us = hbm_budget_bytes, linger_us
+        arr = (C.c_void_p * len(self.scenes))(*[vg.handle for vg in self.scenes])
+        self.handle = C.c_void_p()
+        check(lib().vgc_server_create(arr, len(self.scenes), C.byref(o), C.byref(self.handle)))
+
+    def submit(self, scene: int, view: View) -> int:
+        t = C.c_uint64()
+        check(lib().vgc_server_submit(self.handle, scene, C.byref(view), C.byref(t)))
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = 60_000) -> dict:
+        r = ServeResult()
+        check(lib().vgc_server_wait(self.handle, ticket, timeout_ms, C.byref(r)))
+        out = {k: getattr(r, k) for k, _ in ServeResult._fields_ if k != "stats"}
+        out["stats"] = r.stats.as_dict()
+        return out
+
+    def release(self, ticket: int) -> None:
+        check(lib().vgc_server_release(self.handle, ticket))
+
+    def drain(self, timeout_ms: int = 60_000) -> None:
+        check(lib().vgc_server_drain(self.handle, timeout_ms))
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        check(lib().vgc_server_stats_get(self.handle, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in ServerStats._fields_}
+
+    def close(self) -> None:
+        if self.handle:
+            lib().vgc_server_destroy(self.handle)
+            self.handle = C.c_void_p()
