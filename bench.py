@@ -42,6 +42,9 @@ def parse():
     ap.add_argument("--poses", type=int, default=32, help="views per step (the spline's pose count)")
     ap.add_argument("--profile-case", action="store_true", help="small case for an ncu capture (not a bench line)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bound of the CPU-baseline sample")
+    ap.add_argument("--no-extras", action="store_true", help="skip the large-world and serving sections")
+    ap.add_argument("--serve-rate", type=float, default=10_000.0, help="Poisson request rate of the serving section")
+    ap.add_argument("--serve-requests", type=int, default=20_000)
     return ap.parse_args()
 
 
@@ -278,14 +281,14 @@ def run_ours(args, world, rank, local):
     value = world * P * args.steps / (total_ms / 1e3)
 
     # per-view work counters of the last step (algorithmic bytes of the dominant kernel, k_chunks: the meshlet
-    # tests read 64 B of bounds per tested meshlet and write 16 B per drawn entry; a chunk record is 16 B and its
-    # instance matrix 64 B, at most one chunk per 256 tested meshlets plus one per item)
+    # tests read 64 B of bounds per tested meshlet and write 16 B per drawn entry; a span record is 16 B plus its
+    # instance matrix 64 B, one per item and 512-meshlet window crossed; a chunk record is 16 B per window)
     st = [vg.read_stats(k) for k in range(P)]
     b_select = 0.0
     for s in st:
         sel = s["selected"][0] + s["selected"][1]
-        chunks = s["work"][0] + s["work"][1] + s["meshlets_tested"] / 256.0
-        b_select += 64 * s["meshlets_tested"] + 16 * (sel - s["fast_emitted"]) + 80 * chunks
+        spans = s["work"][0] + s["work"][1] + s["meshlets_tested"] / 512.0
+        b_select += 64 * s["meshlets_tested"] + 16 * (sel - s["fast_emitted"]) + 80 * spans + 16 * s["meshlets_tested"] / 512.0
     b_hzb = (4 * W * H + 4 * W * H * 4 / 3) * (P if occl else 0)  # read mip 0, write the whole chain
     work = {k: statistics.mean(float(s[k] if not isinstance(s[k], list) else s[k][0]) for s in st)
             for k in ("visible_cells", "instances_tested", "meshlets_tested", "fast_emitted", "selected", "survived",
@@ -374,8 +377,8 @@ def run_ours(args, world, rank, local):
                       traffic=traffic, kernel="k_chunks", peak_source=f"{peak_kind} hbm_gbs",
                       algorithmic_bytes_per_launch=b_select, avg_launch_ms=select_avg_ms,
                       note="k_chunks algorithmic bytes per view = 64 M (bounds of tested meshlets) + 16 (S - F) (drawn "
-                           "entries) + 80 (items + M/256) (chunk records + instance matrices); the scene's bounds sit in "
-                           "L2, so algorithmic GB/s can exceed DRAM GB/s"),
+                           "entries) + 80 (items + M/512) (span records + instance matrices) + 16 M/512 (chunk records); "
+                           "the scene's bounds sit in L2, so algorithmic GB/s can exceed DRAM GB/s"),
         kernels_plain={k: dict(ms=v[0], launches=v[1]) for k, v in kt.items() if v[1]},
         kernels_batched={k: dict(ms=v[0], launches=v[1]) for k, v in kb.items() if v[1]},
         work_per_view=work,
@@ -383,13 +386,152 @@ def run_ours(args, world, rank, local):
         gpu_launches=args.steps * ((2 if occl else 0) + 11),
         clocks=clk,
     )
+    vg.dispose()
+    if world == 1 and args.config == "ruins" and not args.no_extras:
+        line["large_world"] = run_large_world(spec, args, flush, stream)
+        line["serve"] = run_serve(spec, args)
     if rank == 0:
         vps, cores, sample = cpu_baseline(spec, args.cpu_seconds, occl)
         line["cpu_baseline"] = dict(value=vps, unit="views/s", cores=cores, kind="port", sample=sample)
         print(json.dumps(line), flush=True)
-    for b in list(vg._batches.values()):
-        pass
+
+
+def percentile(sorted_values, q: float) -> float:
+    return sorted_values[min(len(sorted_values) - 1, max(0, int(math.ceil(q * len(sorted_values))) - 1))]
+
+
+def run_large_world(ruins, args, flush, stream):
+    """3M instances over 6 km x 6 km, 16 poses at 3840 x 2160, triangleBudget 6M by the device histogram search,
+    maxDrawDistance 400 m on the small-mesh bucket: batched views/s and how the search met the budget."""
+    import torch
+    from vgcut import engine, scenes
+    spec = scenes.large_world(ruins.meshes, ruins.mesh_triangles, ruins.notes["weight_exponent"])
+    small = set(spec.notes["small_meshes"])
+    vg = engine.VirtualGeometry(max_triangles=12_000_000, max_shadow_triangles=4_000_000, max_meshlets=1 << 18,
+                                output_slots=len(spec.cameras))
+    for i, (data, mats) in enumerate(zip(spec.meshes, spec.instances)):
+        vg.create_mesh(data, mats, max_draw_distance=(400.0 if i in small else float("inf")))
+    budget = spec.notes["triangle_budget"]
+    # the search range reaches 24 px: at 3840 x 2160 over 3M instances no threshold in the reference's default
+    # [0.5, 3] brings the camera cut down to 6M triangles
+    trange = (0.5, 24.0)
+    views = [engine.make_view(c, engine.ViewParams(triangle_budget=budget, threshold_range=trange, state_slot=k,
+                                                   fresh_state=True))
+             for k, c in enumerate(spec.cameras)]
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    for _ in range(max(3, args.warmup)):
+        vg.cut(views, first_slot=0, stream=sp, graph=True)
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        vg.cut(views, first_slot=0, stream=sp, graph=True)
+        b.record(stream)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+    st = [vg.read_stats(k) for k in range(len(views))]
+    drawn = [s["requested_indices"][0] // 3 for s in st]
+    pred = [s["predicted_triangles"] for s in st]
+    out = dict(workload=f"large world: {spec.instance_count} instances of {len(spec.meshes)} meshes over 6x6 km "
+                        f"({spec.notes['placement']}), {len(views)} poses at 3840x2160, triangleBudget 6M, "
+                        f"maxDrawDistance 400 m on the 10 smallest meshes",
+               views_per_sec=len(views) * len(ms) / (sum(ms) / 1e3), ms_per_step=statistics.mean(ms),
+               budget=budget, predicted_triangles_mean=statistics.mean(pred), predicted_over_budget=max(pred) / budget,
+               camera_cut_triangles_mean=statistics.mean(drawn),
+               threshold_range=list(trange),
+               thresholds=[min(s["effective_threshold"] for s in st), max(s["effective_threshold"] for s in st)],
+               note="predicted = the histogram's plain-cut triangles at the chosen threshold; the drawn camera cut adds "
+                    "the LOD-blend band's overlap")
     vg.dispose()
+    return out
+
+
+def run_serve(ruins, args):
+    """The serving loop: 16 resident scenes of 10k-3M instances, a seeded Poisson request stream (pose, 720p / 1080p
+    / 4K, threshold U[0.5, 2], budget on a quarter), admission by output slots and HBM budget, 4 streams."""
+    from vgcut import engine, scenes
+    specs = scenes.serving_scenes(ruins.meshes, ruins.mesh_triangles, ruins.notes["weight_exponent"])
+    vgs = []
+    for sp in specs:
+        vg = engine.VirtualGeometry(max_triangles=10_000_000, max_shadow_triangles=2_000_000, max_meshlets=1 << 17,
+                                    output_slots=1)
+        scenes.load_into(vg, sp)
+        vgs.append(vg)
+    import numpy as np
+    reqs = scenes.request_stream(specs, args.serve_requests, args.serve_rate)
+    views = [engine.make_view(cam, engine.ViewParams(error_threshold=t, triangle_budget=b, threshold_range=(0.5, 3.0)))
+             for _, _, cam, t, b in reqs]
+    budget = 4 << 30
+    server = engine.Server(vgs, streams=4, max_batch=64, slots_per_scene=64, hbm_budget_bytes=budget)
+
+    def run_stream(items, paced: bool):
+        """Submits (arrival s, index) items (paced: at their arrival times), waits and releases each; returns the
+        results and the server-stat deltas."""
+        base = server.stats()
+        tickets = [0] * len(items)
+        results = [None] * len(items)
+        ready = threading.Semaphore(0)
+
+        def submitter():
+            t0 = time.perf_counter()
+            for j, (at, i) in enumerate(items):
+                while paced:
+                    dt = t0 + at - time.perf_counter()
+                    if dt <= 0:
+                        break
+                    if dt > 3e-4:
+                        time.sleep(dt - 2e-4)
+                tickets[j] = server.submit(reqs[i][1], views[i])
+                ready.release()
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        for j in range(len(items)):
+            ready.acquire()
+            results[j] = server.wait(tickets[j])
+            server.release(tickets[j])
+        th.join()
+        st = server.stats()
+        return results, {k: st[k] - base[k] for k in ("batches", "views_launched")}, st
+
+    def summary(results, delta):
+        lat = sorted((r["done_us"] - r["submit_us"]) / 1e3 for r in results)
+        span_s = (max(r["done_us"] for r in results) - min(r["submit_us"] for r in results)) / 1e6
+        return dict(views_per_sec=len(results) / span_s, p50_ms=percentile(lat, 0.5), p99_ms=percentile(lat, 0.99),
+                    p999_ms=percentile(lat, 0.999), mean_batch=delta["views_launched"] / max(1, delta["batches"]),
+                    batches=delta["batches"],
+                    batch_gpu_ms_mean=statistics.mean(r["batch_gpu_ms"] for r in results))
+
+    try:
+        run_stream([(0.0, i) for i in range(256)], False)  # warm-up
+        # capacity: the whole burst submitted at once
+        n_sat = min(len(reqs), 4096)
+        res, delta, _ = run_stream([(0.0, i) for i in range(n_sat)], False)
+        saturated = summary(res, delta)
+        # latency under a Poisson stream at 70% of that capacity (or the requested rate, if lower)
+        rate = min(args.serve_rate, 0.7 * saturated["views_per_sec"])
+        n = min(len(reqs), max(1000, int(rate * 4.0)))
+        gaps = np.random.default_rng(17).exponential(1.0 / rate, n)
+        arrivals = np.cumsum(gaps)
+        res, delta, st = run_stream([(float(arrivals[j]), j % len(reqs)) for j in range(n)], True)
+        paced = summary(res, delta)
+        paced.update(offered_per_sec=n / float(arrivals[-1]), requests=n)
+    finally:
+        server.close()
+        for vg in vgs:
+            vg.dispose()
+    return dict(workload=f"serving: {len(specs)} resident scenes of {min(s.instance_count for s in specs)}-"
+                         f"{max(s.instance_count for s in specs)} instances ({sum(s.instance_count for s in specs)} total) "
+                         f"of the ruins meshes; seeded requests (scene, ground pose, 720p/1080p/4K, threshold U[0.5,2], "
+                         f"triangleBudget 2M/4M/8M on ~25%)",
+                saturated=dict(saturated, requests=n_sat, note="burst submitted at once: the server's capacity"),
+                poisson=dict(paced, note="Poisson arrivals at min(requested rate, 70% of capacity)"),
+                max_in_flight=st["max_in_flight"], hbm_budget_bytes=budget, max_bytes_in_use=st["max_bytes_in_use"],
+                latency_note="submit -> completion seen by the server, host steady clock",
+                config=dict(streams=4, max_batch=64, slots_per_scene=64))
 
 
 def main():

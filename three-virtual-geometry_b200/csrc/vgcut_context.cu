@@ -237,7 +237,7 @@ int ensure_scratch(vgc_context *ctx, LaunchScratch &s, uint32_t views, size_t un
   // meshlet work queue: about one span per instance with a level range and cut, one chunk per 512 meshlets of a
   // warp's items. Sized for 64k entries per view; a warp that cannot reserve tests its items itself, so a full
   // queue costs time, not correctness.
-  const uint32_t want_chunks = std::max<uint32_t>(65536, views * 65536u);
+  const uint32_t want_chunks = std::max<uint32_t>(std::max<uint32_t>(65536, views * 65536u), s.queue_want);
   if (want_chunks > s.chunk_capacity) {
     if (s.d_chunks) {
       cudaFree(s.d_chunks);
@@ -249,6 +249,10 @@ int ensure_scratch(vgc_context *ctx, LaunchScratch &s, uint32_t views, size_t un
     s.chunk_capacity = want_chunks;
   }
   if (!s.done) CUDA_TRY(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
+  if (!s.h_ctl) {
+    CUDA_TRY(cudaMallocHost(&s.h_ctl, 64));
+    std::memset(s.h_ctl, 0, 64);
+  }
   return VGC_OK;
 }
 
@@ -259,6 +263,7 @@ void free_scratch(LaunchScratch &s) {
   if (s.d_units) cudaFree(s.d_units);
   if (s.d_unit_count) cudaFree(s.d_unit_count);
   if (s.d_chunks) cudaFree(s.d_chunks);
+  if (s.h_ctl) cudaFreeHost(s.h_ctl);
   if (s.done) cudaEventDestroy(s.done);
   s = LaunchScratch();
 }
@@ -396,9 +401,14 @@ int prepare(vgc_context *ctx, LaunchScratch &s, const vgc_view *views, uint32_t 
     for (uint32_t i = 0; i < count; i++) slot_end = std::max(slot_end, slots[i] + 1);
   }
   if ((rc = ensure_outputs(ctx, slot_end))) return rc;
+  if (s.pending) CUDA_TRY(cudaEventSynchronize(s.done));
+  s.pending = false;
+  if (s.h_ctl) {  // the last sequence's peak queue demand (spans take 3/4 of the entries, chunks 1/4), plus 25%
+    const uint64_t need = std::max<uint64_t>((uint64_t)s.h_ctl[6] * 4 / 3, (uint64_t)s.h_ctl[7] * 4) * 5 / 4;
+    if (need > s.chunk_capacity) s.queue_want = (uint32_t)std::min<uint64_t>((need + 65535) & ~65535ull, 1u << 28);
+  }
   const uint32_t cells = pad32((uint32_t)ctx->cells.size());
   if ((rc = ensure_scratch(ctx, s, count, (size_t)count * cells))) return rc;
-  if (s.pending) CUDA_TRY(cudaEventSynchronize(s.done));
   bool changed = false;
   s.hzb_w = s.hzb_h = 0;
   s.hzb_tail = false;
@@ -487,6 +497,8 @@ int enqueue(vgc_context *ctx, LaunchScratch &s, uint32_t count, cudaStream_t st,
       return launch_finish(s.d_views, count, S.slot_capacity, S.slots_used, s.d_unit_count, round, st);
     }));
   }
+  // control words (peak queue demand) for the next prepare
+  CUDA_TRY(cudaMemcpyAsync(s.h_ctl, s.d_unit_count, 64, cudaMemcpyDeviceToHost, st));
   return VGC_OK;
 }
 
@@ -891,7 +903,7 @@ int vgc_batch_run(vgc_batch *b, const vgc_view *views, uint32_t count, uint32_t 
   const uint32_t cells = (uint32_t)ctx->cells.size();
   if (!b->exec || b->graph_views != count || b->graph_cells != cells || b->graph_slots != ctx->slot_capacity ||
       b->graph_hzb_w != b->scratch.hzb_w || b->graph_hzb_h != b->scratch.hzb_h || b->graph_hzb_tail != b->scratch.hzb_tail ||
-      b->graph_budget != b->scratch.any_budget) {
+      b->graph_budget != b->scratch.any_budget || b->graph_queue != b->scratch.d_chunks) {
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     b->exec = nullptr;
@@ -914,6 +926,7 @@ int vgc_batch_run(vgc_batch *b, const vgc_view *views, uint32_t count, uint32_t 
     b->graph_hzb_h = b->scratch.hzb_h;
     b->graph_hzb_tail = b->scratch.hzb_tail;
     b->graph_budget = b->scratch.any_budget;
+    b->graph_queue = b->scratch.d_chunks;
   }
   CUDA_TRY(cudaGraphLaunch(b->exec, st));
   CUDA_TRY(cudaEventRecord(b->scratch.done, st));

@@ -60,8 +60,10 @@ struct LaunchScratch {
   ViewConst *d_views = nullptr;
   uint2 *d_units = nullptr;
   uint32_t *d_unit_count = nullptr;  // control words (see launch_reset)
-  uint4 *d_chunks = nullptr;
-  uint32_t chunk_capacity = 0;
+  uint4 *d_chunks = nullptr;      // meshlet work queue (spans and chunks)
+  uint32_t chunk_capacity = 0;    // its entries
+  uint32_t queue_want = 0;        // entries the last launch sequence asked for (grown to before the next one)
+  uint32_t *h_ctl = nullptr;      // pinned copy of the control words at the end of the last launch sequence
   uint32_t view_capacity = 0;
   size_t unit_capacity = 0;
   cudaEvent_t done = nullptr;
@@ -126,6 +128,7 @@ struct vgc_batch {
   uint32_t graph_hzb_w = 0, graph_hzb_h = 0;
   bool graph_hzb_tail = false;
   bool graph_budget = false;
+  const uint4 *graph_queue = nullptr;  // work queue the graph was captured with
 };
 
 namespace vgch {

@@ -255,6 +255,15 @@ __device__ __forceinline__ unsigned long long *queue_counter(uint32_t *ctl) {
   return reinterpret_cast<unsigned long long *>(ctl + 4);
 }
 
+// End of a pass over the work queue (one thread): ctl[6] / ctl[7] keep the most spans / chunks any pass of the
+// launch sequence asked for (the host grows the queue from them for the next launch), and the queue empties.
+__device__ __forceinline__ void retire_queue(uint32_t *ctl) {
+  const unsigned long long q = *queue_counter(ctl);
+  ctl[6] = max(ctl[6], uint32_t(q));
+  ctl[7] = max(ctl[7], uint32_t(q >> 32));
+  *queue_counter(ctl) = 0;
+}
+
 // Band values of a view for the current round, written by k_reset and by the capacity check (dyn[1..5]).
 struct ViewBands {
   float low0, low1, high0, high1, fade_scale;
@@ -888,7 +897,7 @@ __global__ void __launch_bounds__(128) k_chunks(Scene S, const ViewConst *__rest
 // frame's first selection round.
 __global__ void __launch_bounds__(128) k_budget(const ViewConst *__restrict__ views, uint32_t nviews,
                                                 uint32_t *__restrict__ ctl) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) *queue_counter(ctl) = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) retire_queue(ctl);
   const uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t lane = threadIdx.x & 31;
   if (v >= nviews) return;
@@ -938,7 +947,7 @@ __global__ void __launch_bounds__(128) k_finish(const ViewConst *__restrict__ vi
                                                 int round) {
   const uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t lane = threadIdx.x & 31;
-  if (blockIdx.x == 0 && threadIdx.x == 0) *queue_counter(ctl) = 0;  // the next round's work queue starts empty
+  if (blockIdx.x == 0 && threadIdx.x == 0) retire_queue(ctl);  // the next round's work queue starts empty
   if (v >= nviews) return;
   const ViewConst &V = views[v];
   uint32_t *ctr = V.counters;

@@ -12,6 +12,14 @@ workloads here are seeded synthetic scenes with the published shapes and sizes:
   full-detail total lands near the reference ruins scene's 5.73 billion triangles (docs/benchmarks.json);
   1080p camera on a seeded 32-pose spline at 2 m height; HZB from a 1920 x 1080 depth image of 64 screen-aligned
   occluder quads at U[5, 500] m.
+* ``large_world``: 3,000,000 instances of the same 40 meshes over 6 km x 6 km, 80% on a jittered grid (blue noise
+  with a guaranteed minimum spacing, standing in for Poisson-disk placement) and 20% in 50 seeded towns of 150 m
+  radius; 16 poses of a 3840 x 2160 camera at 2 m height; triangleBudget 6,000,000; maxDrawDistance 400 m on the
+  bucket of small meshes (the 10 with the fewest triangles: none of the 50k-2M meshes is under 10k triangles).
+* ``serving_scenes``: 16 scenes of 10k-3M instances (log-uniform) of the same meshes at the ruins density, and a
+  seeded request stream over them (pose, resolution 720p / 1080p / 4K, threshold U[0.5, 2], budget on a quarter).
+
+Instance fields of the large scenes come from numpy's seeded PCG64 stream (vectorised; millions of instances).
 """
 from __future__ import annotations
 
@@ -57,7 +65,7 @@ def icosphere_mesh(n: int, radius: float = 1.0, amplitude: float = 0.02, seed: i
 
 
 def plain_small(n: int = 229, seed: int = 1, grid: int = 8, threads: int = 0) -> SceneSpec:
-    """BASELINE config 1 (see module docstring); `n` may be lowered for CPU-sized tests."""
+    """The small plain scene of the module docstring; `n` may be lowered for CPU-sized tests."""
     r = B.Mulberry32(seed)
     R = 1.0
     data = icosphere_mesh(n, R, 0.02, seed, threads)
@@ -111,7 +119,7 @@ def _ruins_meshes(count: int, tri_lo: float, tri_hi: float, seed: int, threads: 
 def ruins(seed: int = 2, mesh_count: int = 40, tri_lo: float = 50_000, tri_hi: float = 2_000_000,
           instances: int = 113_106, extent: float = 1000.0, poses: int = 32, width: int = 1920, height: int = 1080,
           target_full_detail: float = 5.73e9, quads: int = 64, threads: int = 0) -> SceneSpec:
-    """BASELINE config 2 (see module docstring). Smaller arguments give CPU-sized variants for tests."""
+    """The ruins-like scene of the module docstring. Smaller arguments give CPU-sized variants for tests."""
     meshes = _ruins_meshes(mesh_count, tri_lo, tri_hi, seed, threads)
     tris = np.array([m.stats["leafTriangles"] for m in meshes], np.float64)
     # weights ~ tris^-a; pick a so the expected full-detail total is near the target
@@ -190,4 +198,110 @@ def load_into(vg, spec: SceneSpec, **mesh_options) -> list:
     out = []
     for data, mats in zip(spec.meshes, spec.instances):
         out.append(vg.create_mesh(data, mats, **mesh_options))
+    return out
+
+
+# ---------------------------------------------------------------------------------------------------- large scenes
+def _weights(tris: np.ndarray, exponent: float) -> np.ndarray:
+    w = tris.astype(np.float64) ** (-exponent)
+    return w / w.sum()
+
+
+def _matrices(rng: np.random.Generator, xs: np.ndarray, zs: np.ndarray, scale_sigma: float) -> np.ndarray:
+    n = len(xs)
+    yaw = rng.uniform(0.0, 2 * math.pi, n)
+    sc = np.exp(scale_sigma * rng.standard_normal(n))
+    c, s = np.cos(yaw), np.sin(yaw)
+    mat = np.zeros((n, 16), np.float32)
+    mat[:, 0], mat[:, 2] = c * sc, -s * sc
+    mat[:, 5] = sc
+    mat[:, 8], mat[:, 10] = s * sc, c * sc
+    mat[:, 12], mat[:, 14], mat[:, 15] = xs, zs, 1.0
+    return mat
+
+
+def _jittered_grid(rng: np.random.Generator, n: int, extent: float) -> tuple[np.ndarray, np.ndarray]:
+    """n points on distinct cells of a square grid over [-extent/2, extent/2]^2, each jittered inside the middle
+    70% of its cell: blue noise whose points are at least 0.3 cell apart."""
+    g = int(math.ceil(math.sqrt(n * 1.25)))
+    cells = rng.choice(g * g, n, replace=False)
+    size = extent / g
+    cx, cz = cells % g, cells // g
+    xs = (cx + 0.5 + rng.uniform(-0.35, 0.35, n)) * size - extent / 2
+    zs = (cz + 0.5 + rng.uniform(-0.35, 0.35, n)) * size - extent / 2
+    return xs, zs
+
+
+def _ground_cameras(rng: np.random.Generator, n: int, extent: float, sizes, near=0.1, far=10000.0) -> list:
+    cams = []
+    for _ in range(n):
+        x, z = rng.uniform(-0.45, 0.45, 2) * extent
+        yaw = rng.uniform(0.0, 2 * math.pi)
+        width, height = sizes[int(rng.integers(len(sizes)))]
+        eye = (float(x), 2.0, float(z))
+        target = (float(x + math.cos(yaw)), 2.0 - 0.02, float(z + math.sin(yaw)))
+        cams.append(Camera(view=invert_rigid(look_at_world(eye, target)), proj=perspective(60.0, width / height, near, far),
+                           near=near, height=float(height), width=float(width), extra={"eye": np.array(eye)}))
+    return cams
+
+
+def _assign(rng: np.random.Generator, weights: np.ndarray, xs, zs, scale_sigma: float) -> list:
+    choice = rng.choice(len(weights), len(xs), p=weights)
+    mats = _matrices(rng, xs, zs, scale_sigma)
+    return [mats[choice == m] for m in range(len(weights))]
+
+
+def large_world(meshes: list, mesh_triangles: list, weight_exponent: float, seed: int = 5, instances: int = 3_000_000,
+                extent: float = 6000.0, towns: int = 50, town_fraction: float = 0.2, town_radius: float = 150.0,
+                poses: int = 16, width: int = 3840, height: int = 2160) -> SceneSpec:
+    """The large-world scene of the module docstring over already built meshes."""
+    rng = np.random.default_rng(seed)
+    n_town = int(instances * town_fraction)
+    xs, zs = _jittered_grid(rng, instances - n_town, extent)
+    centres = rng.uniform(-0.45, 0.45, (towns, 2)) * extent
+    which = rng.integers(towns, size=n_town)
+    r = town_radius * np.sqrt(rng.uniform(0.0, 1.0, n_town))
+    a = rng.uniform(0.0, 2 * math.pi, n_town)
+    xs = np.concatenate([xs, centres[which, 0] + r * np.cos(a)])
+    zs = np.concatenate([zs, centres[which, 1] + r * np.sin(a)])
+    tris = np.asarray(mesh_triangles, np.float64)
+    per_mesh = _assign(rng, _weights(tris, weight_exponent), xs, zs, 0.3)
+    cams = _ground_cameras(rng, poses, extent, [(width, height)])
+    small = [int(i) for i in np.argsort(tris)[:10]]
+    spec = SceneSpec("large_world", meshes, [int(t) for t in tris], per_mesh, cams, [])
+    spec.notes = dict(small_meshes=small, max_draw_distance=400.0, triangle_budget=6_000_000.0,
+                      placement="jittered grid (min spacing 0.3 cell) + 50 towns", seed=seed)
+    return spec
+
+
+def serving_scenes(meshes: list, mesh_triangles: list, weight_exponent: float, seed: int = 9, count: int = 16,
+                   lo: int = 10_000, hi: int = 3_000_000, density_per_km2: float = 113_106.0) -> list:
+    """`count` scenes of log-uniform instance counts in [lo, hi] at the ruins density (list of SceneSpec)."""
+    rng = np.random.default_rng(seed)
+    tris = np.asarray(mesh_triangles, np.float64)
+    w = _weights(tris, weight_exponent)
+    out = []
+    for k in range(count):
+        n = int(round(math.exp(rng.uniform(math.log(lo), math.log(hi)))))
+        extent = 1000.0 * math.sqrt(n / density_per_km2)
+        xs = rng.uniform(-0.5, 0.5, n) * extent
+        zs = rng.uniform(-0.5, 0.5, n) * extent
+        spec = SceneSpec(f"serve{k}", meshes, [int(t) for t in tris], _assign(rng, w, xs, zs, 0.3), [], [])
+        spec.notes = dict(extent=extent)
+        out.append(spec)
+    return out
+
+
+def request_stream(specs: list, count: int, rate_per_s: float, seed: int = 13, budget_fraction: float = 0.25) -> list:
+    """Seeded requests over `specs`: (arrival seconds (Poisson process), scene index, camera, threshold, budget)."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate_per_s, count))
+    out = []
+    sizes = [(1280, 720), (1920, 1080), (3840, 2160)]
+    for i in range(count):
+        k = int(rng.integers(len(specs)))
+        cam = _ground_cameras(rng, 1, specs[k].notes["extent"], sizes)[0]
+        threshold = float(rng.uniform(0.5, 2.0))
+        budget = float(rng.choice([2e6, 4e6, 8e6])) if rng.random() < budget_fraction else 0.0
+        out.append((float(t[i]), k, cam, threshold, budget))
     return out
