@@ -14,6 +14,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _native
+from .budget import GlideController, stats_drawn_and_use
 from .camera import Camera
 
 VGC_OK = 0
@@ -305,7 +306,10 @@ class VirtualGeometry:
     """GPU culling + LOD-cut context (VirtualGeometry.ts:77-633), one resident scene."""
 
     def __init__(self, max_triangles: int = 10_000_000, max_shadow_triangles: int = 4_000_000,
-                 max_meshlets: int = 1 << 20, output_slots: int = 1, device: int = 0, hbm_budget_bytes: int = 0):
+                 max_meshlets: int = 1 << 20, output_slots: int = 1, device: int = 0, hbm_budget_bytes: int = 0,
+                 budget_mode: str = "search"):
+        """budget_mode: how `triangle_budget` steers the threshold in `update` — "search" (the device histogram
+        search of each frame's own cut) or "glide" (the reference's CPU controller over stats readbacks)."""
         o = Options()
         lib().vgc_default_options(C.byref(o))
         o.max_triangles, o.max_shadow_triangles = max_triangles, max_shadow_triangles
@@ -319,6 +323,10 @@ class VirtualGeometry:
         self.params = ViewParams()
         self.last_stats: dict | None = None
         self._batches: dict[int, C.c_void_p] = {}
+        if budget_mode not in ("search", "glide"):
+            raise ValueError("budget_mode is 'search' or 'glide'")
+        self.budget_mode = budget_mode
+        self.glide: GlideController | None = None
 
     # ------------------------------------------------------------------ levers (VirtualGeometry.ts:78-183)
     def __getattr__(self, name):
@@ -354,10 +362,26 @@ class VirtualGeometry:
 
     # ------------------------------------------------------------------ the cut
     def update(self, camera: Camera, slot: int = 0, stream=None, **overrides) -> None:
-        """Runs the cut for `camera` into output slot `slot` (VirtualGeometry.update, :392)."""
+        """Runs the cut for `camera` into output slot `slot` (VirtualGeometry.update, :392). With a triangle budget
+        and budget_mode "glide", the reference's controller steps the threshold first and reads the stats back every
+        few frames (budget.GlideController)."""
         p = ViewParams(**{**self.params.__dict__, **overrides})
+        glide = self.budget_mode == "glide" and p.triangle_budget > 0
+        if glide:
+            g = self.glide
+            if g is None:
+                g = self.glide = GlideController(p.error_threshold, p.triangle_budget, p.threshold_range)
+            elif g.written != p.error_threshold:
+                g.error_threshold = p.error_threshold  # the user's value (step() then drops the glide)
+            g.triangle_budget, g.threshold_range = p.triangle_budget, tuple(p.threshold_range)
+            p.error_threshold = self.params.error_threshold = g.step()
+            p.triangle_budget = 0.0
         v = make_view(camera, p)
         check(lib().vgc_cut(self.handle, C.byref(v), 1, slot, stream))
+        if glide and self.glide.end_frame():
+            drawn, use = stats_drawn_and_use(self.read_stats(slot), self.options.max_triangles,
+                                             self.options.max_shadow_triangles, self.options.max_meshlets)
+            self.glide.adapt(drawn, use)
 
     def cut(self, views: list[View], first_slot: int = 0, stream=None, graph: bool = False) -> None:
         arr = (View * len(views))(*views)
