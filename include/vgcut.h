@@ -76,9 +76,14 @@ typedef struct vgc_mesh_opts {
 
 /* vgc_view.flags */
 enum {
-  VGC_VIEW_FRESH_STATE = 1 /* the capacity controller starts this cut from its initial state (threshold scale 1, no
-                              fill history) instead of the state slot's contents; the slot then holds this cut's
-                              state as usual */
+  VGC_VIEW_FRESH_STATE = 1, /* the capacity controller starts this cut from its initial state (threshold scale 1, no
+                               fill history) instead of the state slot's contents; the slot then holds this cut's
+                               state as usual */
+  VGC_VIEW_CASCADE = 2      /* the view is one shadow cascade of its camera (no counterpart in the reference, whose
+                               shadow cut keeps the casters inside the camera frustum swept along shadowSweep): no
+                               camera cut; the shadow cut keeps its reference semantics (LOD from the camera: view,
+                               projection, threshold x shadowErrorScale; no occlusion) but culls against the clip
+                               volume of `cascade_clip`; shadowSweep is not used; triangle_budget must be 0 */
 };
 
 /* One cut request: the uniforms VirtualGeometry.update() writes (VirtualGeometry.ts:414-442) and the levers
@@ -105,6 +110,9 @@ typedef struct vgc_view {
      kernels to the frame's compute submission (VirtualGeometry.ts:482-484). NULL: use the slot as built. */
   const float *depth;
   uint32_t depth_width, depth_height;
+  /* VGC_VIEW_CASCADE: the cascade's clip matrix (light projection x light view, column-major, [0, 1] depth),
+     world -> clip; its six planes bound the shadow cut */
+  double cascade_clip[16];
 } vgc_view;
 
 /* Device pointers of one output slot. */
@@ -208,6 +216,18 @@ int vgc_cut_noalloc(vgc_context *ctx, const vgc_view *view, uint32_t slot, vgc_s
 int vgc_batch_create(vgc_context *ctx, uint32_t max_views, vgc_batch **out);
 int vgc_batch_run(vgc_batch *batch, const vgc_view *views, uint32_t count, uint32_t first_slot, vgc_stream stream);
 int vgc_batch_destroy(vgc_batch *batch);
+
+/* Autotuner (no counterpart in the reference): times the batch's launch sequence for `views` (reps replays each,
+   median) under every pair of persistent grid sizes for the instance and meshlet kernels (blocks per SM: quarters
+   of each kernel's occupancy limit) and keeps the fastest for the batch's later runs. Results are the same under
+   every candidate: the grids only decide which warp takes which unit of work. Runs the views' cut (outputs are
+   left as a normal run leaves them). */
+typedef struct {
+  uint32_t instances_blocks_per_sm, chunks_blocks_per_sm;
+  float ms; /* median device time of one run */
+} vgc_tune_result;
+int vgc_batch_autotune(vgc_batch *batch, const vgc_view *views, uint32_t count, uint32_t first_slot, vgc_stream stream,
+                       uint32_t reps, vgc_tune_result *best);
 
 /* ---------------------------------------------------------------- serving (no counterpart in the reference) */
 /* A request loop over several resident scenes (one context each). The reference cuts once per rendered frame of

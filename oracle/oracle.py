@@ -164,7 +164,8 @@ class _View(C.Structure):
                 ("hzb_offset", C.c_uint32 * 16), ("hzb_width", C.c_uint32 * 16), ("hzb_height", C.c_uint32 * 16),
                 ("max_drawn", C.c_uint32), ("index_capacity", C.c_uint32 * 2), ("state", C.c_uint32 * 8),
                 ("triangle_budget", C.c_double), ("threshold_range", C.c_double * 2),
-                ("chosen_threshold", C.c_double), ("predicted_triangles", C.c_uint64)]
+                ("chosen_threshold", C.c_double), ("predicted_triangles", C.c_uint64), ("cascade", C.c_uint32),
+                ("cascade_clip", C.c_double * 16)]
 
 
 class _Result(C.Structure):
@@ -267,6 +268,11 @@ def make_view(camera, params, max_drawn=1 << 20, index_capacity=(30_000_000, 12_
     for i in range(8):
         v.state[i] = int(st[i])
     v.triangle_budget = float(getattr(params, "triangle_budget", 0.0))
+    clip = getattr(params, "cascade_clip", None)
+    v.cascade = 1 if clip is not None else 0
+    if clip is not None:
+        for k in range(16):
+            v.cascade_clip[k] = float(clip[k])
     tr = getattr(params, "threshold_range", (0.5, 3.0))
     v.threshold_range[0], v.threshold_range[1] = float(tr[0]), float(tr[1])
     v.occlusion_active = 0

@@ -103,6 +103,8 @@ typedef struct vgo_view {
   double threshold_range[2];
   double chosen_threshold;    /* out: errorThreshold the budget search picked */
   uint64_t predicted_triangles; /* out: plain camera-cut triangles the histogram predicts at that threshold */
+  uint32_t cascade;           /* shadow cascade: no camera cut, the shadow cut bounded by cascade_clip's planes */
+  double cascade_clip[16];    /* world -> clip of the cascade, column-major, [0,1] depth */
 } vgo_view;
 
 typedef struct vgo_result {

@@ -40,6 +40,19 @@ float vgo_logf(float x) {
   return fe * 0.693145752f + (fe * 1.42860677e-06f + lnm);
 }
 
+/* Inverse of a rigid column-major 4x4 (rotation + translation): R^T and -R^T t. */
+static void oracle_rigid_inverse(const double *m, double *out) {
+  for (int c = 0; c < 3; c++)
+    for (int r = 0; r < 3; r++) out[c * 4 + r] = m[r * 4 + c];
+  for (int r = 0; r < 3; r++) {
+    double s = 0;
+    for (int i = 0; i < 3; i++) s += m[r * 4 + i] * m[12 + i];
+    out[12 + r] = -s;
+  }
+  out[3] = out[7] = out[11] = 0;
+  out[15] = 1;
+}
+
 /* Frustum planes of a column-major matrix, [0,1] depth (WebGPU), each normalised by its normal's length:
    Gribb & Hartmann plane extraction from the rows of the clip matrix. */
 static void oracle_planes(const double *me, double out[6][4]) {

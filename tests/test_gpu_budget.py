@@ -80,3 +80,28 @@ def test_budget_mixed_batch(plain):
             assert s["effective_threshold"] == np.float32(res["threshold"])
             assert s["predicted_triangles"] == (res["predicted"] if p.triangle_budget > 0 else 0)
             assert key_set(h.vg.draw_list(i, 0), (0, 1, 3)) == key_set(res["entries"][0], (0, 1, 2))
+
+
+def test_reference_glide_controller_on_the_gpu(plain):
+    """budget_mode="glide": the reference's CPU controller steers the threshold over frames from stats readbacks
+    until the camera cut's triangles sit inside its +-15% band around the budget."""
+    spec = plain.spec
+    cam = spec.cameras[0]
+    target_t = 1.5
+    res, _ = plain.oracle(cam, engine.ViewParams(error_threshold=target_t))
+    budget = float(res["counters"][2 + 4] // 3)
+    vg = engine.VirtualGeometry(max_meshlets=1 << 16, budget_mode="glide")
+    try:
+        scenes.load_into(vg, spec)
+        vg.error_threshold = 0.5
+        vg.triangle_budget = budget
+        vg.threshold_range = (0.5, 3.0)
+        ts = []
+        for _ in range(400):
+            vg.update(cam)
+            ts.append(vg.error_threshold)
+        drawn = vg.read_stats(0)["requested_indices"][0] / 3
+        assert abs(drawn / budget - 1) < 0.15, f"drawn {drawn} budget {budget} threshold {ts[-1]}"
+        assert ts[0] == 0.5 and all(b <= a * 1.03 + 1e-9 for a, b in zip(ts, ts[1:]))  # glided, never jumped
+    finally:
+        vg.dispose()

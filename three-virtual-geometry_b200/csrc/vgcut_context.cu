@@ -286,6 +286,29 @@ void planes_of(const double *me, double out[6][4]) {
   }
 }
 
+// Inverse of a rigid column-major 4x4 (rotation + translation): R^T and -R^T t.
+void rigid_inverse(const double *m, double *out) {
+  for (int c = 0; c < 3; c++)
+    for (int r = 0; r < 3; r++) out[c * 4 + r] = m[r * 4 + c];
+  for (int r = 0; r < 3; r++) {
+    double s = 0;
+    for (int i = 0; i < 3; i++) s += m[r * 4 + i] * m[12 + i];
+    out[12 + r] = -s;
+  }
+  out[3] = out[7] = out[11] = 0;
+  out[15] = 1;
+}
+
+// a * b, column-major 4x4
+void mat4_mul(const double *a, const double *b, double *out) {
+  for (int c = 0; c < 4; c++)
+    for (int r = 0; r < 4; r++) {
+      double s = 0;
+      for (int i = 0; i < 4; i++) s += a[i * 4 + r] * b[c * 4 + i];
+      out[c * 4 + r] = s;
+    }
+}
+
 HzbDesc hzb_layout(uint32_t width, uint32_t height, size_t *total_floats) {
   HzbDesc desc{};
   uint32_t lw = width, lh = height, n = 0;
@@ -345,11 +368,21 @@ int view_constants(vgc_context *ctx, const vgc_view &in, uint32_t out_slot, uint
   planes_of(pvm, pw);
   for (int r = 0; r < 3; r++)
     for (int c = 0; c < 4; c++) k.V[r * 4 + c] = (float)in.view[c * 4 + r];
+  const bool cascade = (in.flags & VGC_VIEW_CASCADE) != 0;
+  if (cascade) {
+    if (in.triangle_budget > 0) return fail(VGC_INVALID_ARG, "view: a cascade has no camera cut to budget");
+    // the cascade's planes in camera view space: clip = C * V^-1 * x_view
+    double vinv[16], cm[16];
+    rigid_inverse(in.view, vinv);
+    mat4_mul(in.cascade_clip, vinv, cm);
+    planes_of(cm, pv);
+  }
   for (int p = 0; p < 6; p++) {
     for (int i = 0; i < 4; i++) k.plane[p * 4 + i] = (float)pv[p][i];
     double d = pw[p][0] * in.shadow_sweep[0] + pw[p][1] * in.shadow_sweep[1] + pw[p][2] * in.shadow_sweep[2];
-    k.sweep[p] = (float)(d > 0 ? d : 0);
+    k.sweep[p] = cascade ? 0.0f : (float)(d > 0 ? d : 0);
   }
+  k.cascade = cascade ? 1u : 0u;
   k.proj_scale = (float)(in.proj[5] * in.viewport_height * 0.5);
   k.near_ = (float)in.near_;
   k.P0 = (float)in.proj[0];
@@ -464,6 +497,8 @@ cudaError_t timed(vgc_context *ctx, bool capture, int kind, cudaStream_t st, F &
 // (GeometryPool.ts:1081-1092 without the dispatch-argument kernels, which persistent launches do not need).
 int enqueue(vgc_context *ctx, LaunchScratch &s, uint32_t count, cudaStream_t st, bool capture) {
   const Scene S = scene_of(ctx);
+  const uint32_t select_grid = s.grid_instances ? s.grid_instances : ctx->select_grid;
+  const uint32_t chunk_grid = s.grid_chunks ? s.grid_chunks : ctx->chunk_grid;
   const uint32_t cells = pad32(S.cell_count);
   const HzbDesc *hzbs = (const HzbDesc *)ctx->d_hzb_desc.ptr;
   CUDA_TRY(cudaMemcpyAsync(s.d_views, s.h_views, sizeof(ViewConst) * count, cudaMemcpyHostToDevice, st));
@@ -478,9 +513,9 @@ int enqueue(vgc_context *ctx, LaunchScratch &s, uint32_t count, cudaStream_t st,
   if (s.any_budget) {  // the triangleBudget search: histogram pass, then the threshold of each budget view
     CUDA_TRY(timed(ctx, capture, VGC_KERNEL_BUDGET, st, [&] {
       cudaError_t e = launch_instances(S, s.d_views, hzbs, s.d_units, s.d_unit_count, s.d_chunks, s.chunk_capacity, -1,
-                                       ctx->select_grid, st);
+                                       select_grid, st);
       if (e == cudaSuccess)
-        e = launch_chunks(S, s.d_views, hzbs, s.d_chunks, s.d_unit_count, s.chunk_capacity, -1, ctx->chunk_grid, st);
+        e = launch_chunks(S, s.d_views, hzbs, s.d_chunks, s.d_unit_count, s.chunk_capacity, -1, chunk_grid, st);
       if (e == cudaSuccess) e = launch_budget(s.d_views, count, s.d_unit_count, st);
       return e;
     }));
@@ -488,10 +523,10 @@ int enqueue(vgc_context *ctx, LaunchScratch &s, uint32_t count, cudaStream_t st,
   for (int round = 0; round < 3; round++) {
     CUDA_TRY(timed(ctx, capture, round == 0 ? VGC_KERNEL_SELECT0 : VGC_KERNEL_SELECT_RETRY, st, [&] {
       return launch_instances(S, s.d_views, hzbs, s.d_units, s.d_unit_count, s.d_chunks, s.chunk_capacity, round,
-                              ctx->select_grid, st);
+                              select_grid, st);
     }));
     CUDA_TRY(timed(ctx, capture, round == 0 ? VGC_KERNEL_CHUNKS0 : VGC_KERNEL_SELECT_RETRY, st, [&] {
-      return launch_chunks(S, s.d_views, hzbs, s.d_chunks, s.d_unit_count, s.chunk_capacity, round, ctx->chunk_grid, st);
+      return launch_chunks(S, s.d_views, hzbs, s.d_chunks, s.d_unit_count, s.chunk_capacity, round, chunk_grid, st);
     }));
     CUDA_TRY(timed(ctx, capture, VGC_KERNEL_FINISH, st, [&] {
       return launch_finish(s.d_views, count, S.slot_capacity, S.slots_used, s.d_unit_count, round, st);
@@ -903,7 +938,8 @@ int vgc_batch_run(vgc_batch *b, const vgc_view *views, uint32_t count, uint32_t 
   const uint32_t cells = (uint32_t)ctx->cells.size();
   if (!b->exec || b->graph_views != count || b->graph_cells != cells || b->graph_slots != ctx->slot_capacity ||
       b->graph_hzb_w != b->scratch.hzb_w || b->graph_hzb_h != b->scratch.hzb_h || b->graph_hzb_tail != b->scratch.hzb_tail ||
-      b->graph_budget != b->scratch.any_budget || b->graph_queue != b->scratch.d_chunks) {
+      b->graph_budget != b->scratch.any_budget || b->graph_queue != b->scratch.d_chunks ||
+      b->graph_grids[0] != b->scratch.grid_instances || b->graph_grids[1] != b->scratch.grid_chunks) {
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     b->exec = nullptr;
@@ -927,10 +963,69 @@ int vgc_batch_run(vgc_batch *b, const vgc_view *views, uint32_t count, uint32_t 
     b->graph_hzb_tail = b->scratch.hzb_tail;
     b->graph_budget = b->scratch.any_budget;
     b->graph_queue = b->scratch.d_chunks;
+    b->graph_grids[0] = b->scratch.grid_instances;
+    b->graph_grids[1] = b->scratch.grid_chunks;
   }
   CUDA_TRY(cudaGraphLaunch(b->exec, st));
   CUDA_TRY(cudaEventRecord(b->scratch.done, st));
   b->scratch.pending = true;
+  return VGC_OK;
+}
+
+int vgc_batch_autotune(vgc_batch *b, const vgc_view *views, uint32_t count, uint32_t first_slot, vgc_stream stream,
+                       uint32_t reps, vgc_tune_result *best) {
+  if (!b || !views || !best || count == 0) return fail(VGC_INVALID_ARG, "bad arguments");
+  vgc_context *ctx = b->ctx;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  const uint32_t sms = (uint32_t)ctx->sm_count;
+  const uint32_t max_i = std::max(1u, ctx->select_grid / sms), max_c = std::max(1u, ctx->chunk_grid / sms);
+  // candidate blocks per SM: quarters of the occupancy limit, each at least 1
+  auto steps = [](uint32_t mx) {
+    std::vector<uint32_t> v;
+    for (uint32_t q = 1; q <= 4; q++) {
+      const uint32_t x = std::max(1u, (mx * q + 3) / 4);
+      if (v.empty() || v.back() != x) v.push_back(x);
+    }
+    return v;
+  };
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0));
+  CUDA_TRY(cudaEventCreate(&e1));
+  reps = std::max(1u, reps);
+  vgc_tune_result top{0, 0, INFINITY};
+  int rc = VGC_OK;
+  for (uint32_t bi : steps(max_i)) {
+    for (uint32_t bc : steps(max_c)) {
+      b->scratch.grid_instances = bi * sms;
+      b->scratch.grid_chunks = bc * sms;
+      if ((rc = vgc_batch_run(b, views, count, first_slot, stream))) break;  // capture + warm-up
+      std::vector<float> ms;
+      for (uint32_t r = 0; r < reps; r++) {  // replays of the captured graph: device time only
+        cudaEventRecord(e0, st);
+        cudaGraphLaunch(b->exec, st);
+        cudaEventRecord(e1, st);
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+          rc = fail(VGC_DEVICE_ERROR, "autotune replay failed");
+          break;
+        }
+        float t = 0;
+        cudaEventElapsedTime(&t, e0, e1);
+        ms.push_back(t);
+      }
+      if (rc) break;
+      std::sort(ms.begin(), ms.end());
+      const float med = ms[ms.size() / 2];
+      if (med < top.ms) top = vgc_tune_result{bi, bc, med};
+    }
+    if (rc) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  b->scratch.grid_instances = top.instances_blocks_per_sm * sms;
+  b->scratch.grid_chunks = top.chunks_blocks_per_sm * sms;
+  *best = top;
   return VGC_OK;
 }
 

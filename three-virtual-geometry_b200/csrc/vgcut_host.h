@@ -64,6 +64,8 @@ struct LaunchScratch {
   uint32_t chunk_capacity = 0;    // its entries
   uint32_t queue_want = 0;        // entries the last launch sequence asked for (grown to before the next one)
   uint32_t *h_ctl = nullptr;      // pinned copy of the control words at the end of the last launch sequence
+  uint32_t grid_instances = 0;    // persistent grids of k_instances / k_chunks (0: the context's occupancy defaults)
+  uint32_t grid_chunks = 0;
   uint32_t view_capacity = 0;
   size_t unit_capacity = 0;
   cudaEvent_t done = nullptr;
@@ -129,6 +131,7 @@ struct vgc_batch {
   bool graph_hzb_tail = false;
   bool graph_budget = false;
   const uint4 *graph_queue = nullptr;  // work queue the graph was captured with
+  uint32_t graph_grids[2] = {0, 0};    // persistent grids the graph was captured with
 };
 
 namespace vgch {

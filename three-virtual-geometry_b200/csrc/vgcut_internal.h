@@ -3,11 +3,11 @@
 // HBM layout of a resident scene (one context):
 //   meshes      MeshRec[slot_capacity]            mesh table (GeometryPool.ts:449-460: spheres, levers, flags)
 //   levels      LevelRec[]                        level tables (GeometryPool.ts:432-445), 32 B per level
-//   m_lod       float4[M]  LOD sphere             \
-//   m_parent    float4[M]  parent LOD sphere       | meshletBounds (buildVirtualMesh.ts:85-91) split into
-//   m_err       float4[M]  (error, parentError,    | structure-of-arrays so each pass reads only the 16-byte
-//                           triCount bits, 0)      | columns it needs, coalesced (one float4 per lane)
-//   m_cull      float4[M]  culling sphere         /
+//   m_lod       float4[M]  LOD sphere              | meshletBounds (buildVirtualMesh.ts:85-91) split into
+//   m_parent    float4[M]  parent LOD sphere       | structure-of-arrays so each pass reads only the 16-byte
+//   m_err       float4[M]  (error, parentError,    | columns it needs, coalesced (one float4 per lane), in
+//                           triCount bits, id)     | the engine's test order (m_err.w: pool-global meshlet id)
+//   m_cull      float4[M]  culling sphere          |
 //   m_info      uint4[M]   triangleCount, firstIndex (pool-global), lodLevel, vertexOffset
 //   m_tris      u32[]      packed local triangles (meshletTriangles), pool-global
 //   inst        float4[4 I] instance matrix columns, Morton order per mesh (GeometryPool.ts:484-497)
@@ -73,7 +73,7 @@ struct HzbDesc {
 // Per-view constants derived on the host in double precision (VirtualGeometry.ts:414-442) and stored as float.
 struct ViewConst {
   float V[12];        // rows 0..2 of world->view, row-major 3x4
-  float plane[24];    // 6 view-space frustum planes (xyz normal, w), normalised
+  float plane[24];    // 6 view-space frustum planes (xyz normal, w), normalised (a cascade's: its clip volume)
   float sweep[6];     // per-plane max(dot(world normal, shadowSweep), 0)
   float proj_scale, near_, P0, P5, P8, P9, P10, P14;
   float error_threshold, lod_blend_max, shadow_error_scale, lod_scale_limit, min_pixel_radius;
@@ -85,6 +85,7 @@ struct ViewConst {
   int32_t hzb;          // HZB slot or -1
   uint32_t build_hzb;   // 1: build HZB slot `hzb` from `depth` before the cut
   uint32_t fresh_state; // 1: k_reset puts the controller state back to its initial words first
+  uint32_t cascade;     // 1: shadow cascade (no camera cut; plane[] are the cascade's planes, sweep[] zero)
   const float *depth;   // occluder depth of this frame (build_hzb)
   uint32_t *counters;   // VGC_COUNTER_* header, then per (cut, slot, part): count, start
   uint32_t *state;      // kStateWords, carried between frames

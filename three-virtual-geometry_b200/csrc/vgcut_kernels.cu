@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(256) k_cells(Scene S, const ViewConst *__restr
   if (cell < S.cell_count) {
     CellRec cr = S.cells[cell];
     const MeshRec &mesh = S.meshes[cr.slot];
-    vis = mesh.enabled != 0;
+    vis = mesh.enabled != 0 && (!V.cascade || mesh.shadow != 0);  // a cascade draws shadow casters only
     float c[3];
     xform(V.V, cr.sphere.x, cr.sphere.y, cr.sphere.z, c);
     float radius = cr.sphere.w;
@@ -649,7 +649,7 @@ __global__ void __launch_bounds__(128) k_instances(Scene S, const ViewConst *__r
       xform(VM, mesh.sphere.x, mesh.sphere.y, mesh.sphere.z, c);
       const float radius = mesh.sphere.w * scale;
       const bool no_frustum = !V.frustum;
-      bool in_camera = no_frustum || frustum(V, c, false) >= -radius;
+      bool in_camera = !V.cascade && (no_frustum || frustum(V, c, false) >= -radius);
       bool in_shadow = mesh.shadow != 0 && (no_frustum || frustum(V, c, true) >= -radius);
       in_camera = in_camera && redo0;
       in_shadow = in_shadow && redo1;

@@ -109,3 +109,35 @@ class Camera:
         world = look_at_world(eye, target)
         return Camera(view=invert_rigid(world), proj=perspective(fov, width / height, near, far), near=near,
                       height=float(height), width=float(width), extra={"eye": np.asarray(eye, float)})
+
+
+def cascade_clips(camera, light_dir, splits, caster_reach: float = 200.0) -> list:
+    """World -> clip matrices of orthographic shadow cascades for `camera` (cascaded shadow maps): cascade i bounds
+    the slice [splits[i], splits[i+1]] of the camera frustum in light space, its near plane pulled `caster_reach`
+    toward the light so casters outside the slice that shade it stay inside. `light_dir` points from the light into
+    the scene."""
+    d = np.asarray(light_dir, float)
+    d = d / np.linalg.norm(d)
+    cam_world = invert_rigid(camera.view)
+    W = np.asarray(cam_world, float).reshape(4, 4).T
+    P = np.asarray(camera.proj, float).reshape(4, 4).T
+    tan_y = 1.0 / P[1, 1]
+    tan_x = 1.0 / P[0, 0]
+    out = []
+    for a, b in zip(splits[:-1], splits[1:]):
+        corners = []
+        for z in (a, b):
+            for sx in (-1, 1):
+                for sy in (-1, 1):
+                    corners.append(W @ np.array([sx * tan_x * z, sy * tan_y * z, -z, 1.0]))
+        corners = np.array(corners)[:, :3]
+        centre = corners.mean(axis=0)
+        up = (0.0, 1.0, 0.0) if abs(d[1]) < 0.99 else (0.0, 0.0, 1.0)
+        light_view = invert_rigid(look_at_world(centre - d, centre, up))
+        L = np.asarray(light_view, float).reshape(4, 4).T
+        ls = (L[:3, :3] @ corners.T).T + L[:3, 3]
+        lo, hi = ls.min(axis=0), ls.max(axis=0)
+        # light looks down -z: near = -max z (pulled toward the light), far = -min z
+        proj = orthographic(lo[0], hi[0], hi[1], lo[1], -hi[2] - caster_reach, -lo[2])
+        out.append(mat_mul(proj, light_view))
+    return out

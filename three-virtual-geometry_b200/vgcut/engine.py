@@ -58,7 +58,11 @@ class View(C.Structure):
                 ("triangle_budget", C.c_double), ("threshold_range", C.c_double * 2),
                 ("frustum_culling", C.c_uint32), ("hzb", C.c_int32), ("state_slot", C.c_uint32),
                 ("flags", C.c_uint32), ("depth", C.c_void_p), ("depth_width", C.c_uint32),
-                ("depth_height", C.c_uint32)]
+                ("depth_height", C.c_uint32), ("cascade_clip", C.c_double * 16)]
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("instances_blocks_per_sm", C.c_uint32), ("chunks_blocks_per_sm", C.c_uint32), ("ms", C.c_float)]
 
 
 class ServerOptions(C.Structure):
@@ -127,6 +131,7 @@ def lib() -> C.CDLL:
         "vgc_batch_create": ([vp, C.c_uint32, P(vp)], C.c_int),
         "vgc_batch_run": ([vp, P(View), C.c_uint32, C.c_uint32, vp], C.c_int),
         "vgc_batch_destroy": ([vp], C.c_int),
+        "vgc_batch_autotune": ([vp, P(View), C.c_uint32, C.c_uint32, vp, C.c_uint32, P(TuneResult)], C.c_int),
         "vgc_get_output": ([vp, C.c_uint32, P(Output)], C.c_int),
         "vgc_read_stats": ([vp, C.c_uint32, P(Stats), vp], C.c_int),
         "vgc_read_draw_list": ([vp, C.c_uint32, C.c_uint32, P(C.c_uint32), C.c_uint32, P(C.c_uint32), vp], C.c_int),
@@ -206,9 +211,11 @@ class ViewParams:
     hzb: int = -1
     state_slot: int = 0
     fresh_state: bool = False  # VGC_VIEW_FRESH_STATE: the capacity controller starts from its initial state
+    cascade_clip: object = None  # VGC_VIEW_CASCADE: 16 floats, the cascade's world -> clip matrix (column-major)
 
 
 VGC_VIEW_FRESH_STATE = 1
+VGC_VIEW_CASCADE = 2
 
 
 def make_view(camera: Camera, p: ViewParams | None = None, depth=None) -> View:
@@ -233,7 +240,10 @@ def make_view(camera: Camera, p: ViewParams | None = None, depth=None) -> View:
     v.frustum_culling = 1 if p.frustum_culling else 0
     v.hzb = p.hzb
     v.state_slot = p.state_slot
-    v.flags = VGC_VIEW_FRESH_STATE if p.fresh_state else 0
+    v.flags = (VGC_VIEW_FRESH_STATE if p.fresh_state else 0) | (VGC_VIEW_CASCADE if p.cascade_clip is not None else 0)
+    if p.cascade_clip is not None:
+        for k in range(16):
+            v.cascade_clip[k] = float(p.cascade_clip[k])
     if depth is not None:
         v.depth, v.depth_width, v.depth_height = depth
     return v
@@ -394,6 +404,19 @@ class VirtualGeometry:
             check(lib().vgc_batch_create(self.handle, len(views), C.byref(b)))
             self._batches[len(views)] = b
         check(lib().vgc_batch_run(b, arr, len(views), first_slot, stream))
+
+    def autotune(self, views: list[View], first_slot: int = 0, stream=None, reps: int = 3) -> dict:
+        """Picks the persistent grid sizes of the batched launch for `len(views)` views (vgc_batch_autotune); later
+        `cut(..., graph=True)` calls with that many views use them."""
+        arr = (View * len(views))(*views)
+        b = self._batches.get(len(views))
+        if b is None:
+            b = C.c_void_p()
+            check(lib().vgc_batch_create(self.handle, len(views), C.byref(b)))
+            self._batches[len(views)] = b
+        r = TuneResult()
+        check(lib().vgc_batch_autotune(b, arr, len(views), first_slot, stream, reps, C.byref(r)))
+        return {k: getattr(r, k) for k, _ in TuneResult._fields_}
 
     def cut_noalloc(self, view: View, slot: int = 0, stream=None) -> None:
         """The single-view cut that allocates nothing on the call (see vgc_cut_noalloc in include/vgcut.h)."""
