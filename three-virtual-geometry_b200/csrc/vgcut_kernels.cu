@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(256) k_cells(Scene S, const ViewConst *__restr
 }
 
 // ------------------------------------------------------------------------------------------------ k_instances
-constexpr int kWarpStage = 96;   // staged draw entries per warp and cut (a step adds <= 32)
+constexpr int kWarpStage = 96;   // staged draw entries per warp (a step adds <= 32; one cut at a time)
 constexpr uint32_t kChunk = 512;  // meshlets per chunk (one warp in k_chunks)
 
 // The meshlet work queue between k_instances and k_chunks, in one buffer of `capacity` uint4: spans (one item's
@@ -286,8 +286,8 @@ __device__ __forceinline__ void store_bands(const ViewConst &V, float threshold)
 }
 
 // Drawn entries of one warp waiting for their draw-list positions; the counts are warp-uniform registers.
-struct WarpStage {
-  uint4 e[2][kWarpStage];
+struct WarpStage {  // a warp stages one cut at a time: every stage is flushed before the warp switches cut
+  uint4 e[kWarpStage];
 };
 
 struct WarpCount {
@@ -323,7 +323,7 @@ __device__ __forceinline__ void warp_flush(WarpStage &ws, WarpCount &wc, const V
     if (kept != n) {  // overflow: re-pack the kept prefix
       add0 = add1 = 0;
       for (uint32_t s = 0; s < kept; s++) {
-        uint4 &e = ws.e[cut][s];
+        uint4 &e = ws.e[s];
         const uint32_t tri3 = (e.w & 255u) * 3u;
         if (part_of(e.w)) {
           e.z = add1;
@@ -344,7 +344,7 @@ __device__ __forceinline__ void warp_flush(WarpStage &ws, WarpCount &wc, const V
   __syncwarp();
   uint4 *dst = V.draw_list + (size_t)cut * V.max_drawn + base;
   for (uint32_t s = lane; s < kept; s += 32) {
-    uint4 e = ws.e[cut][s];
+    uint4 e = ws.e[s];
     e.z += part_of(e.w) ? b1 : b0;
     dst[s] = e;
   }
@@ -369,7 +369,7 @@ __device__ __forceinline__ void warp_stage(WarpStage &ws, WarpCount &wc, const V
   if (drawn) {
     const uint32_t excl = incl - mine;
     const uint32_t local = part == 0 ? wc.idx0 + (excl & 0xffffu) : wc.idx1 + (excl >> 16);
-    ws.e[cut][wc.n + __popc(mask & ((1u << lane) - 1u))] = make_uint4(instance, meshlet, local, packed);
+    ws.e[wc.n + __popc(mask & ((1u << lane) - 1u))] = make_uint4(instance, meshlet, local, packed);
   }
   wc.n += __popc(mask);
   wc.idx0 += total & 0xffffu;
@@ -608,7 +608,7 @@ __device__ __forceinline__ void drain_queue(const Scene &S, const ViewConst &V, 
 // HIST: the budget search's pass (views with a triangleBudget only): the camera cut's level range over the whole
 // threshold range, no fast path, no counters.
 template <bool HIST>
-__global__ void __launch_bounds__(128) k_instances(Scene S, const ViewConst *__restrict__ views,
+__global__ void __launch_bounds__(128, 6) k_instances(Scene S, const ViewConst *__restrict__ views,
                                                    const HzbDesc *__restrict__ hzbs, const uint2 *__restrict__ units,
                                                    uint32_t *__restrict__ ctl, uint4 *__restrict__ queue,
                                                    uint32_t capacity, int round) {
@@ -787,7 +787,7 @@ __global__ void __launch_bounds__(128) k_instances(Scene S, const ViewConst *__r
 // meshlets that pass queue up and finish 32 at a time (drain_queue). One draw-list flush per chunk.
 // HIST: the budget histogram of the chunks the budget pass queued.
 template <bool HIST>
-__global__ void __launch_bounds__(128) k_chunks(Scene S, const ViewConst *__restrict__ views,
+__global__ void __launch_bounds__(128, 8) k_chunks(Scene S, const ViewConst *__restrict__ views,
                                                 const HzbDesc *__restrict__ hzbs, uint4 *__restrict__ queue,
                                                 uint32_t *__restrict__ ctl, uint32_t capacity, int round) {
   __shared__ WarpStage stage[4];
