@@ -291,7 +291,8 @@ def run_ours(args, world, rank, local):
         b_select += 64 * s["meshlets_tested"] + 16 * (sel - s["fast_emitted"]) + 80 * spans + 16 * s["meshlets_tested"] / 512.0
     b_hzb = (4 * W * H + 4 * W * H * 4 / 3) * (P if occl else 0)  # read mip 0, write the whole chain
     work = {k: statistics.mean(float(s[k] if not isinstance(s[k], list) else s[k][0]) for s in st)
-            for k in ("visible_cells", "instances_tested", "meshlets_tested", "fast_emitted", "selected", "survived",
+            for k in ("visible_cells", "instances_tested", "meshlets_tested", "meshlets_queued", "fast_emitted",
+                      "selected", "survived",
                       "occluded_instances", "requested_indices", "rounds")}
 
     # plain per-view launches, timed per kernel kind on the launching stream

@@ -141,6 +141,8 @@ enum {
   VGC_COUNTER_PREDICTED_LO = 20,     /* triangleBudget search: plain camera-cut triangles predicted at the */
   VGC_COUNTER_PREDICTED_HI = 21,     /*   chosen threshold (64-bit, low and high words) */
   VGC_COUNTER_BUDGET_BIN = 22,       /* the chosen threshold bin k: t = lo + (hi - lo) k / 255 */
+  VGC_COUNTER_MESHLETS_QUEUED = 23,  /* meshlets of the items after trimming the ones that fail the LOD band for
+                                        certain (tested in the meshlet pass; MESHLETS_TESTED counts the full ranges) */
   VGC_COUNTER_HEADER = 24,
 };
 enum { VGC_CUT_SELECTED = 0, VGC_CUT_DRAWN = 1, VGC_CUT_SURVIVED = 2, VGC_CUT_WORK = 3, VGC_CUT_REQUESTED = 4 };
@@ -157,6 +159,7 @@ typedef struct vgc_stats {
   float effective_threshold;    /* errorThreshold used (after a budget search) */
   uint32_t instances_tested, meshlets_tested, fast_emitted, levels_read; /* work done, all rounds */
   uint64_t predicted_triangles; /* triangleBudget search: predicted plain camera-cut triangles */
+  uint32_t meshlets_queued;     /* meshlets the meshlet pass tested after item trimming (all rounds) */
 } vgc_stats;
 
 const char *vgc_last_error(void);

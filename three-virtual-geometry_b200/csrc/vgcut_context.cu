@@ -48,6 +48,7 @@ void decode_stats(const vgc_context *ctx, const uint32_t *c, float threshold, vg
   s->fast_emitted = c[VGC_COUNTER_FAST_EMITTED];
   s->levels_read = c[VGC_COUNTER_LEVELS_READ];
   s->predicted_triangles = (uint64_t)c[VGC_COUNTER_PREDICTED_LO] | ((uint64_t)c[VGC_COUNTER_PREDICTED_HI] << 32);
+  s->meshlets_queued = c[VGC_COUNTER_MESHLETS_QUEUED];
   s->effective_threshold = threshold;
 }
 
@@ -133,6 +134,7 @@ int sync_scene(vgc_context *ctx) {
   if ((rc = upload(ctx, ctx->d_m_cull, ctx->m_cull))) return rc;
   if ((rc = upload(ctx, ctx->d_m_info, ctx->m_info))) return rc;
   if ((rc = upload(ctx, ctx->d_m_tris, ctx->m_tris))) return rc;
+  if ((rc = upload(ctx, ctx->d_lsamples, ctx->lsamples))) return rc;
   if ((rc = upload(ctx, ctx->d_inst, ctx->inst))) return rc;
   if ((rc = upload(ctx, ctx->d_inst_slot, ctx->inst_slot))) return rc;
   if ((rc = upload(ctx, ctx->d_cells, ctx->cells))) return rc;
@@ -150,6 +152,7 @@ Scene scene_of(const vgc_context *ctx) {
   S.m_cull = (const float4 *)ctx->d_m_cull.ptr;
   S.m_info = (const uint4 *)ctx->d_m_info.ptr;
   S.m_tris = (const uint32_t *)ctx->d_m_tris.ptr;
+  S.lsamples = (const float2 *)ctx->d_lsamples.ptr;
   S.inst = (const float4 *)ctx->d_inst.ptr;
   S.inst_slot = (const uint32_t *)ctx->d_inst_slot.ptr;
   S.cells = (const CellRec *)ctx->d_cells.ptr;
@@ -695,6 +698,7 @@ int vgc_context_destroy(vgc_context *ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   free_scratch(ctx->scratch);
   for (DevBuf *b : {&ctx->d_meshes, &ctx->d_levels, &ctx->d_m_lod, &ctx->d_m_parent, &ctx->d_m_err, &ctx->d_m_cull,
+                    &ctx->d_lsamples,
                     &ctx->d_m_info, &ctx->d_m_tris, &ctx->d_inst, &ctx->d_inst_slot, &ctx->d_cells, &ctx->d_counters,
                     &ctx->d_draw, &ctx->d_args, &ctx->d_dyn, &ctx->d_hist, &ctx->d_state, &ctx->d_hzb_desc})
     dev_free(ctx, *b);
@@ -784,6 +788,34 @@ int vgc_mesh_add(vgc_context *ctx, const vgc_mesh_data *d, const float *matrices
     ctx->m_info.push_back(make_uint4(info[0], info[1] + m.triangle_base * 3, info[2], info[3]));
   }
   if (d->meshlet_triangles) ctx->m_tris.insert(ctx->m_tris.end(), d->meshlet_triangles, d->meshlet_triangles + d->meshlet_triangle_count);
+  // item trimming data: per level, samples of the parent errors (non-decreasing in test order) and suffix minima of
+  // the own errors; valid only when every meshlet's LOD and parent spheres lie inside the mesh's LOD sphere
+  // (then max(|V M c| - r s, near) >= max(d - R s, near) for each of them, the bound k_instances relies on)
+  for (uint32_t l = 0; l < d->level_count; l++) {
+    const uint32_t f = d->level_ranges[l * 2], c = d->level_ranges[l * 2 + 1];
+    std::vector<float> sufmin(c);
+    float mn = INFINITY;
+    for (uint32_t k = c; k-- > 0;) {
+      mn = std::min(mn, d->meshlet_bounds[(size_t)order_of_test[f + k] * 16 + 8]);
+      sufmin[k] = mn;
+    }
+    for (uint32_t k = 0; k < kLevelSamples; k++) {
+      const uint32_t pos = (uint32_t)(((uint64_t)k * c) / kLevelSamples);
+      const float parent = d->meshlet_bounds[(size_t)order_of_test[f + pos] * 16 + 9];
+      ctx->lsamples.push_back(make_float2(parent, sufmin[pos]));
+    }
+  }
+  bool contained = true;
+  {
+    const double C[3] = {d->lod_bounds_sphere[0], d->lod_bounds_sphere[1], d->lod_bounds_sphere[2]};
+    const double R = d->lod_bounds_sphere[3];
+    for (uint32_t i = 0; i < d->meshlet_count && contained; i++)
+      for (int sph = 0; sph < 2; sph++) {
+        const float *b = d->meshlet_bounds + (size_t)i * 16 + sph * 4;
+        const double dx = b[0] - C[0], dy = b[1] - C[1], dz = b[2] - C[2];
+        if (!(std::sqrt(dx * dx + dy * dy + dz * dz) + b[3] <= R)) contained = false;
+      }
+  }
   for (uint32_t l = 0; l < d->level_count; l++) {
     LevelRec L;
     L.first = d->level_ranges[l * 2] + m.meshlet_base;
@@ -812,6 +844,7 @@ int vgc_mesh_add(vgc_context *ctx, const vgc_mesh_data *d, const float *matrices
   r.level_count = d->level_count;
   r.level_base = m.level_base;
   r.meshlet_base = m.meshlet_base;
+  r.range_cut = contained ? 1u : 0u;
   vgc_mesh_opts def = {0.0f, 0.0f, 1u, 0u, 0u};
   write_flags(ctx, slot, opts ? opts : &def);
   ctx->slots_used = std::max(ctx->slots_used, slot + 1);

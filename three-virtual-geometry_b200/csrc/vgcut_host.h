@@ -86,6 +86,7 @@ struct vgc_context {
   std::vector<MeshRec> meshes;
   std::vector<LevelRec> levels;
   std::vector<float4> m_lod, m_parent, m_err, m_cull;
+  std::vector<float2> lsamples;  // kLevelSamples per level
   std::vector<uint4> m_info;
   std::vector<uint32_t> m_tris;
   std::vector<float4> inst;
@@ -96,6 +97,7 @@ struct vgc_context {
   bool dirty = true;
   // device copies
   DevBuf d_meshes, d_levels, d_m_lod, d_m_parent, d_m_err, d_m_cull, d_m_info, d_m_tris, d_inst, d_inst_slot, d_cells;
+  DevBuf d_lsamples;
   // output slots
   uint32_t out_slots = 0;
   uint32_t out_slot_capacity = 0;  // slot_capacity the output buffers were sized for

@@ -10,6 +10,8 @@
 //   m_cull      float4[M]  culling sphere          |
 //   m_info      uint4[M]   triangleCount, firstIndex (pool-global), lodLevel, vertexOffset
 //   m_tris      u32[]      packed local triangles (meshletTriangles), pool-global
+//   lsamples    float2[64 * levels]  per level, at positions k * count / 64 of its meshlets in test order: the
+//                          parent error there (non-decreasing) and the smallest own error from there to the level's end
 //   inst        float4[4 I] instance matrix columns, Morton order per mesh (GeometryPool.ts:484-497)
 //   inst_slot   u32[I]     mesh slot of each instance
 //   cells       CellRec[C] 128 consecutive instances of one mesh (GeometryPool.ts:519-545)
@@ -30,14 +32,17 @@ constexpr uint32_t kLocalVertexBits = 7;   // ceil(log2(MAX_MESHLET_VERTICES = 1
 constexpr uint32_t kMaxHzbLevels = 16;
 constexpr uint32_t kStateWords = 8;        // S_SCALE 0..1, S_FILL 2..3, S_RETRY 4..5
 constexpr uint32_t kBudgetBins = 256;
+constexpr uint32_t kLevelSamples = 64;     // per level: samples of the meshlets in test order (item trimming)
 
-struct MeshRec {  // 80 bytes
+struct MeshRec {  // 96 bytes
   float4 sphere;
   float4 lod;
   float4 cull;
   float max_draw_distance, min_pixel_radius;
   uint32_t level_count, level_base;
   uint32_t enabled, shadow, occlusion, meshlet_base;
+  uint32_t range_cut;  // 1: every meshlet's LOD and parent spheres lie in `lod`, so items may be trimmed
+  uint32_t pad[3];
 };
 
 struct LevelRec {  // 32 bytes
@@ -58,6 +63,7 @@ struct Scene {
   const float4 *m_lod, *m_parent, *m_err, *m_cull;
   const uint4 *m_info;
   const uint32_t *m_tris;
+  const float2 *lsamples;  // kLevelSamples per level (global level index)
   const float4 *inst;
   const uint32_t *inst_slot;
   const CellRec *cells;

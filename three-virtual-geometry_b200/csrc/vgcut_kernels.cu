@@ -406,19 +406,22 @@ __device__ __forceinline__ bool test_meshlet(const Scene &S, const ViewConst &V,
 
 struct LevelRange {
   uint32_t first, last, possible, guaranteed;
+  uint32_t lfirst, llast;  // first and last possible level
 };
 
 // selectLevels' level loop (GeometryPool.ts:788-812) over the mesh's level table (read through L1: every lane
 // of a warp reads the same entries)
 __device__ __forceinline__ LevelRange level_range(const LevelRec *L, uint32_t levels, float low, float high,
                                                   float px_min, float px_max) {
-  LevelRange r{0xffffffffu, 0u, 0u, 0u};
+  LevelRange r{0xffffffffu, 0u, 0u, 0u, 0u, 0u};
   for (uint32_t l = 0; l < levels; l++) {
     const LevelRec e = L[l];
     const bool possible = e.min_own * px_max <= high && (e.max_parent >= float(1e30 * 0.5) || e.max_parent * px_min > low);
     const bool sure = e.max_own * px_min <= low * float(1 - 1e-3) &&
                       (e.min_parent >= float(1e30 * 0.5) || e.min_parent * px_max > high * float(1 + 1e-3));
     if (possible) {
+      if (r.possible == 0) r.lfirst = l;
+      r.llast = l;
       r.first = min(r.first, e.first);
       r.last = max(r.last, e.first + e.count);
       r.possible += e.count;
@@ -426,6 +429,39 @@ __device__ __forceinline__ LevelRange level_range(const LevelRec *L, uint32_t le
     }
   }
   return r;
+}
+
+// The meshlets of an item that can pass the LOD band (own <= high && parent > low). With every meshlet's LOD and
+// parent spheres inside the mesh's LOD sphere, each meshlet's max(|V M c| - r s, near) lies between the mesh's
+// max(d - R s, near) and max(d + R s, near), so its projected parent error is at most parentError * px_min and its
+// own at least ownError * px_max. Within a level the meshlets are in parent-error order: the first possible level's
+// meshlets with parentError * px_min below `low` form a prefix, and the last possible level's meshlets from the point
+// where the smallest remaining ownError * px_max exceeds `high` form a suffix; both fail for certain and are cut.
+// The level samples give the cut points to 1/64 of a level; the margin of 1e-4 covers float rounding.
+__device__ __forceinline__ void trim_item(const Scene &S, const MeshRec &mesh, const LevelRec *L, const LevelRange &r,
+                                          float low, float high, float px_min, float px_max, uint32_t &first,
+                                          uint32_t &last) {
+  first = r.first;
+  last = r.last;
+  if (!mesh.range_cut || !(r.last > r.first)) return;
+  const float2 *a = S.lsamples + (size_t)(mesh.level_base + r.lfirst) * kLevelSamples;
+  int k = -1;  // last sample whose parent error surely fails (samples are non-decreasing)
+#pragma unroll
+  for (int step = 32; step > 0; step >>= 1) {
+    const float e = a[k + step].x;
+    if (k + step < int(kLevelSamples) && e < float(1e30 * 0.5) && (e * px_min) * 1.0001f <= low) k += step;
+  }
+  const LevelRec lf = L[r.lfirst];
+  if (k > 0) first = lf.first + uint32_t(((uint64_t)k * lf.count) / kLevelSamples);
+  const float2 *b = S.lsamples + (size_t)(mesh.level_base + r.llast) * kLevelSamples;
+  int j = int(kLevelSamples);  // first sample from which every own error surely fails (suffix minima non-decreasing)
+#pragma unroll
+  for (int step = 32; step > 0; step >>= 1) {
+    if (j - step >= 0 && (b[j - step].y * px_max) > high * 1.0001f) j -= step;
+  }
+  const LevelRec ll = L[r.llast];
+  if (j < int(kLevelSamples)) last = ll.first + uint32_t(((uint64_t)j * ll.count) / kLevelSamples);
+  if (last < first) last = first;
 }
 
 // Fast-path entries of one cut for a warp (GeometryPool.ts:827-836): up to 4 meshlets per lane, placed with one
@@ -640,7 +676,8 @@ __global__ void __launch_bounds__(128, 6) k_instances(Scene S, const ViewConst *
     const bool occl_on = mesh.occlusion != 0;
     float VM[13];
     bool occluded_now = false;
-    LevelRange r0{0xffffffffu, 0, 0, 0}, r1{0xffffffffu, 0, 0, 0};
+    LevelRange r0{0xffffffffu, 0, 0, 0, 0, 0}, r1{0xffffffffu, 0, 0, 0, 0, 0};
+    uint32_t t0f = 0, t0l = 0, t1f = 0, t1l = 0;  // the items' trimmed meshlet ranges
     bool fast0 = false, fast1 = false, inside0 = true, inside1 = true;
     if (valid) {
       model_view(V.V, S.inst + (size_t)instance * 4, VM, VM[12]);
@@ -673,19 +710,23 @@ __global__ void __launch_bounds__(128, 6) k_instances(Scene S, const ViewConst *
         // inside: the cullBoundsSphere lies in the frustum, so every meshlet passes its frustum test
         if (HIST && in_camera) {
           const float sc = get_state(V.state, 0);
-          r0 = level_range(L, levels, budget_e(V, sc, 0), budget_e(V, sc, 255), px_min, px_max);
+          const float e0 = budget_e(V, sc, 0), e255 = budget_e(V, sc, 255);
+          r0 = level_range(L, levels, e0, e255, px_min, px_max);
           inside0 = no_frustum || frustum(V, cc, false) >= cr;
+          trim_item(S, mesh, L, r0, e0, e255, px_min, px_max, t0f, t0l);
         } else if (in_camera) {
           r0 = level_range(L, levels, b.low0, b.high0, px_min, px_max);
           inside0 = no_frustum || frustum(V, cc, false) >= cr;
           fast0 = r0.last > r0.first && r0.possible == r0.last - r0.first && r0.guaranteed == r0.possible &&
                   r0.possible <= kFastPathMax && inside0;
+          trim_item(S, mesh, L, r0, b.low0, b.high0, px_min, px_max, t0f, t0l);
         }
         if (in_shadow) {
           r1 = level_range(L, levels, b.low1, b.high1, px_min, px_max);
           inside1 = no_frustum || frustum(V, cc, true) >= cr;
           fast1 = r1.last > r1.first && r1.possible == r1.last - r1.first && r1.guaranteed == r1.possible &&
                   r1.possible <= kFastPathMax && inside1;
+          trim_item(S, mesh, L, r1, b.low1, b.high1, px_min, px_max, t1f, t1l);
         }
       }
     }
@@ -698,6 +739,7 @@ __global__ void __launch_bounds__(128, 6) k_instances(Scene S, const ViewConst *
     const uint32_t n_i0 = __popc(__ballot_sync(0xffffffffu, item0)), n_i1 = __popc(__ballot_sync(0xffffffffu, item1));
     const uint32_t fast_m = __reduce_add_sync(0xffffffffu, (fast0 ? r0.possible : 0u) + (fast1 ? r1.possible : 0u));
     const uint32_t tested = __reduce_add_sync(0xffffffffu, (item0 ? r0.last - r0.first : 0u) + (item1 ? r1.last - r1.first : 0u));
+    const uint32_t queued = __reduce_add_sync(0xffffffffu, (item0 ? t0l - t0f : 0u) + (item1 ? t1l - t1f : 0u));
     if (lane == 0) {
       uint32_t *ctr = V.counters;
       if (n_occl) atomicAdd(ctr + VGC_COUNTER_OCCLUDED, n_occl);
@@ -707,6 +749,7 @@ __global__ void __launch_bounds__(128, 6) k_instances(Scene S, const ViewConst *
       if (n_i1) atomicAdd(ctr + C_CUT(1) + VGC_CUT_WORK, n_i1);
       if (fast_m) atomicAdd(ctr + VGC_COUNTER_FAST_EMITTED, fast_m);
       if (tested) atomicAdd(ctr + VGC_COUNTER_MESHLETS_TESTED, tested);
+      if (queued) atomicAdd(ctr + VGC_COUNTER_MESHLETS_QUEUED, queued);
       atomicAdd(ctr + VGC_COUNTER_INSTANCES_TESTED, min(32u, cell.count - ((w & 3u) << 5)));
       if ((w & 3u) == 0) atomicAdd(ctr + VGC_COUNTER_LEVELS_READ, levels);
     }
@@ -715,7 +758,7 @@ __global__ void __launch_bounds__(128, 6) k_instances(Scene S, const ViewConst *
     }
     // items -> spans -> chunks: per cut, the warp's items laid end to end in lane order and cut into kChunk windows;
     // a window's spans (<= 32, one per item) form one chunk of one (view, cell, cut)
-    const uint32_t n0 = item0 ? r0.last - r0.first : 0u, n1 = item1 ? r1.last - r1.first : 0u;
+    const uint32_t n0 = item0 ? t0l - t0f : 0u, n1 = item1 ? t1l - t1f : 0u;
     const uint32_t s0 = warp_scan_incl(n0) - n0, s1 = warp_scan_incl(n1) - n1;  // starts in the laid-out items
     const uint32_t T0 = __shfl_sync(0xffffffffu, s0 + n0, 31), T1 = __shfl_sync(0xffffffffu, s1 + n1, 31);
     if (T0 + T1 == 0) continue;
@@ -734,7 +777,7 @@ __global__ void __launch_bounds__(128, 6) k_instances(Scene S, const ViewConst *
 #pragma unroll
       for (uint32_t cut = 0; cut < 2; cut++) {
         const uint32_t n = cut ? n1 : n0, st = cut ? s1 : s0, np = cut ? p1 : p0;
-        const uint32_t first = cut ? r1.first : r0.first;
+        const uint32_t first = cut ? t1f : t0f;
         const uint32_t flags = il | ((cut ? inside1 : inside0) ? 1u << 7 : 0u);
         uint4 *dst = Q.spans + span_at + (cut ? P0 + q1 : q0);
         for (uint32_t k = 0; k < np; k++) {
@@ -770,8 +813,8 @@ __global__ void __launch_bounds__(128, 6) k_instances(Scene S, const ViewConst *
         for (int i = 0; i < 13; i++) vmj[i] = __shfl_sync(0xffffffffu, VM[i], j);
         const bool jin0 = __shfl_sync(0xffffffffu, inside0 ? 1 : 0, j) != 0;
         const bool jin1 = __shfl_sync(0xffffffffu, inside1 ? 1 : 0, j) != 0;
-        const uint32_t f0 = __shfl_sync(0xffffffffu, r0.first, j), c0 = __shfl_sync(0xffffffffu, n0, j);
-        const uint32_t f1 = __shfl_sync(0xffffffffu, r1.first, j), c1 = __shfl_sync(0xffffffffu, n1, j);
+        const uint32_t f0 = __shfl_sync(0xffffffffu, t0f, j), c0 = __shfl_sync(0xffffffffu, n0, j);
+        const uint32_t f1 = __shfl_sync(0xffffffffu, t1f, j), c1 = __shfl_sync(0xffffffffu, n1, j);
         const uint32_t inst = cell.first + ((w & 3u) << 5) + j;
         if (c0) warp_item<HIST>(S, V, hzbs, ws, cell.slot, 0, occl_on, jin0, vmj, inst, f0, c0);
         if (c1) warp_item<HIST>(S, V, hzbs, ws, cell.slot, 1, false, jin1, vmj, inst, f1, c1);
