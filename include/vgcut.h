@@ -249,6 +249,8 @@ typedef struct {
   uint32_t slots_per_scene;  /* output slots reserved per scene (default streams * max_batch) */
   uint64_t hbm_budget_bytes; /* admission limit on the output-slot bytes of admitted, unreleased requests (0: none) */
   uint32_t linger_us;        /* a batch smaller than max_batch waits up to this long for more requests (default 0) */
+  uint64_t max_batch_instances; /* views x scene instances per batch at most (default 32M; 0: no limit): large
+                                   scenes go in smaller batches, which keeps their latency and work queue bounded */
 } vgc_server_options;
 typedef struct {
   uint64_t ticket;

@@ -47,6 +47,20 @@ def test_plain_small_levers(plain):
         plain.compare(cam, p)
 
 
+def test_untrimmed_mesh_without_sphere_containment():
+    """A mesh whose LOD sphere does not hold its meshlets' spheres (data not from a conforming builder) gets no item
+    trimming, and the cut still equals the oracle's."""
+    import dataclasses
+    spec = scenes.plain_small(n=24, seed=2)
+    data = spec.meshes[0]
+    shrunk = data.lod_bounds_sphere.copy()
+    shrunk[3] *= 0.5
+    spec.meshes[0] = dataclasses.replace(data, lod_bounds_sphere=shrunk)
+    h = Harness(spec)
+    for t, cam in zip([0.7, 1.5, 3.0], cameras_around(3, 22, 6, seed=4)):
+        h.compare(cam, engine.ViewParams(error_threshold=t))
+
+
 def test_gpu_vs_reference_semantics(plain):
     """Differences between the GPU selection and the double restatement are all decisions within the margin."""
     total = near = 0

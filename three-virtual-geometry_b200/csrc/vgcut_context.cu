@@ -212,6 +212,8 @@ int ensure_state(vgc_context *ctx, uint32_t slot) {
 }
 
 int ensure_scratch(vgc_context *ctx, LaunchScratch &s, uint32_t views, size_t units) {
+  if (!s.owner) s.owner = ctx;  // growth below is counted where the scratch was first counted
+  ctx = s.owner;
   if (views > s.view_capacity) {
     if (s.h_views) cudaFreeHost(s.h_views);
     if (s.d_views) {

@@ -53,6 +53,7 @@ using namespace vgch;
 
 // Launch scratch: view constants and the (view, cell) unit list of one launch sequence.
 struct LaunchScratch {
+  vgc_context *owner = nullptr;   // the context whose byte count holds this scratch's device buffers
   uint32_t hzb_w = 0, hzb_h = 0;  // largest depth image the views of this launch build an HZB from (0: none)
   bool hzb_tail = false;
   bool any_budget = false;        // a view of this launch searches its threshold for a triangleBudget

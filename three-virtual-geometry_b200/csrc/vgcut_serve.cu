@@ -110,7 +110,13 @@ bool pick_batch(vgc_server *s, Lane &lane, std::vector<uint32_t> &slots, std::ve
   lane.tickets.clear();
   slots.clear();
   views.clear();
-  while (!sc.pending.empty() && !sc.free_slots.empty() && lane.tickets.size() < s->opts.max_batch) {
+  // views of this batch: max_batch, fewer for scenes so large that a full batch would queue too much work at once
+  uint32_t cap = s->opts.max_batch;
+  if (s->opts.max_batch_instances) {
+    const uint64_t inst = std::max<uint64_t>(1, sc.ctx->inst_slot.size());
+    cap = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(cap, s->opts.max_batch_instances / inst));
+  }
+  while (!sc.pending.empty() && !sc.free_slots.empty() && lane.tickets.size() < cap) {
     if (s->opts.hbm_budget_bytes && s->bytes_in_use + sc.slot_bytes > s->opts.hbm_budget_bytes) break;
     const uint64_t t = sc.pending.front();
     sc.pending.pop_front();
@@ -230,6 +236,7 @@ void vgc_server_default_options(vgc_server_options *o) {
   std::memset(o, 0, sizeof *o);
   o->streams = 2;
   o->max_batch = 64;
+  o->max_batch_instances = 32u << 20;
 }
 
 int vgc_server_create(vgc_context *const *scenes, uint32_t scene_count, const vgc_server_options *opts,

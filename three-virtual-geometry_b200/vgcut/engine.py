@@ -67,7 +67,7 @@ class TuneResult(C.Structure):
 
 class ServerOptions(C.Structure):
     _fields_ = [("streams", C.c_uint32), ("max_batch", C.c_uint32), ("slots_per_scene", C.c_uint32),
-                ("hbm_budget_bytes", C.c_uint64), ("linger_us", C.c_uint32)]
+                ("hbm_budget_bytes", C.c_uint64), ("linger_us", C.c_uint32), ("max_batch_instances", C.c_uint64)]
 
 
 class ServerStats(C.Structure):
@@ -512,12 +512,14 @@ class Server:
     `streams` CUDA streams with continuous batching. Results stay in the scene's output slot until released."""
 
     def __init__(self, scenes: list, streams: int = 2, max_batch: int = 64, slots_per_scene: int = 0,
-                 hbm_budget_bytes: int = 0, linger_us: int = 0):
+                 hbm_budget_bytes: int = 0, linger_us: int = 0, max_batch_instances: int | None = None):
         self.scenes = list(scenes)
         o = ServerOptions()
         lib().vgc_server_default_options(C.byref(o))
         o.streams, o.max_batch, o.slots_per_scene = streams, max_batch, slots_per_scene
         o.hbm_budget_bytes, o.linger_us = hbm_budget_bytes, linger_us
+        if max_batch_instances is not None:
+            o.max_batch_instances = max_batch_instances
         arr = (C.c_void_p * len(self.scenes))(*[vg.handle for vg in self.scenes])
         self.handle = C.c_void_p()
         check(lib().vgc_server_create(arr, len(self.scenes), C.byref(o), C.byref(self.handle)))
