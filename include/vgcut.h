@@ -179,10 +179,13 @@ int vgc_context_footprint(const vgc_context *ctx, uint64_t *bytes);
    into device memory and returns the mesh slot. gpu_to_input (optional, n entries) receives the Morton order. */
 int vgc_mesh_add(vgc_context *ctx, const vgc_mesh_data *data, const float *matrices, uint32_t instance_count,
                  const vgc_mesh_opts *opts, uint32_t *slot, uint32_t *gpu_to_input);
-/* mesh.maxDrawDistance / minPixelRadius / visible / castShadow / occlusionCulling (GeometryPool.writeFlags :463-477) */
+/* mesh.maxDrawDistance / minPixelRadius / visible / castShadow / occlusionCulling (GeometryPool.writeFlags :463-477);
+   a resident scene gets the one mesh record uploaded (synchronous). */
 int vgc_mesh_set_flags(vgc_context *ctx, uint32_t slot, const vgc_mesh_opts *opts);
 /* mesh.setMatrixAt + commitInstances (VirtualMesh.ts:305-314, GeometryPool.ts:499-512): `count` matrices for GPU
-   (Morton) indices [first, first + count) of the mesh; the cells they touch are recomputed. */
+   (Morton) indices [first, first + count) of the mesh; the cells they touch are recomputed. With the scene resident,
+   only the changed matrices are uploaded and the cells are recomputed on the device (synchronous: it waits for the
+   device's earlier work and finishes before returning); the Morton order of the instances is kept. */
 int vgc_instances_update(vgc_context *ctx, uint32_t slot, uint32_t first, uint32_t count, const float *matrices);
 /* mesh.dispose() (GeometryPool.remove :358-363) */
 int vgc_mesh_remove(vgc_context *ctx, uint32_t slot);
@@ -322,6 +325,9 @@ int vgc_kernel_times(vgc_context *ctx, double *ms, uint32_t *launches, int reset
    count; GeometryPool.ts:544 layout) and of the Morton-ordered instance matrices (16 floats each). */
 int vgc_debug_scene(const vgc_context *ctx, float *cells, uint32_t cell_capacity, float *matrices,
                     uint32_t matrix_capacity, uint32_t *cell_count, uint32_t *instance_count);
+/* The device's cell records in the same 8-float form (after the pending upload, if any): instance updates recompute
+   them on the device, and they must equal the host's. */
+int vgc_debug_cells_device(vgc_context *ctx, float *cells, uint32_t capacity, uint32_t *count);
 
 #ifdef __cplusplus
 }

@@ -362,15 +362,16 @@ def compute_cells(matrices_gpu: np.ndarray, sphere, slot: int, instance_base: in
     return np.array(out, np.float32).reshape(-1, 8)
 
 
-def scene_from_spec(meshes, instances, flags=None) -> tuple[OracleScene, np.ndarray, list]:
+def scene_from_spec(meshes, instances, flags=None, orders_in=None) -> tuple[OracleScene, np.ndarray, list]:
     """OracleScene for meshes added in order (slot i = mesh i); returns it, the GPU-order matrices and the per-mesh
-    Morton orders."""
+    Morton orders. `orders_in`: GPU orders to keep (a scene whose instances moved after it was added keeps the order
+    it was added with)."""
     flags = flags or [{} for _ in meshes]
     mats, cells, orders = [], [], []
     base = 0
     for slot, (d, m) in enumerate(zip(meshes, instances)):
         m = np.asarray(m, np.float32).reshape(-1, 16)
-        order = morton_order(m, d.bounding_sphere)
+        order = morton_order(m, d.bounding_sphere) if orders_in is None else np.asarray(orders_in[slot])
         g = m[order]
         mats.append(g)
         cells.append(compute_cells(g, d.bounding_sphere, slot, base))

@@ -251,6 +251,36 @@ def test_instance_update_and_flags(plain):
     assert key_set(lists[0], (0, 1, 3)) == key_set(before[0], (0, 1, 3))
 
 
+def test_instance_updates_on_device():
+    """setMatrixAt + commitInstances on a resident scene: only the moved matrices are uploaded and their cells are
+    recomputed on the device; the device cells equal the host's and the oracle's computeCell bit for bit, and the cut
+    equals the oracle's on the moved scene (the GPU order of the instances is kept)."""
+    spec = scenes.plain_small(n=24, seed=6)
+    h = Harness(spec)
+    cam = cameras_around(1, 24, 7, seed=2)[0]
+    h.compare(cam, engine.ViewParams())  # resident: the updates below take the device path
+    rng = np.random.default_rng(5)
+    mats = [np.array(m, np.float32).reshape(-1, 16) for m in spec.instances]
+    mesh = h.vg.meshes[0]
+    for i in rng.choice(len(mats[0]), 20, replace=False):
+        m = mats[0][i].copy()
+        m[12] += rng.uniform(-6, 6)
+        m[14] += rng.uniform(-6, 6)
+        m[[0, 5, 10]] *= rng.uniform(0.6, 1.6)
+        mats[0][i] = m
+        mesh.set_matrix_at(int(i), m)
+    mesh.commit_instances()
+    dev = h.vg.debug_cells_device()
+    host, gpu_mats = h.vg.debug_scene()
+    assert np.array_equal(dev.view(np.uint32), host.view(np.uint32)), "device cells differ from the host's"
+    h.scene, h.mats, _ = O.scene_from_spec(spec.meshes, mats, h.flags, orders_in=h.orders)
+    assert np.array_equal(gpu_mats, h.mats)
+    ocells = np.asarray(h.scene.keep[-1]).reshape(-1, 8)
+    assert np.array_equal(dev.view(np.uint32), ocells.view(np.uint32)), "device cells differ from the oracle's"
+    for t in (0.8, 2.0):
+        h.compare(cam, engine.ViewParams(error_threshold=t))
+
+
 def test_hzb_built_in_cut_sequence(ruins_small):
     """A view that carries its depth image builds the HZB inside the cut's launches (plain and graph) with the same
     result as a separately built HZB."""

@@ -619,6 +619,19 @@ void morton_order(const float *m, uint32_t n, const float *sphere, std::vector<u
   for (uint32_t i = 0; i < n; i++) order[i] = keys[i].second;
 }
 
+// A changed mesh record goes to the device at once when the scene is resident (after every launch that may still
+// read it); otherwise the pending full upload carries it.
+int publish_mesh_record(vgc_context *ctx, uint32_t slot) {
+  if (ctx->dirty || !ctx->d_meshes.ptr) {
+    ctx->dirty = true;
+    return VGC_OK;
+  }
+  cudaSetDevice(ctx->device);
+  CUDA_TRY(cudaDeviceSynchronize());
+  CUDA_TRY(cudaMemcpy((MeshRec *)ctx->d_meshes.ptr + slot, &ctx->meshes[slot], sizeof(MeshRec), cudaMemcpyHostToDevice));
+  return VGC_OK;
+}
+
 void write_flags(vgc_context *ctx, uint32_t slot, const vgc_mesh_opts *o) {
   MeshRec &r = ctx->meshes[slot];
   double dd = o ? o->max_draw_distance : 0;
@@ -860,8 +873,7 @@ int vgc_mesh_set_flags(vgc_context *ctx, uint32_t slot, const vgc_mesh_opts *opt
   if (!ctx || !opts) return fail(VGC_INVALID_ARG, "null argument");
   if (slot >= ctx->slots_used || !ctx->mesh_host[slot].used) return fail(VGC_NOT_FOUND, "no mesh in slot");
   write_flags(ctx, slot, opts);
-  ctx->dirty = true;
-  return VGC_OK;
+  return publish_mesh_record(ctx, slot);
 }
 
 int vgc_instances_update(vgc_context *ctx, uint32_t slot, uint32_t first, uint32_t count, const float *matrices) {
@@ -869,13 +881,25 @@ int vgc_instances_update(vgc_context *ctx, uint32_t slot, uint32_t first, uint32
   if (slot >= ctx->slots_used || !ctx->mesh_host[slot].used) return fail(VGC_NOT_FOUND, "no mesh in slot");
   MeshHost &m = ctx->mesh_host[slot];
   if ((uint64_t)first + count > m.instance_count) return fail(VGC_INVALID_ARG, "instance range out of bounds");
+  if (count == 0) return VGC_OK;
   for (uint32_t g = 0; g < count; g++) {
     const float *e = matrices + (size_t)g * 16;
     for (int c = 0; c < 4; c++) ctx->inst[(size_t)(m.instance_base + first + g) * 4 + c] = make_float4(e[c * 4], e[c * 4 + 1], e[c * 4 + 2], e[c * 4 + 3]);
   }
-  if (count)
-    for (uint32_t c = first / kCellSize; c <= (first + count - 1) / kCellSize; c++) compute_cell(ctx, slot, c);
-  ctx->dirty = true;
+  const uint32_t c0 = first / kCellSize, c1 = (first + count - 1) / kCellSize;
+  for (uint32_t c = c0; c <= c1; c++) compute_cell(ctx, slot, c);  // the host mirror stays current
+  if (ctx->dirty) return VGC_OK;  // a full upload is pending anyway
+  // resident scene: upload the changed matrices and recompute their cells on the device (GeometryPool.ts:505-512
+  // commitInstances), after every launch that may still read them and before any later one
+  cudaSetDevice(ctx->device);
+  CUDA_TRY(cudaDeviceSynchronize());
+  float4 *d_inst = (float4 *)ctx->d_inst.ptr + (size_t)(m.instance_base + first) * 4;
+  CUDA_TRY(cudaMemcpyAsync(d_inst, &ctx->inst[(size_t)(m.instance_base + first) * 4], (size_t)count * 64,
+                           cudaMemcpyHostToDevice, ctx->stream));
+  const double sphere[4] = {m.sphere[0], m.sphere[1], m.sphere[2], m.sphere[3]};
+  CUDA_TRY(launch_cells_update((const float4 *)ctx->d_inst.ptr, sphere, m.instance_base, m.instance_count, m.cell_base,
+                               slot, c0, c1 - c0 + 1, (CellRec *)ctx->d_cells.ptr, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   return VGC_OK;
 }
 
@@ -885,7 +909,26 @@ int vgc_mesh_remove(vgc_context *ctx, uint32_t slot) {
   // its cells stay in the cell buffer but point at a disabled slot (GeometryPool.ts:358-363)
   ctx->meshes[slot].enabled = 0;
   ctx->mesh_host[slot].used = false;
-  ctx->dirty = true;
+  return publish_mesh_record(ctx, slot);
+}
+
+int vgc_debug_cells_device(vgc_context *ctx, float *cells, uint32_t capacity, uint32_t *count) {
+  if (!ctx || !count) return fail(VGC_INVALID_ARG, "null argument");
+  int rc = sync_scene(ctx);
+  if (rc) return rc;
+  const uint32_t n = (uint32_t)ctx->cells.size();
+  *count = n;
+  if (!cells) return VGC_OK;
+  std::vector<CellRec> tmp(std::min(capacity, n));
+  CUDA_TRY(cudaDeviceSynchronize());
+  if (!tmp.empty())
+    CUDA_TRY(cudaMemcpy(tmp.data(), ctx->d_cells.ptr, tmp.size() * sizeof(CellRec), cudaMemcpyDeviceToHost));
+  for (size_t i = 0; i < tmp.size(); i++) {
+    const CellRec &c = tmp[i];
+    float *o = cells + i * 8;
+    o[0] = c.sphere.x; o[1] = c.sphere.y; o[2] = c.sphere.z; o[3] = c.sphere.w;
+    o[4] = c.max_radius; o[5] = (float)c.slot; o[6] = (float)c.first; o[7] = (float)c.count;
+  }
   return VGC_OK;
 }
 

@@ -1339,7 +1339,78 @@ __global__ void __launch_bounds__(32) k_gather_stats(const ViewConst *__restrict
   out[v * 32 + t] = w;
 }
 
+// ------------------------------------------------------------------------------------------------ cell update
+// computeCell (GeometryPool.ts:519-545) on the device for cells [c0, c0 + gridDim.x) of one mesh after an instance
+// update: the box of the instances' world spheres gives the centre, the radius reaches every instance sphere, both
+// inflated (1e-4 / 1e-3). Double precision in the host's operation order (min / max reductions are exact in any
+// order), so each record equals the host's computation bit for bit. One block of kCellSize threads per cell.
+__global__ void __launch_bounds__(128) k_cells_update(const float4 *__restrict__ inst, double sx, double sy, double sz,
+                                                      double sr, uint32_t instance_base, uint32_t instance_count,
+                                                      uint32_t cell_base, uint32_t slot, uint32_t c0,
+                                                      CellRec *__restrict__ cells) {
+  __shared__ double red[7][kCellSize];
+  const uint32_t cell = c0 + blockIdx.x, t = threadIdx.x;
+  const uint32_t first = cell * kCellSize, end = min(first + kCellSize, instance_count);
+  const uint32_t g = first + t;
+  const bool on = g < end;
+  double s[4] = {0, 0, 0, 0};
+  if (on) {
+    const float4 *c = inst + (size_t)(instance_base + g) * 4;
+    const float4 a = c[0], b = c[1], d = c[2], e = c[3];
+    s[0] = (double)a.x * sx + (double)b.x * sy + (double)d.x * sz + (double)e.x;
+    s[1] = (double)a.y * sx + (double)b.y * sy + (double)d.y * sz + (double)e.y;
+    s[2] = (double)a.z * sx + (double)b.z * sy + (double)d.z * sz + (double)e.z;
+    const double n0 = sqrt((double)a.x * a.x + (double)a.y * a.y + (double)a.z * a.z);
+    const double n1 = sqrt((double)b.x * b.x + (double)b.y * b.y + (double)b.z * b.z);
+    const double n2 = sqrt((double)d.x * d.x + (double)d.y * d.y + (double)d.z * d.z);
+    s[3] = sr * fmax(n0, fmax(n1, n2));
+  }
+  for (int a = 0; a < 3; a++) {
+    red[a][t] = on ? s[a] - s[3] : INFINITY;
+    red[3 + a][t] = on ? s[a] + s[3] : -INFINITY;
+  }
+  red[6][t] = on ? s[3] : 0.0;
+  __syncthreads();
+  for (uint32_t w = kCellSize / 2; w > 0; w >>= 1) {
+    if (t < w) {
+      for (int a = 0; a < 3; a++) {
+        red[a][t] = fmin(red[a][t], red[a][t + w]);
+        red[3 + a][t] = fmax(red[3 + a][t], red[3 + a][t + w]);
+      }
+      red[6][t] = fmax(red[6][t], red[6][t + w]);
+    }
+    __syncthreads();
+  }
+  const double cx = (red[0][0] + red[3][0]) / 2, cy = (red[1][0] + red[4][0]) / 2, cz = (red[2][0] + red[5][0]) / 2;
+  const double max_radius = red[6][0];
+  __syncthreads();
+  red[0][t] = on ? sqrt((s[0] - cx) * (s[0] - cx) + (s[1] - cy) * (s[1] - cy) + (s[2] - cz) * (s[2] - cz)) + s[3] : 0.0;
+  __syncthreads();
+  for (uint32_t w = kCellSize / 2; w > 0; w >>= 1) {
+    if (t < w) red[0][t] = fmax(red[0][t], red[0][t + w]);
+    __syncthreads();
+  }
+  if (t == 0) {
+    CellRec r;
+    r.sphere = make_float4((float)cx, (float)cy, (float)cz, (float)(red[0][0] * (1 + 1e-4) + 1e-3));
+    r.max_radius = (float)(max_radius * (1 + 1e-4) + 1e-4);
+    r.slot = slot;
+    r.first = instance_base + first;
+    r.count = end - first;
+    cells[cell_base + cell] = r;
+  }
+}
+
 // ------------------------------------------------------------------------------------------------ launchers
+cudaError_t launch_cells_update(const float4 *inst, const double sphere[4], uint32_t instance_base,
+                                uint32_t instance_count, uint32_t cell_base, uint32_t slot, uint32_t c0, uint32_t n,
+                                CellRec *cells, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  k_cells_update<<<n, kCellSize, 0, st>>>(inst, sphere[0], sphere[1], sphere[2], sphere[3], instance_base,
+                                          instance_count, cell_base, slot, c0, cells);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_gather_stats(const ViewConst *views, uint32_t nviews, uint32_t *out, cudaStream_t st) {
   k_gather_stats<<<nviews, 32, 0, st>>>(views, nviews, out);
   return cudaGetLastError();

@@ -24,6 +24,10 @@ cudaError_t launch_chunks(const Scene &S, const ViewConst *views, const HzbDesc 
                           uint32_t *ctl, uint32_t capacity, int round, uint32_t grid, cudaStream_t st);
 // 32 words per view: the VGC_COUNTER_HEADER counter words, then the threshold the cut used (float bits).
 cudaError_t launch_gather_stats(const ViewConst *views, uint32_t nviews, uint32_t *out, cudaStream_t st);
+// computeCell on the device for n cells from c0 of one mesh (bit-identical to the host's computation).
+cudaError_t launch_cells_update(const float4 *inst, const double sphere[4], uint32_t instance_base,
+                                uint32_t instance_count, uint32_t cell_base, uint32_t slot, uint32_t c0, uint32_t n,
+                                CellRec *cells, cudaStream_t st);
 cudaError_t launch_finish(const ViewConst *views, uint32_t nviews, uint32_t slot_capacity, uint32_t slots_used,
                           uint32_t *ctl, int round, cudaStream_t st);
 cudaError_t launch_expand(const Scene &S, const ViewConst *view, uint32_t cut, uint32_t *out, uint64_t capacity,

@@ -144,6 +144,7 @@ def lib() -> C.CDLL:
         "vgc_set_profiling": ([vp, C.c_int], C.c_int),
         "vgc_kernel_times": ([vp, P(C.c_double), P(C.c_uint32), C.c_int], C.c_int),
         "vgc_debug_scene": ([vp, P(C.c_float), C.c_uint32, P(C.c_float), C.c_uint32, P(C.c_uint32), P(C.c_uint32)], C.c_int),
+        "vgc_debug_cells_device": ([vp, P(C.c_float), C.c_uint32, P(C.c_uint32)], C.c_int),
         "vgc_server_default_options": ([P(ServerOptions)], None),
         "vgc_server_create": ([P(vp), C.c_uint32, P(ServerOptions), P(vp)], C.c_int),
         "vgc_server_submit": ([vp, C.c_uint32, P(View), P(C.c_uint64)], C.c_int),
@@ -472,6 +473,14 @@ class VirtualGeometry:
         mats = np.zeros((ni.value, 16), np.float32)
         check(lib().vgc_debug_scene(self.handle, _fp(cells), nc.value, _fp(mats), ni.value, None, None))
         return cells, mats
+
+    def debug_cells_device(self) -> np.ndarray:
+        """The device's cell records (8 floats each), as the kernels read them."""
+        n = C.c_uint32()
+        check(lib().vgc_debug_cells_device(self.handle, None, 0, C.byref(n)))
+        cells = np.zeros((n.value, 8), np.float32)
+        check(lib().vgc_debug_cells_device(self.handle, _fp(cells), n.value, C.byref(n)))
+        return cells
 
     def select_cut(self, slot: int, viewmodels: np.ndarray, proj_scale, near, scale, threshold: float,
                    blend: float = 1.0) -> tuple[np.ndarray, np.ndarray]:
