@@ -63,6 +63,12 @@ typedef struct vgc_mesh_data {
   float lod_bounds_sphere[4];
   float cull_bounds_sphere[4];
   float bounding_sphere[4];
+  /* Optional vertex data (VirtualMeshData.positions / meshletVertices, buildVirtualMesh.ts:75-98), needed only by
+     meshes drawn in the occluder depth pass (vgc_mesh_opts.occluder); NULL / 0 otherwise. */
+  const float *positions;           /* xyz per vertex */
+  uint32_t vertex_count;
+  const uint32_t *meshlet_vertices; /* vertex ids, per meshlet in meshlet-local order (meshlet_info.vertexOffset) */
+  uint32_t meshlet_vertex_count;
 } vgc_mesh_data;
 
 /* Per-mesh levers: VirtualMeshOptions (VirtualMesh.ts:39-62) and the mesh-table flags (GeometryPool.ts:449-477). */
@@ -72,6 +78,7 @@ typedef struct vgc_mesh_opts {
   uint32_t enabled;         /* mesh.visible */
   uint32_t shadow;          /* the shadow cut includes this mesh */
   uint32_t occlusion;       /* occlusion culling may remove this mesh's instances and meshlets */
+  uint32_t occluder;        /* mesh.occluder: drawn by vgc_occluder_depth (needs the mesh's vertex data) */
 } vgc_mesh_opts;
 
 /* vgc_view.flags */
@@ -282,6 +289,16 @@ int vgc_server_release(vgc_server *server, uint64_t ticket);
 int vgc_server_drain(vgc_server *server, uint32_t timeout_ms);
 int vgc_server_stats_get(vgc_server *server, vgc_server_stats *out);
 int vgc_server_destroy(vgc_server *server);
+
+/* Occluder depth pass (OcclusionCulling.ts:244-273, step 1): draws the camera cut held in output slot `src_slot` -
+   the previous frame's - depth-only with this frame's camera `view` into `depth` (device memory, width x height
+   floats, row 0 at the top, NDC depth in [0, 1], 1 where nothing is drawn), for the meshes flagged occluder. As in the
+   reference, only the meshlets drawn over every pixel (part 0) are drawn, back faces are culled, and a triangle is
+   sampled at pixel centres; triangles reaching in front of the near plane are left out (fewer occluders only cull
+   less). Pass `depth` as this frame's vgc_view.depth to build the HZB from it in the cut's own launch sequence.
+   Asynchronous on `stream`. */
+int vgc_occluder_depth(vgc_context *ctx, uint32_t src_slot, const vgc_view *view, float *depth, uint32_t width,
+                       uint32_t height, vgc_stream stream);
 
 /* Layout of HZB slot `hzb`: levels, per-level offset (floats) / width / height (16 entries each), and the device
    pointer of the mip chain (level i at data + offset[i], row-major). */

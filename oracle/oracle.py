@@ -380,3 +380,42 @@ def scene_from_spec(meshes, instances, flags=None, orders_in=None) -> tuple[Orac
     allm = np.concatenate(mats) if mats else np.zeros((0, 16), np.float32)
     allc = np.concatenate(cells) if cells else np.zeros((0, 8), np.float32)
     return OracleScene(list(zip(meshes, flags)), allm, allc), allm, orders
+
+
+def occluder_depth(meshes, occluder_flags, gpu_mats, inst_slot, entries, camera, width: int, height: int) -> np.ndarray:
+    """The occluder depth pass restated (vg_raster.c) over the same pool layout the engine builds: meshes in add
+    order, meshlet / triangle / meshlet-vertex / vertex ids rebased to pool-global, vertex data only for occluders.
+    `entries`: (n, 4) uint32 draw-list entries of the source cut; returns the (height, width) float32 depth."""
+    infos, tris, mverts, pos = [], [], [], []
+    tri_base = mv_base = v_base = 0
+    for d, occ in zip(meshes, occluder_flags):
+        info = np.asarray(d.meshlet_info, np.uint32).reshape(-1, 4).copy()
+        info[:, 1] += np.uint32(tri_base * 3)
+        info[:, 3] += np.uint32(mv_base)
+        infos.append(info)
+        t = np.asarray(d.meshlet_triangles, np.uint32)
+        tris.append(t)
+        tri_base += len(t)
+        if occ:
+            mv = np.asarray(d.meshlet_vertices, np.uint32) + np.uint32(v_base)
+            p = np.asarray(d.positions, np.float32).reshape(-1, 3)
+            mverts.append(mv)
+            pos.append(p)
+            mv_base += len(mv)
+            v_base += len(p)
+    m_info = np.ascontiguousarray(np.concatenate(infos), np.uint32)
+    m_tris = np.ascontiguousarray(np.concatenate(tris), np.uint32)
+    m_verts = np.ascontiguousarray(np.concatenate(mverts) if mverts else np.zeros(1, np.uint32), np.uint32)
+    positions = np.ascontiguousarray(np.concatenate(pos) if pos else np.zeros((1, 3), np.float32), np.float32)
+    e = np.ascontiguousarray(entries, np.uint32).reshape(-1, 4)
+    mats = np.ascontiguousarray(gpu_mats, np.float32)
+    slots = np.ascontiguousarray(inst_slot, np.uint32)
+    flags = np.ascontiguousarray([1 if f else 0 for f in occluder_flags], np.uint32)
+    view = np.ascontiguousarray(camera.view, np.float64)
+    proj = np.ascontiguousarray(camera.proj, np.float64)
+    out = np.zeros((height, width), np.float32)
+    L = lib()
+    L.vgo_occluder_depth(_u(e), len(e), _f(mats), _u(slots), _u(flags), _u(m_info), _u(m_tris), _u(m_verts),
+                         _f(positions), view.ctypes.data_as(C.POINTER(C.c_double)),
+                         proj.ctypes.data_as(C.POINTER(C.c_double)), width, height, _f(out))
+    return out

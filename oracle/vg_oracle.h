@@ -118,6 +118,14 @@ typedef struct vgo_result {
   uint32_t rounds;            /* selection rounds run (1 + retries) */
 } vgo_result;
 
+/* Occluder depth pass (vg_raster.c): entries n x 4 u32 (instance, pool-global meshlet, firstIndex, packed), instance
+   matrices 16 floats (4 columns) in GPU order, per-instance mesh slot, per-slot occluder flag, pool-global meshlet
+   info (4 u32), packed triangles, meshlet vertex ids and xyz positions; depth receives width x height floats. */
+int vgo_occluder_depth(const uint32_t *entries, uint32_t n, const float *inst, const uint32_t *inst_slot,
+                       const uint32_t *slot_occluder, const uint32_t *m_info, const uint32_t *m_tris,
+                       const uint32_t *m_verts, const float *positions, const double *view, const double *proj,
+                       uint32_t width, uint32_t height, float *depth);
+
 /* Full per-frame pass, float mirror of the kernels / double semantics. threads: 0 = all. */
 int vgo_cull_pass_f32(const vgo_scene *scene, vgo_view *view, vgo_result *result, int threads);
 int vgo_cull_pass_f64(const vgo_scene *scene, vgo_view *view, vgo_result *result, int threads);

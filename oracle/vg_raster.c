@@ -1,0 +1,100 @@
+/* Oracle (test infrastructure only): C restatement of the occluder depth pass of the cut engine, which stands in for
+ * the reference's occluder render (OcclusionCulling.ts:244-273: the occluders' previous-frame camera cuts drawn
+ * depth-only with the current camera, vertices pulled as in GeometryPool.ts:1095-1131). Same arithmetic, in the
+ * same order, as the CUDA rasterizer, so the depth images agree bit for bit:
+ *   clip = (P V M) p; a triangle is dropped when a vertex has clip.w <= 0 or clip.z < 0, or when it faces away;
+ *   pixel centres inside the three edge functions (edges included) take the screen-space interpolation of the
+ *   vertices' NDC depths, kept as a per-pixel minimum over an image cleared to 1.
+ * Built with -ffp-contract=off. */
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include "vg_oracle.h"
+
+typedef struct {
+  float ax, ay, az, bx, by, bz, cx, cy, cz, area;
+  int x0, x1, y0, y1;
+} raster_tri;
+
+static int raster_setup(const float c[3][4], float W, float H, raster_tri *t) {
+  float sx[3], sy[3], sz[3];
+  for (int k = 0; k < 3; k++) {
+    if (!(c[k][3] > 0.0f) || !(c[k][2] >= 0.0f)) return 0;
+    const float nx = c[k][0] / c[k][3], ny = c[k][1] / c[k][3], nz = c[k][2] / c[k][3];
+    sx[k] = (nx * 0.5f + 0.5f) * W;
+    sy[k] = (0.5f - ny * 0.5f) * H;
+    sz[k] = nz;
+  }
+  const float area0 = (sx[1] - sx[0]) * (sy[2] - sy[0]) - (sx[2] - sx[0]) * (sy[1] - sy[0]);
+  if (!(area0 < 0.0f)) return 0;
+  t->ax = sx[0], t->ay = sy[0], t->az = sz[0];
+  t->bx = sx[2], t->by = sy[2], t->bz = sz[2];
+  t->cx = sx[1], t->cy = sy[1], t->cz = sz[1];
+  t->area = (t->bx - t->ax) * (t->cy - t->ay) - (t->cx - t->ax) * (t->by - t->ay);
+  if (!(t->area > 0.0f)) return 0;
+  float mnx = fminf(fminf(t->ax, t->bx), t->cx), mxx = fmaxf(fmaxf(t->ax, t->bx), t->cx);
+  float mny = fminf(fminf(t->ay, t->by), t->cy), mxy = fmaxf(fmaxf(t->ay, t->by), t->cy);
+  mnx = fmaxf(mnx, -1.0f), mxx = fminf(mxx, W + 1.0f);
+  mny = fmaxf(mny, -1.0f), mxy = fminf(mxy, H + 1.0f);
+  int x0 = (int)ceilf(mnx - 0.5f), x1 = (int)floorf(mxx - 0.5f);
+  int y0 = (int)ceilf(mny - 0.5f), y1 = (int)floorf(mxy - 0.5f);
+  t->x0 = x0 > 0 ? x0 : 0;
+  t->x1 = x1 < (int)W - 1 ? x1 : (int)W - 1;
+  t->y0 = y0 > 0 ? y0 : 0;
+  t->y1 = y1 < (int)H - 1 ? y1 : (int)H - 1;
+  return t->x0 <= t->x1 && t->y0 <= t->y1;
+}
+
+int vgo_occluder_depth(const uint32_t *entries, uint32_t n, const float *inst, const uint32_t *inst_slot,
+                       const uint32_t *slot_occluder, const uint32_t *m_info, const uint32_t *m_tris,
+                       const uint32_t *m_verts, const float *positions, const double *view, const double *proj,
+                       uint32_t width, uint32_t height, float *depth) {
+  float vp[16];
+  for (int r = 0; r < 4; r++)
+    for (int c = 0; c < 4; c++) {
+      double s = 0;
+      for (int i = 0; i < 4; i++) s += proj[i * 4 + r] * view[c * 4 + i];
+      vp[r * 4 + c] = (float)s;
+    }
+  for (size_t i = 0; i < (size_t)width * height; i++) depth[i] = 1.0f;
+  const float W = (float)width, H = (float)height;
+  for (uint32_t e = 0; e < n; e++) {
+    const uint32_t *d = entries + (size_t)e * 4;
+    if ((d[3] & 0xffff00u) != (255u << 16)) continue;
+    if (!slot_occluder[inst_slot[d[0]]]) continue;
+    const float *col = inst + (size_t)d[0] * 16; /* 4 columns */
+    float m[4][4], mvp[4][4];
+    for (int r = 0; r < 4; r++)
+      for (int c = 0; c < 4; c++) m[r][c] = col[c * 4 + r];
+    for (int r = 0; r < 4; r++)
+      for (int k = 0; k < 4; k++)
+        mvp[r][k] = ((vp[r * 4] * m[0][k] + vp[r * 4 + 1] * m[1][k]) + vp[r * 4 + 2] * m[2][k]) + vp[r * 4 + 3] * m[3][k];
+    const uint32_t *info = m_info + (size_t)d[1] * 4;
+    const uint32_t tris = d[3] & 255u, first_tri = info[1] / 3, voff = info[3];
+    for (uint32_t ti = 0; ti < tris; ti++) {
+      const uint32_t p = m_tris[first_tri + ti];
+      float c[3][4];
+      for (int k = 0; k < 3; k++) {
+        const float *v = positions + (size_t)m_verts[voff + ((p >> (8 * k)) & 255u)] * 3;
+        for (int r = 0; r < 4; r++) c[k][r] = ((mvp[r][0] * v[0] + mvp[r][1] * v[1]) + mvp[r][2] * v[2]) + mvp[r][3];
+      }
+      raster_tri t;
+      if (!raster_setup(c, W, H, &t)) continue;
+      for (int py = t.y0; py <= t.y1; py++)
+        for (int px = t.x0; px <= t.x1; px++) {
+          const float x = (float)px + 0.5f, y = (float)py + 0.5f;
+          const float wa = (t.cx - t.bx) * (y - t.by) - (t.cy - t.by) * (x - t.bx);
+          const float wb = (t.ax - t.cx) * (y - t.cy) - (t.ay - t.cy) * (x - t.cx);
+          const float wc = (t.bx - t.ax) * (y - t.ay) - (t.by - t.ay) * (x - t.ax);
+          if (wa >= 0.0f && wb >= 0.0f && wc >= 0.0f) {
+            float z = ((wa * t.az + wb * t.bz) + wc * t.cz) / t.area;
+            z = z > 0.0f ? z : 0.0f;
+            float *o = depth + (size_t)py * width + px;
+            if (z < *o) *o = z;
+          }
+        }
+    }
+  }
+  return 0;
+}

@@ -1,0 +1,74 @@
+"""The occluder depth pass (vgc_occluder_depth) and the two-pass occlusion loop it closes: the previous frame's
+camera cut of the occluder meshes, drawn depth-only with this frame's camera, must equal the oracle's rasterizer bit
+for bit; an HZB built from it then culls this frame's cut exactly as the oracle does with the same HZB."""
+import numpy as np
+import pytest
+
+import oracle as O
+from parity_util import Harness, d2h, key_set, small_ruins
+from vgcut import engine
+from vgcut.camera import Camera
+
+pytestmark = pytest.mark.gpu
+
+W, H = 480, 270
+
+
+@pytest.fixture(scope="module")
+def occluding():
+    spec = small_ruins(seed=9, poses=3, quads=0)
+    flags = [dict(occlusion=True, occluder=True) for _ in spec.meshes]
+    h = Harness(spec, flags)
+    return h
+
+
+def moved(cam, dx, dyaw):
+    eye = cam.extra["eye"]
+    inv = np.asarray(cam.view).reshape(4, 4).T
+    fwd = -inv[2, :3]  # camera -z in world
+    c, s = np.cos(dyaw), np.sin(dyaw)
+    f = np.array([c * fwd[0] - s * fwd[2], fwd[1], s * fwd[0] + c * fwd[2]])
+    e = eye + dx * fwd
+    return Camera.perspective_look_at(tuple(e), tuple(e + f), 60, 960, 540, 0.1, 5000.0)
+
+
+def gpu_depth(h, src_slot, cam):
+    import torch
+    d = torch.empty((H, W), dtype=torch.float32, device="cuda")
+    h.vg.occluder_depth(src_slot, cam, d.data_ptr(), W, H)
+    torch.cuda.synchronize()
+    return d
+
+
+def oracle_depth(h, src_slot, cam):
+    entries = h.vg.draw_list(src_slot, 0)
+    return O.occluder_depth(h.spec.meshes, [True] * len(h.spec.meshes), h.mats, h.inst_slot, entries, cam, W, H)
+
+
+def test_occluder_depth_matches_the_oracle(occluding):
+    h = occluding
+    for k, cam in enumerate(h.spec.cameras):
+        h.gpu(cam, engine.ViewParams(error_threshold=1.0), slot=0)  # the "previous frame"
+        now = moved(cam, 1.5, 0.03 * (k + 1))
+        d = gpu_depth(h, 0, now)
+        got = d.cpu().numpy()
+        want = oracle_depth(h, 0, now)
+        assert (got < 1).mean() > 0.05, "the occluders cover part of the image"
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), \
+            f"pose {k}: {int((got != want).sum())} pixels differ"
+
+
+def test_two_pass_occlusion_matches_the_oracle(occluding):
+    h = occluding
+    culled = 0
+    for k, cam in enumerate(h.spec.cameras):
+        h.gpu(cam, engine.ViewParams(error_threshold=1.0), slot=0)
+        now = moved(cam, 1.0, -0.02 * (k + 1))
+        d = gpu_depth(h, 0, now)
+        engine.check(engine.lib().vgc_hzb_build(h.vg.handle, 30, d.data_ptr(), W, H, 1, None))
+        hzb = O.hzb_build(oracle_depth(h, 0, now))
+        p = engine.ViewParams(error_threshold=1.0, hzb=30)
+        lists, res = h.compare(now, p, hzb_oracle=hzb, slot=1)
+        open_res, _ = h.oracle(now, engine.ViewParams(error_threshold=1.0))
+        culled += len(open_res["entries"][0]) - len(lists[0])
+    assert culled > 0, "the previous frame's occluders hide part of this frame's cut"

@@ -1,0 +1,77 @@
+"""The oracle's occluder depth pass on hand-built triangles (known answers): depth of a plane at a known distance,
+coverage of the pixel centres inside a triangle, back faces, triangles reaching in front of the near plane, and the
+entries it must skip (blended part 1, meshes that are not occluders)."""
+import numpy as np
+
+import oracle as O
+from vgcut.camera import Camera, perspective
+
+W, H = 64, 48
+
+
+def run(positions, tris, entries, occluder=(1,), near=0.1, far=100.0):
+    cam = Camera(view=np.eye(4).reshape(-1), proj=perspective(60.0, W / H, near, far), near=near, height=float(H),
+                 width=float(W))
+    m_info = np.array([[len(tris), 0, 0, 0]], np.uint32)
+    m_tris = np.array([a | (b << 8) | (c << 16) for a, b, c in tris], np.uint32)
+    m_verts = np.arange(len(positions), dtype=np.uint32)
+    inst = np.eye(4, dtype=np.float32).reshape(1, 16)  # columns of the identity
+    out = np.zeros((H, W), np.float32)
+    e = np.ascontiguousarray(entries, np.uint32).reshape(-1, 4)
+    O.lib().vgo_occluder_depth(O._u(e), len(e), O._f(inst), O._u(np.zeros(1, np.uint32)),
+                               O._u(np.asarray(occluder, np.uint32)), O._u(m_info), O._u(m_tris), O._u(m_verts),
+                               O._f(np.ascontiguousarray(positions, np.float32)),
+                               np.ascontiguousarray(cam.view, np.float64).ctypes.data_as(O.C.POINTER(O.C.c_double)),
+                               np.ascontiguousarray(cam.proj, np.float64).ctypes.data_as(O.C.POINTER(O.C.c_double)),
+                               W, H, O._f(out))
+    return out, cam
+
+
+PART0 = (1 | (255 << 16))  # one triangle, fade range [0, 255]: drawn over every pixel
+
+
+def test_plane_depth_and_coverage():
+    z = -5.0
+    # a big counter-clockwise (front-facing) triangle covering the view at distance 5
+    pos = [(-20, -20, z), (20, -20, z), (0, 30, z)]
+    out, cam = run(pos, [(0, 1, 2)], [(0, 0, 0, PART0)])
+    p10, p14 = cam.proj[10], cam.proj[14]
+    want = np.float32((p10 * z + p14) / -z)
+    covered = out < 1.0
+    assert covered.all(), "the triangle spans the whole view"
+    assert np.allclose(out, want, rtol=0, atol=2e-6), (out.min(), out.max(), want)
+
+
+def test_pixel_centres_inside_only():
+    # NDC triangle (-0.5,-0.5), (0.5,-0.5), (0,0.5) at depth 5 (x, y scaled by 5 tan(fov/2) per axis)
+    t = np.tan(np.radians(30.0))
+    sx, sy = 5 * t * W / H, 5 * t
+    pos = [(-0.5 * sx, -0.5 * sy, -5), (0.5 * sx, -0.5 * sy, -5), (0.0, 0.5 * sy, -5)]
+    out, _ = run(pos, [(0, 1, 2)], [(0, 0, 0, PART0)])
+    covered = out < 1.0
+    # screen vertices (16, 36), (48, 36), (32, 12): pixel centres inside the three edges
+    expect = np.zeros((H, W), bool)
+    for py in range(H):
+        for px in range(W):
+            x, y = px + 0.5, py + 0.5
+            e = [(48 - 16) * (y - 36) - (36 - 36) * (x - 16), (32 - 48) * (y - 36) - (12 - 36) * (x - 48),
+                 (16 - 32) * (y - 12) - (36 - 12) * (x - 32)]
+            expect[py, px] = all(v <= 0 for v in e) or all(v >= 0 for v in e)
+    assert covered.sum() > 100
+    assert abs(int(covered.sum()) - int(expect.sum())) <= 2 * (24 + 32), "coverage follows the pixel-centre rule"
+    assert not covered[:11].any() and not covered[37:].any()
+
+
+def test_back_faces_near_plane_and_skipped_entries():
+    z = -5.0
+    front = [(-20, -20, z), (20, -20, z), (0, 30, z)]
+    back, _ = run(front, [(0, 2, 1)], [(0, 0, 0, PART0)])
+    assert (back == 1.0).all(), "a clockwise (back-facing) triangle is not drawn"
+    crossing = [(-20, -20, z), (20, -20, z), (0, 30, 1.0)]  # one vertex behind the camera
+    out, _ = run(crossing, [(0, 1, 2)], [(0, 0, 0, PART0)])
+    assert (out == 1.0).all(), "a triangle reaching in front of the near plane is left out"
+    blended = 1 | (10 << 8) | (200 << 16)
+    out, _ = run(front, [(0, 1, 2)], [(0, 0, 0, blended)])
+    assert (out == 1.0).all(), "blended (part 1) meshlets are not occluders"
+    out, _ = run(front, [(0, 1, 2)], [(0, 0, 0, PART0)], occluder=(0,))
+    assert (out == 1.0).all(), "meshes that are not occluders are not drawn"

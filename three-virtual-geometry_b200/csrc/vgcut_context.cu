@@ -135,6 +135,8 @@ int sync_scene(vgc_context *ctx) {
   if ((rc = upload(ctx, ctx->d_m_info, ctx->m_info))) return rc;
   if ((rc = upload(ctx, ctx->d_m_tris, ctx->m_tris))) return rc;
   if ((rc = upload(ctx, ctx->d_lsamples, ctx->lsamples))) return rc;
+  if ((rc = upload(ctx, ctx->d_positions, ctx->positions))) return rc;
+  if ((rc = upload(ctx, ctx->d_m_verts, ctx->m_verts))) return rc;
   if ((rc = upload(ctx, ctx->d_inst, ctx->inst))) return rc;
   if ((rc = upload(ctx, ctx->d_inst_slot, ctx->inst_slot))) return rc;
   if ((rc = upload(ctx, ctx->d_cells, ctx->cells))) return rc;
@@ -153,6 +155,8 @@ Scene scene_of(const vgc_context *ctx) {
   S.m_info = (const uint4 *)ctx->d_m_info.ptr;
   S.m_tris = (const uint32_t *)ctx->d_m_tris.ptr;
   S.lsamples = (const float2 *)ctx->d_lsamples.ptr;
+  S.positions = (const float4 *)ctx->d_positions.ptr;
+  S.m_verts = (const uint32_t *)ctx->d_m_verts.ptr;
   S.inst = (const float4 *)ctx->d_inst.ptr;
   S.inst_slot = (const uint32_t *)ctx->d_inst_slot.ptr;
   S.cells = (const CellRec *)ctx->d_cells.ptr;
@@ -640,6 +644,7 @@ void write_flags(vgc_context *ctx, uint32_t slot, const vgc_mesh_opts *o) {
   r.enabled = o ? (o->enabled ? 1u : 0u) : 1u;
   r.shadow = o ? (o->shadow ? 1u : 0u) : 0u;
   r.occlusion = o ? (o->occlusion ? 1u : 0u) : 0u;
+  r.occluder = (o && o->occluder && ctx->mesh_host[slot].vertex_count) ? 1u : 0u;
 }
 
 }  // namespace vgch
@@ -713,7 +718,7 @@ int vgc_context_destroy(vgc_context *ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   free_scratch(ctx->scratch);
   for (DevBuf *b : {&ctx->d_meshes, &ctx->d_levels, &ctx->d_m_lod, &ctx->d_m_parent, &ctx->d_m_err, &ctx->d_m_cull,
-                    &ctx->d_lsamples,
+                    &ctx->d_lsamples, &ctx->d_positions, &ctx->d_m_verts,
                     &ctx->d_m_info, &ctx->d_m_tris, &ctx->d_inst, &ctx->d_inst_slot, &ctx->d_cells, &ctx->d_counters,
                     &ctx->d_draw, &ctx->d_args, &ctx->d_dyn, &ctx->d_hist, &ctx->d_state, &ctx->d_hzb_desc})
     dev_free(ctx, *b);
@@ -755,6 +760,28 @@ int vgc_mesh_add(vgc_context *ctx, const vgc_mesh_data *d, const float *matrices
     if (tc == 0 || tc > 128) return fail(VGC_INVALID_ARG, "meshlet triangle count outside 1..128");
     tri_total += tc;
   }
+  // every index the kernels follow must stay inside the arrays: triangles (expand, occluder pass), vertices
+  const bool has_vertices = d->positions || d->meshlet_vertices;
+  if (has_vertices && (!d->positions || !d->meshlet_vertices || !d->vertex_count || !d->meshlet_vertex_count ||
+                       !d->meshlet_triangles))
+    return fail(VGC_INVALID_ARG, "vertex data needs positions, meshlet_vertices and meshlet_triangles");
+  if (d->meshlet_triangles)
+    for (uint32_t i = 0; i < d->meshlet_count; i++) {
+      const uint32_t *info = d->meshlet_info + (size_t)i * 4;
+      if (info[1] % 3 || (uint64_t)info[1] / 3 + info[0] > d->meshlet_triangle_count)
+        return fail(VGC_INVALID_ARG, "meshlet " + std::to_string(i) + ": triangles outside meshlet_triangles");
+      if (!has_vertices) continue;
+      uint32_t top = 0;
+      for (uint32_t t = 0; t < info[0]; t++) {
+        const uint32_t p = d->meshlet_triangles[info[1] / 3 + t];
+        top = std::max(top, std::max(p & 255u, std::max((p >> 8) & 255u, (p >> 16) & 255u)));
+      }
+      if ((uint64_t)info[3] + top >= d->meshlet_vertex_count)
+        return fail(VGC_INVALID_ARG, "meshlet " + std::to_string(i) + ": vertices outside meshlet_vertices");
+    }
+  if (has_vertices)
+    for (uint32_t i = 0; i < d->meshlet_vertex_count; i++)
+      if (d->meshlet_vertices[i] >= d->vertex_count) return fail(VGC_INVALID_ARG, "meshlet_vertices id out of range");
   std::lock_guard<std::mutex> lock(ctx->mu);
   uint32_t slot = 0;
   while (slot < ctx->slots_used && ctx->mesh_host[slot].used) slot++;
@@ -772,6 +799,15 @@ int vgc_mesh_add(vgc_context *ctx, const vgc_mesh_data *d, const float *matrices
   m.level_base = (uint32_t)ctx->levels.size();
   m.level_count = d->level_count;
   m.triangle_base = (uint32_t)ctx->m_tris.size();
+  // vertex data (occluders): positions and meshletVertices rebased to pool-global ids (GeometryPool.ts:424-429)
+  const uint32_t meshlet_vertex_base = (uint32_t)ctx->m_verts.size();
+  if (d->positions && d->meshlet_vertices && d->vertex_count && d->meshlet_vertex_count) {
+    m.vertex_base = (uint32_t)ctx->positions.size();
+    m.vertex_count = d->vertex_count;
+    for (uint32_t v = 0; v < d->vertex_count; v++)
+      ctx->positions.push_back(make_float4(d->positions[v * 3], d->positions[v * 3 + 1], d->positions[v * 3 + 2], 1.0f));
+    for (uint32_t i = 0; i < d->meshlet_vertex_count; i++) ctx->m_verts.push_back(d->meshlet_vertices[i] + m.vertex_base);
+  }
   m.triangle_count = d->meshlet_triangles ? d->meshlet_triangle_count : 0;
   m.instance_base = (uint32_t)ctx->inst_slot.size();
   m.instance_count = n;
@@ -800,7 +836,7 @@ int vgc_mesh_add(vgc_context *ctx, const vgc_mesh_data *d, const float *matrices
   for (uint32_t i = 0; i < d->meshlet_count; i++) {
     const uint32_t *info = d->meshlet_info + (size_t)i * 4;
     // rebased to pool-global index / vertex ranges (GeometryPool.ts:417-426)
-    ctx->m_info.push_back(make_uint4(info[0], info[1] + m.triangle_base * 3, info[2], info[3]));
+    ctx->m_info.push_back(make_uint4(info[0], info[1] + m.triangle_base * 3, info[2], info[3] + meshlet_vertex_base));
   }
   if (d->meshlet_triangles) ctx->m_tris.insert(ctx->m_tris.end(), d->meshlet_triangles, d->meshlet_triangles + d->meshlet_triangle_count);
   // item trimming data: per level, samples of the parent errors (non-decreasing in test order) and suffix minima of

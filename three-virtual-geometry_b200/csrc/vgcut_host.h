@@ -36,6 +36,7 @@ struct MeshHost {
   uint32_t triangle_base = 0, triangle_count = 0;
   uint32_t instance_base = 0, instance_count = 0;
   uint32_t cell_base = 0, cell_count = 0;
+  uint32_t vertex_base = 0, vertex_count = 0;  // vertex data (0 when the mesh has none)
   float sphere[4];
 };
 
@@ -88,6 +89,8 @@ struct vgc_context {
   std::vector<LevelRec> levels;
   std::vector<float4> m_lod, m_parent, m_err, m_cull;
   std::vector<float2> lsamples;  // kLevelSamples per level
+  std::vector<float4> positions;
+  std::vector<uint32_t> m_verts;
   std::vector<uint4> m_info;
   std::vector<uint32_t> m_tris;
   std::vector<float4> inst;
@@ -98,7 +101,7 @@ struct vgc_context {
   bool dirty = true;
   // device copies
   DevBuf d_meshes, d_levels, d_m_lod, d_m_parent, d_m_err, d_m_cull, d_m_info, d_m_tris, d_inst, d_inst_slot, d_cells;
-  DevBuf d_lsamples;
+  DevBuf d_lsamples, d_positions, d_m_verts;
   // output slots
   uint32_t out_slots = 0;
   uint32_t out_slot_capacity = 0;  // slot_capacity the output buffers were sized for

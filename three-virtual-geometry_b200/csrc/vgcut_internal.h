@@ -8,7 +8,9 @@
 //   m_err       float4[M]  (error, parentError,    | columns it needs, coalesced (one float4 per lane), in
 //                           triCount bits, id)     | the engine's test order (m_err.w: pool-global meshlet id)
 //   m_cull      float4[M]  culling sphere          |
-//   m_info      uint4[M]   triangleCount, firstIndex (pool-global), lodLevel, vertexOffset
+//   m_info      uint4[M]   triangleCount, firstIndex (pool-global), lodLevel, vertexOffset (pool-global)
+//   positions   float4[]   vertex positions of the meshes that carry vertex data (occluders), pool-global
+//   m_verts     u32[]      meshlet-local -> pool-global vertex id (meshletVertices)
 //   m_tris      u32[]      packed local triangles (meshletTriangles), pool-global
 //   lsamples    float2[64 * levels]  per level, at positions k * count / 64 of its meshlets in test order: the
 //                          parent error there (non-decreasing) and the smallest own error from there to the level's end
@@ -42,7 +44,8 @@ struct MeshRec {  // 96 bytes
   uint32_t level_count, level_base;
   uint32_t enabled, shadow, occlusion, meshlet_base;
   uint32_t range_cut;  // 1: every meshlet's LOD and parent spheres lie in `lod`, so items may be trimmed
-  uint32_t pad[3];
+  uint32_t occluder;   // 1: drawn by the occluder depth pass (has vertex data)
+  uint32_t pad[2];
 };
 
 struct LevelRec {  // 32 bytes
@@ -64,6 +67,8 @@ struct Scene {
   const uint4 *m_info;
   const uint32_t *m_tris;
   const float2 *lsamples;  // kLevelSamples per level (global level index)
+  const float4 *positions;  // vertex positions (meshes with vertex data)
+  const uint32_t *m_verts;  // meshletVertices
   const float4 *inst;
   const uint32_t *inst_slot;
   const CellRec *cells;

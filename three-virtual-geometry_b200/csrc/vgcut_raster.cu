@@ -1,0 +1,195 @@
+// Occluder depth pass (vgc_occluder_depth): the reference draws the occluder meshes' previous-frame camera cuts
+// depth-only with the current camera into a small depth target before the HZB build (OcclusionCulling.ts:244-273,
+// through the pools' vertex pulling, GeometryPool.ts:1095-1131). Here it is a CUDA rasterizer over the draw list of
+// an output slot:
+//
+//  * one warp per draw-list entry of part 0 (drawn over every pixel; the blended ones are left out, as in the
+//    reference's proxy) whose mesh is an occluder; clip = (P V M) p with the instance's model matrix;
+//  * a triangle is dropped when a vertex lies behind the near plane (clip.z < 0 or clip.w <= 0) or when it faces
+//    away (the reference's proxy is single-sided): fewer occluders only cull less;
+//  * pixel centres (x + 0.5, y + 0.5) inside all three edge functions (edges included) take the depth interpolated
+//    from the vertices' NDC depths (affine in screen space) through an atomic minimum on the float's bits (depth is
+//    >= 0, so the unsigned order is the float order); the image starts at 1 (far);
+//  * small triangles (bounding box of at most kWarpRasterMin pixels) are drawn by their lane; larger ones one at a
+//    time by the whole warp, so a near, screen-filling occluder costs pixels / 32 steps.
+//
+// Every expression rounds step by step in the written order (the library is compiled with -fmad=false), so the
+// oracle's C restatement reproduces the image bit for bit.
+#include "vgcut_host.h"
+#include "vgcut_kernels.h"
+
+namespace {
+
+constexpr uint32_t kWarpRasterMin = 64;  // bounding-box pixels from which the whole warp draws a triangle
+
+struct RasterArgs {
+  float vp[16];  // P * V, row-major 4x4 (float of the double product)
+  uint32_t width, height;
+  uint32_t *depth;             // float bits
+  const uint4 *draw_list;      // cut 0 entries of the source slot
+  const uint32_t *counters;    // its counter header
+  uint32_t max_drawn;
+};
+
+struct ScreenTri {
+  float ax, ay, az, bx, by, bz, cx, cy, cz, area;
+  int x0, x1, y0, y1;  // pixel bounding box, inclusive
+};
+
+// Setup of one triangle from its clip-space corners; false when it is dropped.
+__device__ __forceinline__ bool setup_triangle(const float c[3][4], float W, float H, ScreenTri &t) {
+  float sx[3], sy[3], sz[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    if (!(c[k][3] > 0.0f) || !(c[k][2] >= 0.0f)) return false;
+    const float nx = c[k][0] / c[k][3], ny = c[k][1] / c[k][3], nz = c[k][2] / c[k][3];
+    sx[k] = (nx * 0.5f + 0.5f) * W;
+    sy[k] = (0.5f - ny * 0.5f) * H;
+    sz[k] = nz;
+  }
+  // screen space is y-down: a triangle facing the camera (counter-clockwise in NDC) has a negative area here
+  const float area0 = (sx[1] - sx[0]) * (sy[2] - sy[0]) - (sx[2] - sx[0]) * (sy[1] - sy[0]);
+  if (!(area0 < 0.0f)) return false;  // back-facing, degenerate or not finite
+  // order A, B, C = 0, 2, 1: positive area
+  t.ax = sx[0], t.ay = sy[0], t.az = sz[0];
+  t.bx = sx[2], t.by = sy[2], t.bz = sz[2];
+  t.cx = sx[1], t.cy = sy[1], t.cz = sz[1];
+  t.area = (t.bx - t.ax) * (t.cy - t.ay) - (t.cx - t.ax) * (t.by - t.ay);
+  if (!(t.area > 0.0f)) return false;
+  float mnx = fminf(fminf(t.ax, t.bx), t.cx), mxx = fmaxf(fmaxf(t.ax, t.bx), t.cx);
+  float mny = fminf(fminf(t.ay, t.by), t.cy), mxy = fmaxf(fmaxf(t.ay, t.by), t.cy);
+  // pixel centres px + 0.5 in [mn, mx]; clamped in float before the integer conversion
+  mnx = fmaxf(mnx, -1.0f), mxx = fminf(mxx, W + 1.0f);
+  mny = fmaxf(mny, -1.0f), mxy = fminf(mxy, H + 1.0f);
+  t.x0 = max(0, int(ceilf(mnx - 0.5f)));
+  t.x1 = min(int(W) - 1, int(floorf(mxx - 0.5f)));
+  t.y0 = max(0, int(ceilf(mny - 0.5f)));
+  t.y1 = min(int(H) - 1, int(floorf(mxy - 0.5f)));
+  return t.x0 <= t.x1 && t.y0 <= t.y1;
+}
+
+__device__ __forceinline__ void shade_pixel(const ScreenTri &t, int px, int py, uint32_t W, uint32_t *depth) {
+  const float x = float(px) + 0.5f, y = float(py) + 0.5f;
+  const float wa = (t.cx - t.bx) * (y - t.by) - (t.cy - t.by) * (x - t.bx);  // edge B -> C
+  const float wb = (t.ax - t.cx) * (y - t.cy) - (t.ay - t.cy) * (x - t.cx);  // edge C -> A
+  const float wc = (t.bx - t.ax) * (y - t.ay) - (t.by - t.ay) * (x - t.ax);  // edge A -> B
+  if (wa >= 0.0f && wb >= 0.0f && wc >= 0.0f) {
+    float z = ((wa * t.az + wb * t.bz) + wc * t.cz) / t.area;
+    z = z > 0.0f ? z : 0.0f;  // +0 for rounding below zero (and never -0, whose bits would sort last)
+    atomicMin(depth + (size_t)py * W + px, __float_as_uint(z));
+  }
+}
+
+__global__ void __launch_bounds__(256) k_depth_clear(uint32_t *depth, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    depth[i] = 0x3f800000u;  // 1.0f
+}
+
+__global__ void __launch_bounds__(128) k_raster_occluders(Scene S, RasterArgs A) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t n = min(A.counters[VGC_COUNTER_CUT0 + VGC_CUT_SELECTED], A.max_drawn);
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  const float W = float(A.width), H = float(A.height);
+  for (uint32_t e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < n; e += warps) {
+    const uint4 d = A.draw_list[e];
+    if ((d.w & 0xffff00u) != (255u << 16)) continue;  // part 1 (blended): not an occluder
+    const uint32_t slot = S.inst_slot[d.x];
+    if (!S.meshes[slot].occluder) continue;
+    // M's rows from the instance's columns, then clip = (P V) M p
+    const float4 *col = S.inst + (size_t)d.x * 4;
+    const float4 c0 = col[0], c1 = col[1], c2 = col[2], c3 = col[3];
+    const float m[4][4] = {{c0.x, c1.x, c2.x, c3.x}, {c0.y, c1.y, c2.y, c3.y}, {c0.z, c1.z, c2.z, c3.z},
+                           {c0.w, c1.w, c2.w, c3.w}};
+    float mvp[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+        mvp[r][k] = ((A.vp[r * 4] * m[0][k] + A.vp[r * 4 + 1] * m[1][k]) + A.vp[r * 4 + 2] * m[2][k]) +
+                    A.vp[r * 4 + 3] * m[3][k];
+    const uint4 info = S.m_info[d.y];
+    const uint32_t tris = d.w & 255u, first_tri = info.y / 3, voff = info.w;
+    uint32_t big = 0;  // this lane's triangles left for the whole warp (bit per round)
+    for (uint32_t round = 0; round * 32 < tris; round++) {
+      const uint32_t ti = round * 32 + lane;
+      ScreenTri t;
+      bool ok = false;
+      if (ti < tris) {
+        const uint32_t p = S.m_tris[first_tri + ti];
+        float c[3][4];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+          const float4 v = S.positions[S.m_verts[voff + ((p >> (8 * k)) & 255u)]];
+#pragma unroll
+          for (int r = 0; r < 4; r++) c[k][r] = ((mvp[r][0] * v.x + mvp[r][1] * v.y) + mvp[r][2] * v.z) + mvp[r][3];
+        }
+        ok = setup_triangle(c, W, H, t);
+      }
+      if (ok && uint32_t(t.x1 - t.x0 + 1) * uint32_t(t.y1 - t.y0 + 1) > kWarpRasterMin) {
+        big |= 1u << round;
+        ok = false;
+      }
+      if (ok)
+        for (int py = t.y0; py <= t.y1; py++)
+          for (int px = t.x0; px <= t.x1; px++) shade_pixel(t, px, py, A.width, A.depth);
+    }
+    // large triangles: one at a time, the warp's lanes over its pixels
+    for (uint32_t round = 0; round * 32 < tris; round++) {
+      uint32_t pending = __ballot_sync(0xffffffffu, (big >> round) & 1u);
+      while (pending) {
+        const uint32_t owner = __ffs(pending) - 1;
+        pending &= pending - 1;
+        ScreenTri t;
+        {  // the owner's setup, recomputed by every lane from the same inputs
+          const uint32_t ti = round * 32 + owner;
+          const uint32_t p = S.m_tris[first_tri + ti];
+          float c[3][4];
+#pragma unroll
+          for (int k = 0; k < 3; k++) {
+            const float4 v = S.positions[S.m_verts[voff + ((p >> (8 * k)) & 255u)]];
+#pragma unroll
+            for (int r = 0; r < 4; r++) c[k][r] = ((mvp[r][0] * v.x + mvp[r][1] * v.y) + mvp[r][2] * v.z) + mvp[r][3];
+          }
+          setup_triangle(c, W, H, t);
+        }
+        const uint32_t bw = uint32_t(t.x1 - t.x0 + 1), count = bw * uint32_t(t.y1 - t.y0 + 1);
+        for (uint32_t i = lane; i < count; i += 32) shade_pixel(t, t.x0 + int(i % bw), t.y0 + int(i / bw), A.width, A.depth);
+      }
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" int vgc_occluder_depth(vgc_context *ctx, uint32_t src_slot, const vgc_view *view, float *depth,
+                                  uint32_t width, uint32_t height, vgc_stream stream) {
+  if (!ctx || !view || !depth) return fail(VGC_INVALID_ARG, "null argument");
+  if (width == 0 || height == 0 || width > 16384 || height > 16384)
+    return fail(VGC_INVALID_ARG, "occluder depth size must be 1..16384 per side");
+  if (src_slot >= ctx->out_slots) return fail(VGC_NOT_FOUND, "output slot not allocated");
+  cudaSetDevice(ctx->device);
+  int rc = sync_scene(ctx);
+  if (rc) return rc;
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  RasterArgs A{};
+  for (int r = 0; r < 4; r++)
+    for (int c = 0; c < 4; c++) {
+      double s = 0;
+      for (int i = 0; i < 4; i++) s += view->proj[i * 4 + r] * view->view[c * 4 + i];
+      A.vp[r * 4 + c] = (float)s;
+    }
+  A.width = width;
+  A.height = height;
+  A.depth = reinterpret_cast<uint32_t *>(depth);
+  A.draw_list = (const uint4 *)ctx->d_draw.ptr + (size_t)src_slot * 2 * ctx->opts.max_meshlets;
+  A.counters = (const uint32_t *)ctx->d_counters.ptr + (size_t)src_slot * ctx->counter_words;
+  A.max_drawn = ctx->opts.max_meshlets;
+  const size_t pixels = (size_t)width * height;
+  k_depth_clear<<<(unsigned)std::min<size_t>((pixels + 255) / 256, (size_t)ctx->sm_count * 16), 256, 0, st>>>(
+      A.depth, pixels);
+  CUDA_TRY(cudaGetLastError());
+  if (ctx->positions.empty()) return VGC_OK;  // no mesh carries vertex data: nothing is an occluder
+  k_raster_occluders<<<ctx->sm_count * 8, 128, 0, st>>>(scene_of(ctx), A);
+  CUDA_TRY(cudaGetLastError());
+  return VGC_OK;
+}

@@ -42,12 +42,14 @@ class MeshData(C.Structure):
                 ("meshlet_triangles", C.POINTER(C.c_uint32)), ("level_count", C.c_uint32),
                 ("level_ranges", C.POINTER(C.c_uint32)), ("level_errors", C.POINTER(C.c_float)),
                 ("level_guard_errors", C.POINTER(C.c_float)), ("lod_bounds_sphere", C.c_float * 4),
-                ("cull_bounds_sphere", C.c_float * 4), ("bounding_sphere", C.c_float * 4)]
+                ("cull_bounds_sphere", C.c_float * 4), ("bounding_sphere", C.c_float * 4),
+                ("positions", C.POINTER(C.c_float)), ("vertex_count", C.c_uint32),
+                ("meshlet_vertices", C.POINTER(C.c_uint32)), ("meshlet_vertex_count", C.c_uint32)]
 
 
 class MeshOpts(C.Structure):
     _fields_ = [("max_draw_distance", C.c_float), ("min_pixel_radius", C.c_float), ("enabled", C.c_uint32),
-                ("shadow", C.c_uint32), ("occlusion", C.c_uint32)]
+                ("shadow", C.c_uint32), ("occlusion", C.c_uint32), ("occluder", C.c_uint32)]
 
 
 class View(C.Structure):
@@ -145,6 +147,7 @@ def lib() -> C.CDLL:
         "vgc_kernel_times": ([vp, P(C.c_double), P(C.c_uint32), C.c_int], C.c_int),
         "vgc_debug_scene": ([vp, P(C.c_float), C.c_uint32, P(C.c_float), C.c_uint32, P(C.c_uint32), P(C.c_uint32)], C.c_int),
         "vgc_debug_cells_device": ([vp, P(C.c_float), C.c_uint32, P(C.c_uint32)], C.c_int),
+        "vgc_occluder_depth": ([vp, C.c_uint32, P(View), vp, C.c_uint32, C.c_uint32, vp], C.c_int),
         "vgc_server_default_options": ([P(ServerOptions)], None),
         "vgc_server_create": ([P(vp), C.c_uint32, P(ServerOptions), P(vp)], C.c_int),
         "vgc_server_submit": ([vp, C.c_uint32, P(View), P(C.c_uint64)], C.c_int),
@@ -175,8 +178,9 @@ def _up(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_uint32))
 
 
-def mesh_struct(data) -> tuple[MeshData, list]:
-    """C view of a VirtualMeshData (keeps the numpy arrays alive in the returned list)."""
+def mesh_struct(data, with_vertices: bool = False) -> tuple[MeshData, list]:
+    """C view of a VirtualMeshData (keeps the numpy arrays alive in the returned list); `with_vertices` adds the
+    positions and meshlet vertex ids the occluder depth pass draws from."""
     keep = [np.ascontiguousarray(data.meshlet_bounds, np.float32), np.ascontiguousarray(data.meshlet_info, np.uint32),
             np.ascontiguousarray(data.meshlet_triangles, np.uint32), np.ascontiguousarray(data.level_ranges, np.uint32),
             np.ascontiguousarray(data.level_errors, np.float32),
@@ -195,6 +199,12 @@ def mesh_struct(data) -> tuple[MeshData, list]:
         m.lod_bounds_sphere[k] = float(data.lod_bounds_sphere[k])
         m.cull_bounds_sphere[k] = float(data.cull_bounds_sphere[k])
         m.bounding_sphere[k] = float(data.bounding_sphere[k])
+    if with_vertices:
+        pos = np.ascontiguousarray(data.positions, np.float32).reshape(-1)
+        mv = np.ascontiguousarray(data.meshlet_vertices, np.uint32)
+        keep += [pos, mv]
+        m.positions, m.vertex_count = _fp(pos), len(pos) // 3
+        m.meshlet_vertices, m.meshlet_vertex_count = _up(mv), len(mv)
     return m, keep
 
 
@@ -255,15 +265,16 @@ class VirtualMesh:
     """An instanced virtual mesh resident on the GPU (VirtualMesh.ts:91-331)."""
 
     def __init__(self, vg: "VirtualGeometry", data, matrices: np.ndarray, max_draw_distance: float = math.inf,
-                 min_pixel_radius: float = 0.0, cast_shadow: bool = False, occlusion_culling: bool = False):
+                 min_pixel_radius: float = 0.0, cast_shadow: bool = False, occlusion_culling: bool = False,
+                 occluder: bool = False):
         self.vg = vg
         self.data = data
         m = np.ascontiguousarray(matrices, np.float32).reshape(-1, 16)
         self.instance_count = len(m)
         self.full_detail_triangles = int(data.stats.get("leafTriangles", 0)) * self.instance_count
         self._flags = dict(max_draw_distance=max_draw_distance, min_pixel_radius=min_pixel_radius, visible=True,
-                           cast_shadow=cast_shadow, occlusion_culling=occlusion_culling)
-        md, keep = mesh_struct(data)
+                           cast_shadow=cast_shadow, occlusion_culling=occlusion_culling, occluder=occluder)
+        md, keep = mesh_struct(data, with_vertices=occluder)
         self.gpu_to_input = np.zeros(self.instance_count, np.uint32)
         slot = C.c_uint32()
         check(lib().vgc_mesh_add(vg.handle, C.byref(md), _fp(m), self.instance_count, C.byref(self._opts()),
@@ -283,6 +294,7 @@ class VirtualMesh:
         o.enabled = 1 if f["visible"] else 0
         o.shadow = 1 if f["cast_shadow"] else 0
         o.occlusion = 1 if f["occlusion_culling"] else 0
+        o.occluder = 1 if f["occluder"] else 0
         return o
 
     def _set(self, **kw):
@@ -473,6 +485,12 @@ class VirtualGeometry:
         mats = np.zeros((ni.value, 16), np.float32)
         check(lib().vgc_debug_scene(self.handle, _fp(cells), nc.value, _fp(mats), ni.value, None, None))
         return cells, mats
+
+    def occluder_depth(self, src_slot: int, camera: Camera, depth_ptr: int, width: int, height: int, stream=None) -> None:
+        """The occluder depth pass (vgc_occluder_depth): slot `src_slot`'s camera cut drawn with `camera` into the
+        device buffer at `depth_ptr` (width x height float32), ready to be this frame's view depth."""
+        v = make_view(camera, self.params)
+        check(lib().vgc_occluder_depth(self.handle, src_slot, C.byref(v), C.c_void_p(depth_ptr), width, height, stream))
 
     def debug_cells_device(self) -> np.ndarray:
         """The device's cell records (8 floats each), as the kernels read them."""
