@@ -10,8 +10,10 @@
 //  * pixel centres (x + 0.5, y + 0.5) inside all three edge functions (edges included) take the depth interpolated
 //    from the vertices' NDC depths (affine in screen space) through an atomic minimum on the float's bits (depth is
 //    >= 0, so the unsigned order is the float order); the image starts at 1 (far);
+//  * each meshlet vertex is transformed once, into the warp's shared-memory vertex buffer (meshlet-local ids < 256);
 //  * small triangles (bounding box of at most kWarpRasterMin pixels) are drawn by their lane; larger ones one at a
-//    time by the whole warp, so a near, screen-filling occluder costs pixels / 32 steps.
+//    time by the whole warp, its lanes over the bounding box's pixels. The atomics' results are unused, so they
+//    do not wait (a load-then-atomic early depth test measured slower: it puts an L2 round trip on every pixel).
 //
 // Every expression rounds step by step in the written order (the library is compiled with -fmad=false), so the
 // oracle's C restatement reproduces the image bit for bit.
@@ -36,24 +38,26 @@ struct ScreenTri {
   int x0, x1, y0, y1;  // pixel bounding box, inclusive
 };
 
-// Setup of one triangle from its clip-space corners; false when it is dropped.
-__device__ __forceinline__ bool setup_triangle(const float c[3][4], float W, float H, ScreenTri &t) {
-  float sx[3], sy[3], sz[3];
+// A vertex in screen space: x, y (pixels, y down), NDC depth; w = 1 when usable (in front of the near plane).
+__device__ __forceinline__ float4 screen_vertex(const float mvp[4][4], float4 v, float W, float H) {
+  float c[4];
 #pragma unroll
-  for (int k = 0; k < 3; k++) {
-    if (!(c[k][3] > 0.0f) || !(c[k][2] >= 0.0f)) return false;
-    const float nx = c[k][0] / c[k][3], ny = c[k][1] / c[k][3], nz = c[k][2] / c[k][3];
-    sx[k] = (nx * 0.5f + 0.5f) * W;
-    sy[k] = (0.5f - ny * 0.5f) * H;
-    sz[k] = nz;
-  }
+  for (int r = 0; r < 4; r++) c[r] = ((mvp[r][0] * v.x + mvp[r][1] * v.y) + mvp[r][2] * v.z) + mvp[r][3];
+  if (!(c[3] > 0.0f) || !(c[2] >= 0.0f)) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const float nx = c[0] / c[3], ny = c[1] / c[3], nz = c[2] / c[3];
+  return make_float4((nx * 0.5f + 0.5f) * W, (0.5f - ny * 0.5f) * H, nz, 1.0f);
+}
+
+// Setup of one triangle from its screen-space corners; false when it is dropped.
+__device__ __forceinline__ bool setup_triangle(float4 v0, float4 v1, float4 v2, float W, float H, ScreenTri &t) {
+  if (v0.w == 0.0f || v1.w == 0.0f || v2.w == 0.0f) return false;  // a corner behind the near plane
   // screen space is y-down: a triangle facing the camera (counter-clockwise in NDC) has a negative area here
-  const float area0 = (sx[1] - sx[0]) * (sy[2] - sy[0]) - (sx[2] - sx[0]) * (sy[1] - sy[0]);
+  const float area0 = (v1.x - v0.x) * (v2.y - v0.y) - (v2.x - v0.x) * (v1.y - v0.y);
   if (!(area0 < 0.0f)) return false;  // back-facing, degenerate or not finite
   // order A, B, C = 0, 2, 1: positive area
-  t.ax = sx[0], t.ay = sy[0], t.az = sz[0];
-  t.bx = sx[2], t.by = sy[2], t.bz = sz[2];
-  t.cx = sx[1], t.cy = sy[1], t.cz = sz[1];
+  t.ax = v0.x, t.ay = v0.y, t.az = v0.z;
+  t.bx = v2.x, t.by = v2.y, t.bz = v2.z;
+  t.cx = v1.x, t.cy = v1.y, t.cz = v1.z;
   t.area = (t.bx - t.ax) * (t.cy - t.ay) - (t.cx - t.ax) * (t.by - t.ay);
   if (!(t.area > 0.0f)) return false;
   float mnx = fminf(fminf(t.ax, t.bx), t.cx), mxx = fmaxf(fmaxf(t.ax, t.bx), t.cx);
@@ -76,7 +80,7 @@ __device__ __forceinline__ void shade_pixel(const ScreenTri &t, int px, int py, 
   if (wa >= 0.0f && wb >= 0.0f && wc >= 0.0f) {
     float z = ((wa * t.az + wb * t.bz) + wc * t.cz) / t.area;
     z = z > 0.0f ? z : 0.0f;  // +0 for rounding below zero (and never -0, whose bits would sort last)
-    atomicMin(depth + (size_t)py * W + px, __float_as_uint(z));
+    atomicMin(depth + (size_t)py * W + px, __float_as_uint(z));  // result unused: a fire-and-forget reduction
   }
 }
 
@@ -86,6 +90,8 @@ __global__ void __launch_bounds__(256) k_depth_clear(uint32_t *depth, size_t n) 
 }
 
 __global__ void __launch_bounds__(128) k_raster_occluders(Scene S, RasterArgs A) {
+  __shared__ float4 verts[4][256];  // per warp: the current meshlet's vertices in screen space (local ids < 256)
+  float4 *sv = verts[threadIdx.x >> 5];
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t n = min(A.counters[VGC_COUNTER_CUT0 + VGC_CUT_SELECTED], A.max_drawn);
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
@@ -109,6 +115,16 @@ __global__ void __launch_bounds__(128) k_raster_occluders(Scene S, RasterArgs A)
                     A.vp[r * 4 + 3] * m[3][k];
     const uint4 info = S.m_info[d.y];
     const uint32_t tris = d.w & 255u, first_tri = info.y / 3, voff = info.w;
+    // the meshlet's vertices (local ids 0 .. the largest its triangles use), each transformed once
+    uint32_t top = 0;
+    for (uint32_t ti = lane; ti < tris; ti += 32) {
+      const uint32_t p = S.m_tris[first_tri + ti];
+      top = max(top, max(p & 255u, max((p >> 8) & 255u, (p >> 16) & 255u)));
+    }
+    top = __reduce_max_sync(0xffffffffu, top);
+    __syncwarp();
+    for (uint32_t v = lane; v <= top; v += 32) sv[v] = screen_vertex(mvp, S.positions[S.m_verts[voff + v]], W, H);
+    __syncwarp();
     uint32_t big = 0;  // this lane's triangles left for the whole warp (bit per round)
     for (uint32_t round = 0; round * 32 < tris; round++) {
       const uint32_t ti = round * 32 + lane;
@@ -116,14 +132,7 @@ __global__ void __launch_bounds__(128) k_raster_occluders(Scene S, RasterArgs A)
       bool ok = false;
       if (ti < tris) {
         const uint32_t p = S.m_tris[first_tri + ti];
-        float c[3][4];
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-          const float4 v = S.positions[S.m_verts[voff + ((p >> (8 * k)) & 255u)]];
-#pragma unroll
-          for (int r = 0; r < 4; r++) c[k][r] = ((mvp[r][0] * v.x + mvp[r][1] * v.y) + mvp[r][2] * v.z) + mvp[r][3];
-        }
-        ok = setup_triangle(c, W, H, t);
+        ok = setup_triangle(sv[p & 255u], sv[(p >> 8) & 255u], sv[(p >> 16) & 255u], W, H, t);
       }
       if (ok && uint32_t(t.x1 - t.x0 + 1) * uint32_t(t.y1 - t.y0 + 1) > kWarpRasterMin) {
         big |= 1u << round;
@@ -140,22 +149,13 @@ __global__ void __launch_bounds__(128) k_raster_occluders(Scene S, RasterArgs A)
         const uint32_t owner = __ffs(pending) - 1;
         pending &= pending - 1;
         ScreenTri t;
-        {  // the owner's setup, recomputed by every lane from the same inputs
-          const uint32_t ti = round * 32 + owner;
-          const uint32_t p = S.m_tris[first_tri + ti];
-          float c[3][4];
-#pragma unroll
-          for (int k = 0; k < 3; k++) {
-            const float4 v = S.positions[S.m_verts[voff + ((p >> (8 * k)) & 255u)]];
-#pragma unroll
-            for (int r = 0; r < 4; r++) c[k][r] = ((mvp[r][0] * v.x + mvp[r][1] * v.y) + mvp[r][2] * v.z) + mvp[r][3];
-          }
-          setup_triangle(c, W, H, t);
-        }
+        const uint32_t p = S.m_tris[first_tri + round * 32 + owner];
+        setup_triangle(sv[p & 255u], sv[(p >> 8) & 255u], sv[(p >> 16) & 255u], W, H, t);
         const uint32_t bw = uint32_t(t.x1 - t.x0 + 1), count = bw * uint32_t(t.y1 - t.y0 + 1);
         for (uint32_t i = lane; i < count; i += 32) shade_pixel(t, t.x0 + int(i % bw), t.y0 + int(i / bw), A.width, A.depth);
       }
     }
+    __syncwarp();  // the vertex buffer is rewritten by the next entry
   }
 }
 
