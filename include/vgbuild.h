@@ -111,6 +111,8 @@ int vgb_gen_depth_image(uint32_t width, uint32_t height, uint32_t quads, float d
 /* 30-bit Morton order of instance sphere centres (GeometryPool.ts:1263-1311 behaviour: stable LSD radix sort).
    matrices: 16 floats column-major per instance; sphere: the mesh's bounding sphere. out: n indices. */
 int vgb_morton_order(const float *matrices, uint32_t n, const float sphere[4], uint32_t *out);
+/* Checksum of a .vgeo file (serialize.ts:429-437) over the u32 words from byte `start`. */
+uint32_t vgb_vgeo_checksum(const uint8_t *bytes, uint64_t length, uint64_t start);
 
 const char *vgb_last_error(void);
 

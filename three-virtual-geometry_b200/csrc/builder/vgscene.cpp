@@ -361,4 +361,18 @@ int vgb_morton_order(const float *m, uint32_t n, const float sphere[4], uint32_t
   return 0;
 }
 
+// The .vgeo container checksum (serialize.ts:429-437): a 32-bit multiplicative hash over the little-endian u32 words
+// from byte `start` (whole words only): h = 0x811c9dc5 ^ words; per word h = (h ^ w) * 0x01000193, h ^= h >> 15.
+uint32_t vgb_vgeo_checksum(const uint8_t *bytes, uint64_t length, uint64_t start) {
+  const uint64_t n = length > start ? (length - start) >> 2 : 0;
+  uint32_t h = 0x811c9dc5u ^ (uint32_t)n;
+  for (uint64_t i = 0; i < n; i++) {
+    uint32_t w;
+    std::memcpy(&w, bytes + start + i * 4, 4);
+    h = (h ^ w) * 0x01000193u;
+    h ^= h >> 15;
+  }
+  return h;
+}
+
 }  // extern "C"

@@ -73,6 +73,8 @@ def _lib() -> C.CDLL:
         lib.vgb_gen_depth_image.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.c_float, C.c_float,
                                             C.c_float, C.c_uint32, P(C.c_float)]
         lib.vgb_morton_order.argtypes = [P(C.c_float), C.c_uint32, P(C.c_float), P(C.c_uint32)]
+        lib.vgb_vgeo_checksum.argtypes = [C.c_char_p, C.c_uint64, C.c_uint64]
+        lib.vgb_vgeo_checksum.restype = C.c_uint32
         lib.vgb_mulberry32_next.argtypes = [P(C.c_uint32)]
         lib.vgb_mulberry32_next.restype = C.c_uint32
         lib.vgb_perlin3.argtypes = [C.c_uint32, C.c_float, C.c_float, C.c_float]
@@ -112,6 +114,7 @@ class VirtualMeshData:
     replacement_start: np.ndarray
     replacement_indices: np.ndarray
     stats: dict = field(default_factory=dict)
+    extra: dict = field(default_factory=dict)  # fields this builder does not produce (normals, colors, uvs, ...)
 
     @property
     def level_count(self) -> int:
