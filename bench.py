@@ -42,7 +42,10 @@ def parse():
     ap.add_argument("--poses", type=int, default=32, help="views per step (the spline's pose count)")
     ap.add_argument("--profile-case", action="store_true", help="small case for an ncu capture (not a bench line)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bound of the CPU-baseline sample")
-    ap.add_argument("--no-extras", action="store_true", help="skip the large-world and serving sections")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batching, occluder, large-world and serving sections")
+    ap.add_argument("--extras", default="batching,occluders,large_world,serve",
+                    help="comma-separated sections to run after the headline line's measurement")
     ap.add_argument("--serve-rate", type=float, default=10_000.0, help="Poisson request rate of the serving section")
     ap.add_argument("--serve-requests", type=int, default=20_000)
     return ap.parse_args()
@@ -389,10 +392,15 @@ def run_ours(args, world, rank, local):
     )
     vg.dispose()
     if world == 1 and args.config == "ruins" and not args.no_extras:
-        line["batching"] = run_batching(spec, args, flush, stream)
-        line["occluders"] = run_occluders(spec, args, flush, stream)
-        line["large_world"] = run_large_world(spec, args, flush, stream)
-        line["serve"] = run_serve(spec, args)
+        extras = set(args.extras.split(","))
+        if "batching" in extras:
+            line["batching"] = run_batching(spec, args, flush, stream)
+        if "occluders" in extras:
+            line["occluders"] = run_occluders(spec, args, flush, stream)
+        if "large_world" in extras:
+            line["large_world"] = run_large_world(spec, args, flush, stream)
+        if "serve" in extras:
+            line["serve"] = run_serve(spec, args)
     if rank == 0:
         vps, cores, sample = cpu_baseline(spec, args.cpu_seconds, occl)
         line["cpu_baseline"] = dict(value=vps, unit="views/s", cores=cores, kind="port", sample=sample)

@@ -72,3 +72,49 @@ def test_two_pass_occlusion_matches_the_oracle(occluding):
         open_res, _ = h.oracle(now, engine.ViewParams(error_threshold=1.0))
         culled += len(open_res["entries"][0]) - len(lists[0])
     assert culled > 0, "the previous frame's occluders hide part of this frame's cut"
+
+
+def large_triangles(h, entries, cam, width, height, min_pixels=1024):
+    """Front-facing part-0 triangles of `entries` in front of the camera whose pixel bounding box at width x height
+    exceeds `min_pixels` (float64 estimate): those the rasterizer hands to its grid-wide tile pass."""
+    e = entries[(entries[:, 3] & 0xFFFF00) == (255 << 16)]
+    vp = np.asarray(cam.proj, np.float64).reshape(4, 4).T @ np.asarray(cam.view, np.float64).reshape(4, 4).T
+    bases = np.cumsum([0] + [len(d.meshlet_info) // 4 for d in h.spec.meshes])
+    found = 0
+    for inst, mid, _, w in e:
+        k = int(np.searchsorted(bases, mid, side="right")) - 1
+        d = h.spec.meshes[k]
+        info = np.asarray(d.meshlet_info, np.uint32).reshape(-1, 4)[mid - bases[k]]
+        packed = np.asarray(d.meshlet_triangles, np.uint32)[info[1] // 3: info[1] // 3 + (w & 255)]
+        local = np.stack([packed & 255, (packed >> 8) & 255, (packed >> 16) & 255], 1)
+        ids = np.asarray(d.meshlet_vertices, np.uint32)[info[3] + local]
+        p = np.asarray(d.positions, np.float64).reshape(-1, 3)[ids]
+        m = np.asarray(h.mats[inst], np.float64).reshape(4, 4).T
+        clip = np.einsum("ij,tvj->tvi", vp @ m, np.concatenate([p, np.ones(p.shape[:2] + (1,))], 2))
+        ok = (clip[..., 3] > 0).all(1) & (clip[..., 2] >= 0).all(1)
+        sx = (clip[..., 0] / clip[..., 3] * 0.5 + 0.5) * width
+        sy = (0.5 - clip[..., 1] / clip[..., 3] * 0.5) * height
+        area = (sx[:, 1] - sx[:, 0]) * (sy[:, 2] - sy[:, 0]) - (sx[:, 2] - sx[:, 0]) * (sy[:, 1] - sy[:, 0])
+        bw = np.clip(sx.max(1), 0, width) - np.clip(sx.min(1), 0, width)
+        bh = np.clip(sy.max(1), 0, height) - np.clip(sy.min(1), 0, height)
+        found += int((ok & (area < 0) & (bw * bh > min_pixels)).sum())
+    return found
+
+
+def test_large_triangles_match_the_oracle(occluding):
+    """A coarse cut drawn at 1920x1080: many triangles cover thousands of pixels, and those go through the tile pass;
+    the image is still the oracle's bit for bit."""
+    import torch
+    h = occluding
+    w2, h2 = 1920, 1080
+    cam = h.spec.cameras[1]
+    h.gpu(cam, engine.ViewParams(error_threshold=24.0), slot=0)
+    now = moved(cam, 0.5, 0.02)
+    entries = h.vg.draw_list(0, 0)
+    assert large_triangles(h, entries, now, w2, h2) > 50, "the case reaches the tile pass"
+    d = torch.empty((h2, w2), dtype=torch.float32, device="cuda")
+    h.vg.occluder_depth(0, now, d.data_ptr(), w2, h2)
+    torch.cuda.synchronize()
+    got = d.cpu().numpy()
+    want = O.occluder_depth(h.spec.meshes, [True] * len(h.spec.meshes), h.mats, h.inst_slot, entries, now, w2, h2)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), f"{int((got != want).sum())} pixels differ"

@@ -12,8 +12,11 @@
 //    >= 0, so the unsigned order is the float order); the image starts at 1 (far);
 //  * each meshlet vertex is transformed once, into the warp's shared-memory vertex buffer (meshlet-local ids < 256);
 //  * small triangles (bounding box of at most kWarpRasterMin pixels) are drawn by their lane; larger ones one at a
-//    time by the whole warp, its lanes over the bounding box's pixels. The atomics' results are unused, so they
-//    do not wait (a load-then-atomic early depth test measured slower: it puts an L2 round trip on every pixel).
+//    time by the whole warp, its lanes over the bounding box's pixels; the largest (more than kTileRasterMin) are
+//    queued as 32 x 16 pixel tiles of their bounding box that a second kernel spreads over the whole grid, so that
+//    a few near triangles covering much of the image do not leave single warps drawing while the rest idle. The
+//    atomics' results are unused, so they do not wait (a load-then-atomic early depth test measured slower: it
+//    puts an L2 round trip on every pixel). The image is the minimum over all drawn pixels, whatever the order.
 //
 // Every expression rounds step by step in the written order (the library is compiled with -fmad=false), so the
 // oracle's C restatement reproduces the image bit for bit.
@@ -22,7 +25,12 @@
 
 namespace {
 
-constexpr uint32_t kWarpRasterMin = 64;  // bounding-box pixels from which the whole warp draws a triangle
+constexpr uint32_t kWarpRasterMin = 64;     // bounding-box pixels from which the whole warp draws a triangle
+constexpr uint32_t kTileRasterMin = 1024;   // ... from which its tiles go to the grid-wide tile pass
+constexpr uint32_t kTileW = 32, kTileH = 16;
+constexpr uint32_t kTileTris = 1u << 16;    // capacity of the tile pass: triangles
+constexpr uint32_t kTileUnits = 1u << 20;   // ... and tiles
+constexpr uint32_t kNoTri = 0xffffffffu;    // an empty tile record
 
 struct RasterArgs {
   float vp[16];  // P * V, row-major 4x4 (float of the double product)
@@ -31,6 +39,11 @@ struct RasterArgs {
   const uint4 *draw_list;      // cut 0 entries of the source slot
   const uint32_t *counters;    // its counter header
   uint32_t max_drawn;
+  // tile pass: tile_ctl[0] = queued triangles, tile_ctl[2..3] = queued tiles (64-bit); triangle records (4 float4
+  // each: the ScreenTri and its tile columns); tile records (triangle, tile index in its bounding box, row-major)
+  uint32_t *tile_ctl;
+  float4 *tile_tris;
+  uint2 *tiles;
 };
 
 struct ScreenTri {
@@ -84,9 +97,38 @@ __device__ __forceinline__ void shade_pixel(const ScreenTri &t, int px, int py, 
   }
 }
 
-__global__ void __launch_bounds__(256) k_depth_clear(uint32_t *depth, size_t n) {
+__global__ void __launch_bounds__(256) k_depth_clear(uint32_t *depth, size_t n, uint32_t *tile_ctl) {
+  if (blockIdx.x == 0 && threadIdx.x < 4) tile_ctl[threadIdx.x] = 0;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     depth[i] = 0x3f800000u;  // 1.0f
+}
+
+// Queues triangle t's bounding box as tiles for k_raster_tiles (whole warp, t the same in every lane); false when
+// the tile pass is full (its reserved tile records are then left empty and the warp draws t itself).
+__device__ bool queue_tiles(const RasterArgs &A, const ScreenTri &t, uint32_t bw, uint32_t bh, uint32_t lane) {
+  const uint32_t tx = (bw + kTileW - 1) / kTileW, n = tx * ((bh + kTileH - 1) / kTileH);
+  uint32_t tri = 0;
+  unsigned long long at = 0;
+  if (lane == 0) {
+    tri = atomicAdd(A.tile_ctl, 1u);
+    if (tri < kTileTris) at = atomicAdd(reinterpret_cast<unsigned long long *>(A.tile_ctl + 2), (unsigned long long)n);
+  }
+  tri = __shfl_sync(0xffffffffu, tri, 0);
+  if (tri >= kTileTris) return false;
+  at = __shfl_sync(0xffffffffu, at, 0);
+  if (at + n > kTileUnits) {
+    for (unsigned long long i = at + lane; i < kTileUnits; i += 32) A.tiles[i] = make_uint2(kNoTri, 0u);
+    return false;
+  }
+  float4 *r = A.tile_tris + (size_t)tri * 4;
+  if (lane == 0) {
+    r[0] = make_float4(t.ax, t.ay, t.az, t.bx);
+    r[1] = make_float4(t.by, t.bz, t.cx, t.cy);
+    r[2] = make_float4(t.cz, t.area, __int_as_float(t.x0), __int_as_float(t.y0));
+    r[3] = make_float4(__int_as_float(t.x1), __int_as_float(t.y1), __uint_as_float(tx), 0.0f);
+  }
+  for (uint32_t i = lane; i < n; i += 32) A.tiles[at + i] = make_uint2(tri, i);
+  return true;
 }
 
 __global__ void __launch_bounds__(128) k_raster_occluders(Scene S, RasterArgs A) {
@@ -151,11 +193,36 @@ __global__ void __launch_bounds__(128) k_raster_occluders(Scene S, RasterArgs A)
         ScreenTri t;
         const uint32_t p = S.m_tris[first_tri + round * 32 + owner];
         setup_triangle(sv[p & 255u], sv[(p >> 8) & 255u], sv[(p >> 16) & 255u], W, H, t);
-        const uint32_t bw = uint32_t(t.x1 - t.x0 + 1), count = bw * uint32_t(t.y1 - t.y0 + 1);
+        const uint32_t bw = uint32_t(t.x1 - t.x0 + 1), bh = uint32_t(t.y1 - t.y0 + 1), count = bw * bh;
+        if (count > kTileRasterMin && queue_tiles(A, t, bw, bh, lane)) continue;
         for (uint32_t i = lane; i < count; i += 32) shade_pixel(t, t.x0 + int(i % bw), t.y0 + int(i / bw), A.width, A.depth);
       }
     }
     __syncwarp();  // the vertex buffer is rewritten by the next entry
+  }
+}
+
+// The tile pass: one warp per queued 32 x 16 tile of a large triangle, a lane per column.
+__global__ void __launch_bounds__(128) k_raster_tiles(RasterArgs A) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t n = (uint32_t)min(*reinterpret_cast<const unsigned long long *>(A.tile_ctl + 2),
+                                   (unsigned long long)kTileUnits);
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n; u += warps) {
+    const uint2 tile = A.tiles[u];
+    if (tile.x == kNoTri) continue;
+    const float4 *r = A.tile_tris + (size_t)tile.x * 4;
+    const float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
+    ScreenTri t;
+    t.ax = r0.x, t.ay = r0.y, t.az = r0.z, t.bx = r0.w;
+    t.by = r1.x, t.bz = r1.y, t.cx = r1.z, t.cy = r1.w;
+    t.cz = r2.x, t.area = r2.y, t.x0 = __float_as_int(r2.z), t.y0 = __float_as_int(r2.w);
+    t.x1 = __float_as_int(r3.x), t.y1 = __float_as_int(r3.y);
+    const uint32_t tx = __float_as_uint(r3.z);
+    const int px = t.x0 + int((tile.y % tx) * kTileW + lane), py0 = t.y0 + int((tile.y / tx) * kTileH);
+    if (px > t.x1) continue;
+    const int py1 = min(t.y1, py0 + int(kTileH) - 1);
+    for (int py = py0; py <= py1; py++) shade_pixel(t, px, py, A.width, A.depth);
   }
 }
 
@@ -184,12 +251,20 @@ extern "C" int vgc_occluder_depth(vgc_context *ctx, uint32_t src_slot, const vgc
   A.draw_list = (const uint4 *)ctx->d_draw.ptr + (size_t)src_slot * 2 * ctx->opts.max_meshlets;
   A.counters = (const uint32_t *)ctx->d_counters.ptr + (size_t)src_slot * ctx->counter_words;
   A.max_drawn = ctx->opts.max_meshlets;
+  // the tile pass's buffers: control words, triangle records, tile records
+  const size_t tri_bytes = (size_t)kTileTris * 64, tile_bytes = (size_t)kTileUnits * 8;
+  if ((rc = dev_alloc(ctx, ctx->d_raster, 256 + tri_bytes + tile_bytes))) return rc;  // once per context
+  A.tile_ctl = (uint32_t *)ctx->d_raster.ptr;
+  A.tile_tris = (float4 *)((char *)ctx->d_raster.ptr + 256);
+  A.tiles = (uint2 *)((char *)ctx->d_raster.ptr + 256 + tri_bytes);
   const size_t pixels = (size_t)width * height;
   k_depth_clear<<<(unsigned)std::min<size_t>((pixels + 255) / 256, (size_t)ctx->sm_count * 16), 256, 0, st>>>(
-      A.depth, pixels);
+      A.depth, pixels, A.tile_ctl);
   CUDA_TRY(cudaGetLastError());
   if (ctx->positions.empty()) return VGC_OK;  // no mesh carries vertex data: nothing is an occluder
   k_raster_occluders<<<ctx->sm_count * 8, 128, 0, st>>>(scene_of(ctx), A);
+  CUDA_TRY(cudaGetLastError());
+  k_raster_tiles<<<ctx->sm_count * 8, 128, 0, st>>>(A);
   CUDA_TRY(cudaGetLastError());
   return VGC_OK;
 }
