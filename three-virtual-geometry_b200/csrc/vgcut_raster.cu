@@ -11,11 +11,16 @@
 //    from the vertices' NDC depths (affine in screen space) through an atomic minimum on the float's bits (depth is
 //    >= 0, so the unsigned order is the float order); the image starts at 1 (far);
 //  * each meshlet vertex is transformed once, into the warp's shared-memory vertex buffer (meshlet-local ids < 256);
-//  * small triangles (bounding box of at most kWarpRasterMin pixels) are drawn by their lane; larger ones one at a
-//    time by the whole warp, its lanes over the bounding box's pixels; the largest (more than kTileRasterMin) are
-//    queued as 32 x 16 pixel tiles of their bounding box that a second kernel spreads over the whole grid, so that
-//    a few near triangles covering much of the image do not leave single warps drawing while the rest idle. The
-//    atomics' results are unused, so they do not wait (a load-then-atomic early depth test measured slower: it
+//    a meshlet's loads are issued together (its triangles, then its vertex ids, then positions, 128 at a time) and
+//    the warp's next entry is fetched while it draws this one: every step of this pass waits on memory;
+//  * triangles are sorted by the pixels of their bounding box: small ones (at most kLaneRasterMax) are drawn at once
+//    by their lane; medium ones (at most kWarpRasterMax) are queued, one atomic per warp and round of 32 triangles
+//    on one of kSubQueues counters, and drawn by the second kernel, a warp per triangle; larger ones are queued as
+//    32 x 16 pixel tiles of their bounding box, a warp per tile. The second kernel spreads both over the whole
+//    grid: a meshlet close to the camera, with a hundred triangles of a few hundred pixels each, would otherwise
+//    keep one warp drawing long after the rest have finished. When a queue is full its triangles are drawn by the
+//    warp that set them up;
+//  * the atomics' results are unused, so they do not wait (a load-then-atomic early depth test measured slower: it
 //    puts an L2 round trip on every pixel). The image is the minimum over all drawn pixels, whatever the order.
 //
 // Every expression rounds step by step in the written order (the library is compiled with -fmad=false), so the
@@ -25,12 +30,15 @@
 
 namespace {
 
-constexpr uint32_t kWarpRasterMin = 64;     // bounding-box pixels from which the whole warp draws a triangle
-constexpr uint32_t kTileRasterMin = 1024;   // ... from which its tiles go to the grid-wide tile pass
+constexpr uint32_t kLaneRasterMax = 16;     // bounding-box pixels up to which a triangle is drawn by its lane
+constexpr uint32_t kWarpRasterMax = 1024;   // ... by one warp of the second kernel; beyond, as tiles
 constexpr uint32_t kTileW = 32, kTileH = 16;
-constexpr uint32_t kTileTris = 1u << 16;    // capacity of the tile pass: triangles
-constexpr uint32_t kTileUnits = 1u << 20;   // ... and tiles
-constexpr uint32_t kNoTri = 0xffffffffu;    // an empty tile record
+constexpr uint32_t kQueuedMedium = 1u << 18;  // queue capacities: medium triangles,
+constexpr uint32_t kSubQueues = 256;          //   in sub-queues (record i of sub-queue q at i * kSubQueues + q),
+constexpr uint32_t kCtlWords = 4 + kSubQueues;
+constexpr uint32_t kQueuedLarge = 1u << 16;   // large triangles,
+constexpr uint32_t kTileUnits = 1u << 20;     // and their tiles
+constexpr uint32_t kNoTri = 0xffffffffu;      // an empty tile record
 
 struct RasterArgs {
   float vp[16];  // P * V, row-major 4x4 (float of the double product)
@@ -39,10 +47,12 @@ struct RasterArgs {
   const uint4 *draw_list;      // cut 0 entries of the source slot
   const uint32_t *counters;    // its counter header
   uint32_t max_drawn;
-  // tile pass: tile_ctl[0] = queued triangles, tile_ctl[2..3] = queued tiles (64-bit); triangle records (4 float4
-  // each: the ScreenTri and its tile columns); tile records (triangle, tile index in its bounding box, row-major)
-  uint32_t *tile_ctl;
-  float4 *tile_tris;
+  // queues: ctl[1] = large triangles, ctl[2..3] = tiles (64-bit), ctl[4 + q] = medium triangles of sub-queue q;
+  // triangle records (4 float4 each: the ScreenTri and, for large ones, its tile columns); tile records (large
+  // triangle, tile index in its bounding box, row-major)
+  uint32_t *ctl;
+  float4 *medium;
+  float4 *large;
   uint2 *tiles;
 };
 
@@ -97,55 +107,81 @@ __device__ __forceinline__ void shade_pixel(const ScreenTri &t, int px, int py, 
   }
 }
 
-__global__ void __launch_bounds__(256) k_depth_clear(uint32_t *depth, size_t n, uint32_t *tile_ctl) {
-  if (blockIdx.x == 0 && threadIdx.x < 4) tile_ctl[threadIdx.x] = 0;
+__device__ __forceinline__ void write_record(float4 *r, const ScreenTri &t, uint32_t extra) {
+  r[0] = make_float4(t.ax, t.ay, t.az, t.bx);
+  r[1] = make_float4(t.by, t.bz, t.cx, t.cy);
+  r[2] = make_float4(t.cz, t.area, __int_as_float(t.x0), __int_as_float(t.y0));
+  r[3] = make_float4(__int_as_float(t.x1), __int_as_float(t.y1), __uint_as_float(extra), 0.0f);
+}
+
+__device__ __forceinline__ ScreenTri read_record(const float4 *r, uint32_t &extra) {
+  const float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
+  ScreenTri t;
+  t.ax = r0.x, t.ay = r0.y, t.az = r0.z, t.bx = r0.w;
+  t.by = r1.x, t.bz = r1.y, t.cx = r1.z, t.cy = r1.w;
+  t.cz = r2.x, t.area = r2.y, t.x0 = __float_as_int(r2.z), t.y0 = __float_as_int(r2.w);
+  t.x1 = __float_as_int(r3.x), t.y1 = __float_as_int(r3.y);
+  extra = __float_as_uint(r3.z);
+  return t;
+}
+
+// The whole warp over t's bounding box, 32 consecutive pixels (row-major) per step.
+__device__ __forceinline__ void warp_draw(const ScreenTri &t, uint32_t lane, uint32_t W, uint32_t *depth) {
+  const uint32_t bw = uint32_t(t.x1 - t.x0 + 1), count = bw * uint32_t(t.y1 - t.y0 + 1);
+  const uint32_t q = 32 / bw, r = 32 % bw;  // a step of 32 pixels: q rows and r columns
+  uint32_t x = lane % bw, y = lane / bw;
+  for (uint32_t i = lane; i < count; i += 32) {
+    shade_pixel(t, t.x0 + int(x), t.y0 + int(y), W, depth);
+    x += r, y += q;
+    if (x >= bw) x -= bw, y++;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_depth_clear(uint32_t *depth, size_t n, uint32_t *ctl) {
+  if (blockIdx.x == 0)
+    for (uint32_t i = threadIdx.x; i < kCtlWords; i += blockDim.x) ctl[i] = 0;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     depth[i] = 0x3f800000u;  // 1.0f
 }
 
-// Queues triangle t's bounding box as tiles for k_raster_tiles (whole warp, t the same in every lane); false when
-// the tile pass is full (its reserved tile records are then left empty and the warp draws t itself).
-__device__ bool queue_tiles(const RasterArgs &A, const ScreenTri &t, uint32_t bw, uint32_t bh, uint32_t lane) {
-  const uint32_t tx = (bw + kTileW - 1) / kTileW, n = tx * ((bh + kTileH - 1) / kTileH);
-  uint32_t tri = 0;
-  unsigned long long at = 0;
-  if (lane == 0) {
-    tri = atomicAdd(A.tile_ctl, 1u);
-    if (tri < kTileTris) at = atomicAdd(reinterpret_cast<unsigned long long *>(A.tile_ctl + 2), (unsigned long long)n);
+__device__ __forceinline__ uint32_t warp_scan_incl(uint32_t v) {
+  const uint32_t lane = threadIdx.x & 31;
+#pragma unroll
+  for (uint32_t o = 1; o < 32; o <<= 1) {
+    const uint32_t u = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += u;
   }
-  tri = __shfl_sync(0xffffffffu, tri, 0);
-  if (tri >= kTileTris) return false;
-  at = __shfl_sync(0xffffffffu, at, 0);
-  if (at + n > kTileUnits) {
-    for (unsigned long long i = at + lane; i < kTileUnits; i += 32) A.tiles[i] = make_uint2(kNoTri, 0u);
-    return false;
-  }
-  float4 *r = A.tile_tris + (size_t)tri * 4;
-  if (lane == 0) {
-    r[0] = make_float4(t.ax, t.ay, t.az, t.bx);
-    r[1] = make_float4(t.by, t.bz, t.cx, t.cy);
-    r[2] = make_float4(t.cz, t.area, __int_as_float(t.x0), __int_as_float(t.y0));
-    r[3] = make_float4(__int_as_float(t.x1), __int_as_float(t.y1), __uint_as_float(tx), 0.0f);
-  }
-  for (uint32_t i = lane; i < n; i += 32) A.tiles[at + i] = make_uint2(tri, i);
-  return true;
+  return v;
 }
 
-__global__ void __launch_bounds__(128) k_raster_occluders(Scene S, RasterArgs A) {
-  __shared__ float4 verts[4][256];  // per warp: the current meshlet's vertices in screen space (local ids < 256)
+__global__ void __launch_bounds__(128, 6) k_raster_occluders(Scene S, RasterArgs A) {
+  __shared__ float4 verts[4][256];     // per warp: the current meshlet's vertices in screen space (local ids < 256)
+  __shared__ uint32_t packed[4][128];  // ... and its packed triangles
   float4 *sv = verts[threadIdx.x >> 5];
+  uint32_t *st = packed[threadIdx.x >> 5];
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t n = min(A.counters[VGC_COUNTER_CUT0 + VGC_CUT_SELECTED], A.max_drawn);
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
   const float W = float(A.width), H = float(A.height);
-  for (uint32_t e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < n; e += warps) {
-    const uint4 d = A.draw_list[e];
+  const uint32_t sub = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) % kSubQueues;  // this warp's medium sub-queue
+  // Each step waits on memory several times (entry, instance and meshlet, vertices, triangles): the loads of a step
+  // are issued together, and the next entry is fetched while this one is drawn.
+  uint32_t e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  uint4 next = e < n ? A.draw_list[e] : make_uint4(0u, 0u, 0u, 0u);
+  for (; e < n; e += warps) {
+    const uint4 d = next;
+    if (e + warps < n) next = A.draw_list[e + warps];
     if ((d.w & 0xffff00u) != (255u << 16)) continue;  // part 1 (blended): not an occluder
     const uint32_t slot = S.inst_slot[d.x];
-    if (!S.meshes[slot].occluder) continue;
-    // M's rows from the instance's columns, then clip = (P V) M p
     const float4 *col = S.inst + (size_t)d.x * 4;
     const float4 c0 = col[0], c1 = col[1], c2 = col[2], c3 = col[3];
+    const uint4 info = S.m_info[d.y];
+    if (!S.meshes[slot].occluder) continue;
+    const uint32_t tris = d.w & 255u, first_tri = info.y / 3, voff = info.w;
+    uint32_t pk[4];  // the meshlet's packed triangles (at most 128), loaded at once
+#pragma unroll
+    for (uint32_t r = 0; r < 4; r++) pk[r] = r * 32 + lane < tris ? S.m_tris[first_tri + r * 32 + lane] : 0u;
+    // M's rows from the instance's columns, then clip = (P V) M p
     const float m[4][4] = {{c0.x, c1.x, c2.x, c3.x}, {c0.y, c1.y, c2.y, c3.y}, {c0.z, c1.z, c2.z, c3.z},
                            {c0.w, c1.w, c2.w, c3.w}};
     float mvp[4][4];
@@ -155,70 +191,126 @@ __global__ void __launch_bounds__(128) k_raster_occluders(Scene S, RasterArgs A)
       for (int k = 0; k < 4; k++)
         mvp[r][k] = ((A.vp[r * 4] * m[0][k] + A.vp[r * 4 + 1] * m[1][k]) + A.vp[r * 4 + 2] * m[2][k]) +
                     A.vp[r * 4 + 3] * m[3][k];
-    const uint4 info = S.m_info[d.y];
-    const uint32_t tris = d.w & 255u, first_tri = info.y / 3, voff = info.w;
-    // the meshlet's vertices (local ids 0 .. the largest its triangles use), each transformed once
+    // the meshlet's vertices (local ids 0 .. the largest its triangles use), each transformed once, 128 at a time
     uint32_t top = 0;
-    for (uint32_t ti = lane; ti < tris; ti += 32) {
-      const uint32_t p = S.m_tris[first_tri + ti];
-      top = max(top, max(p & 255u, max((p >> 8) & 255u, (p >> 16) & 255u)));
-    }
+#pragma unroll
+    for (uint32_t r = 0; r < 4; r++)
+      top = max(top, max(pk[r] & 255u, max((pk[r] >> 8) & 255u, (pk[r] >> 16) & 255u)));
     top = __reduce_max_sync(0xffffffffu, top);
     __syncwarp();
-    for (uint32_t v = lane; v <= top; v += 32) sv[v] = screen_vertex(mvp, S.positions[S.m_verts[voff + v]], W, H);
+#pragma unroll
+    for (uint32_t r = 0; r < 4; r++) st[r * 32 + lane] = pk[r];
+    for (uint32_t base = 0; base <= top; base += 128) {
+      uint32_t id[4];
+#pragma unroll
+      for (uint32_t k = 0; k < 4; k++) id[k] = base + k * 32 + lane <= top ? S.m_verts[voff + base + k * 32 + lane] : 0u;
+      float4 pos[4];
+#pragma unroll
+      for (uint32_t k = 0; k < 4; k++) pos[k] = base + k * 32 + lane <= top ? S.positions[id[k]] : make_float4(0, 0, 0, 1);
+#pragma unroll
+      for (uint32_t k = 0; k < 4; k++)
+        if (base + k * 32 + lane <= top) sv[base + k * 32 + lane] = screen_vertex(mvp, pos[k], W, H);
+    }
     __syncwarp();
-    uint32_t big = 0;  // this lane's triangles left for the whole warp (bit per round)
+    uint32_t big = 0;  // this lane's triangles left for the whole warp here (bit per round)
     for (uint32_t round = 0; round * 32 < tris; round++) {
-      const uint32_t ti = round * 32 + lane;
+      const uint32_t ti = round * 32 + lane, p = st[ti];
       ScreenTri t;
       bool ok = false;
-      if (ti < tris) {
-        const uint32_t p = S.m_tris[first_tri + ti];
-        ok = setup_triangle(sv[p & 255u], sv[(p >> 8) & 255u], sv[(p >> 16) & 255u], W, H, t);
+      if (ti < tris) ok = setup_triangle(sv[p & 255u], sv[(p >> 8) & 255u], sv[(p >> 16) & 255u], W, H, t);
+      const uint32_t px = ok ? uint32_t(t.x1 - t.x0 + 1) * uint32_t(t.y1 - t.y0 + 1) : 0u;
+      // medium and large triangles: one reservation of each kind for the warp's round, issued before this round's
+      // small triangles are drawn so that the atomics' round trips overlap the drawing
+      const bool medium = px > kLaneRasterMax && px <= kWarpRasterMax, large = px > kWarpRasterMax;
+      const uint32_t mm = __ballot_sync(0xffffffffu, medium), lm = __ballot_sync(0xffffffffu, large);
+      const uint32_t tx = large ? (uint32_t(t.x1 - t.x0) + kTileW) / kTileW : 0u;
+      const uint32_t nt = large ? tx * ((uint32_t(t.y1 - t.y0) + kTileH) / kTileH) : 0u;
+      uint32_t ts = 0, total = 0;
+      if (lm) {
+        ts = warp_scan_incl(nt) - nt;
+        total = __shfl_sync(0xffffffffu, ts + nt, 31);
       }
-      if (ok && uint32_t(t.x1 - t.x0 + 1) * uint32_t(t.y1 - t.y0 + 1) > kWarpRasterMin) {
-        big |= 1u << round;
-        ok = false;
+      uint32_t at_m = 0, tri = 0;
+      unsigned long long at_t = 0;
+      if (lane == 0) {
+        if (mm) at_m = atomicAdd(A.ctl + 4 + sub, __popc(mm));
+        if (lm) {
+          tri = atomicAdd(A.ctl + 1, __popc(lm));
+          at_t = atomicAdd(reinterpret_cast<unsigned long long *>(A.ctl + 2), (unsigned long long)total);
+        }
       }
-      if (ok)
+      if (px && px <= kLaneRasterMax)
         for (int py = t.y0; py <= t.y1; py++)
-          for (int px = t.x0; px <= t.x1; px++) shade_pixel(t, px, py, A.width, A.depth);
+          for (int x = t.x0; x <= t.x1; x++) shade_pixel(t, x, py, A.width, A.depth);
+      if (mm) {
+        const uint32_t at = __shfl_sync(0xffffffffu, at_m, 0) + __popc(mm & ((1u << lane) - 1u));
+        if (medium && at < kQueuedMedium / kSubQueues)
+          write_record(A.medium + ((size_t)at * kSubQueues + sub) * 4, t, 0u);
+        else if (medium) big |= 1u << round;  // the queue is full: drawn below
+      }
+      if (lm) {
+        tri = __shfl_sync(0xffffffffu, tri, 0);
+        at_t = __shfl_sync(0xffffffffu, at_t, 0);
+        if (tri + __popc(lm) <= kQueuedLarge && at_t + total <= kTileUnits) {
+          const uint32_t mine = tri + __popc(lm & ((1u << lane) - 1u));
+          if (large) write_record(A.large + (size_t)mine * 4, t, tx);
+          for (uint32_t rest = lm; rest; rest &= rest - 1) {  // the tile records, a triangle at a time
+            const uint32_t j = __ffs(rest) - 1;
+            const uint32_t nj = __shfl_sync(0xffffffffu, nt, j), sj = __shfl_sync(0xffffffffu, ts, j);
+            const uint32_t tj = __shfl_sync(0xffffffffu, mine, j);
+            for (uint32_t i = lane; i < nj; i += 32) A.tiles[at_t + sj + i] = make_uint2(tj, i);
+          }
+        } else {  // a queue is full: reserved tile slots below its capacity become empty records, drawn below
+          for (unsigned long long i = at_t + lane; i < at_t + total && i < kTileUnits; i += 32)
+            A.tiles[i] = make_uint2(kNoTri, 0u);
+          if (large) big |= 1u << round;
+        }
+      }
     }
-    // large triangles: one at a time, the warp's lanes over its pixels
+    // triangles the queues had no room for: one at a time, the whole warp
     for (uint32_t round = 0; round * 32 < tris; round++) {
       uint32_t pending = __ballot_sync(0xffffffffu, (big >> round) & 1u);
       while (pending) {
         const uint32_t owner = __ffs(pending) - 1;
         pending &= pending - 1;
         ScreenTri t;
-        const uint32_t p = S.m_tris[first_tri + round * 32 + owner];
+        const uint32_t p = st[round * 32 + owner];
         setup_triangle(sv[p & 255u], sv[(p >> 8) & 255u], sv[(p >> 16) & 255u], W, H, t);
-        const uint32_t bw = uint32_t(t.x1 - t.x0 + 1), bh = uint32_t(t.y1 - t.y0 + 1), count = bw * bh;
-        if (count > kTileRasterMin && queue_tiles(A, t, bw, bh, lane)) continue;
-        for (uint32_t i = lane; i < count; i += 32) shade_pixel(t, t.x0 + int(i % bw), t.y0 + int(i / bw), A.width, A.depth);
+        warp_draw(t, lane, A.width, A.depth);
       }
     }
-    __syncwarp();  // the vertex buffer is rewritten by the next entry
+    __syncwarp();  // the vertex and triangle buffers are rewritten by the next entry
   }
 }
 
-// The tile pass: one warp per queued 32 x 16 tile of a large triangle, a lane per column.
-__global__ void __launch_bounds__(128) k_raster_tiles(RasterArgs A) {
+// The queued triangles, spread over the whole grid: a warp per medium triangle, then a warp per tile of a large one
+// (a lane per column of the tile).
+__global__ void __launch_bounds__(128) k_raster_queued(RasterArgs A) {
+  __shared__ uint32_t counts[kSubQueues];  // medium triangles per sub-queue
+  __shared__ uint32_t most;
+  if (threadIdx.x == 0) most = 0;
+  __syncthreads();
+  for (uint32_t q = threadIdx.x; q < kSubQueues; q += blockDim.x) {
+    counts[q] = min(A.ctl[4 + q], kQueuedMedium / kSubQueues);
+    atomicMax(&most, counts[q]);
+  }
+  __syncthreads();
   const uint32_t lane = threadIdx.x & 31;
-  const uint32_t n = (uint32_t)min(*reinterpret_cast<const unsigned long long *>(A.tile_ctl + 2),
-                                   (unsigned long long)kTileUnits);
+  // medium records are interleaved: slot u holds record u / kSubQueues of sub-queue u % kSubQueues
+  const uint32_t n_medium = most * kSubQueues;
+  const uint32_t n = n_medium + (uint32_t)min(*reinterpret_cast<const unsigned long long *>(A.ctl + 2),
+                                              (unsigned long long)kTileUnits);
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n; u += warps) {
-    const uint2 tile = A.tiles[u];
+    uint32_t tx;
+    if (u < n_medium) {
+      if (u / kSubQueues < counts[u % kSubQueues])
+        warp_draw(read_record(A.medium + (size_t)u * 4, tx), lane, A.width, A.depth);
+      continue;
+    }
+    const uint2 tile = A.tiles[u - n_medium];
     if (tile.x == kNoTri) continue;
-    const float4 *r = A.tile_tris + (size_t)tile.x * 4;
-    const float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
-    ScreenTri t;
-    t.ax = r0.x, t.ay = r0.y, t.az = r0.z, t.bx = r0.w;
-    t.by = r1.x, t.bz = r1.y, t.cx = r1.z, t.cy = r1.w;
-    t.cz = r2.x, t.area = r2.y, t.x0 = __float_as_int(r2.z), t.y0 = __float_as_int(r2.w);
-    t.x1 = __float_as_int(r3.x), t.y1 = __float_as_int(r3.y);
-    const uint32_t tx = __float_as_uint(r3.z);
+    const ScreenTri t = read_record(A.large + (size_t)tile.x * 4, tx);
     const int px = t.x0 + int((tile.y % tx) * kTileW + lane), py0 = t.y0 + int((tile.y / tx) * kTileH);
     if (px > t.x1) continue;
     const int py1 = min(t.y1, py0 + int(kTileH) - 1);
@@ -251,20 +343,31 @@ extern "C" int vgc_occluder_depth(vgc_context *ctx, uint32_t src_slot, const vgc
   A.draw_list = (const uint4 *)ctx->d_draw.ptr + (size_t)src_slot * 2 * ctx->opts.max_meshlets;
   A.counters = (const uint32_t *)ctx->d_counters.ptr + (size_t)src_slot * ctx->counter_words;
   A.max_drawn = ctx->opts.max_meshlets;
-  // the tile pass's buffers: control words, triangle records, tile records
-  const size_t tri_bytes = (size_t)kTileTris * 64, tile_bytes = (size_t)kTileUnits * 8;
-  if ((rc = dev_alloc(ctx, ctx->d_raster, 256 + tri_bytes + tile_bytes))) return rc;  // once per context
-  A.tile_ctl = (uint32_t *)ctx->d_raster.ptr;
-  A.tile_tris = (float4 *)((char *)ctx->d_raster.ptr + 256);
-  A.tiles = (uint2 *)((char *)ctx->d_raster.ptr + 256 + tri_bytes);
+  // the queues: control words, medium and large triangle records, tile records
+  const size_t medium_bytes = (size_t)kQueuedMedium * 64, large_bytes = (size_t)kQueuedLarge * 64;
+  const size_t ctl_bytes = 2048;
+  static_assert(kCtlWords * 4 <= ctl_bytes, "control words");
+  if ((rc = dev_alloc(ctx, ctx->d_raster, ctl_bytes + medium_bytes + large_bytes + (size_t)kTileUnits * 8))) return rc;
+  char *q = (char *)ctx->d_raster.ptr;
+  A.ctl = (uint32_t *)q;
+  A.medium = (float4 *)(q + ctl_bytes);
+  A.large = (float4 *)(q + ctl_bytes + medium_bytes);
+  A.tiles = (uint2 *)(q + ctl_bytes + medium_bytes + large_bytes);
   const size_t pixels = (size_t)width * height;
   k_depth_clear<<<(unsigned)std::min<size_t>((pixels + 255) / 256, (size_t)ctx->sm_count * 16), 256, 0, st>>>(
-      A.depth, pixels, A.tile_ctl);
+      A.depth, pixels, A.ctl);
   CUDA_TRY(cudaGetLastError());
   if (ctx->positions.empty()) return VGC_OK;  // no mesh carries vertex data: nothing is an occluder
-  k_raster_occluders<<<ctx->sm_count * 8, 128, 0, st>>>(scene_of(ctx), A);
+  // persistent grids of exactly the resident blocks: a grid-stride loop over a grid larger than one wave leaves the
+  // blocks of the second wave their full share of the work after the first has finished
+  static int per_sm[2] = {0, 0};
+  if (!per_sm[0]) {
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], k_raster_occluders, 128, 0));
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k_raster_queued, 128, 0));
+  }
+  k_raster_occluders<<<ctx->sm_count * std::max(1, per_sm[0]), 128, 0, st>>>(scene_of(ctx), A);
   CUDA_TRY(cudaGetLastError());
-  k_raster_tiles<<<ctx->sm_count * 8, 128, 0, st>>>(A);
+  k_raster_queued<<<ctx->sm_count * std::max(1, per_sm[1]), 128, 0, st>>>(A);
   CUDA_TRY(cudaGetLastError());
   return VGC_OK;
 }
