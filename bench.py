@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bound of the CPU-baseline sample")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batching, occluder, large-world and serving sections")
-    ap.add_argument("--extras", default="batching,occluders,large_world,serve",
+    ap.add_argument("--extras", default="batching,occluders,visibility,large_world,serve",
                     help="comma-separated sections to run after the headline line's measurement")
     ap.add_argument("--serve-rate", type=float, default=10_000.0, help="Poisson request rate of the serving section")
     ap.add_argument("--serve-requests", type=int, default=20_000)
@@ -406,6 +406,8 @@ def run_ours(args, world, rank, local):
             line["batching"] = run_batching(spec, args, flush, stream)
         if "occluders" in extras:
             line["occluders"] = run_occluders(spec, args, flush, stream)
+        if "visibility" in extras:
+            line["visibility"] = run_visibility(spec, args, flush, stream)
         if "large_world" in extras:
             line["large_world"] = run_large_world(spec, args, flush, stream)
         if "serve" in extras:
@@ -541,6 +543,60 @@ def run_occluders(ruins, args, flush, stream):
                 occluder_pass_ms_per_view=occ_ms / P, two_pass_ms_per_step=both_ms, views_per_sec=P / (both_ms / 1e3),
                 occluder_coverage=covered, occluded_instances_mean=statistics.mean(occluded),
                 drawn_meshlets_with_hzb=statistics.mean(drawn_hzb), drawn_meshlets_without=statistics.mean(drawn_open))
+
+
+def run_visibility(ruins, args, flush, stream):
+    """The loop closed headlessly: per pose, the camera cut (batched, 32 views per launch), its index expansion and
+    the visibility buffer drawn from the expanded indices at 1920x1080 (vertex pulling, draw-distance fade, LOD blend
+    mask), one view after the other through one index buffer."""
+    import torch
+    from vgcut import engine
+    vg = engine.VirtualGeometry(max_triangles=10_000_000, max_shadow_triangles=4_000_000, max_meshlets=1 << 18,
+                                output_slots=len(ruins.cameras))
+    for data, mats in zip(ruins.meshes, ruins.instances):
+        vg.create_mesh(data, mats, vertex_data=True)
+    P, W, H = len(ruins.cameras), 1920, 1080
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    views = [engine.make_view(c, engine.ViewParams(error_threshold=1.0, state_slot=k, fresh_state=True))
+             for k, c in enumerate(ruins.cameras)]
+    cap = 10_000_000 * 3
+    idx = torch.empty(cap, dtype=torch.int32, device="cuda")
+    vis = torch.empty((H, W), dtype=torch.int64, device="cuda")
+
+    def draw_all():
+        for k in range(P):
+            vg.expand(k, 0, idx.data_ptr(), cap, stream=sp)
+            vg.visibility(k, 0, ruins.cameras[k], idx.data_ptr(), cap, vis.data_ptr(), W, H, stream=sp)
+
+    def timed(fn):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        return statistics.mean(ms)
+
+    vg.cut(views, first_slot=0, stream=sp, graph=True)
+    torch.cuda.synchronize()
+    draw_ms = timed(draw_all)
+    loop_ms = timed(lambda: (vg.cut(views, first_slot=0, stream=sp, graph=True), draw_all()))
+    torch.cuda.synchronize()
+    tris = statistics.mean(vg.read_stats(k)["requested_indices"][0] / 3 for k in range(P))
+    covered = float((vis != engine.VIS_EMPTY).float().mean())
+    vg.dispose()
+    return dict(workload=f"closed loop, ruins-like scene, {P} poses: batched camera cut, index expansion and a "
+                         f"{W}x{H} visibility buffer from the expanded indices, per view",
+                expand_and_visibility_ms_per_view=draw_ms / P, loop_ms_per_step=loop_ms,
+                views_per_sec=P / (loop_ms / 1e3), triangles_per_view=tris,
+                triangles_per_sec=tris * P / (draw_ms / 1e3), coverage_last_view=covered)
 
 
 def run_large_world(ruins, args, flush, stream):

@@ -300,6 +300,20 @@ int vgc_server_destroy(vgc_server *server);
 int vgc_occluder_depth(vgc_context *ctx, uint32_t src_slot, const vgc_view *view, float *depth, uint32_t width,
                        uint32_t height, vgc_stream stream);
 
+/* Visibility buffer: a headless consumer of a cut's output, after vgc_expand. Draws the index buffer `indices`
+   (device, `capacity` indices) that vgc_expand wrote for output slot `slot` and cut `cut`, region by region as the
+   cut's draw args give them, with the reference's vertex pulling (GeometryPool.ts:1095-1131: draw-list entry,
+   meshletVertices, positions, the instance's model, the draw-distance shrink toward the instance origin measured
+   from `fade_view`, NULL = `view`) and LOD blend mask (lodBlend.ts:36-45: interleaved gradient noise at the pixel
+   centre, `frame` as lodBlendFrame), rasterized with `view` at pixel centres, back faces and triangles reaching in
+   front of the near plane left out, into `vis` (device, width x height u64, row 0 at the top): per pixel the
+   minimum of (NDC depth bits << 32 | drawSlot << 7 | triangle in its meshlet), VGC_VIS_EMPTY where nothing is
+   drawn. Meshes without vertex data are not drawn. Asynchronous on `stream`. */
+#define VGC_VIS_EMPTY 0x3f800000ffffffffull
+int vgc_visibility(vgc_context *ctx, uint32_t slot, uint32_t cut, const vgc_view *view, const vgc_view *fade_view,
+                   const uint32_t *indices, uint64_t capacity, uint64_t *vis, uint32_t width, uint32_t height,
+                   uint32_t frame, vgc_stream stream);
+
 /* Layout of HZB slot `hzb`: levels, per-level offset (floats) / width / height (16 entries each), and the device
    pointer of the mip chain (level i at data + offset[i], row-major). */
 int vgc_hzb_info(const vgc_context *ctx, int32_t hzb, uint32_t *levels, uint32_t *offset, uint32_t *width,

@@ -45,6 +45,11 @@ def lib() -> C.CDLL:
                                                 D16, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                                                 P(C.c_uint32), P(C.c_uint32)]
     L.vgo_cull_pass_f32.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+    U32, F32 = P(C.c_uint32), P(C.c_float)
+    L.vgo_blend_keep.argtypes = [C.c_int, C.c_int, C.c_uint32, C.c_uint32, C.c_uint32]
+    L.vgo_visibility.argtypes = [U32, C.c_uint64, U32, C.c_uint32, U32, C.c_uint32, F32, C.c_uint32, U32, U32, F32,
+                                 U32, C.c_uint32, U32, C.c_uint32, F32, C.c_uint32, P(C.c_double), P(C.c_double),
+                                 P(C.c_double), C.c_uint32, C.c_uint32, C.c_uint32, P(C.c_uint64)]
     L.vgo_cull_pass_f64.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
     L.vgo_explain_f64.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32]
     L.vgo_explain_f64.restype = C.c_double
@@ -382,13 +387,13 @@ def scene_from_spec(meshes, instances, flags=None, orders_in=None) -> tuple[Orac
     return OracleScene(list(zip(meshes, flags)), allm, allc), allm, orders
 
 
-def occluder_depth(meshes, occluder_flags, gpu_mats, inst_slot, entries, camera, width: int, height: int) -> np.ndarray:
-    """The occluder depth pass restated (vg_raster.c) over the same pool layout the engine builds: meshes in add
-    order, meshlet / triangle / meshlet-vertex / vertex ids rebased to pool-global, vertex data only for occluders.
-    `entries`: (n, 4) uint32 draw-list entries of the source cut; returns the (height, width) float32 depth."""
+def _pool_arrays(meshes, vertex_flags):
+    """The engine's pool layout of the meshes (add order): meshlet info with pool-global triangle and
+    meshlet-vertex offsets, packed triangles, and the meshlet vertices / positions of the meshes flagged in
+    `vertex_flags` (pool-global vertex ids)."""
     infos, tris, mverts, pos = [], [], [], []
     tri_base = mv_base = v_base = 0
-    for d, occ in zip(meshes, occluder_flags):
+    for d, occ in zip(meshes, vertex_flags):
         info = np.asarray(d.meshlet_info, np.uint32).reshape(-1, 4).copy()
         info[:, 1] += np.uint32(tri_base * 3)
         info[:, 3] += np.uint32(mv_base)
@@ -407,6 +412,14 @@ def occluder_depth(meshes, occluder_flags, gpu_mats, inst_slot, entries, camera,
     m_tris = np.ascontiguousarray(np.concatenate(tris), np.uint32)
     m_verts = np.ascontiguousarray(np.concatenate(mverts) if mverts else np.zeros(1, np.uint32), np.uint32)
     positions = np.ascontiguousarray(np.concatenate(pos) if pos else np.zeros((1, 3), np.float32), np.float32)
+    return m_info, m_tris, m_verts, positions
+
+
+def occluder_depth(meshes, occluder_flags, gpu_mats, inst_slot, entries, camera, width: int, height: int) -> np.ndarray:
+    """The occluder depth pass restated (vg_raster.c) over the same pool layout the engine builds: meshes in add
+    order, meshlet / triangle / meshlet-vertex / vertex ids rebased to pool-global, vertex data only for occluders.
+    `entries`: (n, 4) uint32 draw-list entries of the source cut; returns the (height, width) float32 depth."""
+    m_info, m_tris, m_verts, positions = _pool_arrays(meshes, occluder_flags)
     e = np.ascontiguousarray(entries, np.uint32).reshape(-1, 4)
     mats = np.ascontiguousarray(gpu_mats, np.float32)
     slots = np.ascontiguousarray(inst_slot, np.uint32)
@@ -418,4 +431,39 @@ def occluder_depth(meshes, occluder_flags, gpu_mats, inst_slot, entries, camera,
     L.vgo_occluder_depth(_u(e), len(e), _f(mats), _u(slots), _u(flags), _u(m_info), _u(m_tris), _u(m_verts),
                          _f(positions), view.ctypes.data_as(C.POINTER(C.c_double)),
                          proj.ctypes.data_as(C.POINTER(C.c_double)), width, height, _f(out))
+    return out
+
+
+def blend_keep(px: int, py: int, frame: int, lo: int, hi: int) -> bool:
+    """lodBlendMask (lodBlend.ts:36-45) at pixel (px, py), as vg_raster.c computes it."""
+    return bool(lib().vgo_blend_keep(px, py, frame, lo, hi))
+
+
+def visibility(meshes, vertex_flags, max_draw_distance, gpu_mats, inst_slot, indices, draw_list, args, camera,
+               width: int, height: int, frame: int = 0, fade_camera=None) -> np.ndarray:
+    """The visibility pass restated (vg_raster.c) over the engine's pool layout: `vertex_flags` per mesh, whether its
+    vertex data was uploaded; `indices` the expanded index buffer, `draw_list` the output slot's entries of both cuts
+    ((2 max_drawn, 4) u32), `args` the cut's draw args ((regions, 5) u32), `max_draw_distance` per mesh (as given to
+    the engine; inf = none). Returns the (height, width) uint64 image."""
+    has_vertices = [bool(f) for f in vertex_flags]
+    m_info, _, m_verts, positions = _pool_arrays(meshes, has_vertices)
+    n_verts = sum(len(np.asarray(d.meshlet_vertices)) for d, f in zip(meshes, has_vertices) if f)
+    n_pos = sum(len(np.asarray(d.positions)) // 3 for d, f in zip(meshes, has_vertices) if f)
+    maxd = np.array([np.float32(x) if (x > 0 and x < 1e30) else np.float32(1e30) for x in max_draw_distance],
+                    np.float32)
+    idx = np.ascontiguousarray(indices, np.uint32)
+    dl = np.ascontiguousarray(draw_list, np.uint32).reshape(-1, 4)
+    a = np.ascontiguousarray(args, np.uint32).reshape(-1, 5)
+    mats = np.ascontiguousarray(gpu_mats, np.float32)
+    slots = np.ascontiguousarray(inst_slot, np.uint32)
+    flags = np.ascontiguousarray([1 if f else 0 for f in has_vertices], np.uint32)
+    fc = fade_camera if fade_camera is not None else camera
+    view = np.ascontiguousarray(camera.view, np.float64)
+    proj = np.ascontiguousarray(camera.proj, np.float64)
+    fview = np.ascontiguousarray(fc.view, np.float64)
+    out = np.zeros((height, width), np.uint64)
+    dp = lambda x: x.ctypes.data_as(C.POINTER(C.c_double))
+    lib().vgo_visibility(_u(idx), len(idx), _u(dl), len(dl), _u(a), len(a), _f(mats), len(mats), _u(slots), _u(flags),
+                         _f(maxd), _u(m_info), len(m_info), _u(m_verts), n_verts, _f(positions), n_pos, dp(view),
+                         dp(proj), dp(fview), width, height, frame, out.ctypes.data_as(C.POINTER(C.c_uint64)))
     return out

@@ -125,6 +125,14 @@ int vgo_occluder_depth(const uint32_t *entries, uint32_t n, const float *inst, c
                        const uint32_t *slot_occluder, const uint32_t *m_info, const uint32_t *m_tris,
                        const uint32_t *m_verts, const float *positions, const double *view, const double *proj,
                        uint32_t width, uint32_t height, float *depth);
+/* visibility buffer of a cut's expanded index buffer (vgc_visibility), and its per-pixel blend keep test */
+int vgo_blend_keep(int px, int py, uint32_t frame, uint32_t lo, uint32_t hi);
+int vgo_visibility(const uint32_t *indices, uint64_t capacity, const uint32_t *draw_list, uint32_t draw_slots,
+                   const uint32_t *args, uint32_t regions, const float *inst, uint32_t instances,
+                   const uint32_t *inst_slot, const uint32_t *slot_vertices, const float *slot_max_draw_distance,
+                   const uint32_t *m_info, uint32_t meshlets, const uint32_t *m_verts, uint32_t meshlet_vertices,
+                   const float *positions, uint32_t vertices, const double *view, const double *proj,
+                   const double *fade_view, uint32_t width, uint32_t height, uint32_t frame, uint64_t *vis);
 
 /* Full per-frame pass, float mirror of the kernels / double semantics. threads: 0 = all. */
 int vgo_cull_pass_f32(const vgo_scene *scene, vgo_view *view, vgo_result *result, int threads);

@@ -98,3 +98,115 @@ int vgo_occluder_depth(const uint32_t *entries, uint32_t n, const float *inst, c
   }
   return 0;
 }
+
+/* ---- visibility buffer: the headless consumer of a cut (vgc_visibility), restated. An index of the expanded
+ * buffer is (drawSlot << 7) | localVertex; vertex pulling follows GeometryPool.ts:1095-1131 (entry, meshletVertices,
+ * position, model, draw-distance shrink toward the instance origin, DRAW_DISTANCE_FADE = 0.15 at :109) and the
+ * fragment keep test lodBlend.ts:36-45 (interleaved gradient noise at the pixel centre, lodBlendFrame = frame).
+ * Every pixel keeps the minimum of (depth bits << 32 | drawSlot << 7 | triangle in its meshlet). */
+static const float kDrawDistanceFade = 0.15f;
+
+typedef struct {
+  const uint32_t *draw_list;
+  uint32_t draw_slots;
+  const float *inst;
+  uint32_t instances;
+  const uint32_t *inst_slot, *slot_vertices;
+  const float *slot_max_draw_distance;
+  const uint32_t *m_info;
+  uint32_t meshlets;
+  const uint32_t *m_verts;
+  uint32_t meshlet_vertices;
+  const float *positions;
+  uint32_t vertices;
+  float vp[16], view[16];
+} vis_scene;
+
+/* clip coordinates of index `idx`; 0 when an array index is out of range or the mesh has no vertex data */
+static int vis_pull(const vis_scene *s, uint32_t idx, float c[4]) {
+  const uint32_t ds = idx >> 7, lv = idx & 127u;
+  if (ds >= s->draw_slots) return 0;
+  const uint32_t *ent = s->draw_list + (size_t)ds * 4;
+  if (ent[0] >= s->instances || ent[1] >= s->meshlets) return 0;
+  const uint32_t slot = s->inst_slot[ent[0]];
+  const uint32_t mv = s->m_info[(size_t)ent[1] * 4 + 3] + lv;
+  if (!s->slot_vertices[slot] || mv >= s->meshlet_vertices) return 0;
+  const uint32_t vid = s->m_verts[mv];
+  if (vid >= s->vertices) return 0;
+  const float *p = s->positions + (size_t)vid * 3;
+  const float *col = s->inst + (size_t)ent[0] * 16;
+  const float *c0 = col, *c1 = col + 4, *c2 = col + 8, *c3 = col + 12;
+  const float *V = s->view;
+  const float ox = ((V[0] * c3[0] + V[1] * c3[1]) + V[2] * c3[2]) + V[3];
+  const float oy = ((V[4] * c3[0] + V[5] * c3[1]) + V[6] * c3[2]) + V[7];
+  const float oz = ((V[8] * c3[0] + V[9] * c3[1]) + V[10] * c3[2]) + V[11];
+  const float dist = sqrtf((ox * ox + oy * oy) + oz * oz);
+  const float maxd = s->slot_max_draw_distance[slot];
+  const float fade = fminf(fmaxf((maxd - dist) / (maxd * kDrawDistanceFade), 0.0f), 1.0f);
+  const float wx = c3[0] + ((c0[0] * p[0] + c1[0] * p[1]) + c2[0] * p[2]) * fade;
+  const float wy = c3[1] + ((c0[1] * p[0] + c1[1] * p[1]) + c2[1] * p[2]) * fade;
+  const float wz = c3[2] + ((c0[2] * p[0] + c1[2] * p[1]) + c2[2] * p[2]) * fade;
+  for (int r = 0; r < 4; r++) c[r] = ((s->vp[r * 4] * wx + s->vp[r * 4 + 1] * wy) + s->vp[r * 4 + 2] * wz) + s->vp[r * 4 + 3];
+  return 1;
+}
+
+int vgo_blend_keep(int px, int py, uint32_t frame, uint32_t lo, uint32_t hi) {
+  const float x = ((float)px + 0.5f) + (float)frame * 5.588238f, y = (float)py + 0.5f;
+  const float a = x * 0.06711056f + y * 0.00583715f;
+  const float b = (a - floorf(a)) * 52.9829189f;
+  const float step = floorf((b - floorf(b)) * 255.0f);
+  return step >= (float)lo && step < (float)hi;
+}
+
+int vgo_visibility(const uint32_t *indices, uint64_t capacity, const uint32_t *draw_list, uint32_t draw_slots,
+                   const uint32_t *args, uint32_t regions, const float *inst, uint32_t instances,
+                   const uint32_t *inst_slot, const uint32_t *slot_vertices, const float *slot_max_draw_distance,
+                   const uint32_t *m_info, uint32_t meshlets, const uint32_t *m_verts, uint32_t meshlet_vertices,
+                   const float *positions, uint32_t vertices, const double *view, const double *proj,
+                   const double *fade_view, uint32_t width, uint32_t height, uint32_t frame, uint64_t *vis) {
+  vis_scene s = {draw_list, draw_slots, inst, instances, inst_slot, slot_vertices, slot_max_draw_distance,
+                 m_info, meshlets, m_verts, meshlet_vertices, positions, vertices, {0}, {0}};
+  for (int r = 0; r < 4; r++)
+    for (int c = 0; c < 4; c++) {
+      double acc = 0;
+      for (int i = 0; i < 4; i++) acc += proj[i * 4 + r] * view[c * 4 + i];
+      s.vp[r * 4 + c] = (float)acc;
+      s.view[r * 4 + c] = (float)fade_view[c * 4 + r];
+    }
+  for (size_t i = 0; i < (size_t)width * height; i++) vis[i] = 0x3f800000ffffffffull;
+  const float W = (float)width, H = (float)height;
+  for (uint32_t rg = 0; rg < regions; rg++) {
+    const uint32_t tris = args[rg * 5] / 3, start = args[rg * 5 + 2];
+    for (uint32_t i = 0; i < tris; i++) {
+      const uint64_t first = (uint64_t)start + 3ull * i;
+      if (first + 2 >= capacity) continue;
+      float c[3][4];
+      int ok = 1;
+      for (int k = 0; k < 3; k++) ok &= vis_pull(&s, indices[first + k], c[k]);
+      if (!ok) continue;
+      const uint32_t ds = indices[first] >> 7;
+      const uint32_t *ent = draw_list + (size_t)ds * 4;
+      const uint32_t lo = (ent[3] >> 8) & 255u, hi = (ent[3] >> 16) & 255u;
+      const uint32_t payload = (ds << 7) | ((uint32_t)((first - start - ent[2]) / 3) & 127u);
+      raster_tri t;
+      if (!raster_setup(c, W, H, &t)) continue;
+      for (int py = t.y0; py <= t.y1; py++)
+        for (int px = t.x0; px <= t.x1; px++) {
+          const float x = (float)px + 0.5f, y = (float)py + 0.5f;
+          const float wa = (t.cx - t.bx) * (y - t.by) - (t.cy - t.by) * (x - t.bx);
+          const float wb = (t.ax - t.cx) * (y - t.cy) - (t.ay - t.cy) * (x - t.cx);
+          const float wc = (t.bx - t.ax) * (y - t.ay) - (t.by - t.ay) * (x - t.ax);
+          if (wa >= 0.0f && wb >= 0.0f && wc >= 0.0f && vgo_blend_keep(px, py, frame, lo, hi)) {
+            float z = ((wa * t.az + wb * t.bz) + wc * t.cz) / t.area;
+            z = z > 0.0f ? z : 0.0f;
+            uint32_t zb;
+            memcpy(&zb, &z, 4);
+            const uint64_t v = ((uint64_t)zb << 32) | payload;
+            uint64_t *o = vis + (size_t)py * width + px;
+            if (v < *o) *o = v;
+          }
+        }
+    }
+  }
+  return 0;
+}

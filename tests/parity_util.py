@@ -62,7 +62,8 @@ class Harness:
         for d, m, f in zip(spec.meshes, spec.instances, self.flags):
             self.vg.create_mesh(d, m, max_draw_distance=f.get("max_draw_distance", float("inf")),
                                 min_pixel_radius=f.get("min_pixel_radius", 0.0), cast_shadow=f.get("shadow", False),
-                                occlusion_culling=f.get("occlusion", False), occluder=f.get("occluder", False))
+                                occlusion_culling=f.get("occlusion", False), occluder=f.get("occluder", False),
+                                vertex_data=f.get("vertex_data", False))
         self.scene, self.mats, self.orders = O.scene_from_spec(spec.meshes, spec.instances, self.flags)
         self.inst_slot = np.concatenate([np.full(len(m), i, np.uint32) for i, m in enumerate(spec.instances)])
         self.max_meshlets, self.caps = max_meshlets, (max_triangles * 3, max_shadow * 3)

@@ -75,3 +75,60 @@ def test_back_faces_near_plane_and_skipped_entries():
     assert (out == 1.0).all(), "blended (part 1) meshlets are not occluders"
     out, _ = run(front, [(0, 1, 2)], [(0, 0, 0, PART0)], occluder=(0,))
     assert (out == 1.0).all(), "meshes that are not occluders are not drawn"
+
+
+def test_blend_mask_known_values_and_tiling():
+    """lodBlendMask (lodBlend.ts:36-45): the step of each pixel is floor(255 n), n the interleaved gradient noise at
+    the pixel centre (float32 arithmetic, step by step); complementary ranges [0, k) and [k, 255) split every pixel
+    between them, and a range keeps about its share of the pixels."""
+    f = np.float32
+
+    def step(px, py, frame):
+        x = f(f(px) + f(0.5)) + f(f(frame) * f(5.588238))
+        y = f(f(py) + f(0.5))
+        a = f(f(x * f(0.06711056)) + f(y * f(0.00583715)))
+        b = f(f(a - np.floor(a)) * f(52.9829189))
+        return int(np.floor(f(f(b - np.floor(b)) * f(255.0))))
+
+    for px, py, frame in [(0, 0, 0), (17, 3, 0), (1919, 1079, 0), (640, 360, 5), (3, 200, 7)]:
+        s = step(px, py, frame)
+        assert O.blend_keep(px, py, frame, s, s + 1) and not O.blend_keep(px, py, frame, s + 1, 255)
+        assert not O.blend_keep(px, py, frame, 0, s)
+    kept = 0
+    for py in range(0, 48):
+        for px in range(0, 64):
+            a, b = O.blend_keep(px, py, 0, 0, 100), O.blend_keep(px, py, 0, 100, 255)
+            assert a != b, "complementary ranges tile every pixel"
+            kept += a
+    assert abs(kept / (48 * 64) - 100 / 255) < 0.05
+
+
+def test_visibility_oracle_single_triangle():
+    """The oracle's visibility pass on one hand-built draw entry: a front-facing triangle covering the view at
+    distance 5 is drawn where the pixel's blend step lies in the entry's range, with the entry's draw slot and the
+    triangle's index in its meshlet; with a draw distance of 4 the instance (origin 5 away) shrinks to its origin and
+    nothing is drawn."""
+    from types import SimpleNamespace
+    z = -5.0
+    pos = np.array([(-20, -20, 0), (20, -20, 0), (0, 30, 0)], np.float32).reshape(-1)  # the instance sits at z
+    mesh = SimpleNamespace(meshlet_info=np.array([1, 0, 0, 0], np.uint32), meshlet_triangles=np.array([0 | (1 << 8) | (2 << 16)], np.uint32),
+                           meshlet_vertices=np.arange(3, dtype=np.uint32), positions=pos)
+    cam = Camera(view=np.eye(4).reshape(-1), proj=perspective(60.0, W / H, 0.1, 100.0), near=0.1, height=float(H),
+                 width=float(W))
+    inst = np.eye(4, dtype=np.float32)
+    inst[3, 2] = z  # columns: a translation to (0, 0, z)
+    inst = inst.reshape(1, 16)
+    draw_list = np.zeros((4, 4), np.uint32)
+    draw_list[2] = (0, 0, 0, 1 | (40 << 8) | (200 << 16))  # draw slot 2: a blended entry, steps [40, 200)
+    indices = np.array([(2 << 7) | 0, (2 << 7) | 1, (2 << 7) | 2], np.uint32)
+    args = np.array([[3, 1, 0, 0, 0], [0, 1, 3, 0, 0]], np.uint32)
+    out = O.visibility([mesh], [True], [float("inf")], inst, np.zeros(1, np.uint32), indices, draw_list, args, cam, W, H)
+    drawn = out != np.uint64(0x3F800000FFFFFFFF)
+    keep = np.array([[O.blend_keep(x, y, 0, 40, 200) for x in range(W)] for y in range(H)])
+    assert np.array_equal(drawn, keep), "the triangle covers the view: the blend mask alone decides"
+    assert (out[drawn] & np.uint64(0xFFFFFFFF) == np.uint64(2 << 7)).all()
+    p10, p14 = cam.proj[10], cam.proj[14]
+    depth = (out[drawn] >> np.uint64(32)).astype(np.uint32).view(np.float32)
+    assert np.allclose(depth, (p10 * z + p14) / -z, rtol=0, atol=2e-6)
+    gone = O.visibility([mesh], [True], [4.0], inst, np.zeros(1, np.uint32), indices, draw_list, args, cam, W, H)
+    assert (gone == np.uint64(0x3F800000FFFFFFFF)).all(), "beyond its draw distance the instance shrinks to a point"

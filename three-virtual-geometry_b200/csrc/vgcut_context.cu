@@ -645,6 +645,7 @@ void write_flags(vgc_context *ctx, uint32_t slot, const vgc_mesh_opts *o) {
   r.shadow = o ? (o->shadow ? 1u : 0u) : 0u;
   r.occlusion = o ? (o->occlusion ? 1u : 0u) : 0u;
   r.occluder = (o && o->occluder && ctx->mesh_host[slot].vertex_count) ? 1u : 0u;
+  r.vertices = ctx->mesh_host[slot].vertex_count ? 1u : 0u;
 }
 
 }  // namespace vgch

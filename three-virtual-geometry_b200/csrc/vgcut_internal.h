@@ -45,7 +45,8 @@ struct MeshRec {  // 96 bytes
   uint32_t enabled, shadow, occlusion, meshlet_base;
   uint32_t range_cut;  // 1: every meshlet's LOD and parent spheres lie in `lod`, so items may be trimmed
   uint32_t occluder;   // 1: drawn by the occluder depth pass (has vertex data)
-  uint32_t pad[2];
+  uint32_t vertices;   // 1: the mesh carries vertex data (positions, meshletVertices)
+  uint32_t pad;
 };
 
 struct LevelRec {  // 32 bytes

@@ -318,6 +318,175 @@ __global__ void __launch_bounds__(128) k_raster_queued(RasterArgs A) {
   }
 }
 
+
+// ------------------------------------------------------------------------------------------------ visibility
+// Headless consumer of a cut (vgc_visibility): the cut's expanded index buffer drawn as the draw args say, with the
+// reference's vertex pulling (GeometryPool.ts:1095-1131) and LOD blend mask (lodBlend.ts:36-45), into a visibility
+// buffer: per pixel the 64-bit minimum of (depth bits << 32 | drawSlot << 7 | triangle in its meshlet).
+//
+//  * an index is (drawSlot << 7) | localVertex; drawSlot picks the draw-list entry (instance, meshlet), the local
+//    vertex its meshletVertices entry and the position; the instance's model maps it to world space, shrunk toward
+//    the instance origin by the draw-distance fade clamp((maxDrawDistance - |V origin|) / (0.15 maxDrawDistance),
+//    0, 1), V the camera's view (GeometryPool.ts:1112-1119);
+//  * triangles are set up as in the occluder pass (pixel centres, edges included, back faces and triangles reaching
+//    in front of the near plane left out), one per lane, the large ones by the whole warp;
+//  * a fragment is kept when the step floor(255 n) of its pixel lies in the entry's blend range [lo, hi), n the
+//    interleaved gradient noise fract(52.9829189 fract(0.06711056 x + 0.00583715 y)) at the pixel centre (x, y),
+//    x shifted by 5.588238 per `frame` (lodBlendFrame);
+//  * indices or entries outside the context's arrays (an index buffer not written by vgc_expand) drop their
+//    triangle.
+constexpr float kDrawDistanceFade = 0.15f;   // GeometryPool.ts:109
+constexpr uint32_t kVisLaneMax = 64;         // bounding-box pixels up to which a lane draws its triangle
+
+struct VisArgs {
+  float vp[16];    // P * V, row-major
+  float view[16];  // the camera's V (draw-distance fade), row-major
+  uint32_t width, height, frame, regions;  // regions: mesh slots * 2 (parts)
+  unsigned long long *vis;
+  const uint32_t *indices;
+  uint64_t capacity;
+  const uint4 *draw_list;  // the output slot's entries (draw slots of both cuts)
+  const uint32_t *args;    // the cut's draw args, 5 u32 per (mesh slot, part)
+  uint32_t draw_slots;     // entries in draw_list
+  uint32_t meshlets, instances, meshlet_vertices, vertices;
+};
+
+// Screen-space vertex of index `idx` (w = 0: unusable), and its entry's draw slot and blend range.
+__device__ __forceinline__ float4 pulled_vertex(const Scene &S, const VisArgs &A, uint32_t idx, bool &ok) {
+  const uint32_t ds = idx >> kLocalVertexBits, lv = idx & ((1u << kLocalVertexBits) - 1u);
+  ok = false;
+  if (ds >= A.draw_slots) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const uint4 ent = A.draw_list[ds];
+  if (ent.x >= A.instances || ent.y >= A.meshlets) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const MeshRec &mesh = S.meshes[S.inst_slot[ent.x]];
+  const uint32_t mv = S.m_info[ent.y].w + lv;
+  if (!mesh.vertices || mv >= A.meshlet_vertices) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const uint32_t vid = S.m_verts[mv];
+  if (vid >= A.vertices) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  ok = true;
+  const float4 p = S.positions[vid];
+  const float4 *col = S.inst + (size_t)ent.x * 4;
+  const float4 c0 = col[0], c1 = col[1], c2 = col[2], c3 = col[3];
+  // draw-distance fade, from the camera's distance to the instance origin
+  const float *V = A.view;
+  const float ox = ((V[0] * c3.x + V[1] * c3.y) + V[2] * c3.z) + V[3];
+  const float oy = ((V[4] * c3.x + V[5] * c3.y) + V[6] * c3.z) + V[7];
+  const float oz = ((V[8] * c3.x + V[9] * c3.y) + V[10] * c3.z) + V[11];
+  const float dist = sqrtf((ox * ox + oy * oy) + oz * oz);
+  const float maxd = mesh.max_draw_distance;
+  const float fade = fminf(fmaxf((maxd - dist) / (maxd * kDrawDistanceFade), 0.0f), 1.0f);
+  const float wx = c3.x + ((c0.x * p.x + c1.x * p.y) + c2.x * p.z) * fade;
+  const float wy = c3.y + ((c0.y * p.x + c1.y * p.y) + c2.y * p.z) * fade;
+  const float wz = c3.z + ((c0.z * p.x + c1.z * p.y) + c2.z * p.z) * fade;
+  float c[4];
+#pragma unroll
+  for (int r = 0; r < 4; r++) c[r] = ((A.vp[r * 4] * wx + A.vp[r * 4 + 1] * wy) + A.vp[r * 4 + 2] * wz) + A.vp[r * 4 + 3];
+  if (!(c[3] > 0.0f) || !(c[2] >= 0.0f)) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const float nx = c[0] / c[3], ny = c[1] / c[3], nz = c[2] / c[3];
+  return make_float4((nx * 0.5f + 0.5f) * float(A.width), (0.5f - ny * 0.5f) * float(A.height), nz, 1.0f);
+}
+
+// lodBlendMask (lodBlend.ts:36-45) at pixel (px, py): true when the pixel's step lies in [lo, hi).
+__device__ __forceinline__ bool blend_keep(int px, int py, uint32_t frame, uint32_t lo, uint32_t hi) {
+  const float x = (float(px) + 0.5f) + float(frame) * 5.588238f, y = float(py) + 0.5f;
+  const float a = x * 0.06711056f + y * 0.00583715f;
+  const float b = (a - floorf(a)) * 52.9829189f;
+  const float step = floorf((b - floorf(b)) * 255.0f);
+  return step >= float(lo) && step < float(hi);
+}
+
+__device__ __forceinline__ void vis_pixel(const ScreenTri &t, int px, int py, const VisArgs &A, uint32_t lo,
+                                          uint32_t hi, uint32_t payload) {
+  const float x = float(px) + 0.5f, y = float(py) + 0.5f;
+  const float wa = (t.cx - t.bx) * (y - t.by) - (t.cy - t.by) * (x - t.bx);
+  const float wb = (t.ax - t.cx) * (y - t.cy) - (t.ay - t.cy) * (x - t.cx);
+  const float wc = (t.bx - t.ax) * (y - t.ay) - (t.by - t.ay) * (x - t.ax);
+  if (wa >= 0.0f && wb >= 0.0f && wc >= 0.0f && blend_keep(px, py, A.frame, lo, hi)) {
+    float z = ((wa * t.az + wb * t.bz) + wc * t.cz) / t.area;
+    z = z > 0.0f ? z : 0.0f;
+    atomicMin(A.vis + (size_t)py * A.width + px, ((unsigned long long)__float_as_uint(z) << 32) | payload);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_vis_clear(unsigned long long *vis, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    vis[i] = VGC_VIS_EMPTY;
+}
+
+// One lane per triangle of the cut, in region order (mesh slot, then part), as the draw args give them.
+__global__ void __launch_bounds__(256) k_visibility(Scene S, VisArgs A) {
+  extern __shared__ uint32_t tri_start[];  // per region: first triangle in the laid-out order; [regions] = total
+  if (threadIdx.x < 32) {  // warp 0 scans the regions' triangle counts
+    uint32_t carry = 0;
+    for (uint32_t r0 = 0; r0 < A.regions; r0 += 32) {
+      const uint32_t r = r0 + threadIdx.x;
+      const uint32_t c = r < A.regions ? A.args[r * 5] / 3 : 0u;
+      const uint32_t incl = warp_scan_incl(c);
+      if (r < A.regions) tri_start[r] = carry + incl - c;
+      carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (threadIdx.x == 0) tri_start[A.regions] = carry;
+  }
+  __syncthreads();
+  const uint32_t total = tri_start[A.regions];
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  // every lane of a warp runs the same number of steps (the warp draws its lanes' large triangles together)
+  for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
+    const uint32_t t_id = base + lane;
+    ScreenTri t;
+    bool ok = false;
+    uint32_t lo = 0, hi = 0, payload = 0;
+    if (t_id < total) {
+      uint32_t r = 0, span = A.regions;  // the last region starting at or before t_id
+      while (span > 1) {
+        const uint32_t half = span >> 1;
+        if (tri_start[r + half] <= t_id) r += half;
+        span -= half;
+      }
+      const uint64_t first = (uint64_t)A.args[r * 5 + 2] + 3ull * (t_id - tri_start[r]);
+      if (first + 2 < A.capacity) {
+        const uint32_t i0 = A.indices[first], i1 = A.indices[first + 1], i2 = A.indices[first + 2];
+        bool k0, k1, k2;
+        const float4 v0 = pulled_vertex(S, A, i0, k0), v1 = pulled_vertex(S, A, i1, k1), v2 = pulled_vertex(S, A, i2, k2);
+        if (k0 && k1 && k2) {
+          const uint32_t ds = i0 >> kLocalVertexBits;
+          const uint4 ent = A.draw_list[ds];
+          lo = (ent.w >> 8) & 255u, hi = (ent.w >> 16) & 255u;
+          const uint32_t tri = uint32_t((first - A.args[r * 5 + 2] - ent.z) / 3);
+          payload = (ds << kLocalVertexBits) | (tri & ((1u << kLocalVertexBits) - 1u));
+          ok = setup_triangle(v0, v1, v2, float(A.width), float(A.height), t);
+        }
+      }
+    }
+    const bool big = ok && uint32_t(t.x1 - t.x0 + 1) * uint32_t(t.y1 - t.y0 + 1) > kVisLaneMax;
+    if (ok && !big)
+      for (int py = t.y0; py <= t.y1; py++)
+        for (int px = t.x0; px <= t.x1; px++) vis_pixel(t, px, py, A, lo, hi, payload);
+    for (uint32_t pending = __ballot_sync(0xffffffffu, big); pending; pending &= pending - 1) {
+      const uint32_t owner = __ffs(pending) - 1;
+      ScreenTri u;
+      u.ax = __shfl_sync(0xffffffffu, t.ax, owner), u.ay = __shfl_sync(0xffffffffu, t.ay, owner);
+      u.az = __shfl_sync(0xffffffffu, t.az, owner), u.bx = __shfl_sync(0xffffffffu, t.bx, owner);
+      u.by = __shfl_sync(0xffffffffu, t.by, owner), u.bz = __shfl_sync(0xffffffffu, t.bz, owner);
+      u.cx = __shfl_sync(0xffffffffu, t.cx, owner), u.cy = __shfl_sync(0xffffffffu, t.cy, owner);
+      u.cz = __shfl_sync(0xffffffffu, t.cz, owner), u.area = __shfl_sync(0xffffffffu, t.area, owner);
+      u.x0 = __shfl_sync(0xffffffffu, t.x0, owner), u.x1 = __shfl_sync(0xffffffffu, t.x1, owner);
+      u.y0 = __shfl_sync(0xffffffffu, t.y0, owner), u.y1 = __shfl_sync(0xffffffffu, t.y1, owner);
+      const uint32_t ulo = __shfl_sync(0xffffffffu, lo, owner), uhi = __shfl_sync(0xffffffffu, hi, owner);
+      const uint32_t upay = __shfl_sync(0xffffffffu, payload, owner);
+      const uint32_t bw = uint32_t(u.x1 - u.x0 + 1), count = bw * uint32_t(u.y1 - u.y0 + 1);
+      const uint32_t q = 32 / bw, rr = 32 % bw;
+      uint32_t x = lane % bw, y = lane / bw;
+      for (uint32_t i = lane; i < count; i += 32) {
+        vis_pixel(u, u.x0 + int(x), u.y0 + int(y), A, ulo, uhi, upay);
+        x += rr, y += q;
+        if (x >= bw) x -= bw, y++;
+      }
+    }
+  }
+}
+
 }  // namespace
 
 extern "C" int vgc_occluder_depth(vgc_context *ctx, uint32_t src_slot, const vgc_view *view, float *depth,
@@ -368,6 +537,57 @@ extern "C" int vgc_occluder_depth(vgc_context *ctx, uint32_t src_slot, const vgc
   k_raster_occluders<<<ctx->sm_count * std::max(1, per_sm[0]), 128, 0, st>>>(scene_of(ctx), A);
   CUDA_TRY(cudaGetLastError());
   k_raster_queued<<<ctx->sm_count * std::max(1, per_sm[1]), 128, 0, st>>>(A);
+  CUDA_TRY(cudaGetLastError());
+  return VGC_OK;
+}
+
+extern "C" int vgc_visibility(vgc_context *ctx, uint32_t slot, uint32_t cut, const vgc_view *view,
+                              const vgc_view *fade_view, const uint32_t *indices, uint64_t capacity, uint64_t *vis,
+                              uint32_t width, uint32_t height, uint32_t frame, vgc_stream stream) {
+  if (!ctx || !view || !indices || !vis || cut > 1) return fail(VGC_INVALID_ARG, "bad arguments");
+  if (width == 0 || height == 0 || width > 16384 || height > 16384)
+    return fail(VGC_INVALID_ARG, "visibility buffer size must be 1..16384 per side");
+  if (slot >= ctx->out_slots) return fail(VGC_NOT_FOUND, "output slot not allocated");
+  if (ctx->out_slot_capacity != ctx->slot_capacity)
+    return fail(VGC_INVALID_ARG, "vgc_visibility: meshes were added since the cut; cut and expand again first");
+  cudaSetDevice(ctx->device);
+  int rc = sync_scene(ctx);
+  if (rc) return rc;
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  const vgc_view *fv = fade_view ? fade_view : view;
+  VisArgs A{};
+  for (int r = 0; r < 4; r++)
+    for (int c = 0; c < 4; c++) {
+      double s = 0;
+      for (int i = 0; i < 4; i++) s += view->proj[i * 4 + r] * view->view[c * 4 + i];
+      A.vp[r * 4 + c] = (float)s;
+      A.view[r * 4 + c] = (float)fv->view[c * 4 + r];
+    }
+  A.width = width;
+  A.height = height;
+  A.frame = frame;
+  A.regions = ctx->out_slot_capacity * 2;
+  A.vis = reinterpret_cast<unsigned long long *>(vis);
+  A.indices = indices;
+  A.capacity = capacity;
+  A.draw_list = (const uint4 *)ctx->d_draw.ptr + (size_t)slot * 2 * ctx->opts.max_meshlets;
+  A.args = (const uint32_t *)ctx->d_args.ptr + (size_t)slot * 2 * ctx->out_slot_capacity * 2 * 5 +
+           (size_t)cut * ctx->out_slot_capacity * 2 * 5;
+  A.draw_slots = 2 * ctx->opts.max_meshlets;
+  A.meshlets = (uint32_t)ctx->m_info.size();
+  A.instances = (uint32_t)ctx->inst_slot.size();
+  A.meshlet_vertices = (uint32_t)ctx->m_verts.size();
+  A.vertices = (uint32_t)ctx->positions.size();
+  const size_t pixels = (size_t)width * height;
+  k_vis_clear<<<(unsigned)std::min<size_t>((pixels + 255) / 256, (size_t)ctx->sm_count * 16), 256, 0, st>>>(A.vis,
+                                                                                                        pixels);
+  CUDA_TRY(cudaGetLastError());
+  if (ctx->positions.empty()) return VGC_OK;  // no mesh carries vertex data
+  const size_t smem = (A.regions + 1) * sizeof(uint32_t);
+  if (smem > 48 * 1024) return fail(VGC_INVALID_ARG, "too many mesh slots for vgc_visibility");
+  int per_sm = 0;
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_visibility, 256, smem));
+  k_visibility<<<ctx->sm_count * std::max(1, per_sm), 256, smem, st>>>(scene_of(ctx), A);
   CUDA_TRY(cudaGetLastError());
   return VGC_OK;
 }

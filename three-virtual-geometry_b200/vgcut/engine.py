@@ -78,6 +78,9 @@ class ServerStats(C.Structure):
                 ("max_in_flight", C.c_uint32)]
 
 
+VIS_EMPTY = 0x3F800000FFFFFFFF  # visibility-buffer pixel where nothing is drawn (VGC_VIS_EMPTY)
+
+
 class Output(C.Structure):
     _fields_ = [("draw_list", C.c_void_p * 2), ("draw_args", C.c_void_p), ("counters", C.c_void_p),
                 ("max_drawn", C.c_uint32), ("mesh_slots", C.c_uint32)]
@@ -148,6 +151,8 @@ def lib() -> C.CDLL:
         "vgc_debug_scene": ([vp, P(C.c_float), C.c_uint32, P(C.c_float), C.c_uint32, P(C.c_uint32), P(C.c_uint32)], C.c_int),
         "vgc_debug_cells_device": ([vp, P(C.c_float), C.c_uint32, P(C.c_uint32)], C.c_int),
         "vgc_occluder_depth": ([vp, C.c_uint32, P(View), vp, C.c_uint32, C.c_uint32, vp], C.c_int),
+        "vgc_visibility": ([vp, C.c_uint32, C.c_uint32, P(View), P(View), vp, C.c_uint64, vp, C.c_uint32, C.c_uint32,
+                            C.c_uint32, vp], C.c_int),
         "vgc_server_default_options": ([P(ServerOptions)], None),
         "vgc_server_create": ([P(vp), C.c_uint32, P(ServerOptions), P(vp)], C.c_int),
         "vgc_server_submit": ([vp, C.c_uint32, P(View), P(C.c_uint64)], C.c_int),
@@ -266,7 +271,9 @@ class VirtualMesh:
 
     def __init__(self, vg: "VirtualGeometry", data, matrices: np.ndarray, max_draw_distance: float = math.inf,
                  min_pixel_radius: float = 0.0, cast_shadow: bool = False, occlusion_culling: bool = False,
-                 occluder: bool = False):
+                 occluder: bool = False, vertex_data: bool = False):
+        """`vertex_data`: upload the mesh's positions and meshlet vertices (always done for an occluder), which the
+        visibility pass (VirtualGeometry.visibility) pulls its vertices from."""
         self.vg = vg
         self.data = data
         m = np.ascontiguousarray(matrices, np.float32).reshape(-1, 16)
@@ -274,7 +281,7 @@ class VirtualMesh:
         self.full_detail_triangles = int(data.stats.get("leafTriangles", 0)) * self.instance_count
         self._flags = dict(max_draw_distance=max_draw_distance, min_pixel_radius=min_pixel_radius, visible=True,
                            cast_shadow=cast_shadow, occlusion_culling=occlusion_culling, occluder=occluder)
-        md, keep = mesh_struct(data, with_vertices=occluder)
+        md, keep = mesh_struct(data, with_vertices=occluder or vertex_data)
         self.gpu_to_input = np.zeros(self.instance_count, np.uint32)
         slot = C.c_uint32()
         check(lib().vgc_mesh_add(vg.handle, C.byref(md), _fp(m), self.instance_count, C.byref(self._opts()),
@@ -491,6 +498,19 @@ class VirtualGeometry:
         device buffer at `depth_ptr` (width x height float32), ready to be this frame's view depth."""
         v = make_view(camera, self.params)
         check(lib().vgc_occluder_depth(self.handle, src_slot, C.byref(v), C.c_void_p(depth_ptr), width, height, stream))
+
+    def expand(self, slot: int, cut: int, index_ptr: int, capacity: int, stream=None) -> None:
+        """Index expansion (vgc_expand) of output slot `slot`'s cut `cut` into the device buffer at `index_ptr`."""
+        check(lib().vgc_expand(self.handle, slot, cut, C.c_void_p(index_ptr), capacity, stream))
+
+    def visibility(self, slot: int, cut: int, camera: Camera, index_ptr: int, capacity: int, vis_ptr: int, width: int,
+                   height: int, frame: int = 0, fade_camera: Camera | None = None, stream=None) -> None:
+        """Visibility buffer of slot `slot`'s cut `cut` from its expanded index buffer (vgc_visibility): per pixel of
+        the device buffer at `vis_ptr` (height x width uint64), depth bits << 32 | drawSlot << 7 | triangle."""
+        v = make_view(camera, self.params)
+        f = make_view(fade_camera, self.params) if fade_camera is not None else None
+        check(lib().vgc_visibility(self.handle, slot, cut, C.byref(v), C.byref(f) if f is not None else None,
+                                   C.c_void_p(index_ptr), capacity, C.c_void_p(vis_ptr), width, height, frame, stream))
 
     def debug_cells_device(self) -> np.ndarray:
         """The device's cell records (8 floats each), as the kernels read them."""
