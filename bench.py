@@ -41,9 +41,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="ruins", choices=["ruins", "plain_small"])
     ap.add_argument("--poses", type=int, default=32, help="views per step (the spline's pose count)")
-    ap.add_argument("--profile-case", nargs="?", const="cut", default=None, choices=["cut", "occluders"],
-                    help="small case for an ncu capture (not a bench line): the batched and plain cuts, or the "
-                         "occluder depth pass over 4 poses")
+    ap.add_argument("--profile-case", nargs="?", const="cut", default=None,
+                    choices=["cut", "occluders", "visibility"],
+                    help="small case for an ncu capture (not a bench line): the batched and plain cuts, the "
+                         "occluder depth pass over 4 poses, or the closed loop (expand + visibility) over 4 poses")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bound of the CPU-baseline sample")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batching, occluder, large-world and serving sections")
@@ -220,11 +221,12 @@ def run_ours(args, world, rank, local):
 
     torch.cuda.set_device(local)
     spec, cfg = build_scene(args.config, args.poses)
-    if args.profile_case == "occluders":
+    if args.profile_case in ("occluders", "visibility"):
         small = copy.copy(spec)
         small.cameras = spec.cameras[:4]
-        res = run_occluders(small, args, torch.empty(256 << 20, dtype=torch.uint8, device="cuda"), torch.cuda.Stream())
-        print(json.dumps(dict(profile_case="ok", occluders=res)), flush=True)
+        run = run_occluders if args.profile_case == "occluders" else run_visibility
+        res = run(small, args, torch.empty(256 << 20, dtype=torch.uint8, device="cuda"), torch.cuda.Stream())
+        print(json.dumps(dict(profile_case="ok", **{args.profile_case: res})), flush=True)
         return
     P = len(spec.cameras)
     occl = args.config == "ruins" and len(spec.depth_images) > 0

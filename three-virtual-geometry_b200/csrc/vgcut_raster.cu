@@ -23,6 +23,9 @@
 //  * the atomics' results are unused, so they do not wait (a load-then-atomic early depth test measured slower: it
 //    puts an L2 round trip on every pixel). The image is the minimum over all drawn pixels, whatever the order.
 //
+// The visibility pass (vgc_visibility, below) draws a cut's expanded index buffer through the same triangle setup,
+// size classes and queues, with 64-bit (depth | triangle id) fragments.
+//
 // Every expression rounds step by step in the written order (the library is compiled with -fmad=false), so the
 // oracle's C restatement reproduces the image bit for bit.
 #include "vgcut_host.h"
@@ -33,32 +36,45 @@ namespace {
 constexpr uint32_t kLaneRasterMax = 16;     // bounding-box pixels up to which a triangle is drawn by its lane
 constexpr uint32_t kWarpRasterMax = 1024;   // ... by one warp of the second kernel; beyond, as tiles
 constexpr uint32_t kTileW = 32, kTileH = 16;
-constexpr uint32_t kQueuedMedium = 1u << 18;  // queue capacities: medium triangles,
+constexpr uint32_t kQueuedMedium = 1u << 19;  // queue capacities: medium triangles,
 constexpr uint32_t kSubQueues = 256;          //   in sub-queues (record i of sub-queue q at i * kSubQueues + q),
 constexpr uint32_t kCtlWords = 4 + kSubQueues;
 constexpr uint32_t kQueuedLarge = 1u << 16;   // large triangles,
 constexpr uint32_t kTileUnits = 1u << 20;     // and their tiles
 constexpr uint32_t kNoTri = 0xffffffffu;      // an empty tile record
+constexpr uint32_t kRecord = 5;               // float4 per queued triangle
 
+// Where the fragments go, and the queues of the second kernel.
 struct RasterArgs {
-  float vp[16];  // P * V, row-major 4x4 (float of the double product)
   uint32_t width, height;
-  uint32_t *depth;             // float bits
-  const uint4 *draw_list;      // cut 0 entries of the source slot
-  const uint32_t *counters;    // its counter header
-  uint32_t max_drawn;
+  uint32_t *depth;               // occluder pass: float bits per pixel
+  unsigned long long *vis;       // visibility pass: (depth bits << 32 | id) per pixel
+  uint32_t frame;                // visibility pass: lodBlendFrame
   // queues: ctl[1] = large triangles, ctl[2..3] = tiles (64-bit), ctl[4 + q] = medium triangles of sub-queue q;
-  // triangle records (4 float4 each: the ScreenTri and, for large ones, its tile columns); tile records (large
-  // triangle, tile index in its bounding box, row-major)
+  // triangle records (kRecord float4: the ScreenTri, its tile columns and its tag); tile records (large triangle,
+  // tile index in its bounding box, row-major)
   uint32_t *ctl;
   float4 *medium;
   float4 *large;
   uint2 *tiles;
 };
 
+// The occluder pass's inputs.
+struct OccluderArgs {
+  float vp[16];  // P * V, row-major 4x4 (float of the double product)
+  const uint4 *draw_list;      // cut 0 entries of the source slot
+  const uint32_t *counters;    // its counter header
+  uint32_t max_drawn;
+};
+
 struct ScreenTri {
   float ax, ay, az, bx, by, bz, cx, cy, cz, area;
   int x0, x1, y0, y1;  // pixel bounding box, inclusive
+};
+
+// What a visibility fragment carries besides its depth: the entry's blend range and the triangle's id.
+struct TriTag {
+  uint32_t lo, hi, id;
 };
 
 // A vertex in screen space: x, y (pixels, y down), NDC depth; w = 1 when usable (in front of the near plane).
@@ -95,53 +111,66 @@ __device__ __forceinline__ bool setup_triangle(float4 v0, float4 v1, float4 v2, 
   return t.x0 <= t.x1 && t.y0 <= t.y1;
 }
 
-__device__ __forceinline__ void shade_pixel(const ScreenTri &t, int px, int py, uint32_t W, uint32_t *depth) {
+// lodBlendMask (lodBlend.ts:36-45) at pixel (px, py): true when the pixel's step lies in [lo, hi).
+__device__ __forceinline__ bool blend_keep(int px, int py, uint32_t frame, uint32_t lo, uint32_t hi) {
+  const float x = (float(px) + 0.5f) + float(frame) * 5.588238f, y = float(py) + 0.5f;
+  const float a = x * 0.06711056f + y * 0.00583715f;
+  const float b = (a - floorf(a)) * 52.9829189f;
+  const float step = floorf((b - floorf(b)) * 255.0f);
+  return step >= float(lo) && step < float(hi);
+}
+
+// One pixel of t: covered when its centre is inside the three edge functions (edges included); the depth is the
+// screen-space interpolation of the corners' NDC depths, kept as a minimum (depth >= 0, so the unsigned order of
+// the bits is the float order; the atomics' results are unused, so they do not wait).
+template <bool VIS>
+__device__ __forceinline__ void shade_pixel(const RasterArgs &R, const ScreenTri &t, const TriTag &g, int px, int py) {
   const float x = float(px) + 0.5f, y = float(py) + 0.5f;
   const float wa = (t.cx - t.bx) * (y - t.by) - (t.cy - t.by) * (x - t.bx);  // edge B -> C
   const float wb = (t.ax - t.cx) * (y - t.cy) - (t.ay - t.cy) * (x - t.cx);  // edge C -> A
   const float wc = (t.bx - t.ax) * (y - t.ay) - (t.by - t.ay) * (x - t.ax);  // edge A -> B
-  if (wa >= 0.0f && wb >= 0.0f && wc >= 0.0f) {
+  if (wa >= 0.0f && wb >= 0.0f && wc >= 0.0f && (!VIS || blend_keep(px, py, R.frame, g.lo, g.hi))) {
     float z = ((wa * t.az + wb * t.bz) + wc * t.cz) / t.area;
     z = z > 0.0f ? z : 0.0f;  // +0 for rounding below zero (and never -0, whose bits would sort last)
-    atomicMin(depth + (size_t)py * W + px, __float_as_uint(z));  // result unused: a fire-and-forget reduction
+    const size_t at = (size_t)py * R.width + px;
+    if (VIS)
+      atomicMin(R.vis + at, ((unsigned long long)__float_as_uint(z) << 32) | g.id);
+    else
+      atomicMin(R.depth + at, __float_as_uint(z));
   }
 }
 
-__device__ __forceinline__ void write_record(float4 *r, const ScreenTri &t, uint32_t extra) {
+__device__ __forceinline__ void write_record(float4 *r, const ScreenTri &t, uint32_t tx, const TriTag &g) {
   r[0] = make_float4(t.ax, t.ay, t.az, t.bx);
   r[1] = make_float4(t.by, t.bz, t.cx, t.cy);
   r[2] = make_float4(t.cz, t.area, __int_as_float(t.x0), __int_as_float(t.y0));
-  r[3] = make_float4(__int_as_float(t.x1), __int_as_float(t.y1), __uint_as_float(extra), 0.0f);
+  r[3] = make_float4(__int_as_float(t.x1), __int_as_float(t.y1), __uint_as_float(tx), 0.0f);
+  r[4] = make_float4(__uint_as_float(g.lo), __uint_as_float(g.hi), __uint_as_float(g.id), 0.0f);
 }
 
-__device__ __forceinline__ ScreenTri read_record(const float4 *r, uint32_t &extra) {
-  const float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
+__device__ __forceinline__ ScreenTri read_record(const float4 *r, uint32_t &tx, TriTag &g) {
+  const float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4];
   ScreenTri t;
   t.ax = r0.x, t.ay = r0.y, t.az = r0.z, t.bx = r0.w;
   t.by = r1.x, t.bz = r1.y, t.cx = r1.z, t.cy = r1.w;
   t.cz = r2.x, t.area = r2.y, t.x0 = __float_as_int(r2.z), t.y0 = __float_as_int(r2.w);
   t.x1 = __float_as_int(r3.x), t.y1 = __float_as_int(r3.y);
-  extra = __float_as_uint(r3.z);
+  tx = __float_as_uint(r3.z);
+  g.lo = __float_as_uint(r4.x), g.hi = __float_as_uint(r4.y), g.id = __float_as_uint(r4.z);
   return t;
 }
 
 // The whole warp over t's bounding box, 32 consecutive pixels (row-major) per step.
-__device__ __forceinline__ void warp_draw(const ScreenTri &t, uint32_t lane, uint32_t W, uint32_t *depth) {
+template <bool VIS>
+__device__ __forceinline__ void warp_draw(const RasterArgs &R, const ScreenTri &t, const TriTag &g, uint32_t lane) {
   const uint32_t bw = uint32_t(t.x1 - t.x0 + 1), count = bw * uint32_t(t.y1 - t.y0 + 1);
   const uint32_t q = 32 / bw, r = 32 % bw;  // a step of 32 pixels: q rows and r columns
   uint32_t x = lane % bw, y = lane / bw;
   for (uint32_t i = lane; i < count; i += 32) {
-    shade_pixel(t, t.x0 + int(x), t.y0 + int(y), W, depth);
+    shade_pixel<VIS>(R, t, g, t.x0 + int(x), t.y0 + int(y));
     x += r, y += q;
     if (x >= bw) x -= bw, y++;
   }
-}
-
-__global__ void __launch_bounds__(256) k_depth_clear(uint32_t *depth, size_t n, uint32_t *ctl) {
-  if (blockIdx.x == 0)
-    for (uint32_t i = threadIdx.x; i < kCtlWords; i += blockDim.x) ctl[i] = 0;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    depth[i] = 0x3f800000u;  // 1.0f
 }
 
 __device__ __forceinline__ uint32_t warp_scan_incl(uint32_t v) {
@@ -154,23 +183,112 @@ __device__ __forceinline__ uint32_t warp_scan_incl(uint32_t v) {
   return v;
 }
 
-__global__ void __launch_bounds__(128, 6) k_raster_occluders(Scene S, RasterArgs A) {
+// One triangle per lane of the warp (ok: set up; t, g: its setup and tag). Small triangles are drawn here; medium
+// and large ones are queued, one reservation of each kind for the whole warp (the atomics are issued before the small
+// triangles are drawn, so that their round trips overlap the drawing). Returns true for a lane whose triangle a full
+// queue turned away: the caller draws it with the whole warp.
+template <bool VIS>
+__device__ bool queue_triangles(const RasterArgs &R, uint32_t sub, uint32_t lane, bool ok, const ScreenTri &t,
+                                const TriTag &g) {
+  const uint32_t px = ok ? uint32_t(t.x1 - t.x0 + 1) * uint32_t(t.y1 - t.y0 + 1) : 0u;
+  const bool medium = px > kLaneRasterMax && px <= kWarpRasterMax, large = px > kWarpRasterMax;
+  const uint32_t mm = __ballot_sync(0xffffffffu, medium), lm = __ballot_sync(0xffffffffu, large);
+  const uint32_t tx = large ? (uint32_t(t.x1 - t.x0) + kTileW) / kTileW : 0u;
+  const uint32_t nt = large ? tx * ((uint32_t(t.y1 - t.y0) + kTileH) / kTileH) : 0u;
+  uint32_t ts = 0, total = 0;
+  if (lm) {
+    ts = warp_scan_incl(nt) - nt;
+    total = __shfl_sync(0xffffffffu, ts + nt, 31);
+  }
+  uint32_t at_m = 0, tri = 0;
+  unsigned long long at_t = 0;
+  if (lane == 0) {
+    if (mm) at_m = atomicAdd(R.ctl + 4 + sub, __popc(mm));
+    if (lm) {
+      tri = atomicAdd(R.ctl + 1, __popc(lm));
+      at_t = atomicAdd(reinterpret_cast<unsigned long long *>(R.ctl + 2), (unsigned long long)total);
+    }
+  }
+  if (px && px <= kLaneRasterMax)
+    for (int py = t.y0; py <= t.y1; py++)
+      for (int x = t.x0; x <= t.x1; x++) shade_pixel<VIS>(R, t, g, x, py);
+  bool left = false;
+  if (mm) {
+    const uint32_t at = __shfl_sync(0xffffffffu, at_m, 0) + __popc(mm & ((1u << lane) - 1u));
+    if (medium && at < kQueuedMedium / kSubQueues)
+      write_record(R.medium + ((size_t)at * kSubQueues + sub) * kRecord, t, 0u, g);
+    else if (medium)
+      left = true;
+  }
+  if (lm) {
+    tri = __shfl_sync(0xffffffffu, tri, 0);
+    at_t = __shfl_sync(0xffffffffu, at_t, 0);
+    if (tri + __popc(lm) <= kQueuedLarge && at_t + total <= kTileUnits) {
+      const uint32_t mine = tri + __popc(lm & ((1u << lane) - 1u));
+      if (large) write_record(R.large + (size_t)mine * kRecord, t, tx, g);
+      for (uint32_t rest = lm; rest; rest &= rest - 1) {  // the tile records, a triangle at a time
+        const uint32_t j = __ffs(rest) - 1;
+        const uint32_t nj = __shfl_sync(0xffffffffu, nt, j), sj = __shfl_sync(0xffffffffu, ts, j);
+        const uint32_t tj = __shfl_sync(0xffffffffu, mine, j);
+        for (uint32_t i = lane; i < nj; i += 32) R.tiles[at_t + sj + i] = make_uint2(tj, i);
+      }
+    } else {  // a queue is full: reserved tile slots below its capacity become empty records
+      for (unsigned long long i = at_t + lane; i < at_t + total && i < kTileUnits; i += 32)
+        R.tiles[i] = make_uint2(kNoTri, 0u);
+      if (large) left = true;
+    }
+  }
+  return left;
+}
+
+// The triangles a full queue turned away, one at a time, by the whole warp (left: this lane's).
+template <bool VIS>
+__device__ __forceinline__ void draw_left(const RasterArgs &R, uint32_t lane, bool left, const ScreenTri &t,
+                                          const TriTag &g) {
+  for (uint32_t pending = __ballot_sync(0xffffffffu, left); pending; pending &= pending - 1) {
+    const uint32_t o = __ffs(pending) - 1;
+    ScreenTri u;
+    u.ax = __shfl_sync(0xffffffffu, t.ax, o), u.ay = __shfl_sync(0xffffffffu, t.ay, o);
+    u.az = __shfl_sync(0xffffffffu, t.az, o), u.bx = __shfl_sync(0xffffffffu, t.bx, o);
+    u.by = __shfl_sync(0xffffffffu, t.by, o), u.bz = __shfl_sync(0xffffffffu, t.bz, o);
+    u.cx = __shfl_sync(0xffffffffu, t.cx, o), u.cy = __shfl_sync(0xffffffffu, t.cy, o);
+    u.cz = __shfl_sync(0xffffffffu, t.cz, o), u.area = __shfl_sync(0xffffffffu, t.area, o);
+    u.x0 = __shfl_sync(0xffffffffu, t.x0, o), u.x1 = __shfl_sync(0xffffffffu, t.x1, o);
+    u.y0 = __shfl_sync(0xffffffffu, t.y0, o), u.y1 = __shfl_sync(0xffffffffu, t.y1, o);
+    TriTag h;
+    h.lo = __shfl_sync(0xffffffffu, g.lo, o), h.hi = __shfl_sync(0xffffffffu, g.hi, o);
+    h.id = __shfl_sync(0xffffffffu, g.id, o);
+    warp_draw<VIS>(R, u, h, lane);
+  }
+}
+
+// Clears the image and the queues' control words.
+template <typename T>
+__global__ void __launch_bounds__(256) k_target_clear(T *image, size_t n, T value, uint32_t *ctl) {
+  if (blockIdx.x == 0)
+    for (uint32_t i = threadIdx.x; i < kCtlWords; i += blockDim.x) ctl[i] = 0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    image[i] = value;
+}
+
+__global__ void __launch_bounds__(128, 6) k_raster_occluders(Scene S, OccluderArgs O, RasterArgs R) {
   __shared__ float4 verts[4][256];     // per warp: the current meshlet's vertices in screen space (local ids < 256)
   __shared__ uint32_t packed[4][128];  // ... and its packed triangles
   float4 *sv = verts[threadIdx.x >> 5];
   uint32_t *st = packed[threadIdx.x >> 5];
   const uint32_t lane = threadIdx.x & 31;
-  const uint32_t n = min(A.counters[VGC_COUNTER_CUT0 + VGC_CUT_SELECTED], A.max_drawn);
+  const uint32_t n = min(O.counters[VGC_COUNTER_CUT0 + VGC_CUT_SELECTED], O.max_drawn);
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-  const float W = float(A.width), H = float(A.height);
+  const float W = float(R.width), H = float(R.height);
   const uint32_t sub = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) % kSubQueues;  // this warp's medium sub-queue
+  const TriTag none{0u, 0u, 0u};
   // Each step waits on memory several times (entry, instance and meshlet, vertices, triangles): the loads of a step
   // are issued together, and the next entry is fetched while this one is drawn.
   uint32_t e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  uint4 next = e < n ? A.draw_list[e] : make_uint4(0u, 0u, 0u, 0u);
+  uint4 next = e < n ? O.draw_list[e] : make_uint4(0u, 0u, 0u, 0u);
   for (; e < n; e += warps) {
     const uint4 d = next;
-    if (e + warps < n) next = A.draw_list[e + warps];
+    if (e + warps < n) next = O.draw_list[e + warps];
     if ((d.w & 0xffff00u) != (255u << 16)) continue;  // part 1 (blended): not an occluder
     const uint32_t slot = S.inst_slot[d.x];
     const float4 *col = S.inst + (size_t)d.x * 4;
@@ -189,8 +307,8 @@ __global__ void __launch_bounds__(128, 6) k_raster_occluders(Scene S, RasterArgs
     for (int r = 0; r < 4; r++)
 #pragma unroll
       for (int k = 0; k < 4; k++)
-        mvp[r][k] = ((A.vp[r * 4] * m[0][k] + A.vp[r * 4 + 1] * m[1][k]) + A.vp[r * 4 + 2] * m[2][k]) +
-                    A.vp[r * 4 + 3] * m[3][k];
+        mvp[r][k] = ((O.vp[r * 4] * m[0][k] + O.vp[r * 4 + 1] * m[1][k]) + O.vp[r * 4 + 2] * m[2][k]) +
+                    O.vp[r * 4 + 3] * m[3][k];
     // the meshlet's vertices (local ids 0 .. the largest its triangles use), each transformed once, 128 at a time
     uint32_t top = 0;
 #pragma unroll
@@ -212,72 +330,20 @@ __global__ void __launch_bounds__(128, 6) k_raster_occluders(Scene S, RasterArgs
         if (base + k * 32 + lane <= top) sv[base + k * 32 + lane] = screen_vertex(mvp, pos[k], W, H);
     }
     __syncwarp();
-    uint32_t big = 0;  // this lane's triangles left for the whole warp here (bit per round)
+    uint32_t left = 0;  // this lane's triangles turned away by a full queue (bit per round)
     for (uint32_t round = 0; round * 32 < tris; round++) {
       const uint32_t ti = round * 32 + lane, p = st[ti];
       ScreenTri t;
       bool ok = false;
       if (ti < tris) ok = setup_triangle(sv[p & 255u], sv[(p >> 8) & 255u], sv[(p >> 16) & 255u], W, H, t);
-      const uint32_t px = ok ? uint32_t(t.x1 - t.x0 + 1) * uint32_t(t.y1 - t.y0 + 1) : 0u;
-      // medium and large triangles: one reservation of each kind for the warp's round, issued before this round's
-      // small triangles are drawn so that the atomics' round trips overlap the drawing
-      const bool medium = px > kLaneRasterMax && px <= kWarpRasterMax, large = px > kWarpRasterMax;
-      const uint32_t mm = __ballot_sync(0xffffffffu, medium), lm = __ballot_sync(0xffffffffu, large);
-      const uint32_t tx = large ? (uint32_t(t.x1 - t.x0) + kTileW) / kTileW : 0u;
-      const uint32_t nt = large ? tx * ((uint32_t(t.y1 - t.y0) + kTileH) / kTileH) : 0u;
-      uint32_t ts = 0, total = 0;
-      if (lm) {
-        ts = warp_scan_incl(nt) - nt;
-        total = __shfl_sync(0xffffffffu, ts + nt, 31);
-      }
-      uint32_t at_m = 0, tri = 0;
-      unsigned long long at_t = 0;
-      if (lane == 0) {
-        if (mm) at_m = atomicAdd(A.ctl + 4 + sub, __popc(mm));
-        if (lm) {
-          tri = atomicAdd(A.ctl + 1, __popc(lm));
-          at_t = atomicAdd(reinterpret_cast<unsigned long long *>(A.ctl + 2), (unsigned long long)total);
-        }
-      }
-      if (px && px <= kLaneRasterMax)
-        for (int py = t.y0; py <= t.y1; py++)
-          for (int x = t.x0; x <= t.x1; x++) shade_pixel(t, x, py, A.width, A.depth);
-      if (mm) {
-        const uint32_t at = __shfl_sync(0xffffffffu, at_m, 0) + __popc(mm & ((1u << lane) - 1u));
-        if (medium && at < kQueuedMedium / kSubQueues)
-          write_record(A.medium + ((size_t)at * kSubQueues + sub) * 4, t, 0u);
-        else if (medium) big |= 1u << round;  // the queue is full: drawn below
-      }
-      if (lm) {
-        tri = __shfl_sync(0xffffffffu, tri, 0);
-        at_t = __shfl_sync(0xffffffffu, at_t, 0);
-        if (tri + __popc(lm) <= kQueuedLarge && at_t + total <= kTileUnits) {
-          const uint32_t mine = tri + __popc(lm & ((1u << lane) - 1u));
-          if (large) write_record(A.large + (size_t)mine * 4, t, tx);
-          for (uint32_t rest = lm; rest; rest &= rest - 1) {  // the tile records, a triangle at a time
-            const uint32_t j = __ffs(rest) - 1;
-            const uint32_t nj = __shfl_sync(0xffffffffu, nt, j), sj = __shfl_sync(0xffffffffu, ts, j);
-            const uint32_t tj = __shfl_sync(0xffffffffu, mine, j);
-            for (uint32_t i = lane; i < nj; i += 32) A.tiles[at_t + sj + i] = make_uint2(tj, i);
-          }
-        } else {  // a queue is full: reserved tile slots below its capacity become empty records, drawn below
-          for (unsigned long long i = at_t + lane; i < at_t + total && i < kTileUnits; i += 32)
-            A.tiles[i] = make_uint2(kNoTri, 0u);
-          if (large) big |= 1u << round;
-        }
-      }
+      if (queue_triangles<false>(R, sub, lane, ok, t, none)) left |= 1u << round;
     }
-    // triangles the queues had no room for: one at a time, the whole warp
     for (uint32_t round = 0; round * 32 < tris; round++) {
-      uint32_t pending = __ballot_sync(0xffffffffu, (big >> round) & 1u);
-      while (pending) {
-        const uint32_t owner = __ffs(pending) - 1;
-        pending &= pending - 1;
-        ScreenTri t;
-        const uint32_t p = st[round * 32 + owner];
-        setup_triangle(sv[p & 255u], sv[(p >> 8) & 255u], sv[(p >> 16) & 255u], W, H, t);
-        warp_draw(t, lane, A.width, A.depth);
-      }
+      const uint32_t ti = round * 32 + lane, p = st[ti];
+      const bool mine = (left >> round) & 1u;
+      ScreenTri t;
+      if (mine) setup_triangle(sv[p & 255u], sv[(p >> 8) & 255u], sv[(p >> 16) & 255u], W, H, t);
+      draw_left<false>(R, lane, mine, t, none);
     }
     __syncwarp();  // the vertex and triangle buffers are rewritten by the next entry
   }
@@ -285,39 +351,42 @@ __global__ void __launch_bounds__(128, 6) k_raster_occluders(Scene S, RasterArgs
 
 // The queued triangles, spread over the whole grid: a warp per medium triangle, then a warp per tile of a large one
 // (a lane per column of the tile).
-__global__ void __launch_bounds__(128) k_raster_queued(RasterArgs A) {
+template <bool VIS>
+__global__ void __launch_bounds__(128) k_raster_queued(RasterArgs R) {
   __shared__ uint32_t counts[kSubQueues];  // medium triangles per sub-queue
   __shared__ uint32_t most;
   if (threadIdx.x == 0) most = 0;
   __syncthreads();
   for (uint32_t q = threadIdx.x; q < kSubQueues; q += blockDim.x) {
-    counts[q] = min(A.ctl[4 + q], kQueuedMedium / kSubQueues);
+    counts[q] = min(R.ctl[4 + q], kQueuedMedium / kSubQueues);
     atomicMax(&most, counts[q]);
   }
   __syncthreads();
   const uint32_t lane = threadIdx.x & 31;
   // medium records are interleaved: slot u holds record u / kSubQueues of sub-queue u % kSubQueues
   const uint32_t n_medium = most * kSubQueues;
-  const uint32_t n = n_medium + (uint32_t)min(*reinterpret_cast<const unsigned long long *>(A.ctl + 2),
+  const uint32_t n = n_medium + (uint32_t)min(*reinterpret_cast<const unsigned long long *>(R.ctl + 2),
                                               (unsigned long long)kTileUnits);
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n; u += warps) {
     uint32_t tx;
+    TriTag g;
     if (u < n_medium) {
-      if (u / kSubQueues < counts[u % kSubQueues])
-        warp_draw(read_record(A.medium + (size_t)u * 4, tx), lane, A.width, A.depth);
+      if (u / kSubQueues < counts[u % kSubQueues]) {
+        const ScreenTri t = read_record(R.medium + (size_t)u * kRecord, tx, g);
+        warp_draw<VIS>(R, t, g, lane);
+      }
       continue;
     }
-    const uint2 tile = A.tiles[u - n_medium];
+    const uint2 tile = R.tiles[u - n_medium];
     if (tile.x == kNoTri) continue;
-    const ScreenTri t = read_record(A.large + (size_t)tile.x * 4, tx);
+    const ScreenTri t = read_record(R.large + (size_t)tile.x * kRecord, tx, g);
     const int px = t.x0 + int((tile.y % tx) * kTileW + lane), py0 = t.y0 + int((tile.y / tx) * kTileH);
     if (px > t.x1) continue;
     const int py1 = min(t.y1, py0 + int(kTileH) - 1);
-    for (int py = py0; py <= py1; py++) shade_pixel(t, px, py, A.width, A.depth);
+    for (int py = py0; py <= py1; py++) shade_pixel<VIS>(R, t, g, px, py);
   }
 }
-
 
 // ------------------------------------------------------------------------------------------------ visibility
 // Headless consumer of a cut (vgc_visibility): the cut's expanded index buffer drawn as the draw args say, with the
@@ -329,20 +398,18 @@ __global__ void __launch_bounds__(128) k_raster_queued(RasterArgs A) {
 //    the instance origin by the draw-distance fade clamp((maxDrawDistance - |V origin|) / (0.15 maxDrawDistance),
 //    0, 1), V the camera's view (GeometryPool.ts:1112-1119);
 //  * triangles are set up as in the occluder pass (pixel centres, edges included, back faces and triangles reaching
-//    in front of the near plane left out), one per lane, the large ones by the whole warp;
+//    in front of the near plane left out), one per lane, and drawn through the same size classes and queues;
 //  * a fragment is kept when the step floor(255 n) of its pixel lies in the entry's blend range [lo, hi), n the
 //    interleaved gradient noise fract(52.9829189 fract(0.06711056 x + 0.00583715 y)) at the pixel centre (x, y),
 //    x shifted by 5.588238 per `frame` (lodBlendFrame);
 //  * indices or entries outside the context's arrays (an index buffer not written by vgc_expand) drop their
 //    triangle.
 constexpr float kDrawDistanceFade = 0.15f;   // GeometryPool.ts:109
-constexpr uint32_t kVisLaneMax = 64;         // bounding-box pixels up to which a lane draws its triangle
 
 struct VisArgs {
   float vp[16];    // P * V, row-major
   float view[16];  // the camera's V (draw-distance fade), row-major
-  uint32_t width, height, frame, regions;  // regions: mesh slots * 2 (parts)
-  unsigned long long *vis;
+  uint32_t width, height, regions;  // regions: mesh slots * 2 (parts)
   const uint32_t *indices;
   uint64_t capacity;
   const uint4 *draw_list;  // the output slot's entries (draw slots of both cuts)
@@ -386,35 +453,8 @@ __device__ __forceinline__ float4 pulled_vertex(const Scene &S, const VisArgs &A
   return make_float4((nx * 0.5f + 0.5f) * float(A.width), (0.5f - ny * 0.5f) * float(A.height), nz, 1.0f);
 }
 
-// lodBlendMask (lodBlend.ts:36-45) at pixel (px, py): true when the pixel's step lies in [lo, hi).
-__device__ __forceinline__ bool blend_keep(int px, int py, uint32_t frame, uint32_t lo, uint32_t hi) {
-  const float x = (float(px) + 0.5f) + float(frame) * 5.588238f, y = float(py) + 0.5f;
-  const float a = x * 0.06711056f + y * 0.00583715f;
-  const float b = (a - floorf(a)) * 52.9829189f;
-  const float step = floorf((b - floorf(b)) * 255.0f);
-  return step >= float(lo) && step < float(hi);
-}
-
-__device__ __forceinline__ void vis_pixel(const ScreenTri &t, int px, int py, const VisArgs &A, uint32_t lo,
-                                          uint32_t hi, uint32_t payload) {
-  const float x = float(px) + 0.5f, y = float(py) + 0.5f;
-  const float wa = (t.cx - t.bx) * (y - t.by) - (t.cy - t.by) * (x - t.bx);
-  const float wb = (t.ax - t.cx) * (y - t.cy) - (t.ay - t.cy) * (x - t.cx);
-  const float wc = (t.bx - t.ax) * (y - t.ay) - (t.by - t.ay) * (x - t.ax);
-  if (wa >= 0.0f && wb >= 0.0f && wc >= 0.0f && blend_keep(px, py, A.frame, lo, hi)) {
-    float z = ((wa * t.az + wb * t.bz) + wc * t.cz) / t.area;
-    z = z > 0.0f ? z : 0.0f;
-    atomicMin(A.vis + (size_t)py * A.width + px, ((unsigned long long)__float_as_uint(z) << 32) | payload);
-  }
-}
-
-__global__ void __launch_bounds__(256) k_vis_clear(unsigned long long *vis, size_t n) {
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    vis[i] = VGC_VIS_EMPTY;
-}
-
 // One lane per triangle of the cut, in region order (mesh slot, then part), as the draw args give them.
-__global__ void __launch_bounds__(256) k_visibility(Scene S, VisArgs A) {
+__global__ void __launch_bounds__(256) k_visibility(Scene S, VisArgs A, RasterArgs R) {
   extern __shared__ uint32_t tri_start[];  // per region: first triangle in the laid-out order; [regions] = total
   if (threadIdx.x < 32) {  // warp 0 scans the regions' triangle counts
     uint32_t carry = 0;
@@ -430,6 +470,7 @@ __global__ void __launch_bounds__(256) k_visibility(Scene S, VisArgs A) {
   __syncthreads();
   const uint32_t total = tri_start[A.regions];
   const uint32_t lane = threadIdx.x & 31;
+  const uint32_t sub = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) % kSubQueues;  // this warp's medium sub-queue
   const uint32_t stride = gridDim.x * blockDim.x;
   // every lane of a warp runs the same number of steps (the warp draws its lanes' large triangles together)
   for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
@@ -459,35 +500,29 @@ __global__ void __launch_bounds__(256) k_visibility(Scene S, VisArgs A) {
         }
       }
     }
-    const bool big = ok && uint32_t(t.x1 - t.x0 + 1) * uint32_t(t.y1 - t.y0 + 1) > kVisLaneMax;
-    if (ok && !big)
-      for (int py = t.y0; py <= t.y1; py++)
-        for (int px = t.x0; px <= t.x1; px++) vis_pixel(t, px, py, A, lo, hi, payload);
-    for (uint32_t pending = __ballot_sync(0xffffffffu, big); pending; pending &= pending - 1) {
-      const uint32_t owner = __ffs(pending) - 1;
-      ScreenTri u;
-      u.ax = __shfl_sync(0xffffffffu, t.ax, owner), u.ay = __shfl_sync(0xffffffffu, t.ay, owner);
-      u.az = __shfl_sync(0xffffffffu, t.az, owner), u.bx = __shfl_sync(0xffffffffu, t.bx, owner);
-      u.by = __shfl_sync(0xffffffffu, t.by, owner), u.bz = __shfl_sync(0xffffffffu, t.bz, owner);
-      u.cx = __shfl_sync(0xffffffffu, t.cx, owner), u.cy = __shfl_sync(0xffffffffu, t.cy, owner);
-      u.cz = __shfl_sync(0xffffffffu, t.cz, owner), u.area = __shfl_sync(0xffffffffu, t.area, owner);
-      u.x0 = __shfl_sync(0xffffffffu, t.x0, owner), u.x1 = __shfl_sync(0xffffffffu, t.x1, owner);
-      u.y0 = __shfl_sync(0xffffffffu, t.y0, owner), u.y1 = __shfl_sync(0xffffffffu, t.y1, owner);
-      const uint32_t ulo = __shfl_sync(0xffffffffu, lo, owner), uhi = __shfl_sync(0xffffffffu, hi, owner);
-      const uint32_t upay = __shfl_sync(0xffffffffu, payload, owner);
-      const uint32_t bw = uint32_t(u.x1 - u.x0 + 1), count = bw * uint32_t(u.y1 - u.y0 + 1);
-      const uint32_t q = 32 / bw, rr = 32 % bw;
-      uint32_t x = lane % bw, y = lane / bw;
-      for (uint32_t i = lane; i < count; i += 32) {
-        vis_pixel(u, u.x0 + int(x), u.y0 + int(y), A, ulo, uhi, upay);
-        x += rr, y += q;
-        if (x >= bw) x -= bw, y++;
-      }
-    }
+    const TriTag g{lo, hi, payload};
+    const bool left = queue_triangles<true>(R, sub, lane, ok, t, g);
+    draw_left<true>(R, lane, left, t, g);
   }
 }
 
 }  // namespace
+
+// The queues of the second kernel (allocated once per context; the passes of one context share them, so calls on
+// different streams must not overlap).
+static int raster_queues(vgc_context *ctx, RasterArgs &R) {
+  const size_t medium_bytes = (size_t)kQueuedMedium * kRecord * 16, large_bytes = (size_t)kQueuedLarge * kRecord * 16;
+  const size_t ctl_bytes = 2048;
+  static_assert(kCtlWords * 4 <= ctl_bytes, "control words");
+  const int rc = dev_alloc(ctx, ctx->d_raster, ctl_bytes + medium_bytes + large_bytes + (size_t)kTileUnits * 8);
+  if (rc) return rc;
+  char *q = (char *)ctx->d_raster.ptr;
+  R.ctl = (uint32_t *)q;
+  R.medium = (float4 *)(q + ctl_bytes);
+  R.large = (float4 *)(q + ctl_bytes + medium_bytes);
+  R.tiles = (uint2 *)(q + ctl_bytes + medium_bytes + large_bytes);
+  return VGC_OK;
+}
 
 extern "C" int vgc_occluder_depth(vgc_context *ctx, uint32_t src_slot, const vgc_view *view, float *depth,
                                   uint32_t width, uint32_t height, vgc_stream stream) {
@@ -499,32 +534,24 @@ extern "C" int vgc_occluder_depth(vgc_context *ctx, uint32_t src_slot, const vgc
   int rc = sync_scene(ctx);
   if (rc) return rc;
   cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
-  RasterArgs A{};
+  OccluderArgs O{};
   for (int r = 0; r < 4; r++)
     for (int c = 0; c < 4; c++) {
       double s = 0;
       for (int i = 0; i < 4; i++) s += view->proj[i * 4 + r] * view->view[c * 4 + i];
-      A.vp[r * 4 + c] = (float)s;
+      O.vp[r * 4 + c] = (float)s;
     }
-  A.width = width;
-  A.height = height;
-  A.depth = reinterpret_cast<uint32_t *>(depth);
-  A.draw_list = (const uint4 *)ctx->d_draw.ptr + (size_t)src_slot * 2 * ctx->opts.max_meshlets;
-  A.counters = (const uint32_t *)ctx->d_counters.ptr + (size_t)src_slot * ctx->counter_words;
-  A.max_drawn = ctx->opts.max_meshlets;
-  // the queues: control words, medium and large triangle records, tile records
-  const size_t medium_bytes = (size_t)kQueuedMedium * 64, large_bytes = (size_t)kQueuedLarge * 64;
-  const size_t ctl_bytes = 2048;
-  static_assert(kCtlWords * 4 <= ctl_bytes, "control words");
-  if ((rc = dev_alloc(ctx, ctx->d_raster, ctl_bytes + medium_bytes + large_bytes + (size_t)kTileUnits * 8))) return rc;
-  char *q = (char *)ctx->d_raster.ptr;
-  A.ctl = (uint32_t *)q;
-  A.medium = (float4 *)(q + ctl_bytes);
-  A.large = (float4 *)(q + ctl_bytes + medium_bytes);
-  A.tiles = (uint2 *)(q + ctl_bytes + medium_bytes + large_bytes);
+  O.draw_list = (const uint4 *)ctx->d_draw.ptr + (size_t)src_slot * 2 * ctx->opts.max_meshlets;
+  O.counters = (const uint32_t *)ctx->d_counters.ptr + (size_t)src_slot * ctx->counter_words;
+  O.max_drawn = ctx->opts.max_meshlets;
+  RasterArgs R{};
+  R.width = width;
+  R.height = height;
+  R.depth = reinterpret_cast<uint32_t *>(depth);
+  if ((rc = raster_queues(ctx, R))) return rc;
   const size_t pixels = (size_t)width * height;
-  k_depth_clear<<<(unsigned)std::min<size_t>((pixels + 255) / 256, (size_t)ctx->sm_count * 16), 256, 0, st>>>(
-      A.depth, pixels, A.ctl);
+  k_target_clear<uint32_t><<<(unsigned)std::min<size_t>((pixels + 255) / 256, (size_t)ctx->sm_count * 16), 256, 0,
+                             st>>>(R.depth, pixels, 0x3f800000u, R.ctl);  // 1.0f
   CUDA_TRY(cudaGetLastError());
   if (ctx->positions.empty()) return VGC_OK;  // no mesh carries vertex data: nothing is an occluder
   // persistent grids of exactly the resident blocks: a grid-stride loop over a grid larger than one wave leaves the
@@ -532,11 +559,11 @@ extern "C" int vgc_occluder_depth(vgc_context *ctx, uint32_t src_slot, const vgc
   static int per_sm[2] = {0, 0};
   if (!per_sm[0]) {
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], k_raster_occluders, 128, 0));
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k_raster_queued, 128, 0));
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k_raster_queued<false>, 128, 0));
   }
-  k_raster_occluders<<<ctx->sm_count * std::max(1, per_sm[0]), 128, 0, st>>>(scene_of(ctx), A);
+  k_raster_occluders<<<ctx->sm_count * std::max(1, per_sm[0]), 128, 0, st>>>(scene_of(ctx), O, R);
   CUDA_TRY(cudaGetLastError());
-  k_raster_queued<<<ctx->sm_count * std::max(1, per_sm[1]), 128, 0, st>>>(A);
+  k_raster_queued<false><<<ctx->sm_count * std::max(1, per_sm[1]), 128, 0, st>>>(R);
   CUDA_TRY(cudaGetLastError());
   return VGC_OK;
 }
@@ -565,9 +592,7 @@ extern "C" int vgc_visibility(vgc_context *ctx, uint32_t slot, uint32_t cut, con
     }
   A.width = width;
   A.height = height;
-  A.frame = frame;
   A.regions = ctx->out_slot_capacity * 2;
-  A.vis = reinterpret_cast<unsigned long long *>(vis);
   A.indices = indices;
   A.capacity = capacity;
   A.draw_list = (const uint4 *)ctx->d_draw.ptr + (size_t)slot * 2 * ctx->opts.max_meshlets;
@@ -578,16 +603,26 @@ extern "C" int vgc_visibility(vgc_context *ctx, uint32_t slot, uint32_t cut, con
   A.instances = (uint32_t)ctx->inst_slot.size();
   A.meshlet_vertices = (uint32_t)ctx->m_verts.size();
   A.vertices = (uint32_t)ctx->positions.size();
+  RasterArgs R{};
+  R.width = width;
+  R.height = height;
+  R.vis = reinterpret_cast<unsigned long long *>(vis);
+  R.frame = frame;
+  if ((rc = raster_queues(ctx, R))) return rc;
   const size_t pixels = (size_t)width * height;
-  k_vis_clear<<<(unsigned)std::min<size_t>((pixels + 255) / 256, (size_t)ctx->sm_count * 16), 256, 0, st>>>(A.vis,
-                                                                                                        pixels);
+  k_target_clear<unsigned long long>
+      <<<(unsigned)std::min<size_t>((pixels + 255) / 256, (size_t)ctx->sm_count * 16), 256, 0, st>>>(
+          R.vis, pixels, (unsigned long long)VGC_VIS_EMPTY, R.ctl);
   CUDA_TRY(cudaGetLastError());
   if (ctx->positions.empty()) return VGC_OK;  // no mesh carries vertex data
   const size_t smem = (A.regions + 1) * sizeof(uint32_t);
   if (smem > 48 * 1024) return fail(VGC_INVALID_ARG, "too many mesh slots for vgc_visibility");
-  int per_sm = 0;
+  int per_sm = 0, per_sm_queued = 0;
   CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_visibility, 256, smem));
-  k_visibility<<<ctx->sm_count * std::max(1, per_sm), 256, smem, st>>>(scene_of(ctx), A);
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_queued, k_raster_queued<true>, 128, 0));
+  k_visibility<<<ctx->sm_count * std::max(1, per_sm), 256, smem, st>>>(scene_of(ctx), A, R);
+  CUDA_TRY(cudaGetLastError());
+  k_raster_queued<true><<<ctx->sm_count * std::max(1, per_sm_queued), 128, 0, st>>>(R);
   CUDA_TRY(cudaGetLastError());
   return VGC_OK;
 }
