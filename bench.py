@@ -76,33 +76,42 @@ def read_traffic(kernel: str):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
+    """nvidia-smi clocks and throttle reasons sampled every 20 ms while the timed region runs. The sampler is live
+    (its first row read) before the region starts, so that a short region still gets samples; the summary uses the
+    rows read inside the region, else the last row read before it (`samples_in_region` says which)."""
 
     FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
 
     def __init__(self, device: int):
         self.device = device
-        self.rows = []
+        self.rows = []  # (time, fields)
         self.proc = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            deadline = time.perf_counter() + 5.0
+            while not self.rows and time.perf_counter() < deadline and self.proc.poll() is None:
+                time.sleep(0.005)
         except OSError:
             self.proc = None
+        self.t0 = time.perf_counter()
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+            self.rows.append((time.perf_counter(), [x.strip() for x in line.split(",")]))
 
     def __exit__(self, *exc):
+        self.t1 = time.perf_counter()
         if self.proc:
+            time.sleep(0.03)  # the row that covers the region's end
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -110,18 +119,21 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        if not self.rows:
+        inside = [r for t, r in self.rows if self.t0 is not None and self.t0 <= t <= self.t1 + 0.03]
+        before = [r for t, r in self.rows if self.t0 is not None and t < self.t0]
+        rows = inside or before[-1:]
+        if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        sm = [float(r[1]) for r in rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = set()
-        for r in self.rows:
+        for r in rows:
             for i, n in enumerate(names):
                 if len(r) > 5 + i and r[5 + i].lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+                "reasons": sorted(reasons), "samples": len(rows), "samples_in_region": len(inside)}
 
 
 def dist_setup():
