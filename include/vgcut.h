@@ -194,6 +194,13 @@ int vgc_mesh_set_flags(vgc_context *ctx, uint32_t slot, const vgc_mesh_opts *opt
    only the changed matrices are uploaded and the cells are recomputed on the device (synchronous: it waits for the
    device's earlier work and finishes before returning); the Morton order of the instances is kept. */
 int vgc_instances_update(vgc_context *ctx, uint32_t slot, uint32_t first, uint32_t count, const float *matrices);
+/* Re-sort of a mesh's instances along the Morton curve of their current positions (mortonOrder,
+   GeometryPool.ts:1263-1284, which the reference runs only when a mesh is added): after instances have moved,
+   consecutive GPU indices are close again and the 128-instance cells compact. With the scene resident the codes,
+   the stable radix sort, the permutation and the cells are computed on the device; the host mirror follows.
+   Stable with respect to the current GPU order. new_to_old (optional, instance_count entries) receives, for each new
+   GPU index, the GPU index the instance had before. Synchronous. */
+int vgc_instances_resort(vgc_context *ctx, uint32_t slot, uint32_t *new_to_old);
 /* mesh.dispose() (GeometryPool.remove :358-363) */
 int vgc_mesh_remove(vgc_context *ctx, uint32_t slot);
 /* Highest used mesh slot + 1 and the slot capacity (mesh table size). */

@@ -338,16 +338,21 @@ def instance_spheres(matrices: np.ndarray, sphere) -> np.ndarray:
     return out
 
 
-def morton_order(matrices: np.ndarray, sphere) -> np.ndarray:
-    """mortonOrder (GeometryPool.ts:1263-1284): stable sort by 30-bit Morton code of the sphere centres."""
+def morton_codes(matrices: np.ndarray, sphere) -> np.ndarray:
+    """The 30-bit Morton codes mortonOrder (GeometryPool.ts:1263-1284) sorts by: sphere centres quantised to 1024
+    steps of the largest extent over the instances."""
     s = instance_spheres(matrices, sphere)
     if len(s) == 0:
         return np.zeros(0, np.uint32)
     lo, hi = s[:, :3].min(0), s[:, :3].max(0)
     extent = max(float((hi - lo).max()), 1e-9)
     q = np.clip(np.floor((s[:, :3] - lo) / extent * 1024), 0, 1023).astype(np.uint32)
-    codes = _spread10(q[:, 0]) | (_spread10(q[:, 1]) << 1) | (_spread10(q[:, 2]) << 2)
-    return np.argsort(codes, kind="stable").astype(np.uint32)
+    return _spread10(q[:, 0]) | (_spread10(q[:, 1]) << 1) | (_spread10(q[:, 2]) << 2)
+
+
+def morton_order(matrices: np.ndarray, sphere) -> np.ndarray:
+    """mortonOrder (GeometryPool.ts:1263-1284): stable sort by 30-bit Morton code of the sphere centres."""
+    return np.argsort(morton_codes(matrices, sphere), kind="stable").astype(np.uint32)
 
 
 def compute_cells(matrices_gpu: np.ndarray, sphere, slot: int, instance_base: int, cell_size: int = 128) -> np.ndarray:

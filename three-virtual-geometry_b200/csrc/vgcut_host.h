@@ -163,5 +163,9 @@ int prepare(vgc_context *ctx, LaunchScratch &s, const vgc_view *views, uint32_t 
 int enqueue(vgc_context *ctx, LaunchScratch &s, uint32_t count, cudaStream_t st, bool capture);
 // vgc_stats of one view from its counter header and dyn[0] (the threshold the cut used).
 void decode_stats(const vgc_context *ctx, const uint32_t *counters, float threshold, vgc_stats *s);
+// Host mirror: cell `cell` of mesh `slot` from its instances (computeCell, GeometryPool.ts:519-545).
+void compute_cell(vgc_context *ctx, uint32_t slot, uint32_t cell);
+// Host mirror: mortonOrder (GeometryPool.ts:1263-1284) of n column-major matrices.
+void morton_order(const float *m, uint32_t n, const float *sphere, std::vector<uint32_t> &order);
 
 }  // namespace vgch

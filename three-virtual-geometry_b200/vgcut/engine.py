@@ -151,6 +151,7 @@ def lib() -> C.CDLL:
         "vgc_debug_scene": ([vp, P(C.c_float), C.c_uint32, P(C.c_float), C.c_uint32, P(C.c_uint32), P(C.c_uint32)], C.c_int),
         "vgc_debug_cells_device": ([vp, P(C.c_float), C.c_uint32, P(C.c_uint32)], C.c_int),
         "vgc_occluder_depth": ([vp, C.c_uint32, P(View), vp, C.c_uint32, C.c_uint32, vp], C.c_int),
+        "vgc_instances_resort": ([vp, C.c_uint32, P(C.c_uint32)], C.c_int),
         "vgc_visibility": ([vp, C.c_uint32, C.c_uint32, P(View), P(View), vp, C.c_uint64, vp, C.c_uint32, C.c_uint32,
                             C.c_uint32, vp], C.c_int),
         "vgc_server_default_options": ([P(ServerOptions)], None),
@@ -327,6 +328,17 @@ class VirtualMesh:
         block = np.ascontiguousarray(self._matrices[lo:hi + 1])
         check(lib().vgc_instances_update(self.vg.handle, self.slot, lo, hi - lo + 1, _fp(block)))
         self._dirty.clear()
+
+    def resort(self) -> np.ndarray:
+        """Morton re-sort of the instances at their current positions (vgc_instances_resort), after pending
+        set_matrix_at calls are committed; returns new_to_old (previous GPU index of each new GPU index)."""
+        self.commit_instances()
+        new_to_old = np.zeros(self.instance_count, np.uint32)
+        check(lib().vgc_instances_resort(self.vg.handle, self.slot, _up(new_to_old)))
+        self.gpu_to_input = self.gpu_to_input[new_to_old]
+        self.gpu_index_of[self.gpu_to_input] = np.arange(self.instance_count, dtype=np.uint32)
+        self._matrices = self._matrices[new_to_old]
+        return new_to_old
 
     def dispose(self) -> None:
         check(lib().vgc_mesh_remove(self.vg.handle, self.slot))
