@@ -219,10 +219,10 @@ int vgc_hzb_build(vgc_context *ctx, int32_t hzb, const float *depth, uint32_t wi
 int vgc_cut(vgc_context *ctx, const vgc_view *views, uint32_t count, uint32_t first_slot, vgc_stream stream);
 
 /* The plain single-view cut with no device allocation on the call. It has no counterpart in the reference. For
-   callers that cannot call cudaMalloc while they run - a renderer's frame loop that records into a CUDA graph or
-   runs on a real-time thread, or a host that reserves all of its GPU memory up front - it keeps its per-call
-   scratch in a fixed 1.5 MiB device array inside the library (held by every GPU that loads it until the process
-   exits) rather than in context allocations. Limits: a scene of at most 65,536 cells (8,388,608 instances); the
+   callers that cannot call cudaMalloc while they run - a renderer's real-time frame thread, which must not stall on
+   the device-wide synchronisation an allocation can cause, or a host that reserves all of its GPU memory up front
+   and hands nothing else out - it keeps its per-call scratch in a fixed 1.5 MiB device array inside the library
+   (held by every GPU that loads it until the process exits) rather than in context allocations. Limits: a scene of at most 65,536 cells (8,388,608 instances); the
    output slot, the view's state slot and (for a view with `depth`) its HZB slot at that size must already exist
    (create the context with enough output_slots; build the HZB once with vgc_hzb_build); the scene must have been
    published by an earlier vgc_cut after the last mesh change. Meshlet chunks past the fixed queue are tested in

@@ -1,7 +1,7 @@
 """vgc_cut_noalloc, the single-view cut that allocates no device memory on the call, against vgc_cut.
 
-Callers such as a renderer's frame loop recorded into a CUDA graph, or a real-time thread where cudaMalloc is not
-allowed, use this entry point; its scratch is a fixed device array inside the library. The results must be the
+Callers that cannot allocate while they run, such as a renderer's real-time frame thread that must not stall on
+cudaMalloc or a host that reserves all of its GPU memory up front, use this entry point; its scratch is a fixed device array inside the library. The results must be the
 ones vgc_cut produces for the same view, call after call (the array keeps the previous call's contents, so a
 second call checks that everything that must start at zero is cleared). This file is collected last on purpose.
 """
