@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bound of the CPU-baseline sample")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batching, occluder, large-world and serving sections")
-    ap.add_argument("--extras", default="batching,occluders,visibility,large_world,serve",
+    ap.add_argument("--extras", default="batching,occluders,visibility,updates,large_world,serve",
                     help="comma-separated sections to run after the headline line's measurement")
     ap.add_argument("--serve-rate", type=float, default=10_000.0, help="Poisson request rate of the serving section")
     ap.add_argument("--serve-requests", type=int, default=20_000)
@@ -457,6 +457,8 @@ def run_ours(args, world, rank, local):
             line["occluders"] = run_occluders(spec, args, flush, stream)
         if "visibility" in extras:
             line["visibility"] = run_visibility(spec, args, flush, stream)
+        if "updates" in extras:
+            line["updates"] = run_updates(spec, args, flush, stream)
         if "large_world" in extras:
             line["large_world"] = run_large_world(spec, args, flush, stream)
         if "serve" in extras:
@@ -646,6 +648,74 @@ def run_visibility(ruins, args, flush, stream):
                 expand_and_visibility_ms_per_view=draw_ms / P, loop_ms_per_step=loop_ms,
                 views_per_sec=P / (loop_ms / 1e3), triangles_per_view=tris,
                 triangles_per_sec=tris * P / (draw_ms / 1e3), coverage_last_view=covered)
+
+
+def run_updates(ruins, args, flush, stream):
+    """Instance updates and the Morton re-sort on the ruins-like scene: every instance of every mesh moves to another
+    instance's place (commitInstances on the device), which leaves the 128-instance cells spread over the whole
+    world; vgc_instances_resort then restores compact cells. Batched views/s of the 32 poses before, after the move
+    and after the re-sort (no occlusion)."""
+    import numpy as np
+    import torch
+    from vgcut import engine, scenes
+    vg = engine.VirtualGeometry(max_triangles=10_000_000, max_shadow_triangles=4_000_000, max_meshlets=1 << 18,
+                                output_slots=len(ruins.cameras))
+    meshes = scenes.load_into(vg, ruins)
+    P = len(ruins.cameras)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    views = [engine.make_view(c, engine.ViewParams(error_threshold=1.0, state_slot=k, fresh_state=True))
+             for k, c in enumerate(ruins.cameras)]
+
+    def views_per_sec():
+        for _ in range(max(3, args.warmup)):
+            vg.cut(views, first_slot=0, stream=sp, graph=True)
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            vg.cut(views, first_slot=0, stream=sp, graph=True)
+            b.record(stream)
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        return P / (statistics.mean(ms) / 1e3)
+
+    def cell_radius():
+        cells, _ = vg.debug_scene()
+        return float(cells[:, 3].mean())
+
+    before, r_before = views_per_sec(), cell_radius()
+    rng = np.random.default_rng(31)
+    moved = []
+    for mats in ruins.instances:
+        m = np.array(mats, np.float32).reshape(-1, 16)
+        perm = rng.permutation(len(m))
+        m[:, 12:15] = m[perm, 12:15]
+        moved.append(m)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for mesh, m in zip(meshes, moved):
+        mesh.set_matrices(m)
+        mesh.commit_instances()  # synchronous: upload + cells on the device
+    commit_ms = (time.perf_counter() - t) * 1e3
+    scattered, r_scattered = views_per_sec(), cell_radius()
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for mesh in meshes:
+        mesh.resort()  # synchronous: codes, sort, permutation, cells on the device; host mirror follows
+    resort_ms = (time.perf_counter() - t) * 1e3
+    resorted, r_resorted = views_per_sec(), cell_radius()
+    n = sum(len(m) for m in moved)
+    vg.dispose()
+    return dict(workload=f"ruins-like scene, {n} instances: every instance moved to another's place, then re-sorted; "
+                         f"{P} poses, batched, no occlusion",
+                commit_ms=commit_ms, resort_ms=resort_ms, instances=n,
+                views_per_sec_before=before, views_per_sec_moved=scattered, views_per_sec_resorted=resorted,
+                mean_cell_radius_before=r_before, mean_cell_radius_moved=r_scattered,
+                mean_cell_radius_resorted=r_resorted,
+                note="commit and re-sort times are host wall clock around the synchronous calls (all meshes)")
 
 
 def run_large_world(ruins, args, flush, stream):

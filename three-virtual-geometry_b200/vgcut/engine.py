@@ -321,6 +321,13 @@ class VirtualMesh:
         self._matrices[g] = np.asarray(matrix, np.float32).reshape(16)
         self._dirty.add(g)
 
+    def set_matrices(self, matrices: np.ndarray) -> None:
+        """Updates every instance (caller order, (n, 16)); ``commit_instances`` uploads them in one call."""
+        m = np.ascontiguousarray(matrices, np.float32).reshape(self.instance_count, 16)
+        self._matrices[:] = m[self.gpu_to_input]
+        if self.instance_count:
+            self._dirty.update((0, self.instance_count - 1))
+
     def commit_instances(self) -> None:
         if not self._dirty:
             return
