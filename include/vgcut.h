@@ -303,7 +303,9 @@ int vgc_server_destroy(vgc_server *server);
    reference, only the meshlets drawn over every pixel (part 0) are drawn, back faces are culled, and a triangle is
    sampled at pixel centres; triangles reaching in front of the near plane are left out (fewer occluders only cull
    less). Pass `depth` as this frame's vgc_view.depth to build the HZB from it in the cut's own launch sequence.
-   Asynchronous on `stream`. */
+   The first call allocates the context's triangle queues (about 53 MB, shared with vgc_visibility); calls on one
+   context whose GPU work overlaps (different streams) race on them: order them on one stream. Asynchronous on
+   `stream`. */
 int vgc_occluder_depth(vgc_context *ctx, uint32_t src_slot, const vgc_view *view, float *depth, uint32_t width,
                        uint32_t height, vgc_stream stream);
 
@@ -315,7 +317,8 @@ int vgc_occluder_depth(vgc_context *ctx, uint32_t src_slot, const vgc_view *view
    centre, `frame` as lodBlendFrame), rasterized with `view` at pixel centres, back faces and triangles reaching in
    front of the near plane left out, into `vis` (device, width x height u64, row 0 at the top): per pixel the
    minimum of (NDC depth bits << 32 | drawSlot << 7 | triangle in its meshlet), VGC_VIS_EMPTY where nothing is
-   drawn. Meshes without vertex data are not drawn. Asynchronous on `stream`. */
+   drawn. Meshes without vertex data are not drawn. Uses the context's triangle queues (see vgc_occluder_depth):
+   calls whose GPU work overlaps race on them. Asynchronous on `stream`. */
 #define VGC_VIS_EMPTY 0x3f800000ffffffffull
 int vgc_visibility(vgc_context *ctx, uint32_t slot, uint32_t cut, const vgc_view *view, const vgc_view *fade_view,
                    const uint32_t *indices, uint64_t capacity, uint64_t *vis, uint32_t width, uint32_t height,
