@@ -51,6 +51,10 @@ def parse():
     ap.add_argument("--extras", default="batching,occluders,visibility,updates,large_world,serve",
                     help="comma-separated sections to run after the headline line's measurement")
     ap.add_argument("--serve-rate", type=float, default=10_000.0, help="Poisson request rate of the serving section")
+    ap.add_argument("--serve-max-meshlets", type=int, default=1 << 17,
+                    help="draw-list capacity (meshlets per cut) of each serving scene's views")
+    ap.add_argument("--serve-max-triangles", type=int, default=10_000_000,
+                    help="triangle capacity (camera cut) of each serving scene's views")
     ap.add_argument("--serve-requests", type=int, default=20_000)
     return ap.parse_args()
 
@@ -774,8 +778,8 @@ def run_serve(ruins, args):
     specs = scenes.serving_scenes(ruins.meshes, ruins.mesh_triangles, ruins.notes["weight_exponent"])
     vgs = []
     for sp in specs:
-        vg = engine.VirtualGeometry(max_triangles=10_000_000, max_shadow_triangles=2_000_000, max_meshlets=1 << 17,
-                                    output_slots=1)
+        vg = engine.VirtualGeometry(max_triangles=args.serve_max_triangles, max_shadow_triangles=2_000_000,
+                                    max_meshlets=args.serve_max_meshlets, output_slots=1)
         scenes.load_into(vg, sp)
         vgs.append(vg)
     import numpy as np
@@ -821,7 +825,9 @@ def run_serve(ruins, args):
         return dict(views_per_sec=len(results) / span_s, p50_ms=percentile(lat, 0.5), p99_ms=percentile(lat, 0.99),
                     p999_ms=percentile(lat, 0.999), mean_batch=delta["views_launched"] / max(1, delta["batches"]),
                     batches=delta["batches"],
-                    batch_gpu_ms_mean=statistics.mean(r["batch_gpu_ms"] for r in results))
+                    batch_gpu_ms_mean=statistics.mean(r["batch_gpu_ms"] for r in results),
+                    rounds_mean=statistics.mean(r["stats"]["rounds"] for r in results),
+                    overflow_share=statistics.mean(1.0 if r["stats"]["overflow"] else 0.0 for r in results))
 
     try:
         run_stream([(0.0, i) for i in range(256)], False)  # warm-up
@@ -849,7 +855,8 @@ def run_serve(ruins, args):
                 poisson=dict(paced, note="Poisson arrivals at min(requested rate, 70% of capacity)"),
                 max_in_flight=st["max_in_flight"], hbm_budget_bytes=budget, max_bytes_in_use=st["max_bytes_in_use"],
                 latency_note="submit -> completion seen by the server, host steady clock",
-                config=dict(streams=4, max_batch=64, slots_per_scene=64))
+                config=dict(streams=4, max_batch=64, slots_per_scene=64, max_meshlets=args.serve_max_meshlets,
+                            max_triangles=args.serve_max_triangles))
 
 
 def main():
