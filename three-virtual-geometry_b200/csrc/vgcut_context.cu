@@ -719,7 +719,7 @@ int vgc_context_destroy(vgc_context *ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   free_scratch(ctx->scratch);
   for (DevBuf *b : {&ctx->d_meshes, &ctx->d_levels, &ctx->d_m_lod, &ctx->d_m_parent, &ctx->d_m_err, &ctx->d_m_cull,
-                    &ctx->d_lsamples, &ctx->d_positions, &ctx->d_m_verts, &ctx->d_raster,
+                    &ctx->d_lsamples, &ctx->d_positions, &ctx->d_m_verts, &ctx->d_raster, &ctx->d_resort,
                     &ctx->d_m_info, &ctx->d_m_tris, &ctx->d_inst, &ctx->d_inst_slot, &ctx->d_cells, &ctx->d_counters,
                     &ctx->d_draw, &ctx->d_args, &ctx->d_dyn, &ctx->d_hist, &ctx->d_state, &ctx->d_hzb_desc})
     dev_free(ctx, *b);

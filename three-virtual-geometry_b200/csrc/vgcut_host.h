@@ -103,6 +103,7 @@ struct vgc_context {
   DevBuf d_meshes, d_levels, d_m_lod, d_m_parent, d_m_err, d_m_cull, d_m_info, d_m_tris, d_inst, d_inst_slot, d_cells;
   DevBuf d_lsamples, d_positions, d_m_verts;
   DevBuf d_raster;  // occluder depth pass: the tile pass's work lists
+  DevBuf d_resort;  // instance re-sort: centres, keys, permutation scratch (grows only)
   // output slots
   uint32_t out_slots = 0;
   uint32_t out_slot_capacity = 0;  // slot_capacity the output buffers were sized for

@@ -128,10 +128,9 @@ extern "C" int vgc_instances_resort(vgc_context *ctx, uint32_t slot, uint32_t *n
                  inst_b = (size_t)n * 64;
     auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
     const size_t total = up(centres_b) + up(partial_b) + 256 + 4 * up(keys_b) + up(inst_b) + up(sort_bytes);
-    DevBuf tmp;
-    int rc = dev_alloc(ctx, tmp, total);
+    int rc = dev_alloc(ctx, ctx->d_resort, total);  // kept for later re-sorts (grows only)
     if (rc) return rc;
-    char *p = (char *)tmp.ptr;
+    char *p = (char *)ctx->d_resort.ptr;
     double *centres = (double *)p;
     p += up(centres_b);
     double *partial = (double *)p;
@@ -170,7 +169,6 @@ extern "C" int vgc_instances_resort(vgc_context *ctx, uint32_t slot, uint32_t *n
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(order.data(), idx_out, keys_b, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    dev_free(ctx, tmp);
     if (e != cudaSuccess) {
       cudaGetLastError();
       return fail(VGC_DEVICE_ERROR, std::string("vgc_instances_resort: ") + cudaGetErrorString(e));
