@@ -199,7 +199,8 @@ int vgc_instances_update(vgc_context *ctx, uint32_t slot, uint32_t first, uint32
    consecutive GPU indices are close again and the 128-instance cells compact. With the scene resident the codes,
    the stable radix sort, the permutation and the cells are computed on the device; the host mirror follows.
    Stable with respect to the current GPU order. new_to_old (optional, instance_count entries) receives, for each new
-   GPU index, the GPU index the instance had before. Synchronous. */
+   GPU index, the GPU index the instance had before; draw lists cut before the call keep the previous indices.
+   Synchronous; the first call allocates the context's re-sort scratch (about 110 bytes per instance, kept). */
 int vgc_instances_resort(vgc_context *ctx, uint32_t slot, uint32_t *new_to_old);
 /* mesh.dispose() (GeometryPool.remove :358-363) */
 int vgc_mesh_remove(vgc_context *ctx, uint32_t slot);
