@@ -14,7 +14,7 @@
 //    a meshlet's loads are issued together (its triangles, then its vertex ids, then positions, 128 at a time) and
 //    the warp's next entry is fetched while it draws this one: every step of this pass waits on memory;
 //  * triangles are sorted by the pixels of their bounding box: small ones (at most kLaneRasterMax) are drawn at once
-//    by their lane; medium ones (at most kWarpRasterMax) are queued, one atomic per warp and round of 32 triangles
+//    by the warp, their pixels laid end to end, a lane per pixel; medium ones (at most kWarpRasterMax) are queued, one atomic per warp and round of 32 triangles
 //    on one of kSubQueues counters, and drawn by the second kernel, a warp per triangle; larger ones are queued as
 //    32 x 16 pixel tiles of their bounding box, a warp per tile. The second kernel spreads both over the whole
 //    grid: a meshlet close to the camera, with a hundred triangles of a few hundred pixels each, would otherwise
@@ -183,13 +183,21 @@ __device__ __forceinline__ uint32_t warp_scan_incl(uint32_t v) {
   return v;
 }
 
+// Per warp: the small triangles of one round, staged so that the warp can draw their pixels 32 at a time whatever
+// triangle they belong to (structure of arrays: lanes reading different triangles hit different banks).
+struct SmallStage {
+  float ax[32], ay[32], az[32], bx[32], by[32], bz[32], cx[32], cy[32], cz[32], area[32];
+  int x0[32], y0[32];
+  uint32_t bw[32], lo[32], hi[32], id[32];
+};
+
 // One triangle per lane of the warp (ok: set up; t, g: its setup and tag). Small triangles are drawn here; medium
 // and large ones are queued, one reservation of each kind for the whole warp (the atomics are issued before the small
 // triangles are drawn, so that their round trips overlap the drawing). Returns true for a lane whose triangle a full
 // queue turned away: the caller draws it with the whole warp.
 template <bool VIS>
-__device__ bool queue_triangles(const RasterArgs &R, uint32_t sub, uint32_t lane, bool ok, const ScreenTri &t,
-                                const TriTag &g) {
+__device__ bool queue_triangles(const RasterArgs &R, SmallStage &sm, uint32_t sub, uint32_t lane, bool ok,
+                                const ScreenTri &t, const TriTag &g) {
   const uint32_t px = ok ? uint32_t(t.x1 - t.x0 + 1) * uint32_t(t.y1 - t.y0 + 1) : 0u;
   const bool medium = px > kLaneRasterMax && px <= kWarpRasterMax, large = px > kWarpRasterMax;
   const uint32_t mm = __ballot_sync(0xffffffffu, medium), lm = __ballot_sync(0xffffffffu, large);
@@ -209,9 +217,39 @@ __device__ bool queue_triangles(const RasterArgs &R, uint32_t sub, uint32_t lane
       at_t = atomicAdd(reinterpret_cast<unsigned long long *>(R.ctl + 2), (unsigned long long)total);
     }
   }
-  if (px && px <= kLaneRasterMax)
-    for (int py = t.y0; py <= t.y1; py++)
-      for (int x = t.x0; x <= t.x1; x++) shade_pixel<VIS>(R, t, g, x, py);
+  // small triangles: their bounding-box pixels laid end to end in lane order, 32 per step (a lane per pixel), so a
+  // step's cost does not follow the largest small triangle of the round
+  const uint32_t n_small = (px && px <= kLaneRasterMax) ? px : 0u;
+  const uint32_t incl = warp_scan_incl(n_small), all = __shfl_sync(0xffffffffu, incl, 31);
+  if (all) {
+    if (n_small) {
+      sm.ax[lane] = t.ax, sm.ay[lane] = t.ay, sm.az[lane] = t.az, sm.bx[lane] = t.bx, sm.by[lane] = t.by;
+      sm.bz[lane] = t.bz, sm.cx[lane] = t.cx, sm.cy[lane] = t.cy, sm.cz[lane] = t.cz, sm.area[lane] = t.area;
+      sm.x0[lane] = t.x0, sm.y0[lane] = t.y0, sm.bw[lane] = uint32_t(t.x1 - t.x0 + 1);
+      sm.lo[lane] = g.lo, sm.hi[lane] = g.hi, sm.id[lane] = g.id;
+    }
+    __syncwarp();
+    for (uint32_t base = 0; base < all; base += 32) {
+      const uint32_t p = base + lane;
+      // owner: the first lane whose inclusive end exceeds p
+      uint32_t j = 0;
+#pragma unroll
+      for (uint32_t k = 16; k > 0; k >>= 1) {
+        const uint32_t e = __shfl_sync(0xffffffffu, incl, j + k - 1);
+        if (e <= p) j += k;
+      }
+      const uint32_t start = __shfl_sync(0xffffffffu, incl - n_small, j);
+      if (p < all) {
+        ScreenTri u;
+        u.ax = sm.ax[j], u.ay = sm.ay[j], u.az = sm.az[j], u.bx = sm.bx[j], u.by = sm.by[j], u.bz = sm.bz[j];
+        u.cx = sm.cx[j], u.cy = sm.cy[j], u.cz = sm.cz[j], u.area = sm.area[j];
+        const TriTag h{sm.lo[j], sm.hi[j], sm.id[j]};
+        const uint32_t q = p - start, w = sm.bw[j];
+        shade_pixel<VIS>(R, u, h, sm.x0[j] + int(q % w), sm.y0[j] + int(q / w));
+      }
+    }
+    __syncwarp();  // the stage is rewritten by the next round
+  }
   bool left = false;
   if (mm) {
     const uint32_t at = __shfl_sync(0xffffffffu, at_m, 0) + __popc(mm & ((1u << lane) - 1u));
@@ -274,6 +312,8 @@ __global__ void __launch_bounds__(256) k_target_clear(T *image, size_t n, T valu
 __global__ void __launch_bounds__(128, 6) k_raster_occluders(Scene S, OccluderArgs O, RasterArgs R) {
   __shared__ float4 verts[4][256];     // per warp: the current meshlet's vertices in screen space (local ids < 256)
   __shared__ uint32_t packed[4][128];  // ... and its packed triangles
+  __shared__ SmallStage stage[4];
+  SmallStage &sm = stage[threadIdx.x >> 5];
   float4 *sv = verts[threadIdx.x >> 5];
   uint32_t *st = packed[threadIdx.x >> 5];
   const uint32_t lane = threadIdx.x & 31;
@@ -336,7 +376,7 @@ __global__ void __launch_bounds__(128, 6) k_raster_occluders(Scene S, OccluderAr
       ScreenTri t;
       bool ok = false;
       if (ti < tris) ok = setup_triangle(sv[p & 255u], sv[(p >> 8) & 255u], sv[(p >> 16) & 255u], W, H, t);
-      if (queue_triangles<false>(R, sub, lane, ok, t, none)) left |= 1u << round;
+      if (queue_triangles<false>(R, sm, sub, lane, ok, t, none)) left |= 1u << round;
     }
     for (uint32_t round = 0; round * 32 < tris; round++) {
       const uint32_t ti = round * 32 + lane, p = st[ti];
@@ -456,6 +496,8 @@ __device__ __forceinline__ float4 pulled_vertex(const Scene &S, const VisArgs &A
 // One lane per triangle of the cut, in region order (mesh slot, then part), as the draw args give them.
 __global__ void __launch_bounds__(256) k_visibility(Scene S, VisArgs A, RasterArgs R) {
   extern __shared__ uint32_t tri_start[];  // per region: first triangle in the laid-out order; [regions] = total
+  __shared__ SmallStage stage[8];
+  SmallStage &sm = stage[threadIdx.x >> 5];
   if (threadIdx.x < 32) {  // warp 0 scans the regions' triangle counts
     uint32_t carry = 0;
     for (uint32_t r0 = 0; r0 < A.regions; r0 += 32) {
@@ -501,7 +543,7 @@ __global__ void __launch_bounds__(256) k_visibility(Scene S, VisArgs A, RasterAr
       }
     }
     const TriTag g{lo, hi, payload};
-    const bool left = queue_triangles<true>(R, sub, lane, ok, t, g);
+    const bool left = queue_triangles<true>(R, sm, sub, lane, ok, t, g);
     draw_left<true>(R, lane, left, t, g);
   }
 }
