@@ -15,6 +15,18 @@ def small_ruins(seed=3, meshes=6, instances=3000, extent=220.0, poses=6, tri_lo=
                         poses=poses, width=width, height=height, target_full_detail=instances * 8_000, quads=quads)
 
 
+def grid_matrices(n: int, spacing: float, seed: int) -> np.ndarray:
+    """n instances on a square grid (column-major 4x4), seeded yaw and lognormal scale."""
+    rng = np.random.default_rng(seed)
+    side = int(np.ceil(np.sqrt(max(n, 1))))
+    out = np.zeros((n, 16), np.float32)
+    for i in range(n):
+        yaw, s = rng.uniform(0, 2 * np.pi), np.exp(rng.normal(0.0, 0.2))
+        c, sn = np.cos(yaw) * s, np.sin(yaw) * s
+        out[i] = [c, 0, -sn, 0, 0, s, 0, 0, sn, 0, c, 0, (i % side) * spacing, 0, (i // side) * spacing, 1]
+    return out
+
+
 def d2h(ptr, count: int, dtype=np.uint32) -> np.ndarray:
     """Copies `count` elements from a device pointer (cudaMemcpy through the CUDA runtime the engine loaded)."""
     import ctypes

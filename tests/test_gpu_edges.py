@@ -6,23 +6,11 @@ from types import SimpleNamespace
 import numpy as np
 import pytest
 
-from parity_util import Harness
+from parity_util import Harness, grid_matrices
 from vgcut import engine, scenes
 from vgcut.camera import Camera
 
 pytestmark = pytest.mark.gpu
-
-
-def grid_matrices(n: int, spacing: float, seed: int) -> np.ndarray:
-    """n instances on a square grid (column-major 4x4), seeded yaw and lognormal scale."""
-    rng = np.random.default_rng(seed)
-    side = int(np.ceil(np.sqrt(max(n, 1))))
-    out = np.zeros((n, 16), np.float32)
-    for i in range(n):
-        yaw, s = rng.uniform(0, 2 * np.pi), np.exp(rng.normal(0.0, 0.2))
-        c, sn = np.cos(yaw) * s, np.sin(yaw) * s
-        out[i] = [c, 0, -sn, 0, 0, s, 0, 0, sn, 0, c, 0, (i % side) * spacing, 0, (i // side) * spacing, 1]
-    return out
 
 
 @pytest.fixture(scope="module")

@@ -1327,10 +1327,10 @@ int vgc_debug_scene(const vgc_context *ctx, float *cells, uint32_t cell_capacity
 
 // ------------------------------------------------------------------------------------------------ no-alloc cut
 // vgc_cut_noalloc: the single-view cut for callers that must not allocate device memory on the call (a renderer's
-// frame loop running inside a CUDA graph capture or a real-time thread that forbids cudaMalloc, a host that
-// pre-reserves all of its GPU memory). Its per-call scratch - the batch control words, the view constants, the
-// (view, cell) unit list and the meshlet chunk queue - lives in this fixed file-scope device array instead of the
-// context's launch scratch. Every GPU that loads the library holds the array until the process exits.
+// real-time frame thread that must not stall on cudaMalloc, a host that pre-reserves all of its GPU memory). Its
+// per-call scratch - the batch control words, the view constants, the (view, cell) unit list and the meshlet chunk
+// queue - lives in this fixed file-scope device array instead of the context's launch scratch. Every GPU that loads
+// the library holds the array until the process exits.
 namespace {
 constexpr size_t kNoAllocCtl = 0;                                   // 16 control words
 constexpr size_t kNoAllocView = 256;                                // one ViewConst
@@ -1347,12 +1347,17 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 std::mutex g_noalloc_mu;
 unsigned char *g_noalloc_ptr[64] = {nullptr};  // device address of g_noalloc_scratch per device ordinal
 
-// Device address of the scratch array on `device` (current), looked up once per device: in host code the array's
-// name only stands in for the symbol, so kernels must receive this address instead.
+// Device address of the scratch array on `device`, looked up once per device with that device current: in host code
+// the array's name only stands in for the symbol, so kernels must receive this address instead.
 int noalloc_scratch(int device, unsigned char **out) {
   if (device < 0 || device >= 64) return fail(VGC_INVALID_ARG, "device ordinal out of range for the no-alloc scratch");
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
   if (!g_noalloc_ptr[device]) {
+    int current = -1;
+    cudaError_t ce = cudaGetDevice(&current);
+    if (ce != cudaSuccess) return fail(VGC_DEVICE_ERROR, std::string("cudaGetDevice: ") + cudaGetErrorString(ce));
+    if (current != device)
+      return fail(VGC_DEVICE_ERROR, "no-alloc scratch: device " + std::to_string(device) + " is not current");
     void *p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return fail(VGC_DEVICE_ERROR, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
@@ -1361,11 +1366,21 @@ int noalloc_scratch(int device, unsigned char **out) {
   *out = g_noalloc_ptr[device];
   return VGC_OK;
 }
+
+// Writes the view constants into the scratch array. They travel as a kernel argument, which the launch copies, so
+// no host buffer has to outlive the call and nothing is copied from host memory.
+__global__ void k_store_view(const ViewConst k, ViewConst *dst) {
+  static_assert(sizeof(ViewConst) % 4 == 0, "view constants are copied as 32-bit words");
+  const uint32_t *src = reinterpret_cast<const uint32_t *>(&k);
+  uint32_t *out = reinterpret_cast<uint32_t *>(dst);
+  for (uint32_t i = threadIdx.x; i < sizeof(ViewConst) / 4; i += blockDim.x) out[i] = src[i];
+}
 }  // namespace
 
 extern "C" int vgc_cut_noalloc(vgc_context *ctx, const vgc_view *view, uint32_t slot, vgc_stream stream) {
   if (!ctx || !view) return fail(VGC_INVALID_ARG, "null argument");
-  cudaSetDevice(ctx->device);
+  cudaError_t se = cudaSetDevice(ctx->device);
+  if (se != cudaSuccess) return fail(VGC_DEVICE_ERROR, std::string("cudaSetDevice: ") + cudaGetErrorString(se));
   // everything this call writes must exist already: it allocates nothing
   if (ctx->dirty)
     return fail(VGC_INVALID_ARG, "vgc_cut_noalloc: the scene changed since the last upload; one allocating call "
@@ -1405,8 +1420,9 @@ extern "C" int vgc_cut_noalloc(vgc_context *ctx, const vgc_view *view, uint32_t 
   ViewConst *d_view = (ViewConst *)(scratch + kNoAllocView);
   uint2 *units = (uint2 *)(scratch + kNoAllocUnits);
   uint4 *chunks = (uint4 *)(scratch + kNoAllocChunks);
-  // `k` is pageable: the copy has read it when cudaMemcpyAsync returns. k_reset clears the control words.
-  CUDA_TRY(cudaMemcpyAsync(d_view, &k, sizeof(ViewConst), cudaMemcpyHostToDevice, st));
+  // the constants go in by value (k_reset clears the control words)
+  k_store_view<<<1, 128, 0, st>>>(k, d_view);
+  CUDA_TRY(cudaGetLastError());
   const Scene S = scene_of(ctx);
   const HzbDesc *hzbs = (const HzbDesc *)ctx->d_hzb_desc.ptr;
   if (build_hzb) {
