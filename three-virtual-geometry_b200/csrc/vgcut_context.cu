@@ -1366,16 +1366,16 @@ int noalloc_scratch(int device, unsigned char **out) {
   *out = g_noalloc_ptr[device];
   return VGC_OK;
 }
+}  // namespace
 
 // Writes the view constants into the scratch array. They travel as a kernel argument, which the launch copies, so
 // no host buffer has to outlive the call and nothing is copied from host memory.
-__global__ void k_store_view(const ViewConst k, ViewConst *dst) {
-  static_assert(sizeof(ViewConst) % 4 == 0, "view constants are copied as 32-bit words");
+static_assert(sizeof(ViewConst) % 4 == 0, "view constants are copied as 32-bit words");
+__global__ void k_noalloc_store_view(const ViewConst k, ViewConst *dst) {
   const uint32_t *src = reinterpret_cast<const uint32_t *>(&k);
   uint32_t *out = reinterpret_cast<uint32_t *>(dst);
   for (uint32_t i = threadIdx.x; i < sizeof(ViewConst) / 4; i += blockDim.x) out[i] = src[i];
 }
-}  // namespace
 
 extern "C" int vgc_cut_noalloc(vgc_context *ctx, const vgc_view *view, uint32_t slot, vgc_stream stream) {
   if (!ctx || !view) return fail(VGC_INVALID_ARG, "null argument");
@@ -1421,7 +1421,7 @@ extern "C" int vgc_cut_noalloc(vgc_context *ctx, const vgc_view *view, uint32_t 
   uint2 *units = (uint2 *)(scratch + kNoAllocUnits);
   uint4 *chunks = (uint4 *)(scratch + kNoAllocChunks);
   // the constants go in by value (k_reset clears the control words)
-  k_store_view<<<1, 128, 0, st>>>(k, d_view);
+  k_noalloc_store_view<<<1, 128, 0, st>>>(k, d_view);
   CUDA_TRY(cudaGetLastError());
   const Scene S = scene_of(ctx);
   const HzbDesc *hzbs = (const HzbDesc *)ctx->d_hzb_desc.ptr;
