@@ -56,6 +56,7 @@ def lib() -> C.CDLL:
     L.vgo_hzb_build.argtypes = [P(C.c_float), C.c_uint32, C.c_uint32, P(C.c_float), C.c_uint64, P(C.c_uint32),
                                 P(C.c_uint32), P(C.c_uint32), P(C.c_uint32)]
     L.vgo_hzb_build.restype = C.c_int64
+    L.vgo_frustum_planes.argtypes = [C.c_double * 16, C.c_double * 24]
     L.vgo_logf.argtypes = [C.c_float]
     L.vgo_logf.restype = C.c_float
     _lib = L
@@ -143,6 +144,14 @@ def instance_guaranteed_range(data, view16, proj_scale, near, threshold, blend=1
     ok = lib().vgo_instance_guaranteed_range(_u(r), _f(e), _f(g), len(r) // 2, _f(L), _v16(view16), proj_scale, near,
                                              scale, threshold, blend, C.byref(s), C.byref(t))
     return (s.value, t.value) if ok else None
+
+
+def frustum_planes(m16) -> np.ndarray:
+    """three's Frustum.setFromProjectionMatrix(m, WebGPUCoordinateSystem) as the oracle computes it: (6, 4) planes in
+    the order right, left, bottom, top, far, near."""
+    out = (C.c_double * 24)()
+    lib().vgo_frustum_planes(_v16(m16), out)
+    return np.array(list(out)).reshape(6, 4)
 
 
 def logf(x: float) -> float:

@@ -151,6 +151,8 @@ int64_t vgo_hzb_build(const float *depth, uint32_t width, uint32_t height, float
 /* Portable natural log used by both the kernels and the float mirror: frexp-style split and the atanh series
    ln(m) = 2 (s + s^3/3 + s^5/5 + ...), s = (m - 1) / (m + 1) (Abramowitz & Stegun 4.1.27), in float basic ops. */
 float vgo_logf(float x);
+/* three.js Frustum.setFromProjectionMatrix(m, WebGPUCoordinateSystem): planes right, left, bottom, top, far, near. */
+void vgo_frustum_planes(const double m[16], double out[24]);
 
 #ifdef __cplusplus
 }

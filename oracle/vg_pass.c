@@ -71,6 +71,15 @@ static void oracle_planes(const double *me, double out[6][4]) {
   }
 }
 
+/* Frustum.setFromProjectionMatrix(m, WebGPUCoordinateSystem) (three.js, used at VirtualGeometry.ts:429-437) as the
+   oracle computes it: six normalised planes (nx, ny, nz, constant) in three's order right, left, bottom, top, far,
+   near. */
+void vgo_frustum_planes(const double m[16], double out[24]) {
+  double p[6][4];
+  oracle_planes(m, p);
+  memcpy(out, p, sizeof p);
+}
+
 #define REAL float
 #define SFX(name) name##_f32
 #define LOG vgo_logf

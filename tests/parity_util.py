@@ -128,3 +128,67 @@ class Harness:
         st = self.vg.state(params.state_slot)
         assert list(st) == res["state"], f"controller state gpu {list(st)} oracle {res['state']}"
         return lists, res
+
+
+# ------------------------------------------------------------------ the hand-derived pass scene (tests/golden)
+def tiny_dag_mesh(t: dict):
+    """The golden vectors' three-meshlet DAG as a VirtualMeshData-shaped record (LOD, cull and bounding spheres
+    (0, 0, 0, 1))."""
+    from types import SimpleNamespace
+    return SimpleNamespace(
+        meshlet_count=3, meshlet_bounds=np.array(t["bounds"], np.float32).reshape(-1),
+        meshlet_info=np.array(t["info"], np.uint32).reshape(-1), level_ranges=np.array(t["level_ranges"], np.uint32),
+        level_errors=np.array(t["level_errors"], np.float32),
+        level_guard_errors=np.array(t["level_guard_errors"], np.float32),
+        lod_bounds_sphere=np.array(t["lod_bounds_sphere"], np.float32),
+        cull_bounds_sphere=np.array([0, 0, 0, 1], np.float32), bounding_sphere=np.array([0, 0, 0, 1], np.float32),
+        meshlet_triangles=np.array([0x020100, 0x030201, 0x020100, 0x030201, 0x020100], np.uint32),
+        replacement_group=np.array(t["replacement_group"], np.int32),
+        replacement_start=np.array(t["replacement_start"], np.uint32),
+        replacement_indices=np.array(t["replacement_indices"], np.uint32), stats={"leafTriangles": 4})
+
+
+def golden_pass_scene(vectors: dict):
+    """(spec, flags, camera, names) of the golden pass scene: one tiny-DAG mesh per instance, camera at the origin
+    looking down -z with fov 90, near 1, far 100 and a 200 x 200 viewport (projScale 100)."""
+    from types import SimpleNamespace
+    from vgcut.camera import Camera, compose
+    g = vectors["pass_scene"]
+    mesh = tiny_dag_mesh(vectors["tiny_dag"])
+    a = -100.0 / 99.0
+    proj = np.array([1, 0, 0, 0, 0, 1, 0, 0, 0, 0, a, -1, 0, 0, a, 0], float)
+    cam = Camera(view=np.eye(4).reshape(-1), proj=proj, near=1.0, height=200.0, width=200.0)
+    instances, flags = [], []
+    for inst in g["instances"]:
+        instances.append(np.array([compose(inst["at"], 0.0, inst["s"])], np.float32))
+        flags.append(dict(max_draw_distance=inst.get("max_draw_distance", float("inf")),
+                          min_pixel_radius=inst.get("min_pixel_radius", 0.0), shadow=inst.get("shadow", False),
+                          occlusion=inst.get("occlusion", False), enabled=inst.get("enabled", True)))
+    spec = SimpleNamespace(meshes=[mesh] * len(instances), instances=instances)
+    return spec, flags, cam, [inst["name"] for inst in g["instances"]]
+
+
+def check_golden_view(view: dict, names: list, cuts: list, counters: dict) -> None:
+    """Asserts a golden pass view's expectations. cuts[c]: (n, 3) (instance, pool-global meshlet, packed);
+    counters: visible_cells, work0, occluded_instances and (GPU only) fast_emitted."""
+    e = view["expect"]
+    idx = {n: i for i, n in enumerate(names)}
+    by_inst = [dict() for _ in range(2)]
+    for c in (0, 1):
+        for inst, m, packed in np.asarray(cuts[c]).reshape(-1, 3).tolist():
+            by_inst[c].setdefault(names[inst], set()).add((m - 3 * inst, packed))
+    for name, want in e.get("cut0", {}).items():
+        assert by_inst[0].get(name, set()) == set(map(tuple, want)), f"view {view['name']}: {name} in the camera cut"
+    for name in e.get("present0", []):
+        assert by_inst[0].get(name), f"view {view['name']}: {name} must be drawn"
+    for name in e.get("absent0", []):
+        assert name not in by_inst[0], f"view {view['name']}: {name} must not be drawn"
+    if "only" not in e and "cut0" in e and "present0" in e:  # the full camera cut is listed
+        listed = set(e["cut0"]) | set(e["present0"])
+        assert set(by_inst[0]) == listed, f"view {view['name']}: drawn {sorted(by_inst[0])}"
+    if "cut1" in e:
+        got = {(names[i], m - 3 * i, p) for i, m, p in np.asarray(cuts[1]).reshape(-1, 3).tolist()}
+        assert got == set(map(tuple, e["cut1"])), f"view {view['name']}: shadow cut {got}"
+    for k in ("visible_cells", "work0", "occluded_instances", "fast_emitted"):
+        if k in e and k in counters:
+            assert counters[k] == e[k], f"view {view['name']}: {k} {counters[k]} != {e[k]}"

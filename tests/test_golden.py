@@ -66,3 +66,28 @@ def test_morton():
     assert O.morton_order(np.array(mats), m["sphere"]).tolist() == m["expect"]
     from vgcut import build as B
     assert B.morton_order(np.array(mats), np.array(m["sphere"], np.float32)).tolist() == m["expect"]
+
+
+@pytest.mark.parametrize("case", V["frustum_planes"])
+def test_frustum_planes(case):
+    """three's Frustum.setFromProjectionMatrix(P * V, WebGPUCoordinateSystem), worked by hand."""
+    got = O.frustum_planes(case["pv"])
+    assert np.allclose(got, np.array(case["expect"]), rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_pass_scene(precision):
+    """The per-frame passes (cells, instances, selectLevels, fast path, meshlets, blend steps, HZB, shadow sweep) on
+    the hand-built scene, both precisions of the oracle against the hand-derived answers."""
+    from parity_util import check_golden_view, golden_pass_scene
+    from vgcut import engine
+    spec, flags, cam, names = golden_pass_scene(V)
+    scene, _, _ = O.scene_from_spec(spec.meshes, spec.instances, flags)
+    hzb = O.hzb_build(np.array(V["pass_scene"]["hzb"], np.float32))
+    for view in V["pass_scene"]["views"]:
+        p = engine.ViewParams(error_threshold=view["t"], lod_blend=view["blend"], shadow_sweep=tuple(view["sweep"]))
+        v = O.make_view(cam, p, 1 << 10, (100_000, 100_000), hzb=hzb if view["hzb"] else None)
+        r = O.cull_pass(scene, v, precision)
+        c = r["counters"]
+        check_golden_view(view, names, r["entries"],
+                          dict(visible_cells=c[0], occluded_instances=c[1], work0=c[5]))
