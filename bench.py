@@ -511,31 +511,14 @@ def percentile(sorted_values, q: float) -> float:
 def run_batching(ruins, args, flush, stream):
     """64 cameras over the ruins-like scene at 1280x720 / 1920x1080 / 3840x2160 with thresholds 0.5 / 1 / 2 px, each
     with 4 orthographic shadow cascades: 320 views in one CUDA-graph launch, grid sizes picked by the autotuner."""
-    import numpy as np
     import torch
-    from vgcut import engine
-    from vgcut.camera import Camera, cascade_clips
+    from vgcut import engine, scenes
     vg = engine.VirtualGeometry(max_triangles=20_000_000, max_shadow_triangles=8_000_000, max_meshlets=1 << 17,
                                 output_slots=320)
     for data, mats in zip(ruins.meshes, ruins.instances):
         vg.create_mesh(data, mats, cast_shadow=True)
-    rng = np.random.default_rng(21)
-    sizes = [(1280, 720), (1920, 1080), (3840, 2160)]
-    thresholds = [0.5, 1.0, 2.0]
-    light = (0.35, -1.0, 0.25)
-    views = []
-    for i in range(64):
-        eye = ruins.cameras[i % len(ruins.cameras)].extra["eye"]
-        yaw = rng.uniform(0, 2 * np.pi)
-        w, h = sizes[i % 3]
-        t = thresholds[(i // 3) % 3]
-        cam = Camera.perspective_look_at(tuple(eye), (eye[0] + np.cos(yaw), eye[1] - 0.02, eye[2] + np.sin(yaw)), 60,
-                                         w, h, 0.1, 5000.0)
-        views.append(engine.make_view(cam, engine.ViewParams(error_threshold=t, state_slot=len(views), fresh_state=True,
-                                                             shadow_sweep=(0.0, 0.0, 0.0))))
-        for clip in cascade_clips(cam, light, [0.1, 10.0, 40.0, 150.0, 600.0]):
-            views.append(engine.make_view(cam, engine.ViewParams(error_threshold=t, state_slot=len(views),
-                                                                 fresh_state=True, cascade_clip=clip)))
+    views = [engine.make_view(cam, engine.ViewParams(state_slot=k, fresh_state=True, **levers))
+             for k, (cam, levers) in enumerate(scenes.batching_views(ruins))]
     sp = ctypes.c_void_p(stream.cuda_stream)
 
     def timed_steps():

@@ -56,6 +56,9 @@ def lib() -> C.CDLL:
     L.vgo_hzb_build.argtypes = [P(C.c_float), C.c_uint32, C.c_uint32, P(C.c_float), C.c_uint64, P(C.c_uint32),
                                 P(C.c_uint32), P(C.c_uint32), P(C.c_uint32)]
     L.vgo_hzb_build.restype = C.c_int64
+    L.vgo_cut_invariant.argtypes = [C.c_void_p, P(C.c_uint32), C.c_uint32, P(C.c_uint32), C.c_uint32, P(C.c_uint32),
+                                     C.c_uint64, P(C.c_uint32), C.c_uint32, C.c_int, P(C.c_uint64)]
+    L.vgo_cut_invariant.restype = C.c_uint64
     L.vgo_frustum_planes.argtypes = [C.c_double * 16, C.c_double * 24]
     L.vgo_logf.argtypes = [C.c_float]
     L.vgo_logf.restype = C.c_float
@@ -152,6 +155,39 @@ def frustum_planes(m16) -> np.ndarray:
     out = (C.c_double * 24)()
     lib().vgo_frustum_planes(_v16(m16), out)
     return np.array(list(out)).reshape(6, 4)
+
+
+class _Dag(C.Structure):
+    _fields_ = [("meshlet_count", C.c_uint32), ("info", C.POINTER(C.c_uint32)), ("group", C.POINTER(C.c_int32)),
+                ("start", C.POINTER(C.c_uint32)), ("list", C.POINTER(C.c_uint32))]
+
+
+def cut_invariant(meshes, instance_slots, entries, steps=(0,), threads: int = 0) -> tuple[int, int]:
+    """verifyCutCoverage + verifyCutOverlap (cut.ts:83-122) for every drawn instance of one cut at every blend step
+    in `steps`: meshes in slot order, instance_slots (I,) mesh slot per GPU-order instance, entries (n, 3)
+    (instance, pool-global meshlet, packed). Returns (failing (instance, step) pairs, instances checked)."""
+    keep = []
+    dags = (_Dag * max(1, len(meshes)))()
+    base = np.zeros(max(1, len(meshes)), np.uint32)
+    b = 0
+    for k, d in enumerate(meshes):
+        arrs = [np.ascontiguousarray(d.meshlet_info, np.uint32), np.ascontiguousarray(d.replacement_group, np.int32),
+                np.ascontiguousarray(d.replacement_start, np.uint32),
+                np.ascontiguousarray(d.replacement_indices, np.uint32)]
+        keep += arrs
+        dags[k].meshlet_count = d.meshlet_count
+        dags[k].info = _u(arrs[0])
+        dags[k].group = arrs[1].ctypes.data_as(C.POINTER(C.c_int32))
+        dags[k].start, dags[k].list = _u(arrs[2]), _u(arrs[3])
+        base[k] = b
+        b += d.meshlet_count
+    slots = np.ascontiguousarray(instance_slots, np.uint32)
+    e = np.ascontiguousarray(entries, np.uint32).reshape(-1, 3)
+    st = np.ascontiguousarray(steps, np.uint32)
+    checked = C.c_uint64()
+    bad = lib().vgo_cut_invariant(C.addressof(dags), _u(base), len(meshes), _u(slots), len(slots), _u(e), len(e),
+                                  _u(st), len(st), threads, C.byref(checked))
+    return int(bad), int(checked.value)
 
 
 def logf(x: float) -> float:

@@ -13,6 +13,7 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#include <omp.h>
 
 #include "vg_oracle.h"
 
@@ -200,4 +201,78 @@ int vgo_instance_guaranteed_range(const uint32_t *ranges, const float *errors, c
   *start = s0;
   *end = e0;
   return 1;
+}
+
+/* The DAG-cut invariant over the full pass's output: verifyCutCoverage and verifyCutOverlap (cut.ts:83-122) applied
+   to each drawn instance at each blend step. `entries` are one cut's (instance, pool-global meshlet, packed) rows;
+   mesh k's meshlets are [base[k], base[k] + dags[k].meshlet_count). At step s an instance's selection is its
+   meshlets with lo <= s < hi (packed bits 8-15 and 16-23). Returns the number of (instance, step) pairs with a hole
+   or an overlap; *checked receives the number of instances with entries. */
+uint64_t vgo_cut_invariant(const vgo_dag *dags, const uint32_t *base, uint32_t mesh_count, const uint32_t *inst_slot,
+                           uint32_t instance_count, const uint32_t *entries, uint64_t n, const uint32_t *steps,
+                           uint32_t nsteps, int threads, uint64_t *checked) {
+  uint64_t *first = (uint64_t *)calloc((size_t)instance_count + 1, sizeof(uint64_t));
+  uint64_t *order = (uint64_t *)malloc((n ? n : 1) * sizeof(uint64_t));
+  uint64_t bad = 0, seen = 0, skipped = 0;
+  for (uint64_t e = 0; e < n; e++) {
+    uint32_t inst = entries[e * 3];
+    if (inst < instance_count) first[inst + 1]++;
+    else skipped++;
+  }
+  for (uint32_t i = 0; i < instance_count; i++) first[i + 1] += first[i];
+  uint64_t *fill = (uint64_t *)malloc(((size_t)instance_count + 1) * sizeof(uint64_t));
+  memcpy(fill, first, ((size_t)instance_count + 1) * sizeof(uint64_t));
+  for (uint64_t e = 0; e < n; e++) {
+    uint32_t inst = entries[e * 3];
+    if (inst < instance_count) order[fill[inst]++] = e;
+  }
+  free(fill);
+  if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel reduction(+ : bad, seen)
+  {
+    uint8_t *sel = NULL;
+    int8_t *memo = NULL;
+    uint32_t cap = 0;
+#pragma omp for schedule(dynamic, 64)
+    for (int64_t ii = 0; ii < (int64_t)instance_count; ii++) {
+      uint32_t inst = (uint32_t)ii;
+      if (first[inst] == first[inst + 1]) continue;
+      uint32_t slot = inst_slot[inst];
+      if (slot >= mesh_count) { bad += nsteps; continue; }
+      const vgo_dag *d = &dags[slot];
+      if (d->meshlet_count > cap) {
+        cap = d->meshlet_count;
+        sel = (uint8_t *)realloc(sel, cap);
+        memo = (int8_t *)realloc(memo, cap);
+      }
+      seen++;
+      for (uint32_t s = 0; s < nsteps; s++) {
+        memset(sel, 0, d->meshlet_count);
+        int broken = 0;
+        for (uint64_t k = first[inst]; k < first[inst + 1]; k++) {
+          const uint32_t *row = entries + order[k] * 3;
+          uint32_t m = row[1] - base[slot], lo = (row[2] >> 8) & 255, hi = (row[2] >> 16) & 255;
+          if (row[1] < base[slot] || m >= d->meshlet_count) { broken = 1; continue; }
+          if (lo <= steps[s] && steps[s] < hi) {
+            if (sel[m]) broken = 1; /* the same meshlet drawn twice */
+            sel[m] = 1;
+          }
+        }
+        walk_ctx c = {d->group, d->start, d->list, sel, memo};
+        memset(memo, -1, d->meshlet_count);
+        for (uint32_t i = 0; i < d->meshlet_count && !broken; i++)
+          if (sel[i] && below(&c, i)) broken = 1;
+        memset(memo, -1, d->meshlet_count);
+        for (uint32_t i = 0; i < d->meshlet_count && !broken; i++)
+          if (d->info[(size_t)i * 4 + 2] == 0 && !covered(&c, i)) broken = 1;
+        bad += (uint64_t)broken;
+      }
+    }
+    free(sel);
+    free(memo);
+  }
+  free(first);
+  free(order);
+  if (checked) *checked = seen;
+  return bad + skipped;
 }

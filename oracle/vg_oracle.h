@@ -44,6 +44,17 @@ uint32_t vgo_verify_overlap(uint32_t meshlet_count, const int32_t *replacement_g
 uint32_t vgo_verify_coverage(uint32_t meshlet_count, const uint32_t *meshlet_info, const int32_t *replacement_group,
                              const uint32_t *replacement_start, const uint32_t *replacement_indices,
                              const uint8_t *selected, uint32_t *out);
+/* Replacement links of one mesh (VirtualMeshData.replacementGroup / replacementStart / replacementIndices). */
+typedef struct vgo_dag {
+  uint32_t meshlet_count;
+  const uint32_t *info; /* meshletInfo, 4 per meshlet (lodLevel at [2]) */
+  const int32_t *group;
+  const uint32_t *start, *list;
+} vgo_dag;
+/* verifyCutCoverage + verifyCutOverlap per drawn instance and blend step of one cut's entries (see vg_cut.c). */
+uint64_t vgo_cut_invariant(const vgo_dag *dags, const uint32_t *base, uint32_t mesh_count, const uint32_t *inst_slot,
+                           uint32_t instance_count, const uint32_t *entries, uint64_t n, const uint32_t *steps,
+                           uint32_t nsteps, int threads, uint64_t *checked);
 void vgo_instance_meshlet_range(const uint32_t *level_ranges, const float *level_errors, uint32_t level_count,
                                 const float lod_bounds[4], const double view16[16], double proj_scale, double near_,
                                 double scale, double threshold, double blend, uint32_t *start, uint32_t *end);

@@ -66,11 +66,12 @@ def check_index_tiling(entries: np.ndarray, inst_slot: np.ndarray, mesh_counts: 
 class Harness:
     """One scene resident on the GPU and in the oracle."""
 
-    def __init__(self, spec, flags=None, max_meshlets=1 << 16, max_triangles=2_000_000, max_shadow=1_000_000):
+    def __init__(self, spec, flags=None, max_meshlets=1 << 16, max_triangles=2_000_000, max_shadow=1_000_000,
+                 output_slots=8):
         self.spec = spec
         self.flags = flags or [{} for _ in spec.meshes]
         self.vg = engine.VirtualGeometry(max_triangles=max_triangles, max_shadow_triangles=max_shadow,
-                                         max_meshlets=max_meshlets, output_slots=8)
+                                         max_meshlets=max_meshlets, output_slots=output_slots)
         for d, m, f in zip(spec.meshes, spec.instances, self.flags):
             self.vg.create_mesh(d, m, max_draw_distance=f.get("max_draw_distance", float("inf")),
                                 min_pixel_radius=f.get("min_pixel_radius", 0.0), cast_shadow=f.get("shadow", False),

@@ -28,6 +28,11 @@ def check_budget(h, cam, params, hzb_oracle=None, graph=False):
     s = h.vg.last_stats
     assert s["predicted_triangles"] == res["predicted"], f"prediction gpu {s['predicted_triangles']} oracle {res['predicted']}"
     assert s["effective_threshold"] == np.float32(res["threshold"]), "chosen threshold differs"
+    drawn = s["requested_indices"][0] // 3
+    if res["threshold"] < params.threshold_range[1]:  # the search found a threshold whose cut fits
+        # the prediction counts the blend band, so the drawn camera cut (both parts) stays within the budget
+        assert drawn <= s["predicted_triangles"] <= params.triangle_budget, \
+            f"drawn {drawn} predicted {s['predicted_triangles']} budget {params.triangle_budget}"
     return lists, res
 
 

@@ -1,0 +1,166 @@
+"""GPU parity at the benchmark workloads' full sizes, through the C ABI:
+
+* the ruins-like scene (113,106 instances of 40 meshes, 355,991 meshlets) at 1920 x 1080 on 4 spline poses, with
+  each pose's HZB and the shadow cut;
+* the small plain scene at full size (one 1,048,820-triangle icosphere x 64 instances, 1920 x 1080);
+* the large world (3,000,000 instances, 3840 x 2160, triangleBudget 6M searched over [0.5, 24] px, maxDrawDistance
+  400 m on the 10 smallest meshes) on 2 poses;
+* the 320-view batch (64 cameras at 720p / 1080p / 4K with 4 orthographic cascades each) in one CUDA graph.
+
+Each case checks (1) the GPU against the oracle's float mirror bit for bit (draw sets, counters, draw args, controller
+state, and for budgets the chosen threshold and predicted triangles); (2) every difference against the double
+restatement of the reference is a decision within the 1e-5 relative margin (counted); (3) with culling off, every
+instance's drawn meshlets form a complete, overlap-free cut at every blend step (verifyCutCoverage /
+verifyCutOverlap of cut.ts:83-122, exact)."""
+import dataclasses
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from parity_util import Harness, MARGIN, key_set
+from vgcut import engine, scenes
+
+pytestmark = pytest.mark.gpu
+
+THREADS = os.cpu_count() or 8
+STEPS = list(range(0, 255, 15))  # blend steps the invariant is checked at (a range is lo <= s < hi <= 255)
+FRESH = np.array([10000, 10000, 0, 0, 0, 0, 0, 0], np.uint32)
+
+
+def explained(h, lists, cam, params, hzb=None):
+    """GPU vs the double restatement: every (cut, instance, meshlet) that differs has a decision within the margin.
+    Returns (differing decisions, entries in the double cut)."""
+    res, v = h.oracle(cam, params, hzb, precision="f64", state=list(FRESH))
+    near, total = set(), 0
+    for cut in (0, 1):
+        g = key_set(lists[cut], (0, 1, 3))
+        o = key_set(res["entries"][cut], (0, 1, 2))
+        total += len(o)
+        for inst, m, _ in g ^ o:
+            if (cut, inst, m) in near:
+                continue
+            slack = O.explain(h.scene, v, cut, inst, m)
+            assert slack <= MARGIN, f"cut {cut} ({inst}, {m}) differs from the double restatement with slack {slack}"
+            near.add((cut, inst, m))
+    return len(near), total
+
+
+def invariant(h, cam, params, expect_instances):
+    """Culling off (frustum, size, distance, occlusion): the GPU equals the mirror and every instance's cut is
+    complete and overlap-free at every blend step, in both cuts."""
+    p = dataclasses.replace(params, frustum_culling=False, min_pixel_radius=0.0, hzb=-1)
+    h.vg.state(p.state_slot, FRESH)
+    lists, res = h.compare(cam, p)
+    for cut in (0, 1):
+        if cut == 1 and len(lists[1]) == 0:
+            continue
+        assert res["counters"][2 + cut * 5] <= h.max_meshlets, "the culling-off cut must fit the draw list"
+        bad, checked = O.cut_invariant(h.spec.meshes, h.inst_slot, lists[cut][:, [0, 1, 3]], STEPS, threads=THREADS)
+        assert bad == 0, f"cut {cut}: {bad} (instance, step) pairs with a hole or an overlap"
+        if cut == 0:
+            assert checked == expect_instances, f"{checked} of {expect_instances} instances drawn with culling off"
+    return checked
+
+
+@pytest.fixture(scope="module")
+def ruins():
+    return scenes.ruins(poses=32, threads=THREADS)
+
+
+def test_ruins_full_size_hzb_and_shadow(ruins):
+    spec = ruins
+    flags = [dict(occlusion=True, shadow=(i % 2 == 0)) for i in range(len(spec.meshes))]
+    h = Harness(spec, flags, max_meshlets=1 << 20, max_triangles=40_000_000, max_shadow=20_000_000)
+    try:
+        h.check_layout()
+        near = total = 0
+        for k in (0, 8, 16, 24):
+            cam = spec.cameras[k]
+            h.vg.build_hzb(k % 8, spec.depth_images[k])
+            hzb = O.hzb_build(spec.depth_images[k])
+            p = engine.ViewParams(error_threshold=1.0, hzb=k % 8, shadow_sweep=(30.0, -60.0, 10.0))
+            h.vg.state(0, FRESH)
+            lists, res = h.compare(cam, p, hzb_oracle=hzb)
+            assert res["counters"][1] > 0 and len(lists[0]) > 10_000 and len(lists[1]) > 0
+            n, t = explained(h, lists, cam, p, hzb)
+            near, total = near + n, total + t
+        print(f"ruins: {near} margin decisions of {total} entries")
+        assert near <= max(10, total // 1000)
+        invariant(h, spec.cameras[0], engine.ViewParams(error_threshold=2.0, shadow_sweep=(30.0, -60.0, 10.0)),
+                  spec.instance_count)
+    finally:
+        h.vg.dispose()
+
+
+def test_plain_small_full_size():
+    spec = scenes.plain_small(threads=THREADS)
+    h = Harness(spec, max_meshlets=1 << 18, max_triangles=20_000_000)
+    try:
+        h.check_layout()
+        cam = spec.cameras[0]
+        for t in (0.5, 1.0, 2.0):
+            p = engine.ViewParams(error_threshold=t)
+            h.vg.state(0, FRESH)
+            lists, _ = h.compare(cam, p)
+            assert len(lists[0]) > 1000
+            explained(h, lists, cam, p)
+        for t in (1.0, 2.5):
+            invariant(h, cam, engine.ViewParams(error_threshold=t), spec.instance_count)
+    finally:
+        h.vg.dispose()
+
+
+def test_large_world_budget(ruins):
+    spec = scenes.large_world(ruins.meshes, ruins.mesh_triangles, ruins.notes["weight_exponent"], poses=2)
+    small = set(spec.notes["small_meshes"])
+    flags = [dict(max_draw_distance=(400.0 if i in small else float("inf"))) for i in range(len(spec.meshes))]
+    h = Harness(spec, flags, max_meshlets=1 << 18, max_triangles=12_000_000, max_shadow=4_000_000)
+    try:
+        for k, cam in enumerate(spec.cameras):
+            p = engine.ViewParams(triangle_budget=spec.notes["triangle_budget"], threshold_range=(0.5, 24.0),
+                                  state_slot=k, fresh_state=True)
+            h.vg.state(k, FRESH)
+            lists, res = h.compare(cam, p)
+            s = h.vg.last_stats
+            assert s["predicted_triangles"] == res["predicted"]
+            assert s["effective_threshold"] == np.float32(res["threshold"])
+            budget = spec.notes["triangle_budget"]
+            drawn = s["requested_indices"][0] // 3
+            # the search counts the blend band: the drawn camera cut lands just under the budget
+            assert 0.95 * budget <= drawn <= res["predicted"] <= budget, f"drawn {drawn} predicted {res['predicted']}"
+            # the double restatement at the threshold the search chose
+            fixed = engine.ViewParams(error_threshold=float(np.float32(res["threshold"])), state_slot=k)
+            explained(h, lists, cam, fixed)
+    finally:
+        h.vg.dispose()
+
+
+def test_batch_320_views_with_cascades(ruins):
+    spec = ruins
+    views = scenes.batching_views(spec)
+    assert len(views) == 320
+    h = Harness(spec, [dict(shadow=True) for _ in spec.meshes], max_meshlets=1 << 17, max_triangles=20_000_000,
+                max_shadow=8_000_000, output_slots=len(views))
+    try:
+        params = [engine.ViewParams(state_slot=k, fresh_state=True, **levers) for k, (_, levers) in enumerate(views)]
+        h.vg.cut([engine.make_view(cam, p) for (cam, _), p in zip(views, params)], first_slot=0, graph=True)
+        compared = 0
+        for k, ((cam, _), p) in enumerate(zip(views, params)):
+            res, _ = h.oracle(cam, p, state=list(FRESH))
+            s = h.vg.read_stats(k)
+            c = res["counters"]
+            assert s["visible_cells"] == c[0]
+            for cut in (0, 1):
+                got = [s["selected"][cut], s["drawn"][cut], s["survived"][cut], s["work"][cut]]
+                assert got == c[2 + cut * 5: 6 + cut * 5], f"view {k} cut {cut}: gpu {got} oracle {c[2 + cut * 5: 6 + cut * 5]}"
+                if c[2 + cut * 5] <= h.max_meshlets:
+                    assert s["requested_indices"][cut] == c[6 + cut * 5]
+                    assert key_set(h.vg.draw_list(k, cut), (0, 1, 3)) == key_set(res["entries"][cut], (0, 1, 2)), \
+                        f"view {k} cut {cut}: draw sets differ"
+                    compared += 1
+            assert s["rounds"] == res["rounds"]
+        assert compared >= 320, "most cuts fit their draw list and are compared entry by entry"
+    finally:
+        h.vg.dispose()

@@ -499,10 +499,33 @@ __device__ __forceinline__ void emit_fast(const Scene &S, const ViewConst &V, ui
 }
 
 // ---- triangleBudget search. Thresholds t_k = lo + (hi - lo) * (k / 255) over thresholdRange, effective
-// e_k = t_k * cameraScale; a meshlet of a visible instance is in the plain camera cut at t_k iff b_own <= k < b_par
-// with b_x = the first k such that x <= e_k. Its triangles enter the histogram at b_own and leave at b_par.
+// e_k = t_k * cameraScale, band high edge high_k (e_k * width while the LOD-blend band is open at t_k, else e_k).
+// A meshlet of a visible instance is drawn in the camera cut at t_k (blend band included) iff b_own <= k < b_par,
+// with b_own = the first k such that own <= high_k and b_par = the first k such that parent <= e_k. Its triangles
+// enter the histogram at b_own and leave at b_par, so T(t_k) counts the triangles the cut at t_k draws.
 __device__ __forceinline__ float budget_e(const ViewConst &V, float s, uint32_t k) {
   return (V.budget_lo + (V.budget_hi - V.budget_lo) * (float(k) / 255.0f)) * s;
+}
+
+// high_k, with load_bands' arithmetic for the threshold t_k (the final pass at the chosen bin uses the same value)
+__device__ __forceinline__ float budget_high(const ViewConst &V, float s, uint32_t k) {
+  const float x = budget_e(V, s, k);
+  float t = (x - 1.25f) / 1.25f;
+  t = fmn(fmx(t, 0.0f), 1.0f);
+  const float smooth = (t * t) * (3.0f - 2.0f * t);
+  const float width = 1.0f + (V.lod_blend_max - 1.0f) * smooth;
+  return width > float(1.001) ? x * width : x;
+}
+
+// first k with x <= high_k (kBudgetBins when none); high_k does not decrease with k
+__device__ __forceinline__ uint32_t budget_bin_high(const ViewConst &V, float s, float x) {
+  uint32_t lo = 0, hi = kBudgetBins;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (x <= budget_high(V, s, mid)) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo;
 }
 
 __device__ __forceinline__ uint32_t budget_bin(const ViewConst &V, float s, float x) {
@@ -520,7 +543,7 @@ __device__ __forceinline__ bool hist_meshlet(const Scene &S, const ViewConst &V,
                                              uint32_t &bo, uint32_t &bp, uint32_t &tris) {
   const float scale = VM[12];
   const float4 ls = __ldg(S.m_lod + meshlet), ps = __ldg(S.m_parent + meshlet), er = __ldg(S.m_err + meshlet);
-  bo = budget_bin(V, s, proj_error(V, VM, scale, ls, er.x));
+  bo = budget_bin_high(V, s, proj_error(V, VM, scale, ls, er.x));
   bp = budget_bin(V, s, proj_error(V, VM, scale, ps, er.y));
   if (!(bo < bp)) return false;
   tris = __float_as_uint(er.z);
@@ -710,10 +733,10 @@ __global__ void __launch_bounds__(128, 6) k_instances(Scene S, const ViewConst *
         // inside: the cullBoundsSphere lies in the frustum, so every meshlet passes its frustum test
         if (HIST && in_camera) {
           const float sc = get_state(V.state, 0);
-          const float e0 = budget_e(V, sc, 0), e255 = budget_e(V, sc, 255);
-          r0 = level_range(L, levels, e0, e255, px_min, px_max);
+          const float e0 = budget_e(V, sc, 0), h255 = budget_high(V, sc, 255);
+          r0 = level_range(L, levels, e0, h255, px_min, px_max);
           inside0 = no_frustum || frustum(V, cc, false) >= cr;
-          trim_item(S, mesh, L, r0, e0, e255, px_min, px_max, t0f, t0l);
+          trim_item(S, mesh, L, r0, e0, h255, px_min, px_max, t0f, t0l);
         } else if (in_camera) {
           r0 = level_range(L, levels, b.low0, b.high0, px_min, px_max);
           inside0 = no_frustum || frustum(V, cc, false) >= cr;
@@ -896,7 +919,7 @@ __global__ void __launch_bounds__(128, 8) k_chunks(Scene S, const ViewConst *__r
         own = proj_error(V, VM, VM[12], ls, er.x);
         parent = proj_error(V, VM, VM[12], ps, er.y);
         if (HIST) {
-          const uint32_t bo = budget_bin(V, sc, own), bp = budget_bin(V, sc, parent);
+          const uint32_t bo = budget_bin_high(V, sc, own), bp = budget_bin(V, sc, parent);
           pass = bo < bp;
           own = __uint_as_float(bo);
           parent = __uint_as_float(bp);

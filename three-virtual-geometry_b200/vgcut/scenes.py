@@ -201,6 +201,31 @@ def load_into(vg, spec: SceneSpec, **mesh_options) -> list:
     return out
 
 
+def batching_views(ruins: SceneSpec, cameras: int = 64, seed: int = 21) -> list:
+    """The batching workload over the ruins-like scene: `cameras` cameras at the spline's eye points with seeded yaw,
+    resolutions cycling 1280x720 / 1920x1080 / 3840x2160 and thresholds 0.5 / 1 / 2 px, each followed by its 4
+    orthographic shadow cascades (splits 0.1-10-40-150-600 m, light direction (0.35, -1, 0.25)). Returns
+    (camera, lever dict) per view in launch order: camera, then its cascades; the dict holds error_threshold and,
+    for a cascade, cascade_clip (a camera view has no shadow sweep)."""
+    from .camera import cascade_clips
+    rng = np.random.default_rng(seed)
+    sizes = [(1280, 720), (1920, 1080), (3840, 2160)]
+    thresholds = [0.5, 1.0, 2.0]
+    light = (0.35, -1.0, 0.25)
+    out = []
+    for i in range(cameras):
+        eye = ruins.cameras[i % len(ruins.cameras)].extra["eye"]
+        yaw = rng.uniform(0, 2 * np.pi)
+        w, h = sizes[i % 3]
+        t = thresholds[(i // 3) % 3]
+        cam = Camera.perspective_look_at(tuple(eye), (eye[0] + np.cos(yaw), eye[1] - 0.02, eye[2] + np.sin(yaw)), 60,
+                                         w, h, 0.1, 5000.0)
+        out.append((cam, dict(error_threshold=t)))
+        for clip in cascade_clips(cam, light, [0.1, 10.0, 40.0, 150.0, 600.0]):
+            out.append((cam, dict(error_threshold=t, cascade_clip=clip)))
+    return out
+
+
 # ---------------------------------------------------------------------------------------------------- large scenes
 def _weights(tris: np.ndarray, exponent: float) -> np.ndarray:
     w = tris.astype(np.float64) ** (-exponent)
