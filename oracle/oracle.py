@@ -215,7 +215,7 @@ class _View(C.Structure):
                 ("max_drawn", C.c_uint32), ("index_capacity", C.c_uint32 * 2), ("state", C.c_uint32 * 8),
                 ("triangle_budget", C.c_double), ("threshold_range", C.c_double * 2),
                 ("chosen_threshold", C.c_double), ("predicted_triangles", C.c_uint64), ("cascade", C.c_uint32),
-                ("cascade_clip", C.c_double * 16)]
+                ("cascade_clip", C.c_double * 16), ("cut_state", (C.c_uint32 * 2) * 2), ("pin_state", C.c_uint32)]
 
 
 class _Result(C.Structure):
@@ -297,8 +297,12 @@ def hzb_build(depth: np.ndarray):
     return out[:n].copy(), levels.value, list(off), list(ww), list(hh)
 
 
-def make_view(camera, params, max_drawn=1 << 20, index_capacity=(30_000_000, 12_000_000), hzb=None, state=None) -> _View:
+def make_view(camera, params, max_drawn=1 << 20, index_capacity=(30_000_000, 12_000_000), hzb=None, state=None,
+              pin_state: bool = False) -> _View:
+    """The oracle's view of a camera and levers. `pin_state`: one round at `state` (no capacity check, retry or
+    steer), to judge a cut's decisions at the controller state another run's final round used."""
     v = _View()
+    v.pin_state = 1 if pin_state else 0
     for i in range(16):
         v.view[i] = float(camera.view[i])
         v.proj[i] = float(camera.proj[i])
@@ -335,6 +339,28 @@ def make_view(camera, params, max_drawn=1 << 20, index_capacity=(30_000_000, 12_
             v.hzb_offset[i], v.hzb_width[i], v.hzb_height[i] = off[i], ww[i], hh[i]
         v.occlusion_active = 1
     return v
+
+
+def cut_state_words(view: _View, state, cut: int) -> list:
+    """The state words a pinned run of cut `cut` starts from: `state` with the scales that cut's final computation
+    in `view`'s pass ran with."""
+    st = list(state)
+    st[0], st[1] = int(view.cut_state[cut][0]), int(view.cut_state[cut][1])
+    return st
+
+
+def pinned_reference(scene: OracleScene, make, mirror_view: _View, state, threads: int = 0):
+    """The double restatement of each cut at the controller scales its final computation in the mirror's pass ran
+    with (one pinned round per cut). `make(state)` builds the pinned view. Returns (entries per cut, view per cut):
+    the views are what `explain` takes for that cut."""
+    entries, views = [], []
+    for cut in (0, 1):
+        v = make(cut_state_words(mirror_view, state, cut))
+        v.pin_state = 1
+        r = cull_pass(scene, v, "f64", threads=threads)
+        entries.append(r["entries"][cut])
+        views.append(v)
+    return entries, views
 
 
 def cull_pass(scene: OracleScene, view: _View, precision: str = "f32", threads: int = 0, capacity: int | None = None):

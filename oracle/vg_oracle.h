@@ -113,9 +113,14 @@ typedef struct vgo_view {
   double triangle_budget;     /* > 0: pick errorThreshold by the histogram search over threshold_range */
   double threshold_range[2];
   double chosen_threshold;    /* out: errorThreshold the budget search picked */
-  uint64_t predicted_triangles; /* out: plain camera-cut triangles the histogram predicts at that threshold */
+  uint64_t predicted_triangles; /* out: camera-cut triangles the histogram predicts at that threshold */
   uint32_t cascade;           /* shadow cascade: no camera cut, the shadow cut bounded by cascade_clip's planes */
   double cascade_clip[16];    /* world -> clip of the cascade, column-major, [0,1] depth */
+  uint32_t cut_state[2][2];   /* out: per cut, the controller scales (state words 0, 1) its final computation ran
+                                 with (a retry round redoes only the cuts that overflowed; the steer after the last
+                                 round moves state[0..1] on for the next frame) */
+  uint32_t pin_state;         /* 1: one round at `state` as given, no capacity check, retry or steer (to judge the
+                                 cut's decisions at the controller state another run ended with) */
 } vgo_view;
 
 typedef struct vgo_result {

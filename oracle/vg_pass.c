@@ -187,14 +187,25 @@ static double occl_slack(const viewk_f64 *k, const vgo_view *v, const bands_f64 
   double grow = (r + margin) * VGO_MARGIN;
   int a = hzb_test_f64(k, v, c, r + margin - grow), bb = hzb_test_f64(k, v, c, r + margin + grow);
   if (a != bb) best = 0;
+  /* the depth comparison itself (nearest depth against the sampled maximum + 1e-6, both near 1) */
+  double zmin, zmax;
+  if (hzb_sample_f64(k, v, c, r + margin, &zmin, &zmax)) best = fmin(best, slack(zmin, zmax + 1e-6));
   return best;
 }
 
 double vgo_explain_f64(const vgo_scene *s, const vgo_view *v, uint32_t cut, uint32_t instance, uint32_t meshlet) {
   viewk_f64 K;
   view_setup_f64(v, &K);
+  /* the bands the frame's final cut ran with: its threshold (the budget search's pick) and controller scales */
+  if (v->triangle_budget > 0) K.error_threshold = v->chosen_threshold;
+  uint32_t state[8];
+  memcpy(state, v->state, sizeof state);
+  if (v->cut_state[cut & 1][0]) {
+    state[0] = v->cut_state[cut & 1][0];
+    state[1] = v->cut_state[cut & 1][1];
+  }
   bands_f64 B;
-  load_bands_f64(&K, v->state, &B);
+  load_bands_f64(&K, state, &B);
   double best = 1e300;
   /* the cell holding the instance */
   uint32_t cell = 0;

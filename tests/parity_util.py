@@ -91,6 +91,19 @@ class Harness:
         v = O.make_view(cam, params, self.max_meshlets, self.caps, hzb=hzb, state=state)
         return O.cull_pass(self.scene, v, precision), v
 
+    def reference(self, cam, params, hzb=None):
+        """The double restatement of the reference's cut, each cut at the controller scales its final computation
+        in the last compared run used (pinned: one round, no capacity check). The controller's own arithmetic is
+        checked bit for bit against the float mirror; pinning keeps one margin decision in an early round from
+        moving a retried cut's scale, which would shift every decision of the view. Returns (entries per cut,
+        oracle view per cut)."""
+        if getattr(params, "triangle_budget", 0.0) > 0:  # judge the cut at the threshold the search picked
+            import dataclasses
+            params = dataclasses.replace(params, triangle_budget=0.0,
+                                         error_threshold=float(self.last_view.chosen_threshold))
+        make = lambda st: O.make_view(cam, params, self.max_meshlets, self.caps, hzb=hzb, state=st)
+        return O.pinned_reference(self.scene, make, self.last_view, self.last_state)
+
     def gpu(self, cam, params, slot=0, graph=False):
         v = engine.make_view(cam, params)
         self.vg.cut([v], first_slot=slot, graph=graph)
@@ -101,7 +114,10 @@ class Harness:
     def compare(self, cam, params, hzb_oracle=None, slot=0, graph=False):
         """GPU result == float mirror (sets, counters, args); returns (gpu lists, oracle result)."""
         state = list(self.vg.state(params.state_slot))  # the controller state both start from
-        res, _ = self.oracle(cam, params, hzb_oracle, "f32", state)
+        if getattr(params, "fresh_state", False):
+            state = [10000, 10000, 0, 0, 0, 0, 0, 0]
+        res, self.last_view = self.oracle(cam, params, hzb_oracle, "f32", state)
+        self.last_state = state
         stats, lists = self.gpu(cam, params, slot, graph)
         c = res["counters"]
         assert stats["visible_cells"] == c[0]

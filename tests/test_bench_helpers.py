@@ -33,3 +33,11 @@ def test_percentile_nearest_rank():
     v = sorted(float(x) for x in range(1, 101))
     assert bench.percentile(v, 0.5) == 50.0 and bench.percentile(v, 0.99) == 99.0 and bench.percentile(v, 1.0) == 100.0
     assert bench.percentile([3.0], 0.999) == 3.0
+
+
+def test_tail_order_keeps_every_key_and_ends_with_the_headline_figures():
+    line = {"metric": "m", "value": 1.0, "serve": {"x": 1}, "p99_ms": 0.2, "batching": {}, "clocks": {}, "unit": "u"}
+    out = bench.tail_order(line)
+    assert out == line
+    keys = list(out)
+    assert keys[:4] == ["metric", "serve", "batching", "unit"] and keys[-1] == "value"
