@@ -160,6 +160,7 @@ Scene scene_of(const vgc_context *ctx) {
   S.inst = (const float4 *)ctx->d_inst.ptr;
   S.inst_slot = (const uint32_t *)ctx->d_inst_slot.ptr;
   S.cells = (const CellRec *)ctx->d_cells.ptr;
+  S.hzbs = (const HzbDesc *)ctx->d_hzb_desc.ptr;
   S.cell_count = (uint32_t)ctx->cells.size();
   S.instance_count = (uint32_t)ctx->inst_slot.size();
   S.meshlet_count = (uint32_t)ctx->m_lod.size();
@@ -267,6 +268,8 @@ int ensure_scratch(vgc_context *ctx, LaunchScratch &s, uint32_t views, size_t un
 
 void free_scratch(LaunchScratch &s) {
   if (s.pending && s.done) cudaEventSynchronize(s.done);
+  if (s.h_scenes) cudaFreeHost(s.h_scenes);
+  if (s.d_scenes) cudaFree(s.d_scenes);
   if (s.h_views) cudaFreeHost(s.h_views);
   if (s.d_views) cudaFree(s.d_views);
   if (s.d_units) cudaFree(s.d_units);
@@ -415,6 +418,11 @@ int view_constants(vgc_context *ctx, const vgc_view &in, uint32_t out_slot, uint
   k.frustum = in.frustum_culling ? 1u : 0u;
   k.occl_active = in.hzb >= 0 ? 1u : 0u;
   k.hzb = in.hzb;
+  k.hzb_desc = in.hzb >= 0 ? (const HzbDesc *)ctx->d_hzb_desc.ptr + in.hzb : nullptr;
+  k.scene = 0;
+  k.slot_capacity = ctx->slot_capacity;
+  k.slots_used = ctx->slots_used;
+  k.counter_words = VGC_COUNTER_HEADER + ctx->slot_capacity * 8;
   k.build_hzb = (in.hzb >= 0 && in.depth) ? 1u : 0u;
   k.fresh_state = (in.flags & VGC_VIEW_FRESH_STATE) ? 1u : 0u;
   k.depth = in.depth;
@@ -451,6 +459,8 @@ int prepare(vgc_context *ctx, LaunchScratch &s, const vgc_view *views, uint32_t 
   }
   const uint32_t cells = pad32((uint32_t)ctx->cells.size());
   if ((rc = ensure_scratch(ctx, s, count, (size_t)count * cells))) return rc;
+  s.multi = false;
+  s.units_total = (size_t)count * cells;
   bool changed = false;
   s.hzb_w = s.hzb_h = 0;
   s.hzb_tail = false;
@@ -504,41 +514,97 @@ cudaError_t timed(vgc_context *ctx, bool capture, int kind, cudaStream_t st, F &
 
 // The launch sequence of one frame: reset, cells, then select + finish for the first round and two retry rounds
 // (GeometryPool.ts:1081-1092 without the dispatch-argument kernels, which persistent launches do not need).
+int prepare_multi(vgc_context *const *ctxs, uint32_t nctx, LaunchScratch &s, const vgc_view *views,
+                  const uint32_t *scene, uint32_t count, const uint32_t *slots) {
+  if (!ctxs || nctx == 0 || !views || !scene || !slots || count == 0) return fail(VGC_INVALID_ARG, "no views");
+  std::vector<uint32_t> slot_end(nctx, 0);
+  for (uint32_t i = 0; i < count; i++) {
+    if (scene[i] >= nctx) return fail(VGC_INVALID_ARG, "view scene index out of range");
+    if (views[i].depth) return fail(VGC_INVALID_ARG, "a multi-scene launch takes built HZB slots, not depth images");
+    slot_end[scene[i]] = std::max(slot_end[scene[i]], slots[i] + 1);
+  }
+  int rc;
+  size_t units = 0;
+  for (uint32_t k = 0; k < nctx; k++) {
+    if ((rc = sync_scene(ctxs[k]))) return rc;
+    if (slot_end[k] && (rc = ensure_outputs(ctxs[k], slot_end[k]))) return rc;
+  }
+  for (uint32_t i = 0; i < count; i++) units += pad32((uint32_t)ctxs[scene[i]]->cells.size());
+  if (s.pending) CUDA_TRY(cudaEventSynchronize(s.done));
+  s.pending = false;
+  if (s.h_ctl) {  // the last sequence's peak queue demand, as in prepare
+    const uint64_t need = std::max<uint64_t>((uint64_t)s.h_ctl[6] * 4 / 3, (uint64_t)s.h_ctl[7] * 4) * 5 / 4;
+    if (need > s.chunk_capacity) s.queue_want = (uint32_t)std::min<uint64_t>((need + 65535) & ~65535ull, 1u << 28);
+  }
+  if ((rc = ensure_scratch(ctxs[0], s, count, units))) return rc;
+  if (nctx > s.scene_capacity) {
+    vgc_context *owner = s.owner ? s.owner : ctxs[0];
+    if (s.h_scenes) cudaFreeHost(s.h_scenes);
+    if (s.d_scenes) {
+      cudaFree(s.d_scenes);
+      owner->bytes -= sizeof(Scene) * s.scene_capacity;
+    }
+    s.h_scenes = nullptr;
+    s.d_scenes = nullptr;
+    s.scene_capacity = 0;
+    CUDA_TRY(cudaMallocHost(&s.h_scenes, sizeof(Scene) * nctx));
+    CUDA_TRY(cudaMalloc(&s.d_scenes, sizeof(Scene) * nctx));
+    owner->bytes += sizeof(Scene) * nctx;
+    s.scene_capacity = nctx;
+  }
+  for (uint32_t k = 0; k < nctx; k++) s.h_scenes[k] = scene_of(ctxs[k]);
+  s.scene_count = nctx;
+  s.multi = true;
+  s.units_total = units;
+  s.hzb_w = s.hzb_h = 0;
+  s.hzb_tail = false;
+  s.any_budget = false;
+  uint32_t offset = 0;
+  for (uint32_t i = 0; i < count; i++) {
+    vgc_context *ctx = ctxs[scene[i]];
+    s.any_budget = s.any_budget || views[i].triangle_budget > 0;
+    if ((rc = view_constants(ctx, views[i], slots[i], offset, s.h_views[i]))) return rc;
+    s.h_views[i].scene = scene[i];
+    offset += pad32((uint32_t)ctx->cells.size());
+  }
+  return VGC_OK;
+}
+
 int enqueue(vgc_context *ctx, LaunchScratch &s, uint32_t count, cudaStream_t st, bool capture) {
   const Scene S = scene_of(ctx);
+  const Scene *scenes = s.multi ? s.d_scenes : nullptr;
   const uint32_t select_grid = s.grid_instances ? s.grid_instances : ctx->select_grid;
   const uint32_t chunk_grid = s.grid_chunks ? s.grid_chunks : ctx->chunk_grid;
-  const uint32_t cells = pad32(S.cell_count);
-  const HzbDesc *hzbs = (const HzbDesc *)ctx->d_hzb_desc.ptr;
   CUDA_TRY(cudaMemcpyAsync(s.d_views, s.h_views, sizeof(ViewConst) * count, cudaMemcpyHostToDevice, st));
+  if (s.multi) CUDA_TRY(cudaMemcpyAsync(s.d_scenes, s.h_scenes, sizeof(Scene) * s.scene_count, cudaMemcpyHostToDevice, st));
   if (s.hzb_w)
     CUDA_TRY(timed(ctx, capture, VGC_KERNEL_HZB, st, [&] {
-      return launch_hzb_views(s.d_views, count, hzbs, s.hzb_w, s.hzb_h, s.hzb_tail, st);
+      return launch_hzb_views(s.d_views, count, s.hzb_w, s.hzb_h, s.hzb_tail, st);
     }));
   CUDA_TRY(timed(ctx, capture, VGC_KERNEL_RESET, st,
-                 [&] { return launch_reset(s.d_views, count, ctx->counter_words, s.d_unit_count, st); }));
+                 [&] { return launch_reset(s.d_views, count, s.d_unit_count, st); }));
   CUDA_TRY(timed(ctx, capture, VGC_KERNEL_CELLS, st,
-                 [&] { return launch_cells(S, s.d_views, count, count * cells, s.d_units, s.d_unit_count, st); }));
+                 [&] { return launch_cells(S, scenes, s.d_views, count, s.units_total, s.d_units, s.d_unit_count, st); }));
   if (s.any_budget) {  // the triangleBudget search: histogram pass, then the threshold of each budget view
     CUDA_TRY(timed(ctx, capture, VGC_KERNEL_BUDGET, st, [&] {
-      cudaError_t e = launch_instances(S, s.d_views, hzbs, s.d_units, s.d_unit_count, s.d_chunks, s.chunk_capacity, -1,
+      cudaError_t e = launch_instances(S, scenes, s.d_views, s.d_units, s.d_unit_count, s.d_chunks, s.chunk_capacity, -1,
                                        select_grid, st);
       if (e == cudaSuccess)
-        e = launch_chunks(S, s.d_views, hzbs, s.d_chunks, s.d_unit_count, s.chunk_capacity, -1, chunk_grid, st);
+        e = launch_chunks(S, scenes, s.d_views, s.d_chunks, s.d_unit_count, s.chunk_capacity, -1, chunk_grid, st);
       if (e == cudaSuccess) e = launch_budget(s.d_views, count, s.d_unit_count, st);
       return e;
     }));
   }
   for (int round = 0; round < 3; round++) {
     CUDA_TRY(timed(ctx, capture, round == 0 ? VGC_KERNEL_SELECT0 : VGC_KERNEL_SELECT_RETRY, st, [&] {
-      return launch_instances(S, s.d_views, hzbs, s.d_units, s.d_unit_count, s.d_chunks, s.chunk_capacity, round,
+      return launch_instances(S, scenes, s.d_views, s.d_units, s.d_unit_count, s.d_chunks, s.chunk_capacity, round,
                               select_grid, st);
     }));
     CUDA_TRY(timed(ctx, capture, round == 0 ? VGC_KERNEL_CHUNKS0 : VGC_KERNEL_SELECT_RETRY, st, [&] {
-      return launch_chunks(S, s.d_views, hzbs, s.d_chunks, s.d_unit_count, s.chunk_capacity, round, chunk_grid, st);
+      return launch_chunks(S, scenes, s.d_views, s.d_chunks, s.d_unit_count, s.chunk_capacity, round, chunk_grid, st);
     }));
     CUDA_TRY(timed(ctx, capture, VGC_KERNEL_FINISH, st, [&] {
-      return launch_finish(s.d_views, count, S.slot_capacity, S.slots_used, s.d_unit_count, round, st);
+      return launch_finish(s.d_views, count, s.d_unit_count, round, st);
     }));
   }
   // control words (peak queue demand) for the next prepare
@@ -692,7 +758,7 @@ int vgc_context_create(const vgc_options *opts, vgc_context **out) {
     return fail(VGC_DEVICE_ERROR, "cudaStreamCreate failed");
   }
   int per_sm = 0, chunks_per_sm = 0;
-  if (configure_select(&per_sm, &chunks_per_sm) != cudaSuccess) {
+  if (configure_select(false, &per_sm, &chunks_per_sm) != cudaSuccess) {
     cudaGetLastError();
     per_sm = chunks_per_sm = 1;
   }
@@ -1424,22 +1490,21 @@ extern "C" int vgc_cut_noalloc(vgc_context *ctx, const vgc_view *view, uint32_t 
   k_noalloc_store_view<<<1, 128, 0, st>>>(k, d_view);
   CUDA_TRY(cudaGetLastError());
   const Scene S = scene_of(ctx);
-  const HzbDesc *hzbs = (const HzbDesc *)ctx->d_hzb_desc.ptr;
   if (build_hzb) {
     const HzbDesc &d = ctx->hzb[view->hzb].desc;
-    CUDA_TRY(launch_hzb_views(d_view, 1, hzbs, d.w[0], d.h[0], d.levels > 7, st));
+    CUDA_TRY(launch_hzb_views(d_view, 1, d.w[0], d.h[0], d.levels > 7, st));
   }
-  CUDA_TRY(launch_reset(d_view, 1, ctx->counter_words, ctl, st));
-  CUDA_TRY(launch_cells(S, d_view, 1, cells, units, ctl, st));
+  CUDA_TRY(launch_reset(d_view, 1, ctl, st));
+  CUDA_TRY(launch_cells(S, nullptr, d_view, 1, cells, units, ctl, st));
   if (view->triangle_budget > 0) {
-    CUDA_TRY(launch_instances(S, d_view, hzbs, units, ctl, chunks, kNoAllocMaxChunks, -1, ctx->select_grid, st));
-    CUDA_TRY(launch_chunks(S, d_view, hzbs, chunks, ctl, kNoAllocMaxChunks, -1, ctx->chunk_grid, st));
+    CUDA_TRY(launch_instances(S, nullptr, d_view, units, ctl, chunks, kNoAllocMaxChunks, -1, ctx->select_grid, st));
+    CUDA_TRY(launch_chunks(S, nullptr, d_view, chunks, ctl, kNoAllocMaxChunks, -1, ctx->chunk_grid, st));
     CUDA_TRY(launch_budget(d_view, 1, ctl, st));
   }
   for (int round = 0; round < 3; round++) {
-    CUDA_TRY(launch_instances(S, d_view, hzbs, units, ctl, chunks, kNoAllocMaxChunks, round, ctx->select_grid, st));
-    CUDA_TRY(launch_chunks(S, d_view, hzbs, chunks, ctl, kNoAllocMaxChunks, round, ctx->chunk_grid, st));
-    CUDA_TRY(launch_finish(d_view, 1, S.slot_capacity, S.slots_used, ctl, round, st));
+    CUDA_TRY(launch_instances(S, nullptr, d_view, units, ctl, chunks, kNoAllocMaxChunks, round, ctx->select_grid, st));
+    CUDA_TRY(launch_chunks(S, nullptr, d_view, chunks, ctl, kNoAllocMaxChunks, round, ctx->chunk_grid, st));
+    CUDA_TRY(launch_finish(d_view, 1, ctl, round, st));
   }
   return VGC_OK;
 }

@@ -70,6 +70,11 @@ struct LaunchScratch {
   uint32_t grid_chunks = 0;
   uint32_t view_capacity = 0;
   size_t unit_capacity = 0;
+  size_t units_total = 0;         // (view, cell) units of the prepared launch (each view: its scene's cells, padded)
+  bool multi = false;             // the prepared views belong to several contexts (a multi-scene launch)
+  Scene *h_scenes = nullptr;      // pinned: the multi-scene launch's scene table (ViewConst::scene indexes it)
+  Scene *d_scenes = nullptr;
+  uint32_t scene_count = 0, scene_capacity = 0;
   cudaEvent_t done = nullptr;
   bool pending = false;
 };
@@ -160,6 +165,10 @@ void free_scratch(LaunchScratch &s);
 // slots is null).
 int prepare(vgc_context *ctx, LaunchScratch &s, const vgc_view *views, uint32_t count, uint32_t first_slot,
             const uint32_t *slots = nullptr);
+// Views of several contexts in one launch sequence: view i is a view of ctxs[scene[i]] and writes that context's
+// output slot slots[i]. Views carry no depth image (their HZB slots must be built). Launch it with enqueue(ctxs[0]).
+int prepare_multi(vgc_context *const *ctxs, uint32_t nctx, LaunchScratch &s, const vgc_view *views,
+                  const uint32_t *scene, uint32_t count, const uint32_t *slots);
 // The launch sequence of `count` prepared views on `st` (capture: recorded into a CUDA graph).
 int enqueue(vgc_context *ctx, LaunchScratch &s, uint32_t count, cudaStream_t st, bool capture);
 // vgc_stats of one view from its counter header and dyn[0] (the threshold the cut used).

@@ -73,6 +73,7 @@ struct Scene {
   const float4 *inst;
   const uint32_t *inst_slot;
   const CellRec *cells;
+  const struct HzbDesc *hzbs;  // the context's HZB slot descriptors (ViewConst::hzb indexes them)
   uint32_t cell_count, instance_count, meshlet_count, slot_capacity, slots_used;
 };
 
@@ -107,6 +108,11 @@ struct ViewConst {
                         // [1..5] its bands: low (cut 0, 1), high (cut 0, 1), fade scale
   unsigned long long *hist;  // 2 * kBudgetBins: triangles entering / leaving the cut per threshold bin
   unsigned long long budget_tris;  // triangleBudget as an integer (the search compares T(t) <= budget_tris)
+  const HzbDesc *hzb_desc;  // the HZB slot's descriptor in the view's context (null without an HZB; HZB builds)
+  uint32_t scene;           // multi-scene launch: the view's entry in the launch's scene table (else 0)
+  uint32_t slot_capacity;   // the view's context: mesh slots its counters and draw args are laid out for,
+  uint32_t slots_used;      //   slots in use,
+  uint32_t counter_words;   //   counter words of one output slot
 };
 
 }  // namespace vgc

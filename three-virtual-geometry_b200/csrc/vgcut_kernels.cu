@@ -154,6 +154,22 @@ __device__ bool hzb_occluded(const ViewConst &V, const HzbDesc &H, const float c
   return min_z > hmax + float(1e-6);
 }
 
+// The scene a view reads. A launch over one context passes its Scene by value (kernel parameter space: no registers
+// held) and its HZB descriptors as a read-only parameter; a multi-scene launch (views of several contexts in one
+// batch) reads the view's entry of a scene table, and that scene's descriptors.
+template <bool MULTI>
+struct SceneOf {
+  __device__ __forceinline__ static const Scene &get(const Scene &S, const Scene *, const ViewConst &) { return S; }
+  __device__ __forceinline__ static const HzbDesc *hzbs(const HzbDesc *hzbs, const Scene &) { return hzbs; }
+};
+template <>
+struct SceneOf<true> {
+  __device__ __forceinline__ static Scene get(const Scene &, const Scene *scenes, const ViewConst &V) {
+    return scenes[V.scene];
+  }
+  __device__ __forceinline__ static const HzbDesc *hzbs(const HzbDesc *, const Scene &S) { return S.hzbs; }
+};
+
 // occludedSphere (GeometryPool.ts:701-705): the sphere grows by the camera band's top error in pixels
 __device__ __forceinline__ bool occluded(const ViewConst &V, const HzbDesc *hzbs, float high0, bool on, const float c[3],
                                          float r) {
@@ -185,7 +201,9 @@ __device__ __forceinline__ uint32_t *mesh_count(const ViewConst &V, uint32_t slo
 }
 
 // ------------------------------------------------------------------------------------------------ k_cells
-__global__ void __launch_bounds__(256) k_cells(Scene S, const ViewConst *__restrict__ views, uint32_t nviews,
+template <bool MULTI>
+__global__ void __launch_bounds__(256) k_cells(Scene S0, const Scene *__restrict__ scenes,
+                                               const ViewConst *__restrict__ views, uint32_t nviews,
                                                uint32_t total_units, uint2 *__restrict__ units,
                                                uint32_t *__restrict__ unit_count) {
   const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
@@ -200,6 +218,7 @@ __global__ void __launch_bounds__(256) k_cells(Scene S, const ViewConst *__restr
   }
   const uint32_t v = lo;
   const ViewConst &V = views[v];
+  const auto &S = SceneOf<MULTI>::get(S0, scenes, V);
   const uint32_t cell = u - V.unit_offset;
   bool vis = false;
   if (cell < S.cell_count) {
@@ -666,9 +685,10 @@ __device__ __forceinline__ void drain_queue(const Scene &S, const ViewConst &V, 
 // instances emit their meshlets; the others hand their level range to k_chunks as chunks of <= kChunk meshlets.
 // HIST: the budget search's pass (views with a triangleBudget only): the camera cut's level range over the whole
 // threshold range, no fast path, no counters.
-template <bool HIST>
-__global__ void __launch_bounds__(128, 6) k_instances(Scene S, const ViewConst *__restrict__ views,
-                                                   const HzbDesc *__restrict__ hzbs, const uint2 *__restrict__ units,
+template <bool HIST, bool MULTI>
+__global__ void __launch_bounds__(128, MULTI ? 5 : 6) k_instances(Scene S0, const Scene *__restrict__ scenes,
+                                                   const ViewConst *__restrict__ views,
+                                                   const HzbDesc *__restrict__ hzbs0, const uint2 *__restrict__ units,
                                                    uint32_t *__restrict__ ctl, uint4 *__restrict__ queue,
                                                    uint32_t capacity, int round) {
   __shared__ WarpStage stage[4];
@@ -687,6 +707,8 @@ __global__ void __launch_bounds__(128, 6) k_instances(Scene S, const ViewConst *
       redo1 = V.counters[VGC_COUNTER_REDO1] != 0;
       if (!redo0 && !redo1) continue;
     }
+    const auto &S = SceneOf<MULTI>::get(S0, scenes, V);
+    const HzbDesc *__restrict__ hzbs = SceneOf<MULTI>::hzbs(hzbs0, S);
     const CellRec cell = S.cells[unit.y];
     const uint32_t il = ((w & 3u) << 5) + lane;
     if (((w & 3u) << 5) >= cell.count) continue;
@@ -852,10 +874,12 @@ __global__ void __launch_bounds__(128, 6) k_instances(Scene S, const ViewConst *
 // walk the chunk's meshlets end to end, 32 per step whatever span they belong to. The LOD band comes first; the
 // meshlets that pass queue up and finish 32 at a time (drain_queue). One draw-list flush per chunk.
 // HIST: the budget histogram of the chunks the budget pass queued.
-template <bool HIST>
-__global__ void __launch_bounds__(128, 8) k_chunks(Scene S, const ViewConst *__restrict__ views,
-                                                const HzbDesc *__restrict__ hzbs, uint4 *__restrict__ queue,
-                                                uint32_t *__restrict__ ctl, uint32_t capacity, int round) {
+template <bool HIST, bool MULTI>
+__global__ void __launch_bounds__(128, MULTI ? 6 : 8) k_chunks(Scene S0, const Scene *__restrict__ scenes,
+                                                            const ViewConst *__restrict__ views,
+                                                            const HzbDesc *__restrict__ hzbs0,
+                                                            uint4 *__restrict__ queue, uint32_t *__restrict__ ctl,
+                                                            uint32_t capacity, int round) {
   __shared__ WarpStage stage[4];
   __shared__ LodQueue queues[4];
   __shared__ SpanFrame frames[4];
@@ -872,6 +896,8 @@ __global__ void __launch_bounds__(128, 8) k_chunks(Scene S, const ViewConst *__r
     const uint32_t ns = ch.z >> 8;
     if (ns == 0) continue;
     const ViewConst &V = views[ch.x];
+    const auto &S = SceneOf<MULTI>::get(S0, scenes, V);
+    const HzbDesc *__restrict__ hzbs = SceneOf<MULTI>::hzbs(hzbs0, S);
     const CellRec cell = S.cells[ch.y];
     const uint32_t cut = ch.z & 1u;
     const bool occl_on = (ch.z & 2u) != 0;
@@ -1009,13 +1035,13 @@ __device__ __forceinline__ float fill_of(const ViewConst &V, uint32_t cut) {
 }
 
 __global__ void __launch_bounds__(128) k_finish(const ViewConst *__restrict__ views, uint32_t nviews,
-                                                uint32_t slot_capacity, uint32_t slots_used, uint32_t *__restrict__ ctl,
-                                                int round) {
+                                                uint32_t *__restrict__ ctl, int round) {
   const uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t lane = threadIdx.x & 31;
   if (blockIdx.x == 0 && threadIdx.x == 0) retire_queue(ctl);  // the next round's work queue starts empty
   if (v >= nviews) return;
   const ViewConst &V = views[v];
+  const uint32_t slot_capacity = V.slot_capacity, slots_used = V.slots_used;
   uint32_t *ctr = V.counters;
   const bool redo[2] = {round == 0 || ctr[VGC_COUNTER_REDO0] != 0, round == 0 || ctr[VGC_COUNTER_REDO1] != 0};
   // prefix (GeometryPool.ts:973-995)
@@ -1228,22 +1254,20 @@ __global__ void __launch_bounds__(256) k_hzb_tiles(const float *__restrict__ dep
 }
 
 // The HZB builds of a batch: grid.z = view, views without a depth image skip.
-__global__ void __launch_bounds__(256) k_hzb_tiles_views(const ViewConst *__restrict__ views,
-                                                         const HzbDesc *__restrict__ hzbs) {
+__global__ void __launch_bounds__(256) k_hzb_tiles_views(const ViewConst *__restrict__ views) {
   __shared__ float sm[2][16][17];
   const ViewConst &V = views[blockIdx.z];
   if (!V.build_hzb) return;
-  const HzbDesc &H = hzbs[V.hzb];
+  const HzbDesc &H = *V.hzb_desc;
   const uint32_t ox = blockIdx.x * kHzbTile, oy = blockIdx.y * kHzbTile;
   if (ox >= H.w[0] || oy >= H.h[0]) return;
   hzb_tile64(V.depth, H, const_cast<float *>(H.data), true, ox, oy, sm);
 }
 
-__global__ void __launch_bounds__(1024) k_hzb_tail_views(const ViewConst *__restrict__ views,
-                                                         const HzbDesc *__restrict__ hzbs) {
+__global__ void __launch_bounds__(1024) k_hzb_tail_views(const ViewConst *__restrict__ views) {
   const ViewConst &V = views[blockIdx.x];
   if (!V.build_hzb) return;
-  const HzbDesc &H = hzbs[V.hzb];
+  const HzbDesc &H = *V.hzb_desc;
   float *out = const_cast<float *>(H.data);
   for (uint32_t l = kHzbTileLevels; l < H.levels; l++) {
     const float *src = out + H.off[l - 1];
@@ -1332,11 +1356,12 @@ __global__ void __launch_bounds__(256) k_select_cut(Scene S, uint32_t slot, uint
 // ------------------------------------------------------------------------------------------------ k_reset
 // Zeroes each view's counter block (reset pass, GeometryPool.ts:714-725) and the batch's unit count; reads the
 // output pointers from the view constants, so a captured graph serves any output slots.
-__global__ void __launch_bounds__(256) k_reset(const ViewConst *__restrict__ views, uint32_t nviews, uint32_t words,
+__global__ void __launch_bounds__(256) k_reset(const ViewConst *__restrict__ views, uint32_t nviews,
                                                uint32_t *__restrict__ ctl) {
   if (blockIdx.x == 0 && threadIdx.x < 16) ctl[threadIdx.x] = 0;
   for (uint32_t v = blockIdx.x; v < nviews; v += gridDim.x) {
     uint32_t *c = views[v].counters;
+    const uint32_t words = views[v].counter_words;
     for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) c[i] = 0;
     if (threadIdx.x == 0) {
       if (views[v].fresh_state) {  // initial controller state: scales 1.0 (fixed point x10000), no fill, no retry
@@ -1439,43 +1464,65 @@ cudaError_t launch_gather_stats(const ViewConst *views, uint32_t nviews, uint32_
   return cudaGetLastError();
 }
 
-cudaError_t launch_reset(const ViewConst *views, uint32_t nviews, uint32_t words, uint32_t *ctl, cudaStream_t st) {
+cudaError_t launch_reset(const ViewConst *views, uint32_t nviews, uint32_t *ctl, cudaStream_t st) {
   const uint32_t blocks = nviews < 1024 ? (nviews ? nviews : 1) : 1024;
-  k_reset<<<blocks, 256, 0, st>>>(views, nviews, words, ctl);
+  k_reset<<<blocks, 256, 0, st>>>(views, nviews, ctl);
   return cudaGetLastError();
 }
 
-
-cudaError_t launch_cells(const Scene &S, const ViewConst *views, uint32_t nviews, uint32_t total_units, uint2 *units,
-                         uint32_t *unit_count, cudaStream_t st) {
+cudaError_t launch_cells(const Scene &S, const Scene *scenes, const ViewConst *views, uint32_t nviews,
+                         uint32_t total_units, uint2 *units, uint32_t *unit_count, cudaStream_t st) {
   if (total_units == 0) return cudaSuccess;
   const uint32_t blocks = (total_units + 255) / 256;
-  k_cells<<<blocks, 256, 0, st>>>(S, views, nviews, total_units, units, unit_count);
+  if (scenes)
+    k_cells<true><<<blocks, 256, 0, st>>>(S, scenes, views, nviews, total_units, units, unit_count);
+  else
+    k_cells<false><<<blocks, 256, 0, st>>>(S, nullptr, views, nviews, total_units, units, unit_count);
   return cudaGetLastError();
 }
 
-cudaError_t configure_select(int *instances_per_sm, int *chunks_per_sm) {
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(instances_per_sm, k_instances<false>, 128, 0);
+cudaError_t configure_select(bool multi, int *instances_per_sm, int *chunks_per_sm) {
+  cudaError_t e = multi ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(instances_per_sm, k_instances<false, true>, 128, 0)
+                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(instances_per_sm, k_instances<false, false>, 128, 0);
   if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(chunks_per_sm, k_chunks<false>, 128, 0);
+  return multi ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(chunks_per_sm, k_chunks<false, true>, 128, 0)
+               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(chunks_per_sm, k_chunks<false, false>, 128, 0);
 }
 
-cudaError_t launch_instances(const Scene &S, const ViewConst *views, const HzbDesc *hzbs, const uint2 *units,
+template <bool MULTI>
+static void instances_kernel(const Scene &S, const Scene *scenes, const ViewConst *views, const uint2 *units,
+                             uint32_t *ctl, uint4 *queue, uint32_t capacity, int round, uint32_t grid, cudaStream_t st) {
+  if (round < 0)  // the budget search's pass
+    k_instances<true, MULTI><<<grid, 128, 0, st>>>(S, scenes, views, S.hzbs, units, ctl, queue, capacity, 0);
+  else
+    k_instances<false, MULTI><<<grid, 128, 0, st>>>(S, scenes, views, S.hzbs, units, ctl, queue, capacity, round);
+}
+
+cudaError_t launch_instances(const Scene &S, const Scene *scenes, const ViewConst *views, const uint2 *units,
                              uint32_t *ctl, uint4 *queue, uint32_t capacity, int round, uint32_t grid,
                              cudaStream_t st) {
-  if (round < 0)  // the budget search's pass
-    k_instances<true><<<grid, 128, 0, st>>>(S, views, hzbs, units, ctl, queue, capacity, 0);
+  if (scenes)
+    instances_kernel<true>(S, scenes, views, units, ctl, queue, capacity, round, grid, st);
   else
-    k_instances<false><<<grid, 128, 0, st>>>(S, views, hzbs, units, ctl, queue, capacity, round);
+    instances_kernel<false>(S, nullptr, views, units, ctl, queue, capacity, round, grid, st);
   return cudaGetLastError();
 }
 
-cudaError_t launch_chunks(const Scene &S, const ViewConst *views, const HzbDesc *hzbs, uint4 *queue,
-                          uint32_t *ctl, uint32_t capacity, int round, uint32_t grid, cudaStream_t st) {
+template <bool MULTI>
+static void chunks_kernel(const Scene &S, const Scene *scenes, const ViewConst *views, uint4 *queue, uint32_t *ctl,
+                          uint32_t capacity, int round, uint32_t grid, cudaStream_t st) {
   if (round < 0)
-    k_chunks<true><<<grid, 128, 0, st>>>(S, views, hzbs, queue, ctl, capacity, 0);
+    k_chunks<true, MULTI><<<grid, 128, 0, st>>>(S, scenes, views, S.hzbs, queue, ctl, capacity, 0);
   else
-    k_chunks<false><<<grid, 128, 0, st>>>(S, views, hzbs, queue, ctl, capacity, round);
+    k_chunks<false, MULTI><<<grid, 128, 0, st>>>(S, scenes, views, S.hzbs, queue, ctl, capacity, round);
+}
+
+cudaError_t launch_chunks(const Scene &S, const Scene *scenes, const ViewConst *views, uint4 *queue, uint32_t *ctl,
+                          uint32_t capacity, int round, uint32_t grid, cudaStream_t st) {
+  if (scenes)
+    chunks_kernel<true>(S, scenes, views, queue, ctl, capacity, round, grid, st);
+  else
+    chunks_kernel<false>(S, nullptr, views, queue, ctl, capacity, round, grid, st);
   return cudaGetLastError();
 }
 
@@ -1485,10 +1532,9 @@ cudaError_t launch_budget(const ViewConst *views, uint32_t nviews, uint32_t *ctl
   return cudaGetLastError();
 }
 
-cudaError_t launch_finish(const ViewConst *views, uint32_t nviews, uint32_t slot_capacity, uint32_t slots_used,
-                          uint32_t *ctl, int round, cudaStream_t st) {
+cudaError_t launch_finish(const ViewConst *views, uint32_t nviews, uint32_t *ctl, int round, cudaStream_t st) {
   const uint32_t blocks = (nviews * 32 + 127) / 128;
-  k_finish<<<blocks, 128, 0, st>>>(views, nviews, slot_capacity, slots_used, ctl, round);
+  k_finish<<<blocks, 128, 0, st>>>(views, nviews, ctl, round);
   return cudaGetLastError();
 }
 
@@ -1507,13 +1553,13 @@ cudaError_t launch_hzb(const float *depth, const HzbDesc &H, float *out, int cop
   return cudaGetLastError();
 }
 
-cudaError_t launch_hzb_views(const ViewConst *views, uint32_t nviews, const HzbDesc *hzbs, uint32_t max_w,
+cudaError_t launch_hzb_views(const ViewConst *views, uint32_t nviews, uint32_t max_w,
                              uint32_t max_h, bool tail, cudaStream_t st) {
   dim3 grid((max_w + kHzbTile - 1) / kHzbTile, (max_h + kHzbTile - 1) / kHzbTile, nviews);
-  k_hzb_tiles_views<<<grid, 256, 0, st>>>(views, hzbs);
+  k_hzb_tiles_views<<<grid, 256, 0, st>>>(views);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || !tail) return e;
-  k_hzb_tail_views<<<nviews, 1024, 0, st>>>(views, hzbs);
+  k_hzb_tail_views<<<nviews, 1024, 0, st>>>(views);
   return cudaGetLastError();
 }
 
