@@ -254,9 +254,10 @@ int vgc_batch_autotune(vgc_batch *batch, const vgc_view *views, uint32_t count, 
 /* A request loop over several resident scenes (one context each). The reference cuts once per rendered frame of
    one camera; a server takes cut requests (scene, view) from any thread as they arrive. One worker thread admits a
    request while an output slot of its scene is free and the output-slot bytes of the admitted, unreleased requests
-   stay within the HBM budget; it batches admitted requests of one scene into one launch sequence and keeps up to
-   `streams` batches in flight, so requests that arrive while others run start as soon as a stream and slots free
-   up (continuous batching). Each request runs as vgc_cut of its view alone would with VGC_VIEW_FRESH_STATE, its
+   stay within the HBM budget; it batches the oldest admitted requests - of any scenes, each view reading its own
+   scene's data in the same kernels (cross_scene), or of the oldest request's scene only - into one launch sequence
+   and keeps up to `streams` batches in flight, so requests that arrive while others run start as soon as a stream
+   and slots free up (continuous batching). Each request runs as vgc_cut of its view alone would with VGC_VIEW_FRESH_STATE, its
    output slot doubling as its state slot: the result is the same alone and in any mix. While a server runs, its
    contexts take no other cut or scene change; completed requests' outputs are read with vgc_get_output /
    vgc_read_draw_list on (scene context, result.slot) until vgc_server_release. */
@@ -269,6 +270,7 @@ typedef struct {
   uint32_t linger_us;        /* a batch smaller than max_batch waits up to this long for more requests (default 0) */
   uint64_t max_batch_instances; /* views x scene instances per batch at most (default 32M; 0: no limit): large
                                    scenes go in smaller batches, which keeps their latency and work queue bounded */
+  uint32_t cross_scene;      /* 1 (default): a batch mixes scenes (all contexts on one device); 0: one scene each */
 } vgc_server_options;
 typedef struct {
   uint64_t ticket;
@@ -278,11 +280,13 @@ typedef struct {
   double submit_us, start_us, done_us; /* host steady clock, microseconds: submitted, launched, seen complete */
   float batch_gpu_ms;         /* device time of that launch (CUDA events on its stream) */
   vgc_stats stats;            /* its counters, copied back with the launch */
+  uint32_t batch_scenes;      /* scenes in that launch */
 } vgc_serve_result;
 typedef struct {
   uint64_t submitted, completed, batches, views_launched;
   uint64_t bytes_in_use, max_bytes_in_use; /* admitted output-slot bytes now / at most */
   uint32_t max_in_flight;                 /* most batches in flight at once */
+  uint64_t multi_scene_batches;           /* batches that mixed scenes */
 } vgc_server_stats;
 void vgc_server_default_options(vgc_server_options *opts);
 int vgc_server_create(vgc_context *const *scenes, uint32_t scene_count, const vgc_server_options *opts,

@@ -1,13 +1,15 @@
 """The serving loop (vgc_server_*): requests against several resident scenes, submitted from two threads with
-uneven timing, admitted by output slots and HBM budget, batched per scene and overlapped on two streams. Every
-result must equal the same view cut alone (fresh controller state) on the same scene: counters, chosen threshold,
-budget prediction and the drawn (instance, meshlet, fade) set of both cuts."""
+uneven timing, admitted by output slots and HBM budget, batched across scenes (one multi-scene launch) or per scene,
+and overlapped on two streams. Every result must equal the same view cut alone (fresh controller state) on the same
+scene - counters, chosen threshold, budget prediction and the drawn (instance, meshlet, fade) set of both cuts - and
+the oracle's float mirror of that view."""
 import random
 import threading
 
 import numpy as np
 import pytest
 
+import oracle as O
 from parity_util import key_set
 from vgcut import engine, scenes
 from vgcut.camera import Camera
@@ -18,17 +20,30 @@ COUNTERS = ("visible_cells", "occluded_instances", "selected", "drawn", "survive
             "rounds", "effective_threshold", "predicted_triangles")
 
 
+MAX_MESHLETS = 1 << 15
+FRESH = [10000, 10000, 0, 0, 0, 0, 0, 0]
+
+
 @pytest.fixture(scope="module")
 def contexts():
     out = []
     for seed, n in ((1, 24), (2, 32), (3, 16)):
         spec = scenes.plain_small(n=n, seed=seed, grid=6 + seed)
-        vg = engine.VirtualGeometry(max_meshlets=1 << 15, output_slots=2)
+        vg = engine.VirtualGeometry(max_meshlets=MAX_MESHLETS, output_slots=2)
         scenes.load_into(vg, spec, cast_shadow=(seed != 2))
         out.append((spec, vg))
     yield out
     for _, vg in out:
         vg.dispose()
+
+
+@pytest.fixture(scope="module")
+def oracle_scenes(contexts):
+    out = []
+    for k, (spec, _) in enumerate(contexts):
+        scene, _, _ = O.scene_from_spec(spec.meshes, spec.instances, [dict(shadow=(k != 1)) for _ in spec.meshes])
+        out.append(scene)
+    return out
 
 
 def random_request(rng, spec):
@@ -47,14 +62,16 @@ def snapshot(vg, slot):
     return {k: s[k] for k in COUNTERS}, [key_set(vg.draw_list(slot, c), (0, 1, 3)) for c in (0, 1)]
 
 
-def test_served_equals_alone(contexts):
+@pytest.mark.parametrize("cross_scene", [True, False])
+def test_served_equals_alone_and_the_oracle(contexts, oracle_scenes, cross_scene):
     rng = random.Random(11)
     reqs = []
     for i in range(72):
         k = rng.randrange(len(contexts))
         cam, p = random_request(rng, contexts[k][0])
         reqs.append((k, cam, p))
-    server = engine.Server([vg for _, vg in contexts], streams=2, max_batch=8, slots_per_scene=24)
+    server = engine.Server([vg for _, vg in contexts], streams=2, max_batch=8, slots_per_scene=24,
+                           cross_scene=cross_scene)
     tickets = [None] * len(reqs)
 
     def submit(idx):
@@ -81,8 +98,14 @@ def test_served_equals_alone(contexts):
         st = server.stats()
         assert st["completed"] == len(reqs) and st["batches"] >= len(reqs) // 8
         assert st["max_in_flight"] >= 1
+        if cross_scene:
+            assert st["multi_scene_batches"] > 0, "some batches mix scenes"
+        else:
+            assert st["multi_scene_batches"] == 0
     finally:
         server.close()
+    if cross_scene:
+        assert any(res["batch_scenes"] > 1 for res, _ in served)
     for (k, cam, p), (res, (counters, sets)) in zip(reqs, served):
         assert res["status"] == 0 and res["done_us"] >= res["start_us"] >= res["submit_us"]
         vg = contexts[k][1]
@@ -92,6 +115,19 @@ def test_served_equals_alone(contexts):
         assert counters == want_counters, f"served counters {counters} alone {want_counters}"
         assert {kk: res["stats"][kk] for kk in COUNTERS} == want_counters
         assert sets == want_sets
+        # the oracle's float mirror of the same view
+        o = O.cull_pass(oracle_scenes[k], O.make_view(cam, p, MAX_MESHLETS, (30_000_000, 12_000_000), state=FRESH),
+                        "f32")
+        c = o["counters"]
+        assert counters["visible_cells"] == c[0] and counters["occluded_instances"] == c[1]
+        for cut in (0, 1):
+            assert [counters["selected"][cut], counters["survived"][cut], counters["work"][cut]] == \
+                [c[2 + cut * 5], c[4 + cut * 5], c[5 + cut * 5]]
+            if c[2 + cut * 5] <= MAX_MESHLETS:
+                assert sets[cut] == key_set(o["entries"][cut], (0, 1, 2)), f"served cut {cut} differs from the oracle"
+        if p.triangle_budget > 0:
+            assert counters["predicted_triangles"] == o["predicted"]
+            assert counters["effective_threshold"] == np.float32(o["threshold"])
     assert any(len(s[1][1][0]) > 0 for s in served)
 
 

@@ -4,8 +4,10 @@
 //
 //  * admission: a request waits until an output slot of its scene is free and the output-slot bytes of all
 //    admitted, unreleased requests plus its own stay within the HBM budget;
-//  * batching: the worker takes the scene whose oldest admissible request is oldest and launches up to max_batch
-//    of its admissible requests as one launch sequence (the plain path's kernels, one view per request);
+//  * batching: the worker launches up to max_batch of the oldest admissible requests as one launch sequence (the
+//    plain path's kernels, one view per request). With cross_scene they may belong to different scenes: each view
+//    then reads its own context's scene through a scene table (the multi-scene kernel variants); otherwise a
+//    batch takes the requests of the oldest admissible request's scene;
 //  * continuous batching: each of `streams` lanes owns a CUDA stream and launch scratch; a lane that finishes is
 //    refilled from whatever is pending, while the other lanes' batches keep running;
 //  * completion: the lane's stream gathers every view's counters into pinned memory and then runs a host callback,
@@ -38,7 +40,6 @@ struct Request {
 struct SceneState {
   vgc_context *ctx = nullptr;
   std::vector<uint32_t> free_slots;
-  std::deque<uint64_t> pending;  // tickets in arrival order
   size_t slot_bytes = 0;
 };
 
@@ -51,7 +52,7 @@ struct Lane {
   bool busy = false;
   bool complete = false;  // set by the stream callback
   double done_us = 0;
-  uint32_t scene = 0;
+  uint32_t scenes = 0;  // distinct scenes in the batch
   double start_us = 0;
   std::vector<uint64_t> tickets;
   int status = VGC_OK;
@@ -62,6 +63,9 @@ struct Lane {
 struct vgc_server {
   vgc_server_options opts{};
   std::vector<SceneState> scenes;
+  std::vector<vgc_context *> ctxs;  // the scene table of multi-scene launches (index = scene)
+  std::deque<uint64_t> pending;     // tickets in arrival order, all scenes
+  uint32_t multi_grid[2] = {0, 0};  // persistent grids of the multi-scene k_instances / k_chunks
   std::vector<Lane> lanes;
   std::vector<std::pair<vgc_server *, Lane *>> callbacks;  // host-callback arguments, one per lane
   std::mutex mu;
@@ -91,39 +95,49 @@ void CUDART_CB lane_done(void *arg) {
   s->wake.notify_all();
 }
 
-// The next batch for an idle lane, chosen under the lock: the scene whose oldest admissible request is oldest, then
-// that scene's admissible requests in arrival order. Returns false when nothing can start now.
-bool pick_batch(vgc_server *s, Lane &lane, std::vector<uint32_t> &slots, std::vector<vgc_view> &views) {
-  int best = -1;
-  double best_t = 0;
-  for (size_t i = 0; i < s->scenes.size(); i++) {
-    SceneState &sc = s->scenes[i];
-    if (sc.pending.empty() || sc.free_slots.empty()) continue;
-    if (s->opts.hbm_budget_bytes && s->bytes_in_use + sc.slot_bytes > s->opts.hbm_budget_bytes) continue;
-    const double t = s->requests[sc.pending.front()].result.submit_us;
-    if (best < 0 || t < best_t) best = (int)i, best_t = t;
-  }
-  if (best < 0) return false;
-  SceneState &sc = s->scenes[best];
-  if (s->opts.linger_us && sc.pending.size() < s->opts.max_batch && now_us() - best_t < s->opts.linger_us)
-    return false;
+// The next batch for an idle lane, chosen under the lock: the oldest admissible requests in arrival order (a request
+// is admissible while its scene has a free output slot and its slot bytes fit the HBM budget), from any scene with
+// cross_scene, else from the oldest one's scene. Returns false when nothing can start now.
+bool pick_batch(vgc_server *s, Lane &lane, std::vector<uint32_t> &slots, std::vector<vgc_view> &views,
+                std::vector<uint32_t> &scene_ids) {
+  auto admissible = [&](const SceneState &sc) {
+    return !sc.free_slots.empty() &&
+           !(s->opts.hbm_budget_bytes && s->bytes_in_use + sc.slot_bytes > s->opts.hbm_budget_bytes);
+  };
+  auto first = s->pending.end();
+  size_t ready = 0;
+  for (auto it = s->pending.begin(); it != s->pending.end(); ++it)
+    if (admissible(s->scenes[s->requests[*it].scene])) {
+      if (first == s->pending.end()) first = it;
+      if (++ready >= s->opts.max_batch) break;
+    }
+  if (first == s->pending.end()) return false;
+  const double oldest = s->requests[*first].result.submit_us;
+  if (s->opts.linger_us && ready < s->opts.max_batch && now_us() - oldest < s->opts.linger_us) return false;
+  const uint32_t lead = s->requests[*first].scene;
   lane.tickets.clear();
   slots.clear();
   views.clear();
-  // views of this batch: max_batch, fewer for scenes so large that a full batch would queue too much work at once
-  uint32_t cap = s->opts.max_batch;
-  if (s->opts.max_batch_instances) {
+  scene_ids.clear();
+  // views x scene instances of the batch: large scenes go in smaller batches, which bounds latency and queued work
+  uint64_t work = 0;
+  std::vector<bool> seen(s->scenes.size(), false);
+  uint32_t distinct = 0;
+  for (auto it = first; it != s->pending.end() && lane.tickets.size() < s->opts.max_batch;) {
+    Request &r = s->requests[*it];
+    SceneState &sc = s->scenes[r.scene];
+    if ((!s->opts.cross_scene && r.scene != lead) || !admissible(sc)) {
+      ++it;
+      continue;
+    }
     const uint64_t inst = std::max<uint64_t>(1, sc.ctx->inst_slot.size());
-    cap = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(cap, s->opts.max_batch_instances / inst));
-  }
-  while (!sc.pending.empty() && !sc.free_slots.empty() && lane.tickets.size() < cap) {
-    if (s->opts.hbm_budget_bytes && s->bytes_in_use + sc.slot_bytes > s->opts.hbm_budget_bytes) break;
-    const uint64_t t = sc.pending.front();
-    sc.pending.pop_front();
+    if (s->opts.max_batch_instances && !lane.tickets.empty() && work + inst > s->opts.max_batch_instances) break;
+    work += inst;
+    const uint64_t t = *it;
+    it = s->pending.erase(it);
     const uint32_t slot = sc.free_slots.back();
     sc.free_slots.pop_back();
     s->bytes_in_use += sc.slot_bytes;
-    Request &r = s->requests[t];
     r.result.slot = slot;
     vgc_view v = r.view;
     v.state_slot = slot;
@@ -131,21 +145,35 @@ bool pick_batch(vgc_server *s, Lane &lane, std::vector<uint32_t> &slots, std::ve
     lane.tickets.push_back(t);
     slots.push_back(slot);
     views.push_back(v);
+    scene_ids.push_back(r.scene);
+    if (!seen[r.scene]) seen[r.scene] = true, distinct++;
   }
   s->stats.max_bytes_in_use = std::max<uint64_t>(s->stats.max_bytes_in_use, s->bytes_in_use);
-  lane.scene = (uint32_t)best;
+  lane.scenes = distinct;
   lane.busy = true;
   lane.complete = false;
   return true;
 }
 
-// Launches a picked batch on its lane (no server lock held: prepare may synchronise the device).
+// Launches a picked batch on its lane (no server lock held: prepare may synchronise the device). A batch of one
+// scene takes that context's plain launch sequence; a mixed batch the multi-scene variant over the server's scene
+// table.
 int launch_batch(vgc_server *s, Lane &lane, const std::vector<uint32_t> &slots, const std::vector<vgc_view> &views,
-                 std::pair<vgc_server *, Lane *> *cb) {
-  vgc_context *ctx = s->scenes[lane.scene].ctx;
+                 const std::vector<uint32_t> &scene_ids, std::pair<vgc_server *, Lane *> *cb) {
+  vgc_context *ctx = s->scenes[scene_ids[0]].ctx;
   cudaSetDevice(ctx->device);
   const uint32_t n = (uint32_t)views.size();
-  int rc = prepare(ctx, lane.scratch, views.data(), n, 0, slots.data());
+  int rc;
+  if (lane.scenes <= 1) {
+    lane.scratch.grid_instances = lane.scratch.grid_chunks = 0;  // the context's single-scene grids
+    rc = prepare(ctx, lane.scratch, views.data(), n, 0, slots.data());
+  } else {
+    lane.scratch.grid_instances = s->multi_grid[0];
+    lane.scratch.grid_chunks = s->multi_grid[1];
+    ctx = s->ctxs[0];
+    rc = prepare_multi(s->ctxs.data(), (uint32_t)s->ctxs.size(), lane.scratch, views.data(), scene_ids.data(), n,
+                       slots.data());
+  }
   if (rc) return rc;
   CUDA_TRY(cudaEventRecord(lane.start, lane.stream));
   if ((rc = enqueue(ctx, lane.scratch, n, lane.stream, false))) return rc;
@@ -160,11 +188,12 @@ int launch_batch(vgc_server *s, Lane &lane, const std::vector<uint32_t> &slots, 
 void finish_lane(vgc_server *s, Lane &lane) {
   float gpu_ms = 0;
   if (lane.status == VGC_OK) cudaEventElapsedTime(&gpu_ms, lane.start, lane.end);
-  vgc_context *ctx = s->scenes[lane.scene].ctx;
   for (size_t i = 0; i < lane.tickets.size(); i++) {
     Request &r = s->requests[lane.tickets[i]];
+    vgc_context *ctx = s->scenes[r.scene].ctx;
     r.result.status = lane.status;
     r.result.batch_views = (uint32_t)lane.tickets.size();
+    r.result.batch_scenes = lane.scenes;
     r.result.start_us = lane.start_us;
     r.result.done_us = lane.status == VGC_OK ? lane.done_us : now_us();
     r.result.batch_gpu_ms = gpu_ms;
@@ -184,7 +213,7 @@ void finish_lane(vgc_server *s, Lane &lane) {
 }
 
 void worker_main(vgc_server *s) {
-  std::vector<uint32_t> slots;
+  std::vector<uint32_t> slots, scene_ids;
   std::vector<vgc_view> views;
   std::unique_lock<std::mutex> lock(s->mu);
   while (!s->stop) {
@@ -197,14 +226,15 @@ void worker_main(vgc_server *s) {
     if (progress) s->done.notify_all();
     for (size_t i = 0; i < s->lanes.size(); i++) {
       Lane &lane = s->lanes[i];
-      if (lane.busy || !pick_batch(s, lane, slots, views)) continue;
+      if (lane.busy || !pick_batch(s, lane, slots, views, scene_ids)) continue;
       lane.start_us = now_us();
       s->in_flight++;
       s->stats.batches++;
+      if (lane.scenes > 1) s->stats.multi_scene_batches++;
       s->stats.views_launched += views.size();
       s->stats.max_in_flight = std::max(s->stats.max_in_flight, s->in_flight);
       lock.unlock();
-      const int rc = launch_batch(s, lane, slots, views, &s->callbacks[i]);
+      const int rc = launch_batch(s, lane, slots, views, scene_ids, &s->callbacks[i]);
       std::string why;
       if (rc) {  // the batch's callback was not queued: wait out what was, then complete it with the error
         why = vgc_last_error();
@@ -237,6 +267,7 @@ void vgc_server_default_options(vgc_server_options *o) {
   o->streams = 2;
   o->max_batch = 64;
   o->max_batch_instances = 32u << 20;
+  o->cross_scene = 1;
 }
 
 int vgc_server_create(vgc_context *const *scenes, uint32_t scene_count, const vgc_server_options *opts,
@@ -270,6 +301,8 @@ int vgc_server_create(vgc_context *const *scenes, uint32_t scene_count, const vg
     if (rc) return cleanup(rc);
     SceneState &sc = s->scenes[i];
     sc.ctx = ctx;
+    s->ctxs.push_back(ctx);
+    if (ctx->device != scenes[0]->device) s->opts.cross_scene = 0;  // a multi-scene launch runs on one device
     sc.slot_bytes = output_slot_bytes(ctx);
     for (uint32_t k = o.slots_per_scene; k-- > 0;) sc.free_slots.push_back(k);
     if (ctx->cells.size() > largest->cells.size()) largest = ctx;
@@ -278,6 +311,13 @@ int vgc_server_create(vgc_context *const *scenes, uint32_t scene_count, const vg
     for (const SceneState &sc : s->scenes)
       if (sc.slot_bytes > o.hbm_budget_bytes) return cleanup(fail(VGC_OVER_BUDGET, "one output slot exceeds the budget"));
   cudaSetDevice(largest->device);
+  int mi = 0, mc = 0;
+  if (configure_select(true, &mi, &mc) != cudaSuccess) {
+    cudaGetLastError();
+    mi = mc = 1;
+  }
+  s->multi_grid[0] = (uint32_t)std::max(1, mi) * largest->sm_count;
+  s->multi_grid[1] = (uint32_t)std::max(1, mc) * largest->sm_count;
   const size_t units = (size_t)o.max_batch * pad32((uint32_t)largest->cells.size());
   for (Lane &lane : s->lanes) {
     int rc = ensure_scratch(largest, lane.scratch, o.max_batch, units);
@@ -306,7 +346,7 @@ int vgc_server_submit(vgc_server *s, uint32_t scene, const vgc_view *view, uint6
     r.result.ticket = t;
     r.result.scene = scene;
     r.result.submit_us = now_us();
-    s->scenes[scene].pending.push_back(t);
+    s->pending.push_back(t);
     s->stats.submitted++;
     *ticket = t;
   }

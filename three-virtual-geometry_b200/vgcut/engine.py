@@ -69,13 +69,14 @@ class TuneResult(C.Structure):
 
 class ServerOptions(C.Structure):
     _fields_ = [("streams", C.c_uint32), ("max_batch", C.c_uint32), ("slots_per_scene", C.c_uint32),
-                ("hbm_budget_bytes", C.c_uint64), ("linger_us", C.c_uint32), ("max_batch_instances", C.c_uint64)]
+                ("hbm_budget_bytes", C.c_uint64), ("linger_us", C.c_uint32), ("max_batch_instances", C.c_uint64),
+                ("cross_scene", C.c_uint32)]
 
 
 class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("batches", C.c_uint64),
                 ("views_launched", C.c_uint64), ("bytes_in_use", C.c_uint64), ("max_bytes_in_use", C.c_uint64),
-                ("max_in_flight", C.c_uint32)]
+                ("max_in_flight", C.c_uint32), ("multi_scene_batches", C.c_uint64)]
 
 
 VIS_EMPTY = 0x3F800000FFFFFFFF  # visibility-buffer pixel where nothing is drawn (VGC_VIS_EMPTY)
@@ -106,7 +107,7 @@ class Stats(C.Structure):
 class ServeResult(C.Structure):
     _fields_ = [("ticket", C.c_uint64), ("scene", C.c_uint32), ("slot", C.c_uint32), ("status", C.c_int32),
                 ("batch_views", C.c_uint32), ("submit_us", C.c_double), ("start_us", C.c_double),
-                ("done_us", C.c_double), ("batch_gpu_ms", C.c_float), ("stats", Stats)]
+                ("done_us", C.c_double), ("batch_gpu_ms", C.c_float), ("stats", Stats), ("batch_scenes", C.c_uint32)]
 
 
 _configured = False
@@ -574,16 +575,19 @@ class VirtualGeometry:
 
 class Server:
     """The serving loop over several resident scenes (vgc_server_* in include/vgcut.h): requests (scene index, view)
-    are submitted from any thread, admitted by free output slots and HBM budget, batched per scene and run on
-    `streams` CUDA streams with continuous batching. Results stay in the scene's output slot until released."""
+    are submitted from any thread, admitted by free output slots and HBM budget, batched oldest first (across scenes
+    with `cross_scene`) and run on `streams` CUDA streams with continuous batching. Results stay in the scene's
+    output slot until released."""
 
     def __init__(self, scenes: list, streams: int = 2, max_batch: int = 64, slots_per_scene: int = 0,
-                 hbm_budget_bytes: int = 0, linger_us: int = 0, max_batch_instances: int | None = None):
+                 hbm_budget_bytes: int = 0, linger_us: int = 0, max_batch_instances: int | None = None,
+                 cross_scene: bool = True):
         self.scenes = list(scenes)
         o = ServerOptions()
         lib().vgc_server_default_options(C.byref(o))
         o.streams, o.max_batch, o.slots_per_scene = streams, max_batch, slots_per_scene
         o.hbm_budget_bytes, o.linger_us = hbm_budget_bytes, linger_us
+        o.cross_scene = 1 if cross_scene else 0
         if max_batch_instances is not None:
             o.max_batch_instances = max_batch_instances
         arr = (C.c_void_p * len(self.scenes))(*[vg.handle for vg in self.scenes])
