@@ -48,13 +48,13 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bound of the CPU-baseline sample")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batching, occluder, large-world and serving sections")
-    ap.add_argument("--extras", default="batching,occluders,visibility,updates,large_world,serve",
+    ap.add_argument("--extras", default="serve_ruins,batching,occluders,visibility,updates,large_world,serve",
                     help="comma-separated sections to run after the headline line's measurement")
     ap.add_argument("--serve-rate", type=float, default=10_000.0, help="Poisson request rate of the serving section")
-    ap.add_argument("--serve-max-meshlets", type=int, default=1 << 17,
-                    help="draw-list capacity (meshlets per cut) of each serving scene's views")
-    ap.add_argument("--serve-max-triangles", type=int, default=10_000_000,
-                    help="triangle capacity (camera cut) of each serving scene's views")
+    ap.add_argument("--serve-max-meshlets", type=int, default=0,
+                    help="draw-list capacity (meshlets per cut) of every serving scene's views (0: by scene size)")
+    ap.add_argument("--serve-max-triangles", type=int, default=0,
+                    help="triangle capacity (camera cut) of every serving scene's views (0: by scene size)")
     ap.add_argument("--serve-requests", type=int, default=20_000)
     return ap.parse_args()
 
@@ -568,6 +568,14 @@ def run_ours(args, world, rank, local):
     vg.dispose()
     if world == 1 and args.config == "ruins" and not args.no_extras:
         extras = set(args.extras.split(","))
+        if "serve_ruins" in extras:
+            line["serve_ruins"] = run_serve_ruins(spec, args, plain_vps)
+            line["served_views_per_sec"] = line["serve_ruins"]["saturated"]["views_per_sec"]
+            line["served_over_plain"] = line["serve_ruins"]["served_over_plain"]
+            rates = line["serve_ruins"]["poisson"]
+            top = max(rates, key=float, default=None)  # p99 at the highest Poisson rate measured
+            line["served_p99_ms"] = rates[top]["p99_ms"] if top else None
+            line["served_p99_rate"] = float(top) if top else None
         if "batching" in extras:
             line["batching"] = run_batching(spec, args, flush, stream)
         if "occluders" in extras:
@@ -589,7 +597,7 @@ def run_ours(args, world, rank, local):
 
 
 TAIL_KEYS = ("cpu_baseline", "parity", "roofline", "e2e", "plain_views_per_sec", "batched_over_plain", "p50_ms",
-             "p99_ms", "clocks", "value", "ms_per_step")
+             "p99_ms", "served_views_per_sec", "served_over_plain", "served_p99_ms", "clocks", "value", "ms_per_step")
 
 
 def tail_order(line: dict) -> dict:
@@ -881,28 +889,16 @@ def run_large_world(ruins, args, flush, stream):
     return out
 
 
-def run_serve(ruins, args):
-    """The serving loop: 16 resident scenes of 10k-3M instances, a seeded Poisson request stream (pose, 720p / 1080p
-    / 4K, threshold U[0.5, 2], budget on a quarter), admission by output slots and HBM budget, 4 streams."""
-    from vgcut import engine, scenes
-    specs = scenes.serving_scenes(ruins.meshes, ruins.mesh_triangles, ruins.notes["weight_exponent"])
-    vgs = []
-    for sp in specs:
-        vg = engine.VirtualGeometry(max_triangles=args.serve_max_triangles, max_shadow_triangles=2_000_000,
-                                    max_meshlets=args.serve_max_meshlets, output_slots=1)
-        scenes.load_into(vg, sp)
-        vgs.append(vg)
-    import numpy as np
-    reqs = scenes.request_stream(specs, args.serve_requests, args.serve_rate)
-    views = [engine.make_view(cam, engine.ViewParams(error_threshold=t, triangle_budget=b, threshold_range=(0.5, 3.0)))
-             for _, _, cam, t, b in reqs]
-    budget = 4 << 30
-    server = engine.Server(vgs, streams=4, max_batch=64, slots_per_scene=64, hbm_budget_bytes=budget)
+class ServeDriver:
+    """Drives a server with a request list: submits (arrival s, request index) items - at their arrival times when
+    paced - from a submitter thread, waits for and releases each, and summarises latency (submit -> completion seen
+    by the server, host steady clock) and throughput."""
 
-    def run_stream(items, paced: bool):
-        """Submits (arrival s, index) items (paced: at their arrival times), waits and releases each; returns the
-        results and the server-stat deltas."""
-        base = server.stats()
+    def __init__(self, server, scene_of, views):
+        self.server, self.scene_of, self.views = server, scene_of, views
+
+    def run(self, items, paced: bool):
+        base = self.server.stats()
         tickets = [0] * len(items)
         results = [None] * len(items)
         ready = threading.Semaphore(0)
@@ -916,43 +912,122 @@ def run_serve(ruins, args):
                         break
                     if dt > 3e-4:
                         time.sleep(dt - 2e-4)
-                tickets[j] = server.submit(reqs[i][1], views[i])
+                tickets[j] = self.server.submit(self.scene_of[i], self.views[i])
                 ready.release()
 
         th = threading.Thread(target=submitter)
         th.start()
         for j in range(len(items)):
             ready.acquire()
-            results[j] = server.wait(tickets[j])
-            server.release(tickets[j])
+            results[j] = self.server.wait(tickets[j])
+            self.server.release(tickets[j])
         th.join()
-        st = server.stats()
-        return results, {k: st[k] - base[k] for k in ("batches", "views_launched")}, st
+        st = self.server.stats()
+        delta = {k: st[k] - base[k] for k in ("batches", "views_launched", "multi_scene_batches")}
+        return results, delta, st
 
+    @staticmethod
     def summary(results, delta):
         lat = sorted((r["done_us"] - r["submit_us"]) / 1e3 for r in results)
         span_s = (max(r["done_us"] for r in results) - min(r["submit_us"] for r in results)) / 1e6
         return dict(views_per_sec=len(results) / span_s, p50_ms=percentile(lat, 0.5), p99_ms=percentile(lat, 0.99),
                     p999_ms=percentile(lat, 0.999), mean_batch=delta["views_launched"] / max(1, delta["batches"]),
-                    batches=delta["batches"],
+                    batches=delta["batches"], multi_scene_batches=delta["multi_scene_batches"],
                     batch_gpu_ms_mean=statistics.mean(r["batch_gpu_ms"] for r in results),
                     rounds_mean=statistics.mean(r["stats"]["rounds"] for r in results),
                     overflow_share=statistics.mean(1.0 if r["stats"]["overflow"] else 0.0 for r in results))
 
+    def poisson(self, rate: float, n: int, n_requests: int, seed: int = 17):
+        import numpy as np
+        arrivals = np.cumsum(np.random.default_rng(seed).exponential(1.0 / rate, n))
+        res, delta, st = self.run([(float(arrivals[j]), j % n_requests) for j in range(n)], True)
+        out = self.summary(res, delta)
+        out.update(offered_per_sec=n / float(arrivals[-1]), requests=n)
+        return out, st
+
+
+def run_serve_ruins(ruins, args, plain_vps: float):
+    """Serving on the ruins-like scene (113,106 instances) at 1920 x 1080: requests (spline pose with its prebuilt
+    HZB, threshold U[0.5, 2] px), continuous batching on 4 streams; a saturated burst and Poisson arrivals at
+    2k-20k requests/s, beside the plain per-view launch."""
+    import numpy as np
+    from vgcut import engine, scenes
+    P = len(ruins.cameras)
+    vg = engine.VirtualGeometry(max_triangles=10_000_000, max_shadow_triangles=4_000_000, max_meshlets=1 << 18,
+                                output_slots=1)
+    scenes.load_into(vg, ruins, occlusion_culling=True)
+    for k in range(P):
+        vg.build_hzb(k, ruins.depth_images[k])
+    rng = np.random.default_rng(23)
+    n_req = 4096
+    poses = rng.integers(P, size=n_req)
+    thresholds = rng.uniform(0.5, 2.0, n_req)
+    views = [engine.make_view(ruins.cameras[int(k)], engine.ViewParams(error_threshold=float(t), hzb=int(k)))
+             for k, t in zip(poses, thresholds)]
+    server = engine.Server([vg], streams=4, max_batch=64, slots_per_scene=512)
+    drv = ServeDriver(server, [0] * n_req, views)
+    rates = {}
     try:
-        run_stream([(0.0, i) for i in range(256)], False)  # warm-up
+        drv.run([(0.0, i) for i in range(512)], False)  # warm-up
+        res, delta, _ = drv.run([(0.0, i) for i in range(n_req)], False)
+        saturated = drv.summary(res, delta)
+        for rate in (2_000.0, 5_000.0, 10_000.0, 20_000.0):
+            if rate > 0.9 * saturated["views_per_sec"]:
+                continue
+            rates[f"{int(rate)}"], _ = drv.poisson(rate, int(min(20_000, rate * 1.0)), n_req)
+    finally:
+        server.close()
+        vg.dispose()
+    return dict(workload=f"serving, ruins-like scene: {ruins.instance_count} instances, 1920x1080 requests (one of "
+                         f"{P} spline poses with its prebuilt HZB, threshold U[0.5, 2] px), 4 streams, batches <= 64",
+                saturated=dict(saturated, requests=n_req, note="burst submitted at once: the server's capacity"),
+                poisson=rates, plain_views_per_sec=plain_vps,
+                served_over_plain=saturated["views_per_sec"] / plain_vps if plain_vps else None,
+                latency_note="submit -> completion seen by the server (host steady clock); Poisson arrivals, about "
+                             "1 s of requests per rate")
+
+
+def serve_capacity(instances: int) -> tuple:
+    """Output capacity of a serving scene's views, by its size: draw-list meshlets and camera-cut triangles grow with
+    the instances a 4K view can see, so that a fresh request's cut fits after its capacity rounds."""
+    meshlets = 1 << max(17, min(20, (max(1, instances) - 1).bit_length()))
+    triangles = int(min(48_000_000, max(10_000_000, 16 * instances)))
+    return meshlets, triangles
+
+
+def run_serve(ruins, args):
+    """The serving loop: 16 resident scenes of 10k-3M instances, a seeded Poisson request stream (pose, 720p / 1080p
+    / 4K, threshold U[0.5, 2], budget on a quarter), admission by output slots and HBM budget, 4 streams, batches
+    across scenes."""
+    from vgcut import engine, scenes
+    specs = scenes.serving_scenes(ruins.meshes, ruins.mesh_triangles, ruins.notes["weight_exponent"])
+    vgs, caps = [], []
+    for sp in specs:
+        meshlets, triangles = serve_capacity(sp.instance_count)
+        if args.serve_max_meshlets:
+            meshlets = args.serve_max_meshlets
+        if args.serve_max_triangles:
+            triangles = args.serve_max_triangles
+        vg = engine.VirtualGeometry(max_triangles=triangles, max_shadow_triangles=2_000_000, max_meshlets=meshlets,
+                                    output_slots=1)
+        scenes.load_into(vg, sp)
+        vgs.append(vg)
+        caps.append((sp.instance_count, meshlets, triangles))
+    reqs = scenes.request_stream(specs, args.serve_requests, args.serve_rate)
+    views = [engine.make_view(cam, engine.ViewParams(error_threshold=t, triangle_budget=b, threshold_range=(0.5, 3.0)))
+             for _, _, cam, t, b in reqs]
+    budget = 16 << 30
+    server = engine.Server(vgs, streams=4, max_batch=64, slots_per_scene=64, hbm_budget_bytes=budget)
+    drv = ServeDriver(server, [r[1] for r in reqs], views)
+    try:
+        drv.run([(0.0, i) for i in range(256)], False)  # warm-up
         # capacity: the whole burst submitted at once
         n_sat = min(len(reqs), 4096)
-        res, delta, _ = run_stream([(0.0, i) for i in range(n_sat)], False)
-        saturated = summary(res, delta)
+        res, delta, _ = drv.run([(0.0, i) for i in range(n_sat)], False)
+        saturated = drv.summary(res, delta)
         # latency under a Poisson stream at 70% of that capacity (or the requested rate, if lower)
         rate = min(args.serve_rate, 0.7 * saturated["views_per_sec"])
-        n = min(len(reqs), max(1000, int(rate * 4.0)))
-        gaps = np.random.default_rng(17).exponential(1.0 / rate, n)
-        arrivals = np.cumsum(gaps)
-        res, delta, st = run_stream([(float(arrivals[j]), j % len(reqs)) for j in range(n)], True)
-        paced = summary(res, delta)
-        paced.update(offered_per_sec=n / float(arrivals[-1]), requests=n)
+        paced, st = drv.poisson(rate, min(len(reqs), max(1000, int(rate * 4.0))), len(reqs))
     finally:
         server.close()
         for vg in vgs:
@@ -965,8 +1040,8 @@ def run_serve(ruins, args):
                 poisson=dict(paced, note="Poisson arrivals at min(requested rate, 70% of capacity)"),
                 max_in_flight=st["max_in_flight"], hbm_budget_bytes=budget, max_bytes_in_use=st["max_bytes_in_use"],
                 latency_note="submit -> completion seen by the server, host steady clock",
-                config=dict(streams=4, max_batch=64, slots_per_scene=64, max_meshlets=args.serve_max_meshlets,
-                            max_triangles=args.serve_max_triangles))
+                config=dict(streams=4, max_batch=64, slots_per_scene=64, cross_scene=True,
+                            capacity_by_scene=[dict(instances=i, max_meshlets=m, max_triangles=t) for i, m, t in caps]))
 
 
 def main():
