@@ -239,16 +239,21 @@ int vgc_batch_run(vgc_batch *batch, const vgc_view *views, uint32_t count, uint3
 int vgc_batch_destroy(vgc_batch *batch);
 
 /* Autotuner (no counterpart in the reference): times the batch's launch sequence for `views` (reps replays each,
-   median) under every pair of persistent grid sizes for the instance and meshlet kernels (blocks per SM: quarters
-   of each kernel's occupancy limit) and keeps the fastest for the batch's later runs. Results are the same under
-   every candidate: the grids only decide which warp takes which unit of work. Runs the views' cut (outputs are
-   left as a normal run leaves them). */
+   median) under every combination of the meshlet kernel's work-unit size (chunks of 256, 512 or 1024 meshlets) and
+   the persistent grid sizes of the instance and meshlet kernels (blocks per SM: quarters of each kernel's occupancy
+   limit), and keeps the fastest for the batch's later runs. Results are the same under every candidate: these only
+   decide how the work is cut up and which warp takes which piece. Runs the views' cut (outputs are left as a normal
+   run leaves them). */
 typedef struct {
   uint32_t instances_blocks_per_sm, chunks_blocks_per_sm;
   float ms; /* median device time of one run */
+  uint32_t chunk_meshlets; /* meshlets per k_chunks work unit */
 } vgc_tune_result;
 int vgc_batch_autotune(vgc_batch *batch, const vgc_view *views, uint32_t count, uint32_t first_slot, vgc_stream stream,
                        uint32_t reps, vgc_tune_result *best);
+/* Applies a tuning (for instance one vgc_batch_autotune returned earlier, kept by the caller) to the batch's later
+   runs: blocks per SM of the two kernels (0: the occupancy default) and meshlets per chunk (256, 512 or 1024). */
+int vgc_batch_set_tuning(vgc_batch *batch, const vgc_tune_result *tuning);
 
 /* ---------------------------------------------------------------- serving (no counterpart in the reference) */
 /* A request loop over several resident scenes (one context each). The reference cuts once per rendered frame of

@@ -76,3 +76,27 @@ def test_uneven_batch_equals_alone_and_autotune_keeps_results(ruins):
             for c in (0, 1):  # a draw list that overflowed keeps an atomic-order-dependent subset
                 if got[2][c] <= h.max_meshlets:
                     assert got[c] == alone[k][c], f"view {k} cut {c} differs in the batch (tuned={tuned})"
+
+
+@pytest.mark.parametrize("chunk", [256, 512, 1024])
+def test_every_chunk_size_gives_the_same_cuts(ruins, chunk):
+    """The autotuner's candidates only cut the meshlet work into different windows (chunks of 256, 512 or 1024
+    meshlets) and spread it over different grids: each must give every view's cut exactly."""
+    h = ruins
+    vs = view_set(h)
+    views = [engine.make_view(cam, engine.ViewParams(**{**p.__dict__, "state_slot": k, "fresh_state": True}))
+             for k, (cam, p) in enumerate(vs)]
+    h.vg.set_tuning(len(views), 0, 0, 512)
+    h.vg.cut(views, first_slot=0, graph=True)
+    want = [([key_set(h.vg.draw_list(k, c), (0, 1, 3)) for c in (0, 1)], h.vg.read_stats(k)) for k in range(len(vs))]
+    h.vg.set_tuning(len(views), 1, 2, chunk)
+    h.vg.cut(views, first_slot=0, graph=True)
+    for k in range(len(vs)):
+        s = h.vg.read_stats(k)
+        assert s["selected"] == want[k][1]["selected"] and s["work"] == want[k][1]["work"]
+        assert s["requested_indices"] == want[k][1]["requested_indices"]
+        for c in (0, 1):
+            if s["selected"][c] <= h.max_meshlets:
+                assert key_set(h.vg.draw_list(k, c), (0, 1, 3)) == want[k][0][c], f"view {k} cut {c}, chunk {chunk}"
+    with pytest.raises(engine.VgcError, match="chunk_meshlets"):
+        h.vg.set_tuning(len(views), 0, 0, 300)

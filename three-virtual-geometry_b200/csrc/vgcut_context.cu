@@ -588,7 +588,7 @@ int enqueue(vgc_context *ctx, LaunchScratch &s, uint32_t count, cudaStream_t st,
   if (s.any_budget) {  // the triangleBudget search: histogram pass, then the threshold of each budget view
     CUDA_TRY(timed(ctx, capture, VGC_KERNEL_BUDGET, st, [&] {
       cudaError_t e = launch_instances(S, scenes, s.d_views, s.d_units, s.d_unit_count, s.d_chunks, s.chunk_capacity, -1,
-                                       select_grid, st);
+                                       select_grid, st, s.chunk_shift);
       if (e == cudaSuccess)
         e = launch_chunks(S, scenes, s.d_views, s.d_chunks, s.d_unit_count, s.chunk_capacity, -1, chunk_grid, st);
       if (e == cudaSuccess) e = launch_budget(s.d_views, count, s.d_unit_count, st);
@@ -598,7 +598,7 @@ int enqueue(vgc_context *ctx, LaunchScratch &s, uint32_t count, cudaStream_t st,
   for (int round = 0; round < 3; round++) {
     CUDA_TRY(timed(ctx, capture, round == 0 ? VGC_KERNEL_SELECT0 : VGC_KERNEL_SELECT_RETRY, st, [&] {
       return launch_instances(S, scenes, s.d_views, s.d_units, s.d_unit_count, s.d_chunks, s.chunk_capacity, round,
-                              select_grid, st);
+                              select_grid, st, s.chunk_shift);
     }));
     CUDA_TRY(timed(ctx, capture, round == 0 ? VGC_KERNEL_CHUNKS0 : VGC_KERNEL_SELECT_RETRY, st, [&] {
       return launch_chunks(S, scenes, s.d_views, s.d_chunks, s.d_unit_count, s.chunk_capacity, round, chunk_grid, st);
@@ -1120,7 +1120,8 @@ int vgc_batch_run(vgc_batch *b, const vgc_view *views, uint32_t count, uint32_t 
   if (!b->exec || b->graph_views != count || b->graph_cells != cells || b->graph_slots != ctx->slot_capacity ||
       b->graph_hzb_w != b->scratch.hzb_w || b->graph_hzb_h != b->scratch.hzb_h || b->graph_hzb_tail != b->scratch.hzb_tail ||
       b->graph_budget != b->scratch.any_budget || b->graph_queue != b->scratch.d_chunks ||
-      b->graph_grids[0] != b->scratch.grid_instances || b->graph_grids[1] != b->scratch.grid_chunks) {
+      b->graph_grids[0] != b->scratch.grid_instances || b->graph_grids[1] != b->scratch.grid_chunks ||
+      b->graph_chunk_shift != b->scratch.chunk_shift) {
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     b->exec = nullptr;
@@ -1146,6 +1147,7 @@ int vgc_batch_run(vgc_batch *b, const vgc_view *views, uint32_t count, uint32_t 
     b->graph_queue = b->scratch.d_chunks;
     b->graph_grids[0] = b->scratch.grid_instances;
     b->graph_grids[1] = b->scratch.grid_chunks;
+    b->graph_chunk_shift = b->scratch.chunk_shift;
   }
   CUDA_TRY(cudaGraphLaunch(b->exec, st));
   CUDA_TRY(cudaEventRecord(b->scratch.done, st));
@@ -1174,12 +1176,14 @@ int vgc_batch_autotune(vgc_batch *b, const vgc_view *views, uint32_t count, uint
   CUDA_TRY(cudaEventCreate(&e0));
   CUDA_TRY(cudaEventCreate(&e1));
   reps = std::max(1u, reps);
-  vgc_tune_result top{0, 0, INFINITY};
+  vgc_tune_result top{0, 0, INFINITY, 0};
   int rc = VGC_OK;
+  for (uint32_t shift = kChunkShiftMin; shift <= kChunkShiftMax && !rc; shift++)
   for (uint32_t bi : steps(max_i)) {
     for (uint32_t bc : steps(max_c)) {
       b->scratch.grid_instances = bi * sms;
       b->scratch.grid_chunks = bc * sms;
+      b->scratch.chunk_shift = shift;
       if ((rc = vgc_batch_run(b, views, count, first_slot, stream))) break;  // capture + warm-up
       std::vector<float> ms;
       for (uint32_t r = 0; r < reps; r++) {  // replays of the captured graph: device time only
@@ -1197,7 +1201,7 @@ int vgc_batch_autotune(vgc_batch *b, const vgc_view *views, uint32_t count, uint
       if (rc) break;
       std::sort(ms.begin(), ms.end());
       const float med = ms[ms.size() / 2];
-      if (med < top.ms) top = vgc_tune_result{bi, bc, med};
+      if (med < top.ms) top = vgc_tune_result{bi, bc, med, 1u << shift};
     }
     if (rc) break;
   }
@@ -1206,7 +1210,22 @@ int vgc_batch_autotune(vgc_batch *b, const vgc_view *views, uint32_t count, uint
   if (rc) return rc;
   b->scratch.grid_instances = top.instances_blocks_per_sm * sms;
   b->scratch.grid_chunks = top.chunks_blocks_per_sm * sms;
+  b->scratch.chunk_shift = (uint32_t)__builtin_ctz(top.chunk_meshlets);
   *best = top;
+  return VGC_OK;
+}
+
+int vgc_batch_set_tuning(vgc_batch *b, const vgc_tune_result *t) {
+  if (!b || !t) return fail(VGC_INVALID_ARG, "null argument");
+  const uint32_t c = t->chunk_meshlets;
+  if (c != 256 && c != 512 && c != 1024) return fail(VGC_INVALID_ARG, "chunk_meshlets must be 256, 512 or 1024");
+  const uint32_t sms = (uint32_t)b->ctx->sm_count;
+  const uint32_t max_i = std::max(1u, b->ctx->select_grid / sms), max_c = std::max(1u, b->ctx->chunk_grid / sms);
+  if (t->instances_blocks_per_sm > max_i || t->chunks_blocks_per_sm > max_c)
+    return fail(VGC_INVALID_ARG, "blocks per SM above the kernels' occupancy limit");
+  b->scratch.grid_instances = t->instances_blocks_per_sm * sms;
+  b->scratch.grid_chunks = t->chunks_blocks_per_sm * sms;
+  b->scratch.chunk_shift = (uint32_t)__builtin_ctz(c);
   return VGC_OK;
 }
 

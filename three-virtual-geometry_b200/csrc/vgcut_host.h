@@ -68,6 +68,7 @@ struct LaunchScratch {
   uint32_t *h_ctl = nullptr;      // pinned copy of the control words at the end of the last launch sequence
   uint32_t grid_instances = 0;    // persistent grids of k_instances / k_chunks (0: the context's occupancy defaults)
   uint32_t grid_chunks = 0;
+  uint32_t chunk_shift = kChunkShiftDefault;  // 2^chunk_shift meshlets per k_chunks work unit
   uint32_t view_capacity = 0;
   size_t unit_capacity = 0;
   size_t units_total = 0;         // (view, cell) units of the prepared launch (each view: its scene's cells, padded)
@@ -145,6 +146,7 @@ struct vgc_batch {
   bool graph_budget = false;
   const uint4 *graph_queue = nullptr;  // work queue the graph was captured with
   uint32_t graph_grids[2] = {0, 0};    // persistent grids the graph was captured with
+  uint32_t graph_chunk_shift = 0;      // chunk size it was captured with
 };
 
 namespace vgch {

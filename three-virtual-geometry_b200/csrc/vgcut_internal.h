@@ -34,6 +34,7 @@ constexpr uint32_t kLocalVertexBits = 7;   // ceil(log2(MAX_MESHLET_VERTICES = 1
 constexpr uint32_t kMaxHzbLevels = 16;
 constexpr uint32_t kStateWords = 8;        // S_SCALE 0..1, S_FILL 2..3, S_RETRY 4..5
 constexpr uint32_t kBudgetBins = 256;
+constexpr uint32_t kChunkShiftMin = 8, kChunkShiftDefault = 9, kChunkShiftMax = 10;  // meshlets per chunk: 256..1024
 constexpr uint32_t kLevelSamples = 64;     // per level: samples of the meshlets in test order (item trimming)
 
 struct MeshRec {  // 96 bytes

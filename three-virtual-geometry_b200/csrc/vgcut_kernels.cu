@@ -251,11 +251,9 @@ __global__ void __launch_bounds__(256) k_cells(Scene S0, const Scene *__restrict
 
 // ------------------------------------------------------------------------------------------------ k_instances
 constexpr int kWarpStage = 96;   // staged draw entries per warp (a step adds <= 32; one cut at a time)
-constexpr uint32_t kChunk = 512;  // meshlets per chunk (one warp in k_chunks)
-
 // The meshlet work queue between k_instances and k_chunks, in one buffer of `capacity` uint4: spans (one item's
-// meshlets inside one kChunk window of its warp's items laid end to end) and chunks (the <= 32 spans of one
-// window: one (view, cell, cut)). ctl[4..5] is the 64-bit reservation counter: spans low, chunks high.
+// meshlets inside one window of 2^chunk_shift meshlets of its warp's items laid end to end; 512 unless the batch's
+// autotuner picked 256 or 1024) and chunks (the <= 32 spans of one window: one (view, cell, cut)). ctl[4..5] is the 64-bit reservation counter: spans low, chunks high.
 struct WorkQueue {
   uint4 *spans, *chunks;
   uint32_t span_cap, chunk_cap;
@@ -682,7 +680,8 @@ __device__ __forceinline__ void drain_queue(const Scene &S, const ViewConst &V, 
 }
 
 // One warp per 32 instances of a visible (view, cell) unit: the instance pass of GeometryPool.ts:846-913. Fast-path
-// instances emit their meshlets; the others hand their level range to k_chunks as chunks of <= kChunk meshlets.
+// instances emit their meshlets; the others hand their level range to k_chunks as chunks of <= 2^chunk_shift
+// meshlets.
 // HIST: the budget search's pass (views with a triangleBudget only): the camera cut's level range over the whole
 // threshold range, no fast path, no counters.
 template <bool HIST, bool MULTI>
@@ -690,7 +689,7 @@ __global__ void __launch_bounds__(128, MULTI ? 5 : 6) k_instances(Scene S0, cons
                                                    const ViewConst *__restrict__ views,
                                                    const HzbDesc *__restrict__ hzbs0, const uint2 *__restrict__ units,
                                                    uint32_t *__restrict__ ctl, uint4 *__restrict__ queue,
-                                                   uint32_t capacity, int round) {
+                                                   uint32_t capacity, int round, uint32_t chunk_shift) {
   __shared__ WarpStage stage[4];
   WarpStage &ws = stage[threadIdx.x >> 5];
   if (round > 0 && ctl[round] == 0) return;  // no view redoes a cut in this round
@@ -801,17 +800,19 @@ __global__ void __launch_bounds__(128, MULTI ? 5 : 6) k_instances(Scene S0, cons
     emit_fast(S, V, cell.slot, 0, fast0 ? r0.possible : 0u, r0.first, instance);
     emit_fast(S, V, cell.slot, 1, fast1 ? r1.possible : 0u, r1.first, instance);
     }
-    // items -> spans -> chunks: per cut, the warp's items laid end to end in lane order and cut into kChunk windows;
+    // items -> spans -> chunks: per cut, the warp's items laid end to end in lane order and cut into windows of
+    // 2^chunk_shift meshlets;
     // a window's spans (<= 32, one per item) form one chunk of one (view, cell, cut)
     const uint32_t n0 = item0 ? t0l - t0f : 0u, n1 = item1 ? t1l - t1f : 0u;
     const uint32_t s0 = warp_scan_incl(n0) - n0, s1 = warp_scan_incl(n1) - n1;  // starts in the laid-out items
     const uint32_t T0 = __shfl_sync(0xffffffffu, s0 + n0, 31), T1 = __shfl_sync(0xffffffffu, s1 + n1, 31);
     if (T0 + T1 == 0) continue;
-    const uint32_t p0 = n0 ? (s0 + n0 - 1) / kChunk - s0 / kChunk + 1 : 0u;  // spans of this lane's item
-    const uint32_t p1 = n1 ? (s1 + n1 - 1) / kChunk - s1 / kChunk + 1 : 0u;
+    const uint32_t chunk = 1u << chunk_shift;
+    const uint32_t p0 = n0 ? ((s0 + n0 - 1) >> chunk_shift) - (s0 >> chunk_shift) + 1 : 0u;  // spans of this lane's item
+    const uint32_t p1 = n1 ? ((s1 + n1 - 1) >> chunk_shift) - (s1 >> chunk_shift) + 1 : 0u;
     const uint32_t q0 = warp_scan_incl(p0) - p0, q1 = warp_scan_incl(p1) - p1;
     const uint32_t P0 = __shfl_sync(0xffffffffu, q0 + p0, 31), P1 = __shfl_sync(0xffffffffu, q1 + p1, 31);
-    const uint32_t N0 = (T0 + kChunk - 1) / kChunk, N1 = (T1 + kChunk - 1) / kChunk;
+    const uint32_t N0 = (T0 + chunk - 1) >> chunk_shift, N1 = (T1 + chunk - 1) >> chunk_shift;
     unsigned long long got = 0;
     if (lane == 0)
       got = atomicAdd(queue_counter(ctl), ((unsigned long long)(N0 + N1) << 32) | (unsigned long long)(P0 + P1));
@@ -826,19 +827,19 @@ __global__ void __launch_bounds__(128, MULTI ? 5 : 6) k_instances(Scene S0, cons
         const uint32_t flags = il | ((cut ? inside1 : inside0) ? 1u << 7 : 0u);
         uint4 *dst = Q.spans + span_at + (cut ? P0 + q1 : q0);
         for (uint32_t k = 0; k < np; k++) {
-          const uint32_t win = st / kChunk + k;
-          const uint32_t lo = max(st, win * kChunk), hi = min(st + n, (win + 1) * kChunk);
+          const uint32_t win = (st >> chunk_shift) + k;
+          const uint32_t lo = max(st, win << chunk_shift), hi = min(st + n, (win + 1) << chunk_shift);
           dst[k] = make_uint4(flags, first + (lo - st), hi - lo, 0u);
         }
-        // chunk t starts at the span holding laid-out position t * kChunk: that of the last item starting at or
+        // chunk t starts at the span holding laid-out position t * chunk: that of the last item starting at or
         // before it, plus the windows that item crossed before t
         const uint32_t N = cut ? N1 : N0;
         for (uint32_t t = 0; t < N; t++) {
-          const uint32_t X = t * kChunk;
+          const uint32_t X = t << chunk_shift;
           const uint32_t owner = 31 - __clz(__ballot_sync(0xffffffffu, st <= X));
           const uint32_t first_span = __shfl_sync(0xffffffffu, cut ? q1 : q0, owner) + t -
-                                      __shfl_sync(0xffffffffu, st, owner) / kChunk;
-          const uint32_t spans = __popc(__ballot_sync(0xffffffffu, n > 0 && st < X + kChunk && st + n > X));
+                                      (__shfl_sync(0xffffffffu, st, owner) >> chunk_shift);
+          const uint32_t spans = __popc(__ballot_sync(0xffffffffu, n > 0 && st < X + chunk && st + n > X));
           if (lane == 0)
             Q.chunks[chunk_at + (cut ? N0 : 0u) + t] =
                 make_uint4(unit.x, unit.y, cut | ((cut == 0 && occl_on) ? 2u : 0u) | (spans << 8),
@@ -1491,20 +1492,24 @@ cudaError_t configure_select(bool multi, int *instances_per_sm, int *chunks_per_
 
 template <bool MULTI>
 static void instances_kernel(const Scene &S, const Scene *scenes, const ViewConst *views, const uint2 *units,
-                             uint32_t *ctl, uint4 *queue, uint32_t capacity, int round, uint32_t grid, cudaStream_t st) {
+                             uint32_t *ctl, uint4 *queue, uint32_t capacity, int round, uint32_t grid,
+                             uint32_t chunk_shift, cudaStream_t st) {
   if (round < 0)  // the budget search's pass
-    k_instances<true, MULTI><<<grid, 128, 0, st>>>(S, scenes, views, S.hzbs, units, ctl, queue, capacity, 0);
+    k_instances<true, MULTI><<<grid, 128, 0, st>>>(S, scenes, views, S.hzbs, units, ctl, queue, capacity, 0,
+                                                   chunk_shift);
   else
-    k_instances<false, MULTI><<<grid, 128, 0, st>>>(S, scenes, views, S.hzbs, units, ctl, queue, capacity, round);
+    k_instances<false, MULTI><<<grid, 128, 0, st>>>(S, scenes, views, S.hzbs, units, ctl, queue, capacity, round,
+                                                    chunk_shift);
 }
 
 cudaError_t launch_instances(const Scene &S, const Scene *scenes, const ViewConst *views, const uint2 *units,
                              uint32_t *ctl, uint4 *queue, uint32_t capacity, int round, uint32_t grid,
-                             cudaStream_t st) {
+                             cudaStream_t st, uint32_t chunk_shift) {
+  if (chunk_shift < kChunkShiftMin || chunk_shift > kChunkShiftMax) return cudaErrorInvalidValue;
   if (scenes)
-    instances_kernel<true>(S, scenes, views, units, ctl, queue, capacity, round, grid, st);
+    instances_kernel<true>(S, scenes, views, units, ctl, queue, capacity, round, grid, chunk_shift, st);
   else
-    instances_kernel<false>(S, nullptr, views, units, ctl, queue, capacity, round, grid, st);
+    instances_kernel<false>(S, nullptr, views, units, ctl, queue, capacity, round, grid, chunk_shift, st);
   return cudaGetLastError();
 }
 

@@ -64,7 +64,8 @@ class View(C.Structure):
 
 
 class TuneResult(C.Structure):
-    _fields_ = [("instances_blocks_per_sm", C.c_uint32), ("chunks_blocks_per_sm", C.c_uint32), ("ms", C.c_float)]
+    _fields_ = [("instances_blocks_per_sm", C.c_uint32), ("chunks_blocks_per_sm", C.c_uint32), ("ms", C.c_float),
+                ("chunk_meshlets", C.c_uint32)]
 
 
 class ServerOptions(C.Structure):
@@ -139,6 +140,7 @@ def lib() -> C.CDLL:
         "vgc_batch_run": ([vp, P(View), C.c_uint32, C.c_uint32, vp], C.c_int),
         "vgc_batch_destroy": ([vp], C.c_int),
         "vgc_batch_autotune": ([vp, P(View), C.c_uint32, C.c_uint32, vp, C.c_uint32, P(TuneResult)], C.c_int),
+        "vgc_batch_set_tuning": ([vp, P(TuneResult)], C.c_int),
         "vgc_get_output": ([vp, C.c_uint32, P(Output)], C.c_int),
         "vgc_read_stats": ([vp, C.c_uint32, P(Stats), vp], C.c_int),
         "vgc_read_draw_list": ([vp, C.c_uint32, C.c_uint32, P(C.c_uint32), C.c_uint32, P(C.c_uint32), vp], C.c_int),
@@ -458,6 +460,18 @@ class VirtualGeometry:
         r = TuneResult()
         check(lib().vgc_batch_autotune(b, arr, len(views), first_slot, stream, reps, C.byref(r)))
         return {k: getattr(r, k) for k, _ in TuneResult._fields_}
+
+    def set_tuning(self, count: int, instances_blocks_per_sm: int = 0, chunks_blocks_per_sm: int = 0,
+                   chunk_meshlets: int = 512) -> None:
+        """Applies a tuning to the batched launch of `count` views (vgc_batch_set_tuning): blocks per SM of the
+        instance and meshlet kernels (0: occupancy default) and meshlets per chunk (256, 512 or 1024)."""
+        b = self._batches.get(count)
+        if b is None:
+            b = C.c_void_p()
+            check(lib().vgc_batch_create(self.handle, count, C.byref(b)))
+            self._batches[count] = b
+        t = TuneResult(instances_blocks_per_sm, chunks_blocks_per_sm, 0.0, chunk_meshlets)
+        check(lib().vgc_batch_set_tuning(b, C.byref(t)))
 
     def cut_noalloc(self, view: View, slot: int = 0, stream=None) -> None:
         """The single-view cut that allocates nothing on the call (see vgc_cut_noalloc in include/vgcut.h)."""
