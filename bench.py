@@ -617,7 +617,9 @@ def run_batching(ruins, args, flush, stream):
     with 4 orthographic shadow cascades: 320 views in one CUDA-graph launch, grid sizes picked by the autotuner."""
     import torch
     from vgcut import engine, scenes
-    vg = engine.VirtualGeometry(max_triangles=20_000_000, max_shadow_triangles=8_000_000, max_meshlets=1 << 17,
+    # draw lists of 2^19 entries: at 2^17, 141 of the 320 views overflowed in a round (4K views at 0.5 px select
+    # up to 1.9M meshlets), and their retried rounds coarsened the cuts
+    vg = engine.VirtualGeometry(max_triangles=40_000_000, max_shadow_triangles=16_000_000, max_meshlets=1 << 19,
                                 output_slots=320)
     for data, mats in zip(ruins.meshes, ruins.instances):
         vg.create_mesh(data, mats, cast_shadow=True)
@@ -645,6 +647,8 @@ def run_batching(ruins, args, flush, stream):
     tuned = vg.autotune(views, stream=sp, reps=3)
     tuned_ms = timed_steps()
     st = [vg.read_stats(k) for k in range(len(views))]
+    overflow_share = statistics.mean(1.0 if s["overflow"] else 0.0 for s in st)
+    rounds_mean = statistics.mean(s["rounds"] for s in st)
     cam_tris = statistics.mean(s["requested_indices"][0] / 3 for k, s in enumerate(st) if k % 5 == 0)
     casc_tris = statistics.mean(s["requested_indices"][1] / 3 for k, s in enumerate(st) if k % 5 != 0)
     vg.dispose()
@@ -657,6 +661,8 @@ def run_batching(ruins, args, flush, stream):
                 camera_views_per_sec=64 / (tuned_ms / 1e3), cascade_views_per_sec=256 / (tuned_ms / 1e3),
                 untuned_ms_per_step=default_ms, autotune=tuned,
                 camera_cut_triangles_mean=cam_tris, cascade_cut_triangles_mean=casc_tris,
+                overflow_share=overflow_share, rounds_mean=rounds_mean,
+                capacity=dict(max_meshlets=1 << 19, max_triangles=40_000_000, max_shadow_triangles=16_000_000),
                 note="cascades: no occlusion (the reference never occlusion-culls shadow cuts)")
 
 
@@ -953,7 +959,10 @@ def run_serve_ruins(ruins, args, plain_vps: float):
     import numpy as np
     from vgcut import engine, scenes
     P = len(ruins.cameras)
-    vg = engine.VirtualGeometry(max_triangles=10_000_000, max_shadow_triangles=4_000_000, max_meshlets=1 << 18,
+    # output capacity for the finest request: at 0.5 px a 1080p view of this scene selects up to 334k meshlets and
+    # 33.8M triangles (oracle, all poses), so a fresh request's cut fits in its first round
+    cap_meshlets, cap_triangles = 1 << 19, 40_000_000
+    vg = engine.VirtualGeometry(max_triangles=cap_triangles, max_shadow_triangles=4_000_000, max_meshlets=cap_meshlets,
                                 output_slots=1)
     scenes.load_into(vg, ruins, occlusion_culling=True)
     for k in range(P):
@@ -964,7 +973,7 @@ def run_serve_ruins(ruins, args, plain_vps: float):
     thresholds = rng.uniform(0.5, 2.0, n_req)
     views = [engine.make_view(ruins.cameras[int(k)], engine.ViewParams(error_threshold=float(t), hzb=int(k)))
              for k, t in zip(poses, thresholds)]
-    server = engine.Server([vg], streams=4, max_batch=64, slots_per_scene=512)
+    server = engine.Server([vg], streams=4, max_batch=64, slots_per_scene=256)
     drv = ServeDriver(server, [0] * n_req, views)
     rates = {}
     try:
@@ -983,6 +992,7 @@ def run_serve_ruins(ruins, args, plain_vps: float):
                 saturated=dict(saturated, requests=n_req, note="burst submitted at once: the server's capacity"),
                 poisson=rates, plain_views_per_sec=plain_vps,
                 served_over_plain=saturated["views_per_sec"] / plain_vps if plain_vps else None,
+                capacity=dict(max_meshlets=cap_meshlets, max_triangles=cap_triangles, slots=256),
                 latency_note="submit -> completion seen by the server (host steady clock); Poisson arrivals, about "
                              "1 s of requests per rate")
 

@@ -221,7 +221,7 @@ class _View(C.Structure):
 class _Result(C.Structure):
     _fields_ = [("entry_capacity", C.c_uint32), ("entries", C.POINTER(C.c_uint32) * 2), ("entry_count", C.c_uint32 * 2),
                 ("counters", C.c_uint32 * 12), ("mesh_counts", C.POINTER(C.c_uint32)),
-                ("draw_args", C.POINTER(C.c_uint32)), ("rounds", C.c_uint32)]
+                ("draw_args", C.POINTER(C.c_uint32)), ("rounds", C.c_uint32), ("max_selected", C.c_uint32 * 2)]
 
 
 class OracleScene:
@@ -379,7 +379,7 @@ def cull_pass(scene: OracleScene, view: _View, precision: str = "f32", threads: 
     return dict(entries=[e0[:r.entry_count[0]].copy(), e1[:r.entry_count[1]].copy()], counters=list(r.counters),
                 mesh_counts=mc.reshape(2, scene.mesh_count, 2), draw_args=args.reshape(2, scene.mesh_count, 2, 5),
                 rounds=r.rounds, state=list(view.state), threshold=view.chosen_threshold,
-                predicted=view.predicted_triangles)
+                predicted=view.predicted_triangles, max_selected=list(r.max_selected))
 
 
 def explain(scene: OracleScene, view: _View, cut: int, instance: int, meshlet: int) -> float:

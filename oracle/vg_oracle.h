@@ -132,6 +132,9 @@ typedef struct vgo_result {
   uint32_t *mesh_counts;      /* 2 cuts x mesh_count x 2 parts: requested indices */
   uint32_t *draw_args;        /* 2 cuts x mesh_count x 2 parts x 5 u32 */
   uint32_t rounds;            /* selection rounds run (1 + retries) */
+  uint32_t max_selected[2];   /* per cut, the most meshlets any round selected: above max_drawn, that round kept an
+                                 atomic-order-dependent subset on a GPU, and the capacity controller's next scale
+                                 (from the kept entries' index count) depends on it */
 } vgo_result;
 
 /* Occluder depth pass (vg_raster.c): entries n x 4 u32 (instance, pool-global meshlet, firstIndex, packed), instance

@@ -2,7 +2,8 @@
  * the reference's occluder render (OcclusionCulling.ts:244-273: the occluders' previous-frame camera cuts drawn
  * depth-only with the current camera, vertices pulled as in GeometryPool.ts:1095-1131). Same arithmetic, in the
  * same order, as the CUDA rasterizer, so the depth images agree bit for bit:
- *   clip = (P V M) p; a triangle is dropped when a vertex has clip.w <= 0 or clip.z < 0, or when it faces away;
+ *   clip = (P V M) p; a triangle is clipped against the near plane (clip.z >= 0) into one or two triangles, and
+ *   dropped when it faces away;
  *   pixel centres inside the three edge functions (edges included) take the screen-space interpolation of the
  *   vertices' NDC depths, kept as a per-pixel minimum over an image cleared to 1.
  * Built with -ffp-contract=off. */
@@ -17,20 +18,26 @@ typedef struct {
   int x0, x1, y0, y1;
 } raster_tri;
 
-static int raster_setup(const float c[3][4], float W, float H, raster_tri *t) {
-  float sx[3], sy[3], sz[3];
-  for (int k = 0; k < 3; k++) {
-    if (!(c[k][3] > 0.0f) || !(c[k][2] >= 0.0f)) return 0;
-    const float nx = c[k][0] / c[k][3], ny = c[k][1] / c[k][3], nz = c[k][2] / c[k][3];
-    sx[k] = (nx * 0.5f + 0.5f) * W;
-    sy[k] = (0.5f - ny * 0.5f) * H;
-    sz[k] = nz;
+/* a clip-space vertex in screen space (x, y in pixels, y down; NDC depth; 1 when in front of the near plane, else all 0) */
+static void raster_screen(const float c[4], float W, float H, float out[4]) {
+  if (!(c[3] > 0.0f) || !(c[2] >= 0.0f)) {
+    out[0] = out[1] = out[2] = out[3] = 0.0f;
+    return;
   }
-  const float area0 = (sx[1] - sx[0]) * (sy[2] - sy[0]) - (sx[2] - sx[0]) * (sy[1] - sy[0]);
+  const float nx = c[0] / c[3], ny = c[1] / c[3], nz = c[2] / c[3];
+  out[0] = (nx * 0.5f + 0.5f) * W;
+  out[1] = (0.5f - ny * 0.5f) * H;
+  out[2] = nz;
+  out[3] = 1.0f;
+}
+
+static int raster_tri_setup(const float *v0, const float *v1, const float *v2, float W, float H, raster_tri *t) {
+  if (v0[3] == 0.0f || v1[3] == 0.0f || v2[3] == 0.0f) return 0;
+  const float area0 = (v1[0] - v0[0]) * (v2[1] - v0[1]) - (v2[0] - v0[0]) * (v1[1] - v0[1]);
   if (!(area0 < 0.0f)) return 0;
-  t->ax = sx[0], t->ay = sy[0], t->az = sz[0];
-  t->bx = sx[2], t->by = sy[2], t->bz = sz[2];
-  t->cx = sx[1], t->cy = sy[1], t->cz = sz[1];
+  t->ax = v0[0], t->ay = v0[1], t->az = v0[2];
+  t->bx = v2[0], t->by = v2[1], t->bz = v2[2];
+  t->cx = v1[0], t->cy = v1[1], t->cz = v1[2];
   t->area = (t->bx - t->ax) * (t->cy - t->ay) - (t->cx - t->ax) * (t->by - t->ay);
   if (!(t->area > 0.0f)) return 0;
   float mnx = fminf(fminf(t->ax, t->bx), t->cx), mxx = fmaxf(fmaxf(t->ax, t->bx), t->cx);
@@ -44,6 +51,54 @@ static int raster_setup(const float c[3][4], float W, float H, raster_tri *t) {
   t->y0 = y0 > 0 ? y0 : 0;
   t->y1 = y1 < (int)H - 1 ? y1 : (int)H - 1;
   return t->x0 <= t->x1 && t->y0 <= t->y1;
+}
+
+/* the crossing point of edge P -> Q (P in front) with the near plane: P + s (Q - P), s = P.z / (P.z - Q.z), depth 0 */
+static void raster_crossing(const float *p, const float *q, float out[4]) {
+  const float s = p[2] / (p[2] - q[2]);
+  out[0] = p[0] + s * (q[0] - p[0]);
+  out[1] = p[1] + s * (q[1] - p[1]);
+  out[2] = 0.0f;
+  out[3] = p[3] + s * (q[3] - p[3]);
+}
+
+/* Near-plane clipping of a triangle in clip space (clip.z >= 0 kept), then its screen triangles: t[0] (and t[1]);
+   returns how many (0..2). With A the corner in front (one in front) or the corner after the one behind (two in
+   front) in the order c0 -> c1 -> c2, and B, C the next ones: one in front -> (A, AB, CA); two in front ->
+   (A, B, BC) and (A, BC, CA). A triangle wholly in front is set up from its screen corners unchanged. */
+static int raster_clipped(const float c[3][4], float W, float H, raster_tri t[2]) {
+  const int in = (c[0][2] >= 0.0f) + (c[1][2] >= 0.0f) + (c[2][2] >= 0.0f);
+  float s0[4], s1[4], s2[4];
+  if (in == 3) {
+    raster_screen(c[0], W, H, s0);
+    raster_screen(c[1], W, H, s1);
+    raster_screen(c[2], W, H, s2);
+    return raster_tri_setup(s0, s1, s2, W, H, &t[0]);
+  }
+  if (in == 0) return 0;
+  const int lone = in == 1 ? (c[0][2] >= 0.0f ? 0 : (c[1][2] >= 0.0f ? 1 : 2))
+                            : (c[0][2] < 0.0f ? 0 : (c[1][2] < 0.0f ? 1 : 2));
+  const int ia = in == 1 ? lone : (lone + 1) % 3;
+  const float *A = c[ia], *B = c[(ia + 1) % 3], *C = c[(ia + 2) % 3];
+  float x[4], y[4], sa[4];
+  raster_screen(A, W, H, sa);
+  if (in == 1) {
+    raster_crossing(A, B, x);
+    raster_crossing(A, C, y);
+    raster_screen(x, W, H, s1);
+    raster_screen(y, W, H, s2);
+    return raster_tri_setup(sa, s1, s2, W, H, &t[0]);
+  }
+  raster_crossing(B, C, x);
+  raster_screen(x, W, H, s2); /* BC */
+  raster_screen(B, W, H, s1);
+  const int first = raster_tri_setup(sa, s1, s2, W, H, &t[0]);
+  raster_crossing(A, C, y);
+  float s3[4];
+  raster_screen(y, W, H, s3);
+  const int second = raster_tri_setup(sa, s2, s3, W, H, &t[1]);
+  if (!first && second) t[0] = t[1];
+  return first + second;
 }
 
 int vgo_occluder_depth(const uint32_t *entries, uint32_t n, const float *inst, const uint32_t *inst_slot,
@@ -79,21 +134,24 @@ int vgo_occluder_depth(const uint32_t *entries, uint32_t n, const float *inst, c
         const float *v = positions + (size_t)m_verts[voff + ((p >> (8 * k)) & 255u)] * 3;
         for (int r = 0; r < 4; r++) c[k][r] = ((mvp[r][0] * v[0] + mvp[r][1] * v[1]) + mvp[r][2] * v[2]) + mvp[r][3];
       }
-      raster_tri t;
-      if (!raster_setup(c, W, H, &t)) continue;
-      for (int py = t.y0; py <= t.y1; py++)
-        for (int px = t.x0; px <= t.x1; px++) {
-          const float x = (float)px + 0.5f, y = (float)py + 0.5f;
-          const float wa = (t.cx - t.bx) * (y - t.by) - (t.cy - t.by) * (x - t.bx);
-          const float wb = (t.ax - t.cx) * (y - t.cy) - (t.ay - t.cy) * (x - t.cx);
-          const float wc = (t.bx - t.ax) * (y - t.ay) - (t.by - t.ay) * (x - t.ax);
-          if (wa >= 0.0f && wb >= 0.0f && wc >= 0.0f) {
-            float z = ((wa * t.az + wb * t.bz) + wc * t.cz) / t.area;
-            z = z > 0.0f ? z : 0.0f;
-            float *o = depth + (size_t)py * width + px;
-            if (z < *o) *o = z;
+      raster_tri tt[2];
+      const int nt = raster_clipped(c, W, H, tt);
+      for (int j = 0; j < nt; j++) {
+        const raster_tri t = tt[j];
+        for (int py = t.y0; py <= t.y1; py++)
+          for (int px = t.x0; px <= t.x1; px++) {
+            const float x = (float)px + 0.5f, y = (float)py + 0.5f;
+            const float wa = (t.cx - t.bx) * (y - t.by) - (t.cy - t.by) * (x - t.bx);
+            const float wb = (t.ax - t.cx) * (y - t.cy) - (t.ay - t.cy) * (x - t.cx);
+            const float wc = (t.bx - t.ax) * (y - t.ay) - (t.by - t.ay) * (x - t.ax);
+            if (wa >= 0.0f && wb >= 0.0f && wc >= 0.0f) {
+              float z = ((wa * t.az + wb * t.bz) + wc * t.cz) / t.area;
+              z = z > 0.0f ? z : 0.0f;
+              float *o = depth + (size_t)py * width + px;
+              if (z < *o) *o = z;
+            }
           }
-        }
+      }
     }
   }
   return 0;
@@ -188,24 +246,27 @@ int vgo_visibility(const uint32_t *indices, uint64_t capacity, const uint32_t *d
       const uint32_t *ent = draw_list + (size_t)ds * 4;
       const uint32_t lo = (ent[3] >> 8) & 255u, hi = (ent[3] >> 16) & 255u;
       const uint32_t payload = (ds << 7) | ((uint32_t)((first - start - ent[2]) / 3) & 127u);
-      raster_tri t;
-      if (!raster_setup(c, W, H, &t)) continue;
-      for (int py = t.y0; py <= t.y1; py++)
-        for (int px = t.x0; px <= t.x1; px++) {
-          const float x = (float)px + 0.5f, y = (float)py + 0.5f;
-          const float wa = (t.cx - t.bx) * (y - t.by) - (t.cy - t.by) * (x - t.bx);
-          const float wb = (t.ax - t.cx) * (y - t.cy) - (t.ay - t.cy) * (x - t.cx);
-          const float wc = (t.bx - t.ax) * (y - t.ay) - (t.by - t.ay) * (x - t.ax);
-          if (wa >= 0.0f && wb >= 0.0f && wc >= 0.0f && vgo_blend_keep(px, py, frame, lo, hi)) {
-            float z = ((wa * t.az + wb * t.bz) + wc * t.cz) / t.area;
-            z = z > 0.0f ? z : 0.0f;
-            uint32_t zb;
-            memcpy(&zb, &z, 4);
-            const uint64_t v = ((uint64_t)zb << 32) | payload;
-            uint64_t *o = vis + (size_t)py * width + px;
-            if (v < *o) *o = v;
+      raster_tri tt[2];
+      const int nt = raster_clipped(c, W, H, tt);
+      for (int j = 0; j < nt; j++) {
+        const raster_tri t = tt[j];
+        for (int py = t.y0; py <= t.y1; py++)
+          for (int px = t.x0; px <= t.x1; px++) {
+            const float x = (float)px + 0.5f, y = (float)py + 0.5f;
+            const float wa = (t.cx - t.bx) * (y - t.by) - (t.cy - t.by) * (x - t.bx);
+            const float wb = (t.ax - t.cx) * (y - t.cy) - (t.ay - t.cy) * (x - t.cx);
+            const float wc = (t.bx - t.ax) * (y - t.ay) - (t.by - t.ay) * (x - t.ax);
+            if (wa >= 0.0f && wb >= 0.0f && wc >= 0.0f && vgo_blend_keep(px, py, frame, lo, hi)) {
+              float z = ((wa * t.az + wb * t.bz) + wc * t.cz) / t.area;
+              z = z > 0.0f ? z : 0.0f;
+              uint32_t zb;
+              memcpy(&zb, &z, 4);
+              const uint64_t v = ((uint64_t)zb << 32) | payload;
+              uint64_t *o = vis + (size_t)py * width + px;
+              if (v < *o) *o = v;
+            }
           }
-        }
+      }
     }
   }
   return 0;

@@ -80,6 +80,7 @@ class Harness:
         self.scene, self.mats, self.orders = O.scene_from_spec(spec.meshes, spec.instances, self.flags)
         self.inst_slot = np.concatenate([np.full(len(m), i, np.uint32) for i, m in enumerate(spec.instances)])
         self.max_meshlets, self.caps = max_meshlets, (max_triangles * 3, max_shadow * 3)
+        self.order_dependent = 0  # compared views whose draw list overflowed in some round (see compare)
 
     def check_layout(self):
         cells, mats = self.vg.debug_scene()
@@ -121,27 +122,29 @@ class Harness:
         stats, lists = self.gpu(cam, params, slot, graph)
         c = res["counters"]
         assert stats["visible_cells"] == c[0]
+        if any(m > self.max_meshlets for m in res["max_selected"]):
+            # A round selected more meshlets than the draw list holds: the GPU kept the subset its atomics reached
+            # first, and the capacity controller's fill (the kept entries' index count) - so the next round's scale,
+            # the final state and everything after - follows from that order (as in the reference, whose controller
+            # counts kept entries too). Only the order-independent part is compared; tests keep this count at 0.
+            self.order_dependent += 1
+            return lists, res
         assert stats["occluded_instances"] == c[1]
         for cut in (0, 1):
             k = c[2 + cut * 5: 7 + cut * 5]
             got = [stats["selected"][cut], stats["drawn"][cut], stats["survived"][cut], stats["work"][cut],
                    stats["requested_indices"][cut]]
-            overflow = k[0] > self.max_meshlets
-            if overflow:  # which entries are kept (and so the requested index count) depends on atomic order
-                got, k = got[:4], k[:4]
             assert got == k, f"cut {cut} counters gpu {got} oracle {k}"
-            if not overflow:
-                g = key_set(lists[cut], (0, 1, 3))
-                o = key_set(res["entries"][cut], (0, 1, 2))
-                assert g == o, f"cut {cut}: {len(g - o)} only on GPU, {len(o - g)} only in the oracle"
-                check_index_tiling(lists[cut], self.inst_slot, res["mesh_counts"], cut)
+            g = key_set(lists[cut], (0, 1, 3))
+            o = key_set(res["entries"][cut], (0, 1, 2))
+            assert g == o, f"cut {cut}: {len(g - o)} only on GPU, {len(o - g)} only in the oracle"
+            check_index_tiling(lists[cut], self.inst_slot, res["mesh_counts"], cut)
         assert stats["rounds"] == res["rounds"]
         out = self.vg.output(slot)
         args = d2h(out.draw_args, 2 * out.mesh_slots * 2 * 5).reshape(2, out.mesh_slots, 2, 5)
         n = len(self.spec.meshes)
         for cut in (0, 1):
-            if c[2 + cut * 5] <= self.max_meshlets:  # under overflow the kept entries depend on atomic order
-                assert np.array_equal(args[cut, :n], res["draw_args"][cut]), "drawIndexedIndirect args differ"
+            assert np.array_equal(args[cut, :n], res["draw_args"][cut]), "drawIndexedIndirect args differ"
         st = self.vg.state(params.state_slot)
         assert list(st) == res["state"], f"controller state gpu {list(st)} oracle {res['state']}"
         return lists, res

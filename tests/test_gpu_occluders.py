@@ -118,3 +118,19 @@ def test_large_triangles_match_the_oracle(occluding):
     got = d.cpu().numpy()
     want = O.occluder_depth(h.spec.meshes, [True] * len(h.spec.meshes), h.mats, h.inst_slot, entries, now, w2, h2)
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), f"{int((got != want).sum())} pixels differ"
+
+
+def test_near_plane_clipping_matches_the_oracle(occluding):
+    """With the near plane 8 m out, many occluder triangles cross it: each is clipped in clip space into one or two
+    triangles (queued and clipped by their own kernel), and the image equals the oracle's bit for bit; the clipped
+    parts reach depth 0 at the near plane."""
+    h = occluding
+    cam = h.spec.cameras[0]
+    h.gpu(cam, engine.ViewParams(error_threshold=1.0), slot=0)
+    fwd = -np.asarray(cam.view).reshape(4, 4).T[2, :3]
+    eye = cam.extra["eye"]
+    near = Camera.perspective_look_at(tuple(eye), tuple(eye + fwd), 60, 960, 540, 8.0, 5000.0)
+    got = gpu_depth(h, 0, near).cpu().numpy()
+    want = oracle_depth(h, 0, near)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), f"{int((got != want).sum())} pixels differ"
+    assert (got < 1e-3).sum() > 20, "clipped triangles reach the near plane"

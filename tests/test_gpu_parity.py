@@ -148,14 +148,19 @@ def test_hzb_mips_odd_sizes(ruins_small, shape):
 
 
 def test_capacity_retry_rounds():
-    """A draw list too small for the cut triggers the same-frame redo at a coarser threshold (GeometryPool.ts:1032)
-    and the steer between frames; counters and controller state match the oracle round for round."""
+    """An index buffer too small for the cut triggers the same-frame redo at a coarser threshold
+    (GeometryPool.ts:1032) and the steer between frames; counters and controller state match the oracle round for
+    round. (A draw list too small is not used here: the entries a GPU keeps past it follow its atomic order, and the
+    controller's fill counts the kept entries' indices, so the retried rounds would follow that order too.)"""
     spec = scenes.plain_small(n=60, seed=2)
-    h = Harness(spec, max_meshlets=300, max_triangles=40_000)
+    h = Harness(spec, max_meshlets=1 << 16, max_triangles=40_000)
     cam = cameras_around(1, 12, 4, seed=3)[0]
     p = engine.ViewParams(error_threshold=0.5, state_slot=3)
+    rounds = []
     for _ in range(3):  # state carries from frame to frame
-        h.compare(cam, p)
+        _, res = h.compare(cam, p)
+        rounds.append(res["rounds"])
+    assert h.order_dependent == 0 and rounds[0] >= 2, f"rounds {rounds}"
 
 
 def test_batch_graph_equals_plain(plain):

@@ -106,8 +106,18 @@ def test_served_equals_alone_and_the_oracle(contexts, oracle_scenes, cross_scene
         server.close()
     if cross_scene:
         assert any(res["batch_scenes"] > 1 for res, _ in served)
+    checked = 0
     for (k, cam, p), (res, (counters, sets)) in zip(reqs, served):
         assert res["status"] == 0 and res["done_us"] >= res["start_us"] >= res["submit_us"]
+        # the oracle's float mirror of the same view; a round that overflowed the draw list makes what follows depend
+        # on the GPU's atomic order (served and alone alike), so such a request is not compared
+        o = O.cull_pass(oracle_scenes[k], O.make_view(cam, p, MAX_MESHLETS, (30_000_000, 12_000_000), state=FRESH),
+                        "f32")
+        c = o["counters"]
+        assert counters["visible_cells"] == c[0]
+        if any(m > MAX_MESHLETS for m in o["max_selected"]):
+            continue
+        checked += 1
         vg = contexts[k][1]
         alone = engine.ViewParams(**{**p.__dict__, "state_slot": 0, "fresh_state": True})
         vg.cut([engine.make_view(cam, alone)], first_slot=0)
@@ -115,11 +125,7 @@ def test_served_equals_alone_and_the_oracle(contexts, oracle_scenes, cross_scene
         assert counters == want_counters, f"served counters {counters} alone {want_counters}"
         assert {kk: res["stats"][kk] for kk in COUNTERS} == want_counters
         assert sets == want_sets
-        # the oracle's float mirror of the same view
-        o = O.cull_pass(oracle_scenes[k], O.make_view(cam, p, MAX_MESHLETS, (30_000_000, 12_000_000), state=FRESH),
-                        "f32")
-        c = o["counters"]
-        assert counters["visible_cells"] == c[0] and counters["occluded_instances"] == c[1]
+        assert counters["occluded_instances"] == c[1]
         for cut in (0, 1):
             assert [counters["selected"][cut], counters["survived"][cut], counters["work"][cut]] == \
                 [c[2 + cut * 5], c[4 + cut * 5], c[5 + cut * 5]]
@@ -128,6 +134,7 @@ def test_served_equals_alone_and_the_oracle(contexts, oracle_scenes, cross_scene
         if p.triangle_budget > 0:
             assert counters["predicted_triangles"] == o["predicted"]
             assert counters["effective_threshold"] == np.float32(o["threshold"])
+    assert checked >= len(reqs) * 3 // 4, f"{checked} of {len(reqs)} served results compared with the oracle"
     assert any(len(s[1][1][0]) > 0 for s in served)
 
 

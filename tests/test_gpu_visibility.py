@@ -68,3 +68,17 @@ def test_blend_pattern_moves_with_the_frame(scene):
     a, _, _, _ = run(scene, cam, 0, 0)
     b, _, _, _ = run(scene, cam, 0, 1)
     assert (a != b).any(), "lodBlendFrame shifts the blend pattern"
+
+
+def test_near_plane_clipping_matches_the_oracle(scene):
+    """The visibility pass with the near plane 8 m out: triangles crossing it are clipped into one or two triangles
+    (the second drawn in the same warp step), carrying the crossing triangle's id, bit for bit as the oracle."""
+    from vgcut.camera import Camera
+    base = scene.spec.cameras[1]
+    fwd = -np.asarray(base.view).reshape(4, 4).T[2, :3]
+    eye = base.extra["eye"]
+    cam = Camera.perspective_look_at(tuple(eye), tuple(eye + fwd), 60, 960, 540, 8.0, 5000.0)
+    got, want, _, _ = run(scene, cam, 0)
+    assert np.array_equal(got, want), f"{int((got != want).sum())} pixels differ"
+    depth = (got >> np.uint64(32)).astype(np.uint32).view(np.float32)
+    assert (depth < 1e-3).sum() > 20, "clipped triangles reach the near plane"

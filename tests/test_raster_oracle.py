@@ -1,7 +1,9 @@
 """The oracle's occluder depth pass on hand-built triangles (known answers): depth of a plane at a known distance,
-coverage of the pixel centres inside a triangle, back faces, triangles reaching in front of the near plane, and the
-entries it must skip (blended part 1, meshes that are not occluders)."""
+coverage of the pixel centres inside a triangle, back faces, triangles crossing the near plane (clipped: the part in
+front is drawn with its plane's depth), and the entries it must skip (blended part 1, meshes that are not
+occluders)."""
 import numpy as np
+import pytest
 
 import oracle as O
 from vgcut.camera import Camera, perspective
@@ -67,9 +69,6 @@ def test_back_faces_near_plane_and_skipped_entries():
     front = [(-20, -20, z), (20, -20, z), (0, 30, z)]
     back, _ = run(front, [(0, 2, 1)], [(0, 0, 0, PART0)])
     assert (back == 1.0).all(), "a clockwise (back-facing) triangle is not drawn"
-    crossing = [(-20, -20, z), (20, -20, z), (0, 30, 1.0)]  # one vertex behind the camera
-    out, _ = run(crossing, [(0, 1, 2)], [(0, 0, 0, PART0)])
-    assert (out == 1.0).all(), "a triangle reaching in front of the near plane is left out"
     blended = 1 | (10 << 8) | (200 << 16)
     out, _ = run(front, [(0, 1, 2)], [(0, 0, 0, blended)])
     assert (out == 1.0).all(), "blended (part 1) meshlets are not occluders"
@@ -132,3 +131,52 @@ def test_visibility_oracle_single_triangle():
     assert np.allclose(depth, (p10 * z + p14) / -z, rtol=0, atol=2e-6)
     gone = O.visibility([mesh], [True], [4.0], inst, np.zeros(1, np.uint32), indices, draw_list, args, cam, W, H)
     assert (gone == np.uint64(0x3F800000FFFFFFFF)).all(), "beyond its draw distance the instance shrinks to a point"
+
+
+def plane_depth(cam, corners, px, py):
+    """The NDC depth where pixel (px, py)'s centre ray meets the plane of `corners` (view space), and whether it hits
+    the triangle in front of the near plane; double precision, from the ray-plane intersection."""
+    P = np.asarray(cam.proj, float).reshape(4, 4).T
+    a, b, c = (np.asarray(v, float) for v in corners)
+    n = np.cross(b - a, c - a)
+    x = (px + 0.5) / W * 2 - 1
+    y = 1 - (py + 0.5) / H * 2
+    d = np.array([x / P[0, 0], y / P[1, 1], -1.0])
+    den = n @ d
+    if abs(den) < 1e-12:
+        return None, False
+    t = (n @ a) / den
+    q = t * d
+    # barycentric inside test of q in (a, b, c)
+    v0, v1, v2 = b - a, c - a, q - a
+    d00, d01, d11, d20, d21 = v0 @ v0, v0 @ v1, v1 @ v1, v2 @ v0, v2 @ v1
+    den2 = d00 * d11 - d01 * d01
+    bb = (d11 * d20 - d01 * d21) / den2
+    cc = (d00 * d21 - d01 * d20) / den2
+    inside = bb >= 0 and cc >= 0 and bb + cc <= 1 and -q[2] >= cam.near
+    z = q[2]
+    return (P[2, 2] * z + P[2, 3]) / -z, inside
+
+
+@pytest.mark.parametrize("corners", [
+    [(-20, -20, -5.0), (20, -20, -5.0), (0, 30, 1.0)],   # two corners in front: a quad, two triangles
+    [(-20, -20, 1.0), (20, -20, 1.0), (0, 30, -5.0)],    # one corner in front: one triangle
+    [(-3, -4, -0.05), (3, -4, -0.05), (0, 4, -20.0)],    # two corners between the camera and the near plane
+])
+def test_near_plane_clipping(corners):
+    out, cam = run(corners, [(0, 1, 2)], [(0, 0, 0, PART0)])
+    covered = out < 1.0
+    hits = err = edge = 0
+    for py in range(H):
+        for px in range(W):
+            want, inside = plane_depth(cam, corners, px, py)
+            if covered[py, px]:
+                assert want is not None
+                err = max(err, abs(float(out[py, px]) - want))
+                hits += 1
+                edge += not inside
+            elif inside:
+                edge += 1
+    assert hits > 50, "the part in front of the near plane is drawn"
+    assert err < 2e-5, f"depth off the triangle's plane by {err}"
+    assert edge <= 2 * (W + H), "coverage follows the clipped triangle (up to its edge pixels)"

@@ -5,8 +5,9 @@
 //
 //  * one warp per draw-list entry of part 0 (drawn over every pixel; the blended ones are left out, as in the
 //    reference's proxy) whose mesh is an occluder; clip = (P V M) p with the instance's model matrix;
-//  * a triangle is dropped when a vertex lies behind the near plane (clip.z < 0 or clip.w <= 0) or when it faces
-//    away (the reference's proxy is single-sided): fewer occluders only cull less;
+//  * a triangle is clipped against the near plane (clip.z >= 0, WebGPU depth) as a GPU's clipper would: the part in
+//    front is a triangle or a quad (two triangles) with the crossing points at depth 0; a triangle that faces away
+//    (the reference's proxy is single-sided) is dropped;
 //  * pixel centres (x + 0.5, y + 0.5) inside all three edge functions (edges included) take the depth interpolated
 //    from the vertices' NDC depths (affine in screen space) through an atomic minimum on the float's bits (depth is
 //    >= 0, so the unsigned order is the float order); the image starts at 1 (far);
@@ -38,7 +39,9 @@ constexpr uint32_t kWarpRasterMax = 1024;   // ... by one warp of the second ker
 constexpr uint32_t kTileW = 32, kTileH = 16;
 constexpr uint32_t kQueuedMedium = 1u << 19;  // queue capacities: medium triangles,
 constexpr uint32_t kSubQueues = 256;          //   in sub-queues (record i of sub-queue q at i * kSubQueues + q),
-constexpr uint32_t kCtlWords = 4 + kSubQueues;
+constexpr uint32_t kClipCtl = 4 + kSubQueues;   // occluder pass: triangles crossing the near plane, queued
+constexpr uint32_t kCtlWords = kClipCtl + 1;
+constexpr uint32_t kClipQueue = 1u << 17;       //   (draw-list entry, triangle) records, clipped by a later kernel
 constexpr uint32_t kQueuedLarge = 1u << 16;   // large triangles,
 constexpr uint32_t kTileUnits = 1u << 20;     // and their tiles
 constexpr uint32_t kNoTri = 0xffffffffu;      // an empty tile record
@@ -57,6 +60,7 @@ struct RasterArgs {
   float4 *medium;
   float4 *large;
   uint2 *tiles;
+  uint2 *clip;  // occluder pass: crossing triangles (ctl[kClipCtl] of them)
 };
 
 // The occluder pass's inputs.
@@ -77,14 +81,24 @@ struct TriTag {
   uint32_t lo, hi, id;
 };
 
-// A vertex in screen space: x, y (pixels, y down), NDC depth; w = 1 when usable (in front of the near plane).
-__device__ __forceinline__ float4 screen_vertex(const float mvp[4][4], float4 v, float W, float H) {
+// Clip coordinates of a position: (P V M) p.
+__device__ __forceinline__ float4 clip_vertex(const float mvp[4][4], float4 v) {
   float c[4];
 #pragma unroll
   for (int r = 0; r < 4; r++) c[r] = ((mvp[r][0] * v.x + mvp[r][1] * v.y) + mvp[r][2] * v.z) + mvp[r][3];
-  if (!(c[3] > 0.0f) || !(c[2] >= 0.0f)) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  const float nx = c[0] / c[3], ny = c[1] / c[3], nz = c[2] / c[3];
+  return make_float4(c[0], c[1], c[2], c[3]);
+}
+
+// A clip-space vertex in screen space: x, y (pixels, y down), NDC depth; w = 1 when usable (in front of the near
+// plane), else all 0.
+__device__ __forceinline__ float4 screen_of(float4 c, float W, float H) {
+  if (!(c.w > 0.0f) || !(c.z >= 0.0f)) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const float nx = c.x / c.w, ny = c.y / c.w, nz = c.z / c.w;
   return make_float4((nx * 0.5f + 0.5f) * W, (0.5f - ny * 0.5f) * H, nz, 1.0f);
+}
+
+__device__ __forceinline__ float4 screen_vertex(const float mvp[4][4], float4 v, float W, float H) {
+  return screen_of(clip_vertex(mvp, v), W, H);
 }
 
 // Setup of one triangle from its screen-space corners; false when it is dropped.
@@ -109,6 +123,38 @@ __device__ __forceinline__ bool setup_triangle(float4 v0, float4 v1, float4 v2, 
   t.y0 = max(0, int(ceilf(mny - 0.5f)));
   t.y1 = min(int(H) - 1, int(floorf(mxy - 0.5f)));
   return t.x0 <= t.x1 && t.y0 <= t.y1;
+}
+
+// Near-plane clipping (Sutherland-Hodgman against clip.z >= 0) of the triangle with clip-space corners c0, c1, c2;
+// the part in front is a triangle or a quad, set up as screen triangles into t0 (and t1); returns how many (0..2),
+// t0 holding the first. With A the corner in front (one in front) or the corner after the one behind (two in front)
+// in the order c0 -> c1 -> c2, and B, C the next ones: one in front -> (A, AB, CA); two in front (A, B) ->
+// (A, B, BC) and (A, BC, CA), where XY = X + s (Y - X), s = X.z / (X.z - Y.z), is the crossing point at depth 0.
+// A triangle wholly in front gives exactly setup_triangle of its screen corners.
+__device__ __forceinline__ float4 crossing(float4 p, float4 q) {
+  const float s = p.z / (p.z - q.z);
+  return make_float4(p.x + s * (q.x - p.x), p.y + s * (q.y - p.y), 0.0f, p.w + s * (q.w - p.w));
+}
+
+__device__ __forceinline__ float4 pick3(int i, float4 a, float4 b, float4 c) { return i == 0 ? a : (i == 1 ? b : c); }
+
+__device__ __forceinline__ int setup_clipped(float4 c0, float4 c1, float4 c2, float W, float H, ScreenTri &t0,
+                                             ScreenTri &t1) {
+  const int in = (c0.z >= 0.0f ? 1 : 0) + (c1.z >= 0.0f ? 1 : 0) + (c2.z >= 0.0f ? 1 : 0);
+  if (in == 3) return setup_triangle(screen_of(c0, W, H), screen_of(c1, W, H), screen_of(c2, W, H), W, H, t0) ? 1 : 0;
+  if (in == 0) return 0;
+  // the corner that starts the polygon: the one in front (in == 1) or the one after the corner behind (in == 2)
+  const int lone = in == 1 ? (c0.z >= 0.0f ? 0 : (c1.z >= 0.0f ? 1 : 2)) : (c0.z < 0.0f ? 0 : (c1.z < 0.0f ? 1 : 2));
+  const int ia = in == 1 ? lone : (lone + 1) % 3;
+  const float4 A = pick3(ia, c0, c1, c2), B = pick3((ia + 1) % 3, c0, c1, c2), C = pick3((ia + 2) % 3, c0, c1, c2);
+  const float4 sa = screen_of(A, W, H);
+  if (in == 1)
+    return setup_triangle(sa, screen_of(crossing(A, B), W, H), screen_of(crossing(A, C), W, H), W, H, t0) ? 1 : 0;
+  const float4 sbc = screen_of(crossing(B, C), W, H);
+  const bool first = setup_triangle(sa, screen_of(B, W, H), sbc, W, H, t0);
+  const bool second = setup_triangle(sa, sbc, screen_of(crossing(A, C), W, H), W, H, t1);
+  if (!first && second) t0 = t1;
+  return int(first) + int(second);
 }
 
 // lodBlendMask (lodBlend.ts:36-45) at pixel (px, py): true when the pixel's step lies in [lo, hi).
@@ -370,12 +416,24 @@ __global__ void __launch_bounds__(128, 6) k_raster_occluders(Scene S, OccluderAr
         if (base + k * 32 + lane <= top) sv[base + k * 32 + lane] = screen_vertex(mvp, pos[k], W, H);
     }
     __syncwarp();
-    uint32_t left = 0;  // this lane's triangles turned away by a full queue (bit per round)
+    uint32_t left = 0;  // this lane's unclipped triangles turned away by a full queue (bit per round)
     for (uint32_t round = 0; round * 32 < tris; round++) {
       const uint32_t ti = round * 32 + lane, p = st[ti];
       ScreenTri t;
-      bool ok = false;
-      if (ti < tris) ok = setup_triangle(sv[p & 255u], sv[(p >> 8) & 255u], sv[(p >> 16) & 255u], W, H, t);
+      bool ok = false, crossing = false;
+      if (ti < tris) {
+        const float4 a = sv[p & 255u], b = sv[(p >> 8) & 255u], c = sv[(p >> 16) & 255u];
+        crossing = a.w == 0.0f || b.w == 0.0f || c.w == 0.0f;  // a corner behind the near plane
+        if (!crossing) ok = setup_triangle(a, b, c, W, H, t);
+      }
+      // crossing triangles (rare) are clipped by k_raster_clipped: (entry, triangle) records, one atomic per warp
+      const uint32_t cm = __ballot_sync(0xffffffffu, crossing);
+      if (cm) {
+        uint32_t at = 0;
+        if (lane == __ffs(cm) - 1) at = atomicAdd(R.ctl + kClipCtl, __popc(cm));
+        at = __shfl_sync(0xffffffffu, at, __ffs(cm) - 1) + __popc(cm & ((1u << lane) - 1u));
+        if (crossing && at < kClipQueue) R.clip[at] = make_uint2(e, ti);
+      }
       if (queue_triangles<false>(R, sm, sub, lane, ok, t, none)) left |= 1u << round;
     }
     for (uint32_t round = 0; round * 32 < tris; round++) {
@@ -386,6 +444,52 @@ __global__ void __launch_bounds__(128, 6) k_raster_occluders(Scene S, OccluderAr
       draw_left<false>(R, lane, mine, t, none);
     }
     __syncwarp();  // the vertex and triangle buffers are rewritten by the next entry
+  }
+}
+
+// The occluder pass's triangles that cross the near plane, a lane each: the draw-list entry's (P V M), the triangle's
+// corners in clip space, clipped (setup_clipped), and its one or two screen triangles through the same size classes
+// and queues (k_raster_queued runs after this kernel).
+__global__ void __launch_bounds__(128) k_raster_clipped(Scene S, OccluderArgs O, RasterArgs R) {
+  __shared__ SmallStage stage[4];
+  SmallStage &sm = stage[threadIdx.x >> 5];
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t n = min(R.ctl[kClipCtl], kClipQueue);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  const uint32_t sub = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) % kSubQueues;
+  const float W = float(R.width), H = float(R.height);
+  const TriTag none{0u, 0u, 0u};
+  for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+    const uint32_t i = base + lane;
+    ScreenTri t, t2;
+    int k = 0;
+    if (i < n) {
+      const uint2 rec = R.clip[i];
+      const uint4 d = O.draw_list[rec.x];
+      const float4 *col = S.inst + (size_t)d.x * 4;
+      const float4 c0 = col[0], c1 = col[1], c2 = col[2], c3 = col[3];
+      const float m[4][4] = {{c0.x, c1.x, c2.x, c3.x}, {c0.y, c1.y, c2.y, c3.y}, {c0.z, c1.z, c2.z, c3.z},
+                             {c0.w, c1.w, c2.w, c3.w}};
+      float mvp[4][4];
+#pragma unroll
+      for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++)
+          mvp[r][kk] = ((O.vp[r * 4] * m[0][kk] + O.vp[r * 4 + 1] * m[1][kk]) + O.vp[r * 4 + 2] * m[2][kk]) +
+                       O.vp[r * 4 + 3] * m[3][kk];
+      const uint4 info = S.m_info[d.y];
+      const uint32_t p = S.m_tris[info.y / 3 + rec.y], voff = info.w;
+      const float4 va = clip_vertex(mvp, S.positions[S.m_verts[voff + (p & 255u)]]);
+      const float4 vb = clip_vertex(mvp, S.positions[S.m_verts[voff + ((p >> 8) & 255u)]]);
+      const float4 vc = clip_vertex(mvp, S.positions[S.m_verts[voff + ((p >> 16) & 255u)]]);
+      k = setup_clipped(va, vb, vc, W, H, t, t2);
+    }
+    const bool l = queue_triangles<false>(R, sm, sub, lane, k >= 1, t, none);
+    draw_left<false>(R, lane, l, t, none);
+    if (__any_sync(0xffffffffu, k == 2)) {
+      const bool l2 = queue_triangles<false>(R, sm, sub, lane, k == 2, t2, none);
+      draw_left<false>(R, lane, l2, t2, none);
+    }
   }
 }
 
@@ -459,7 +563,8 @@ struct VisArgs {
 };
 
 // Screen-space vertex of index `idx` (w = 0: unusable), and its entry's draw slot and blend range.
-__device__ __forceinline__ float4 pulled_vertex(const Scene &S, const VisArgs &A, uint32_t idx, bool &ok) {
+// The clip-space position of index `idx` of the expanded buffer (ok: the index and its data are in range).
+__device__ __forceinline__ float4 pulled_clip(const Scene &S, const VisArgs &A, uint32_t idx, bool &ok) {
   const uint32_t ds = idx >> kLocalVertexBits, lv = idx & ((1u << kLocalVertexBits) - 1u);
   ok = false;
   if (ds >= A.draw_slots) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -488,9 +593,7 @@ __device__ __forceinline__ float4 pulled_vertex(const Scene &S, const VisArgs &A
   float c[4];
 #pragma unroll
   for (int r = 0; r < 4; r++) c[r] = ((A.vp[r * 4] * wx + A.vp[r * 4 + 1] * wy) + A.vp[r * 4 + 2] * wz) + A.vp[r * 4 + 3];
-  if (!(c[3] > 0.0f) || !(c[2] >= 0.0f)) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  const float nx = c[0] / c[3], ny = c[1] / c[3], nz = c[2] / c[3];
-  return make_float4((nx * 0.5f + 0.5f) * float(A.width), (0.5f - ny * 0.5f) * float(A.height), nz, 1.0f);
+  return make_float4(c[0], c[1], c[2], c[3]);
 }
 
 // One lane per triangle of the cut, in region order (mesh slot, then part), as the draw args give them.
@@ -517,8 +620,8 @@ __global__ void __launch_bounds__(256) k_visibility(Scene S, VisArgs A, RasterAr
   // every lane of a warp runs the same number of steps (the warp draws its lanes' large triangles together)
   for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
     const uint32_t t_id = base + lane;
-    ScreenTri t;
-    bool ok = false;
+    ScreenTri t, t2;
+    int n = 0;
     uint32_t lo = 0, hi = 0, payload = 0;
     if (t_id < total) {
       uint32_t r = 0, span = A.regions;  // the last region starting at or before t_id
@@ -531,20 +634,24 @@ __global__ void __launch_bounds__(256) k_visibility(Scene S, VisArgs A, RasterAr
       if (first + 2 < A.capacity) {
         const uint32_t i0 = A.indices[first], i1 = A.indices[first + 1], i2 = A.indices[first + 2];
         bool k0, k1, k2;
-        const float4 v0 = pulled_vertex(S, A, i0, k0), v1 = pulled_vertex(S, A, i1, k1), v2 = pulled_vertex(S, A, i2, k2);
+        const float4 v0 = pulled_clip(S, A, i0, k0), v1 = pulled_clip(S, A, i1, k1), v2 = pulled_clip(S, A, i2, k2);
         if (k0 && k1 && k2) {
           const uint32_t ds = i0 >> kLocalVertexBits;
           const uint4 ent = A.draw_list[ds];
           lo = (ent.w >> 8) & 255u, hi = (ent.w >> 16) & 255u;
           const uint32_t tri = uint32_t((first - A.args[r * 5 + 2] - ent.z) / 3);
           payload = (ds << kLocalVertexBits) | (tri & ((1u << kLocalVertexBits) - 1u));
-          ok = setup_triangle(v0, v1, v2, float(A.width), float(A.height), t);
+          n = setup_clipped(v0, v1, v2, float(A.width), float(A.height), t, t2);
         }
       }
     }
     const TriTag g{lo, hi, payload};
-    const bool left = queue_triangles<true>(R, sm, sub, lane, ok, t, g);
+    const bool left = queue_triangles<true>(R, sm, sub, lane, n >= 1, t, g);
     draw_left<true>(R, lane, left, t, g);
+    if (__any_sync(0xffffffffu, n == 2)) {  // the second triangle of a clipped quad
+      const bool left2 = queue_triangles<true>(R, sm, sub, lane, n == 2, t2, g);
+      draw_left<true>(R, lane, left2, t2, g);
+    }
   }
 }
 
@@ -556,13 +663,15 @@ static int raster_queues(vgc_context *ctx, RasterArgs &R) {
   const size_t medium_bytes = (size_t)kQueuedMedium * kRecord * 16, large_bytes = (size_t)kQueuedLarge * kRecord * 16;
   const size_t ctl_bytes = 2048;
   static_assert(kCtlWords * 4 <= ctl_bytes, "control words");
-  const int rc = dev_alloc(ctx, ctx->d_raster, ctl_bytes + medium_bytes + large_bytes + (size_t)kTileUnits * 8);
+  const size_t tile_bytes = (size_t)kTileUnits * 8;
+  const int rc = dev_alloc(ctx, ctx->d_raster, ctl_bytes + medium_bytes + large_bytes + tile_bytes + (size_t)kClipQueue * 8);
   if (rc) return rc;
   char *q = (char *)ctx->d_raster.ptr;
   R.ctl = (uint32_t *)q;
   R.medium = (float4 *)(q + ctl_bytes);
   R.large = (float4 *)(q + ctl_bytes + medium_bytes);
   R.tiles = (uint2 *)(q + ctl_bytes + medium_bytes + large_bytes);
+  R.clip = (uint2 *)(q + ctl_bytes + medium_bytes + large_bytes + tile_bytes);
   return VGC_OK;
 }
 
@@ -604,6 +713,8 @@ extern "C" int vgc_occluder_depth(vgc_context *ctx, uint32_t src_slot, const vgc
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k_raster_queued<false>, 128, 0));
   }
   k_raster_occluders<<<ctx->sm_count * std::max(1, per_sm[0]), 128, 0, st>>>(scene_of(ctx), O, R);
+  CUDA_TRY(cudaGetLastError());
+  k_raster_clipped<<<ctx->sm_count * 2, 128, 0, st>>>(scene_of(ctx), O, R);
   CUDA_TRY(cudaGetLastError());
   k_raster_queued<false><<<ctx->sm_count * std::max(1, per_sm[1]), 128, 0, st>>>(R);
   CUDA_TRY(cudaGetLastError());
