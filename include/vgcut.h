@@ -311,9 +311,11 @@ int vgc_server_destroy(vgc_server *server);
    the previous frame's - depth-only with this frame's camera `view` into `depth` (device memory, width x height
    floats, row 0 at the top, NDC depth in [0, 1], 1 where nothing is drawn), for the meshes flagged occluder. As in the
    reference, only the meshlets drawn over every pixel (part 0) are drawn, back faces are culled, and a triangle is
-   sampled at pixel centres; triangles reaching in front of the near plane are left out (fewer occluders only cull
-   less). Pass `depth` as this frame's vgc_view.depth to build the HZB from it in the cut's own launch sequence.
-   The first call allocates the context's triangle queues (about 53 MB, shared with vgc_visibility); calls on one
+   sampled at pixel centres. A triangle crossing the near plane (clip z = 0) is clipped in clip space into one or two
+   triangles (crossing points interpolated from the corner in front, at depth 0), as a GPU's clipper does; wholly
+   behind it, it is not drawn. Pass `depth` as this frame's vgc_view.depth to build the HZB from it in the cut's own
+   launch sequence. The first call allocates the context's triangle queues (about 54 MB, shared with
+   vgc_visibility; up to 131,072 near-plane-crossing triangles a call are clipped, more are left out); calls on one
    context whose GPU work overlaps (different streams) race on them: order them on one stream. Asynchronous on
    `stream`. */
 int vgc_occluder_depth(vgc_context *ctx, uint32_t src_slot, const vgc_view *view, float *depth, uint32_t width,
@@ -324,8 +326,8 @@ int vgc_occluder_depth(vgc_context *ctx, uint32_t src_slot, const vgc_view *view
    cut's draw args give them, with the reference's vertex pulling (GeometryPool.ts:1095-1131: draw-list entry,
    meshletVertices, positions, the instance's model, the draw-distance shrink toward the instance origin measured
    from `fade_view`, NULL = `view`) and LOD blend mask (lodBlend.ts:36-45: interleaved gradient noise at the pixel
-   centre, `frame` as lodBlendFrame), rasterized with `view` at pixel centres, back faces and triangles reaching in
-   front of the near plane left out, into `vis` (device, width x height u64, row 0 at the top): per pixel the
+   centre, `frame` as lodBlendFrame), rasterized with `view` at pixel centres, back faces culled and triangles
+   crossing the near plane clipped as in vgc_occluder_depth, into `vis` (device, width x height u64, row 0 at the top): per pixel the
    minimum of (NDC depth bits << 32 | drawSlot << 7 | triangle in its meshlet), VGC_VIS_EMPTY where nothing is
    drawn. Meshes without vertex data are not drawn. Uses the context's triangle queues (see vgc_occluder_depth):
    calls whose GPU work overlaps race on them. Asynchronous on `stream`. */
