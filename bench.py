@@ -952,6 +952,12 @@ class ServeDriver:
         return out, st
 
 
+# Serving on one scene: output slots enough that admission does not cut batches short while results wait to be read
+# and released, and a linger that lets a short batch fill while another one runs (none when the GPU is idle).
+SERVE_SLOTS = 1024
+SERVE_LINGER_US = 300
+
+
 def run_serve_ruins(ruins, args, plain_vps: float):
     """Serving on the ruins-like scene (113,106 instances) at 1920 x 1080: requests (spline pose with its prebuilt
     HZB, threshold U[0.5, 2] px), continuous batching on 4 streams; a saturated burst and Poisson arrivals at
@@ -973,7 +979,7 @@ def run_serve_ruins(ruins, args, plain_vps: float):
     thresholds = rng.uniform(0.5, 2.0, n_req)
     views = [engine.make_view(ruins.cameras[int(k)], engine.ViewParams(error_threshold=float(t), hzb=int(k)))
              for k, t in zip(poses, thresholds)]
-    server = engine.Server([vg], streams=4, max_batch=64, slots_per_scene=256)
+    server = engine.Server([vg], streams=4, max_batch=64, slots_per_scene=SERVE_SLOTS, linger_us=SERVE_LINGER_US)
     drv = ServeDriver(server, [0] * n_req, views)
     rates = {}
     try:
@@ -992,7 +998,8 @@ def run_serve_ruins(ruins, args, plain_vps: float):
                 saturated=dict(saturated, requests=n_req, note="burst submitted at once: the server's capacity"),
                 poisson=rates, plain_views_per_sec=plain_vps,
                 served_over_plain=saturated["views_per_sec"] / plain_vps if plain_vps else None,
-                capacity=dict(max_meshlets=cap_meshlets, max_triangles=cap_triangles, slots=256),
+                capacity=dict(max_meshlets=cap_meshlets, max_triangles=cap_triangles, slots=SERVE_SLOTS),
+                linger_us=SERVE_LINGER_US,
                 latency_note="submit -> completion seen by the server (host steady clock); Poisson arrivals, about "
                              "1 s of requests per rate")
 
@@ -1027,7 +1034,8 @@ def run_serve(ruins, args):
     views = [engine.make_view(cam, engine.ViewParams(error_threshold=t, triangle_budget=b, threshold_range=(0.5, 3.0)))
              for _, _, cam, t, b in reqs]
     budget = 16 << 30
-    server = engine.Server(vgs, streams=4, max_batch=64, slots_per_scene=64, hbm_budget_bytes=budget)
+    server = engine.Server(vgs, streams=4, max_batch=64, slots_per_scene=64, hbm_budget_bytes=budget,
+                           linger_us=SERVE_LINGER_US)
     drv = ServeDriver(server, [r[1] for r in reqs], views)
     try:
         drv.run([(0.0, i) for i in range(256)], False)  # warm-up
@@ -1050,7 +1058,7 @@ def run_serve(ruins, args):
                 poisson=dict(paced, note="Poisson arrivals at min(requested rate, 70% of capacity)"),
                 max_in_flight=st["max_in_flight"], hbm_budget_bytes=budget, max_bytes_in_use=st["max_bytes_in_use"],
                 latency_note="submit -> completion seen by the server, host steady clock",
-                config=dict(streams=4, max_batch=64, slots_per_scene=64, cross_scene=True,
+                config=dict(streams=4, max_batch=64, slots_per_scene=64, cross_scene=True, linger_us=SERVE_LINGER_US,
                             capacity_by_scene=[dict(instances=i, max_meshlets=m, max_triangles=t) for i, m, t in caps]))
 
 

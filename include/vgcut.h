@@ -272,7 +272,9 @@ typedef struct {
   uint32_t max_batch;        /* views per launch (default 64) */
   uint32_t slots_per_scene;  /* output slots reserved per scene (default streams * max_batch) */
   uint64_t hbm_budget_bytes; /* admission limit on the output-slot bytes of admitted, unreleased requests (0: none) */
-  uint32_t linger_us;        /* a batch smaller than max_batch waits up to this long for more requests (default 0) */
+  uint32_t linger_us;        /* while another batch runs, a batch smaller than max_batch waits up to this long (from
+                                its oldest request) for more requests; with every stream idle it starts at once
+                                (default 0: never waits) */
   uint64_t max_batch_instances; /* views x scene instances per batch at most (default 32M; 0: no limit): large
                                    scenes go in smaller batches, which keeps their latency and work queue bounded */
   uint32_t cross_scene;      /* 1 (default): a batch mixes scenes (all contexts on one device); 0: one scene each */

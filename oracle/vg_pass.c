@@ -10,8 +10,8 @@
 
 #include "vg_oracle.h"
 
-/* Natural log from float basic operations only (no library call), so the float mirror and the kernels agree
-   bit for bit: x = m * 2^e with m in [sqrt(1/2), sqrt(2)), ln x = e ln 2 + 2 atanh(s), s = (m - 1) / (m + 1),
+/* Natural log from float basic operations and correctly rounded fused multiply-adds only, so the float mirror and
+   the kernels agree bit for bit: x = m * 2^e with m in [sqrt(1/2), sqrt(2)), ln x = e ln 2 + 2 atanh(s), s = (m - 1) / (m + 1),
    2 atanh(s) = 2 (s + s^3/3 + s^5/5 + s^7/7 + s^9/9 + s^11/11) (Abramowitz & Stegun 4.1.27). */
 float vgo_logf(float x) {
   if (!(x > 0.0f)) return x == 0.0f ? -INFINITY : NAN;
@@ -34,10 +34,14 @@ float vgo_logf(float x) {
   }
   float s = (m - 1.0f) / (m + 1.0f);
   float s2 = s * s;
-  float p = s2 * (0.333333343f + s2 * (0.2f + s2 * (0.142857149f + s2 * (0.111111112f + s2 * 0.0909090936f))));
-  float lnm = (s + s * p) * 2.0f;
+  float p = fmaf(s2, 0.0909090936f, 0.111111112f); /* Horner form with fused multiply-adds */
+  p = fmaf(s2, p, 0.142857149f);
+  p = fmaf(s2, p, 0.2f);
+  p = fmaf(s2, p, 0.333333343f);
+  p = s2 * p;
+  float lnm = fmaf(s, p, s) * 2.0f;
   float fe = (float)e;
-  return fe * 0.693145752f + (fe * 1.42860677e-06f + lnm);
+  return fmaf(fe, 0.693145752f, fmaf(fe, 1.42860677e-06f, lnm));
 }
 
 /* Inverse of a rigid column-major 4x4 (rotation + translation): R^T and -R^T t. */
@@ -87,6 +91,7 @@ void vgo_frustum_planes(const double m[16], double out[24]) {
 #define SQRT sqrtf
 #define FLOOR floorf
 #define FABS fabsf
+#define FMA fmaf
 #include "vg_pass.inc"
 #undef REAL
 #undef SFX
@@ -95,6 +100,7 @@ void vgo_frustum_planes(const double m[16], double out[24]) {
 #undef SQRT
 #undef FLOOR
 #undef FABS
+#undef FMA
 
 #define REAL double
 #define SFX(name) name##_f64
@@ -103,6 +109,7 @@ void vgo_frustum_planes(const double m[16], double out[24]) {
 #define SQRT sqrt
 #define FLOOR floor
 #define FABS fabs
+#define FMA fma
 #include "vg_pass.inc"
 
 int64_t vgo_hzb_build(const float *depth, uint32_t width, uint32_t height, float *out, uint64_t cap, uint32_t *levels,

@@ -396,6 +396,7 @@ int view_constants(vgc_context *ctx, const vgc_view &in, uint32_t out_slot, uint
   }
   k.cascade = cascade ? 1u : 0u;
   k.proj_scale = (float)(in.proj[5] * in.viewport_height * 0.5);
+  k.inv_proj_scale = (float)(1.0 / (in.proj[5] * in.viewport_height * 0.5));
   k.near_ = (float)in.near_;
   k.P0 = (float)in.proj[0];
   k.P5 = (float)in.proj[5];

@@ -90,6 +90,7 @@ struct ViewConst {
   float plane[24];    // 6 view-space frustum planes (xyz normal, w), normalised (a cascade's: its clip volume)
   float sweep[6];     // per-plane max(dot(world normal, shadowSweep), 0)
   float proj_scale, near_, P0, P5, P8, P9, P10, P14;
+  float inv_proj_scale;  // 1 / proj_scale, rounded once from double
   float error_threshold, lod_blend_max, shadow_error_scale, lod_scale_limit, min_pixel_radius;
   float budget, budget_lo, budget_hi;  // triangleBudget search (0 = off)
   uint32_t frustum, occl_active;

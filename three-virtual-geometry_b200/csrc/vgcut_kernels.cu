@@ -30,9 +30,9 @@ namespace vgc {
 __device__ __forceinline__ float fmn(float a, float b) { return a < b ? a : b; }
 __device__ __forceinline__ float fmx(float a, float b) { return a > b ? a : b; }
 
-// Natural log from float basic operations (same steps as the oracle's vgo_logf): x = m 2^e, m in
-// [sqrt(1/2), sqrt(2)), ln x = e ln2 + 2 atanh((m-1)/(m+1)) by its odd series (Abramowitz & Stegun 4.1.27),
-// ln2 split in a high part with trailing zero bits and a low correction.
+// Natural log from float basic operations and fused multiply-adds (same steps as the oracle's vgo_logf): x = m 2^e,
+// m in [sqrt(1/2), sqrt(2)), ln x = e ln2 + 2 atanh((m-1)/(m+1)) by its odd series (Abramowitz & Stegun 4.1.27) in
+// Horner form, ln2 split in a high part with trailing zero bits and a low correction.
 __device__ __forceinline__ float vg_logf(float x) {
   if (!(x > 0.0f)) return x == 0.0f ? -__int_as_float(0x7f800000) : __int_as_float(0x7fc00000);
   if (x == __int_as_float(0x7f800000)) return x;
@@ -51,10 +51,14 @@ __device__ __forceinline__ float vg_logf(float x) {
   }
   float s = (m - 1.0f) / (m + 1.0f);
   float s2 = s * s;
-  float p = s2 * (0.333333343f + s2 * (0.2f + s2 * (0.142857149f + s2 * (0.111111112f + s2 * 0.0909090936f))));
-  float lnm = (s + s * p) * 2.0f;
+  float p = __fmaf_rn(s2, 0.0909090936f, 0.111111112f);
+  p = __fmaf_rn(s2, p, 0.142857149f);
+  p = __fmaf_rn(s2, p, 0.2f);
+  p = __fmaf_rn(s2, p, 0.333333343f);
+  p = s2 * p;
+  float lnm = __fmaf_rn(s, p, s) * 2.0f;
   float fe = float(e);
-  return fe * 0.693145752f + (fe * 1.42860677e-06f + lnm);
+  return __fmaf_rn(fe, 0.693145752f, __fmaf_rn(fe, 1.42860677e-06f, lnm));
 }
 
 struct Bands {
@@ -83,12 +87,17 @@ __device__ void load_bands(const ViewConst &V, float threshold, Bands &b) {
   b.high[1] = blending ? t1 * width : t1;
 }
 
+// Products summed with fused multiply-adds from the constant term up (the oracle's float build uses fmaf in the same
+// order): M c = fma(M2, z, fma(M1, y, fma(M0, x, M3))) per row, |v|^2 = fma(v2, v2, fma(v1, v1, v0 v0)).
 __device__ __forceinline__ void xform(const float *M, float x, float y, float z, float out[3]) {
 #pragma unroll
-  for (int r = 0; r < 3; r++) out[r] = ((M[r * 4 + 0] * x + M[r * 4 + 1] * y) + M[r * 4 + 2] * z) + M[r * 4 + 3];
+  for (int r = 0; r < 3; r++)
+    out[r] = __fmaf_rn(M[r * 4 + 2], z, __fmaf_rn(M[r * 4 + 1], y, __fmaf_rn(M[r * 4 + 0], x, M[r * 4 + 3])));
 }
 
-__device__ __forceinline__ float len3(const float v[3]) { return sqrtf((v[0] * v[0] + v[1] * v[1]) + v[2] * v[2]); }
+__device__ __forceinline__ float len3(const float v[3]) {
+  return sqrtf(__fmaf_rn(v[2], v[2], __fmaf_rn(v[1], v[1], v[0] * v[0])));
+}
 
 // VM = V * M (rows 0..2, row-major 3x4) and the instance scale (GeometryPool.ts:670-675)
 __device__ __forceinline__ void model_view(const float *Vr, const float4 *cols, float *VM, float &scale) {
@@ -97,7 +106,8 @@ __device__ __forceinline__ void model_view(const float *Vr, const float4 *cols, 
   for (int r = 0; r < 3; r++)
 #pragma unroll
     for (int k = 0; k < 4; k++)
-      VM[r * 4 + k] = ((Vr[r * 4 + 0] * c[k].x + Vr[r * 4 + 1] * c[k].y) + Vr[r * 4 + 2] * c[k].z) + Vr[r * 4 + 3] * c[k].w;
+      VM[r * 4 + k] = __fmaf_rn(Vr[r * 4 + 3], c[k].w,
+                                __fmaf_rn(Vr[r * 4 + 2], c[k].z, __fmaf_rn(Vr[r * 4 + 1], c[k].y, Vr[r * 4 + 0] * c[k].x)));
   float l0[3] = {c[0].x, c[0].y, c[0].z}, l1[3] = {c[1].x, c[1].y, c[1].z}, l2[3] = {c[2].x, c[2].y, c[2].z};
   scale = fmx(len3(l0), fmx(len3(l1), len3(l2)));
 }
@@ -107,7 +117,7 @@ __device__ __forceinline__ float frustum(const ViewConst &V, const float c[3], b
   float m = 1e30f;
 #pragma unroll
   for (int p = 0; p < 6; p++) {
-    float d = ((V.plane[p * 4] * c[0] + V.plane[p * 4 + 1] * c[1]) + V.plane[p * 4 + 2] * c[2]) + V.plane[p * 4 + 3];
+    float d = __fmaf_rn(V.plane[p * 4 + 2], c[2], __fmaf_rn(V.plane[p * 4 + 1], c[1], __fmaf_rn(V.plane[p * 4], c[0], V.plane[p * 4 + 3])));
     if (swept) d = d + V.sweep[p];
     m = fmn(m, d);
   }
@@ -126,17 +136,17 @@ __device__ bool hzb_occluded(const ViewConst &V, const HzbDesc &H, const float c
   float xlo = c[0] - radius, xhi = c[0] + radius, ylo = c[1] - radius, yhi = c[1] + radius;
   // x / depth as x * (1 / depth): two divisions instead of nine
   const float inv_near = 1.0f / near_depth, inv_far = 1.0f / far_depth;
-  float min_x = fmn(xlo * inv_near, xlo * inv_far) * V.P0 - V.P8;
-  float max_x = fmx(xhi * inv_near, xhi * inv_far) * V.P0 - V.P8;
-  float min_y = fmn(ylo * inv_near, ylo * inv_far) * V.P5 - V.P9;
-  float max_y = fmx(yhi * inv_near, yhi * inv_far) * V.P5 - V.P9;
-  float min_z = V.P14 * inv_near - V.P10;
+  float min_x = __fmaf_rn(fmn(xlo * inv_near, xlo * inv_far), V.P0, -V.P8);
+  float max_x = __fmaf_rn(fmx(xhi * inv_near, xhi * inv_far), V.P0, -V.P8);
+  float min_y = __fmaf_rn(fmn(ylo * inv_near, ylo * inv_far), V.P5, -V.P9);
+  float max_y = __fmaf_rn(fmx(yhi * inv_near, yhi * inv_far), V.P5, -V.P9);
+  float min_z = __fmaf_rn(V.P14, inv_near, -V.P10);
   if (!(min_z < 1.0f)) return false;
   float W = float(H.w[0]), Hh = float(H.h[0]);
-  float fx0 = floorf((min_x * 0.5f + 0.5f) * W);
-  float fx1 = floorf((max_x * 0.5f + 0.5f) * W);
-  float fy0 = floorf((0.5f - max_y * 0.5f) * Hh);
-  float fy1 = floorf((0.5f - min_y * 0.5f) * Hh);
+  float fx0 = floorf(__fmaf_rn(min_x, 0.5f, 0.5f) * W);
+  float fx1 = floorf(__fmaf_rn(max_x, 0.5f, 0.5f) * W);
+  float fy0 = floorf(__fmaf_rn(-max_y, 0.5f, 0.5f) * Hh);
+  float fy1 = floorf(__fmaf_rn(-min_y, 0.5f, 0.5f) * Hh);
   uint32_t x0 = uint32_t(fmn(fmx(fx0, 0.0f), W - 1.0f));
   uint32_t x1 = uint32_t(fmn(fmx(fx1, 0.0f), W - 1.0f));
   uint32_t y0 = uint32_t(fmn(fmx(fy0, 0.0f), Hh - 1.0f));
@@ -174,21 +184,35 @@ struct SceneOf<true> {
 __device__ __forceinline__ bool occluded(const ViewConst &V, const HzbDesc *hzbs, float high0, bool on, const float c[3],
                                          float r) {
   if (!on || !V.occl_active || V.hzb < 0) return false;
-  float margin = (fabsf(c[2]) * high0) / V.proj_scale;
+  float margin = (fabsf(c[2]) * high0) * V.inv_proj_scale;
   return hzb_occluded(V, hzbs[V.hzb], c, r + margin);
 }
 
-// projectedError (GeometryPool.ts:678-683)
-__device__ __forceinline__ float proj_error(const ViewConst &V, const float *VM, float scale, float4 s, float error) {
+// projectedError (GeometryPool.ts:678-683) in two parts: pixels = num / dist, num = (error * scale) * projScale,
+// dist = max(|VM c| - r scale, near) > 0. A band edge x is tested as num <= x * dist (no division); the value itself
+// is divided out only where the fade steps or the budget bins need it. error >= 1e30 / 2 (no parent) is infinite.
+struct ProjErr {
+  float num, dist;
+};
+constexpr float kErrInf = float(1e30 * 0.5);
+
+__device__ __forceinline__ ProjErr proj_parts(const ViewConst &V, const float *VM, float scale, float4 s, float error) {
   float c[3];
   xform(VM, s.x, s.y, s.z, c);
-  float dist = fmx(len3(c) - s.w * scale, V.near_);
-  float pixels = ((error * scale) / dist) * V.proj_scale;
-  return error >= float(1e30 * 0.5) ? 1e30f : pixels;
+  return {(error * scale) * V.proj_scale, fmx(__fmaf_rn(-s.w, scale, len3(c)), V.near_)};
+}
+// pixels <= x
+__device__ __forceinline__ bool err_le(ProjErr p, float error, float x) { return error < kErrInf && p.num <= x * p.dist; }
+// pixels > x
+__device__ __forceinline__ bool err_gt(ProjErr p, float error, float x) { return error >= kErrInf || p.num > x * p.dist; }
+__device__ __forceinline__ float err_value(float num, float dist, float error) {
+  return error >= kErrInf ? 1e30f : num / dist;
 }
 
-__device__ __forceinline__ uint32_t fade_step(float e, float low, float fade_scale) {
-  float x = rintf(vg_logf(fmx(e, float(1e-30)) / low) * fade_scale);
+// lodFadeRange's step of a projected error e against the band's low edge (1 / low passed in): rint(ln(e / low) *
+// fadeScale) clamped to [0, 255]
+__device__ __forceinline__ uint32_t fade_step(float e, float inv_low, float fade_scale) {
+  float x = rintf(vg_logf(fmx(e, float(1e-30)) * inv_low) * fade_scale);
   x = fmn(fmx(x, 0.0f), 255.0f);
   return uint32_t(x);
 }
@@ -403,12 +427,16 @@ __device__ __forceinline__ bool test_meshlet(const Scene &S, const ViewConst &V,
                                              uint32_t &id) {
   const float scale = VM[12];
   const float4 ls = __ldg(S.m_lod + meshlet), ps = __ldg(S.m_parent + meshlet), er = __ldg(S.m_err + meshlet);
-  const float own = proj_error(V, VM, scale, ls, er.x);
-  const float parent = proj_error(V, VM, scale, ps, er.y);
-  if (!(own <= high && parent > low)) return false;
+  const ProjErr own = proj_parts(V, VM, scale, ls, er.x);
+  const ProjErr parent = proj_parts(V, VM, scale, ps, er.y);
+  if (!(err_le(own, er.x, high) && err_gt(parent, er.y, low))) return false;
   id = __float_as_uint(er.w);  // pool-global meshlet id (the columns are in test order)
-  const uint32_t lo = fs > 0.0f ? fade_step(own, low, fs) : 0u;
-  const uint32_t hi = fs > 0.0f ? fade_step(parent, low, fs) : 255u;
+  uint32_t lo = 0u, hi = 255u;
+  if (fs > 0.0f) {
+    const float inv_low = 1.0f / low;
+    lo = fade_step(err_value(own.num, own.dist, er.x), inv_low, fs);
+    hi = fade_step(err_value(parent.num, parent.dist, er.y), inv_low, fs);
+  }
   if (!(hi > lo)) return false;
   packed = __float_as_uint(er.z) | (lo << 8) | (hi << 16);
   const float4 cs = __ldg(S.m_cull + meshlet);
@@ -534,23 +562,28 @@ __device__ __forceinline__ float budget_high(const ViewConst &V, float s, uint32
   return width > float(1.001) ? x * width : x;
 }
 
-// first k with x <= high_k (kBudgetBins when none); high_k does not decrease with k
-__device__ __forceinline__ uint32_t budget_bin_high(const ViewConst &V, float s, float x) {
+// first k with own <= high_k (kBudgetBins when none); high_k does not decrease with k. The comparisons are the
+// cut's own (err_le), so the bins agree with the decisions of the pass at the chosen threshold.
+__device__ __forceinline__ uint32_t budget_bin_high(const ViewConst &V, float s, ProjErr p, float error) {
+  if (error >= kErrInf) return kBudgetBins;
   uint32_t lo = 0, hi = kBudgetBins;
   while (lo < hi) {
     const uint32_t mid = (lo + hi) >> 1;
-    if (x <= budget_high(V, s, mid)) hi = mid;
+    if (err_le(p, error, budget_high(V, s, mid))) hi = mid;
     else lo = mid + 1;
   }
   return lo;
 }
 
-__device__ __forceinline__ uint32_t budget_bin(const ViewConst &V, float s, float x) {
+// first k with parent <= e_k (kBudgetBins when none)
+__device__ __forceinline__ uint32_t budget_bin(const ViewConst &V, float s, ProjErr p, float error) {
+  if (error >= kErrInf) return kBudgetBins;
   // estimate, then exact comparisons with e_k (bounded: the estimate is off by a few bins at most)
+  const float x = p.num / p.dist;
   const float guess = ((x / s - V.budget_lo) / (V.budget_hi - V.budget_lo)) * 255.0f;
   int k = guess != guess ? 0 : (guess < 0.0f ? 0 : (guess > 256.0f ? 256 : int(guess)));
-  for (int i = 0; i < 600 && k > 0 && x <= budget_e(V, s, uint32_t(k - 1)); i++) k--;
-  for (int i = 0; i < 600 && k < int(kBudgetBins) && !(x <= budget_e(V, s, uint32_t(k))); i++) k++;
+  for (int i = 0; i < 600 && k > 0 && err_le(p, error, budget_e(V, s, uint32_t(k - 1))); i++) k--;
+  for (int i = 0; i < 600 && k < int(kBudgetBins) && !err_le(p, error, budget_e(V, s, uint32_t(k))); i++) k++;
   return uint32_t(k);
 }
 
@@ -560,8 +593,8 @@ __device__ __forceinline__ bool hist_meshlet(const Scene &S, const ViewConst &V,
                                              uint32_t &bo, uint32_t &bp, uint32_t &tris) {
   const float scale = VM[12];
   const float4 ls = __ldg(S.m_lod + meshlet), ps = __ldg(S.m_parent + meshlet), er = __ldg(S.m_err + meshlet);
-  bo = budget_bin_high(V, s, proj_error(V, VM, scale, ls, er.x));
-  bp = budget_bin(V, s, proj_error(V, VM, scale, ps, er.y));
+  bo = budget_bin_high(V, s, proj_parts(V, VM, scale, ls, er.x), er.x);
+  bp = budget_bin(V, s, proj_parts(V, VM, scale, ps, er.y), er.y);
   if (!(bo < bp)) return false;
   tris = __float_as_uint(er.z);
   const float4 cs = __ldg(S.m_cull + meshlet);
@@ -621,15 +654,17 @@ __device__ void warp_item(const Scene &S, const ViewConst &V, const HzbDesc *hzb
 // them in place would leave most lanes idle.
 struct LodQueue {
   uint32_t pos[64], span[64];
-  float own[64], parent[64];  // HIST: the bins b_own, b_par as integers
+  float own[64], parent[64];  // the projected errors' distances (ProjErr::dist); HIST: the bins b_own, b_par as integers
 };
 
-// Per warp: the view-model matrix of each span's instance (rows 0..2, scale), its instance and inside flag.
+// Per warp: the view-model matrix of each span's instance (rows 0..2, scale), its instance and inside flag, and the
+// offset from a laid-out position in the chunk to the meshlet it names.
 struct SpanFrame {
-  float4 vm[32][4];  // [3] = (VM[12] scale, instance as bits, inside as bits, 0)
+  float4 vm[32][4];  // [3] = (VM[12] scale, instance as bits, inside as bits, first meshlet - start as bits)
 };
 
-__device__ __forceinline__ void frame_vm(const SpanFrame &F, uint32_t j, float *VM, uint32_t &instance, bool &inside) {
+__device__ __forceinline__ uint32_t frame_vm(const SpanFrame &F, uint32_t j, float *VM, uint32_t &instance,
+                                             bool &inside) {
   const float4 a = F.vm[j][0], b = F.vm[j][1], c = F.vm[j][2], d = F.vm[j][3];
   VM[0] = a.x, VM[1] = a.y, VM[2] = a.z, VM[3] = a.w;
   VM[4] = b.x, VM[5] = b.y, VM[6] = b.z, VM[7] = b.w;
@@ -637,13 +672,15 @@ __device__ __forceinline__ void frame_vm(const SpanFrame &F, uint32_t j, float *
   VM[12] = d.x;
   instance = __float_as_uint(d.y);
   inside = __float_as_uint(d.z) != 0;
+  return __float_as_uint(d.w);
 }
 
-// The rest of the meshlet test for queue entries [0, n): fade steps, culling sphere against the frustum, HZB; then
-// staging (draw list) or the histogram (HIST).
+// The rest of the meshlet test for queue entries [0, n): fade steps (the projected errors divided out here, for the
+// meshlets that passed the band), culling sphere against the frustum, HZB; then staging (draw list) or the histogram
+// (HIST).
 template <bool HIST>
 __device__ __forceinline__ void drain_queue(const Scene &S, const ViewConst &V, const HzbDesc *hzbs, const LodQueue &q,
-                                            const SpanFrame &F, uint32_t n, WarpStage &ws, WarpCount &wc, float low,
+                                            const SpanFrame &F, uint32_t n, WarpStage &ws, WarpCount &wc, float inv_low,
                                             float fs, float high0, uint32_t cut, bool occl_on, uint32_t slot) {
   const uint32_t lane = threadIdx.x & 31;
   bool drawn = false;
@@ -653,15 +690,16 @@ __device__ __forceinline__ void drain_queue(const Scene &S, const ViewConst &V, 
     float VM[13];
     bool inside;
     frame_vm(F, q.span[lane], VM, instance, inside);
+    const float4 er = __ldg(S.m_err + pos);
     if (HIST) {
       lo = __float_as_uint(q.own[lane]);
       hi = __float_as_uint(q.parent[lane]);
     } else if (fs > 0.0f) {
-      lo = fade_step(q.own[lane], low, fs);
-      hi = fade_step(q.parent[lane], low, fs);
+      lo = fade_step(err_value((er.x * VM[12]) * V.proj_scale, q.own[lane], er.x), inv_low, fs);
+      hi = fade_step(err_value((er.y * VM[12]) * V.proj_scale, q.parent[lane], er.y), inv_low, fs);
     }
     if (HIST || hi > lo) {
-      const float4 er = __ldg(S.m_err + pos), cs = __ldg(S.m_cull + pos);
+      const float4 cs = __ldg(S.m_cull + pos);
       id = __float_as_uint(er.w);
       packed = HIST ? __float_as_uint(er.z) : (__float_as_uint(er.z) | (lo << 8) | (hi << 16));
       float c[3];
@@ -904,54 +942,56 @@ __global__ void __launch_bounds__(128, MULTI ? 6 : 8) k_chunks(Scene S0, const S
     const bool occl_on = (ch.z & 2u) != 0;
     const ViewBands b = bands_of(V);
     const float low = cut ? b.low1 : b.low0, high = cut ? b.high1 : b.high0;
+    const float inv_low = 1.0f / low;
     const float sc = HIST ? get_state(V.state, 0) : 0.0f;
-    // spans: one lane each
-    uint32_t sp_first = 0, sp_count = 0;
+    // spans: one lane each, laid end to end from position 0
+    uint4 sp = make_uint4(0u, 0u, 0u, 0u);
+    if (lane < ns) sp = Q.spans[ch.w + lane];
+    const uint32_t sp_off = warp_scan_incl(sp.z) - sp.z;
+    const uint32_t total = __shfl_sync(0xffffffffu, sp_off + sp.z, 31);
     if (lane < ns) {
-      const uint4 sp = Q.spans[ch.w + lane];
-      sp_first = sp.y;
-      sp_count = sp.z;
       const uint32_t instance = cell.first + (sp.x & 127u);
       float VM[13];
       model_view(V.V, S.inst + (size_t)instance * 4, VM, VM[12]);
       F.vm[lane][0] = make_float4(VM[0], VM[1], VM[2], VM[3]);
       F.vm[lane][1] = make_float4(VM[4], VM[5], VM[6], VM[7]);
       F.vm[lane][2] = make_float4(VM[8], VM[9], VM[10], VM[11]);
-      F.vm[lane][3] = make_float4(VM[12], __uint_as_float(instance), __uint_as_float((sp.x >> 7) & 1u), 0.0f);
+      F.vm[lane][3] = make_float4(VM[12], __uint_as_float(instance), __uint_as_float((sp.x >> 7) & 1u),
+                                  __uint_as_float(sp.y - sp_off));
     }
-    const uint32_t sp_off = warp_scan_incl(sp_count) - sp_count;
-    const uint32_t total = __shfl_sync(0xffffffffu, sp_off + sp_count, 31);
     __syncwarp();
     WarpCount wc{0, 0, 0};
-    uint32_t qn = 0;  // warp-uniform
+    uint32_t qn = 0;       // warp-uniform
+    uint32_t started = 0;  // warp-uniform: spans starting before this step's first position
+    const uint32_t lanes_le = (2u << lane) - 1u;
     for (uint32_t base = 0; base < total; base += 32) {
       const uint32_t p = base + lane;
-      // span of position p: the last span starting at or before it (spans are non-empty, in order)
-      uint32_t j = 0;
-#pragma unroll
-      for (uint32_t k = 16; k > 0; k >>= 1) {
-        const uint32_t o = __shfl_sync(0xffffffffu, sp_off, min(j + k, 31u));
-        if (j + k < ns && o <= p) j += k;
-      }
-      const uint32_t m = __shfl_sync(0xffffffffu, sp_first, j) + (p - __shfl_sync(0xffffffffu, sp_off, j));
+      // span of position p: the last span starting at or before it (spans are non-empty and in order, so each step
+      // holds a bit per span starting in it)
+      const uint32_t rel = sp_off - base;
+      const uint32_t starts = __reduce_or_sync(0xffffffffu, lane < ns && rel < 32u ? 1u << rel : 0u);
+      const uint32_t j = started + __popc(starts & lanes_le) - 1u;
+      started += __popc(starts);
       bool pass = false;
       float own = 0.0f, parent = 0.0f;
+      uint32_t m = 0;
       if (p < total) {
         float VM[13];
         uint32_t inst;
         bool inside;
-        frame_vm(F, j, VM, inst, inside);
+        m = p + frame_vm(F, j, VM, inst, inside);
         const float4 ls = __ldg(S.m_lod + m), ps = __ldg(S.m_parent + m);
         const float2 er = __ldg(reinterpret_cast<const float2 *>(S.m_err + m));
-        own = proj_error(V, VM, VM[12], ls, er.x);
-        parent = proj_error(V, VM, VM[12], ps, er.y);
+        const ProjErr po = proj_parts(V, VM, VM[12], ls, er.x), pp = proj_parts(V, VM, VM[12], ps, er.y);
         if (HIST) {
-          const uint32_t bo = budget_bin_high(V, sc, own), bp = budget_bin(V, sc, parent);
+          const uint32_t bo = budget_bin_high(V, sc, po, er.x), bp = budget_bin(V, sc, pp, er.y);
           pass = bo < bp;
           own = __uint_as_float(bo);
           parent = __uint_as_float(bp);
         } else {
-          pass = own <= high && parent > low;
+          pass = err_le(po, er.x, high) && err_gt(pp, er.y, low);
+          own = po.dist;
+          parent = pp.dist;
         }
       }
       const uint32_t mask = __ballot_sync(0xffffffffu, pass);
@@ -965,7 +1005,7 @@ __global__ void __launch_bounds__(128, MULTI ? 6 : 8) k_chunks(Scene S0, const S
       qn += __popc(mask);
       __syncwarp();
       if (qn >= 32) {
-        drain_queue<HIST>(S, V, hzbs, q, F, 32, ws, wc, low, b.fade_scale, b.high0, cut, occl_on, cell.slot);
+        drain_queue<HIST>(S, V, hzbs, q, F, 32, ws, wc, inv_low, b.fade_scale, b.high0, cut, occl_on, cell.slot);
         qn -= 32;
         __syncwarp();
         if (lane < qn) {
@@ -977,7 +1017,7 @@ __global__ void __launch_bounds__(128, MULTI ? 6 : 8) k_chunks(Scene S0, const S
         __syncwarp();
       }
     }
-    if (qn) drain_queue<HIST>(S, V, hzbs, q, F, qn, ws, wc, low, b.fade_scale, b.high0, cut, occl_on, cell.slot);
+    if (qn) drain_queue<HIST>(S, V, hzbs, q, F, qn, ws, wc, inv_low, b.fade_scale, b.high0, cut, occl_on, cell.slot);
     __syncwarp();
     if (!HIST) warp_flush(ws, wc, V, S.slot_capacity, cell.slot, cut);
     __syncwarp();  // the frame and queue are rewritten by the next chunk
@@ -1324,7 +1364,7 @@ __global__ void __launch_bounds__(256) k_select_cut(Scene S, uint32_t slot, uint
     auto project = [&](float4 s, float err) {
       float c[3];
       xform(VM, s.x, s.y, s.z, c);
-      const float dist = fmx(len3(c) - s.w * sc, nr);
+      const float dist = fmx(__fmaf_rn(-s.w, sc, len3(c)), nr);
       return ((err * sc) / dist) * ps;
     };
     const bool own_inf = er.x >= float(1e30 * 0.5), parent_inf = er.y >= float(1e30 * 0.5);

@@ -113,7 +113,10 @@ bool pick_batch(vgc_server *s, Lane &lane, std::vector<uint32_t> &slots, std::ve
     }
   if (first == s->pending.end()) return false;
   const double oldest = s->requests[*first].result.submit_us;
-  if (s->opts.linger_us && ready < s->opts.max_batch && now_us() - oldest < s->opts.linger_us) return false;
+  // linger: while another batch runs, a short batch waits (up to linger_us from its oldest request) for more
+  // requests; with every lane idle it starts at once
+  if (s->opts.linger_us && ready < s->opts.max_batch && s->in_flight > 0 && now_us() - oldest < s->opts.linger_us)
+    return false;
   const uint32_t lead = s->requests[*first].scene;
   lane.tickets.clear();
   slots.clear();
