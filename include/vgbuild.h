@@ -22,6 +22,7 @@
 #ifndef VGBUILD_H
 #define VGBUILD_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -113,6 +114,20 @@ int vgb_gen_depth_image(uint32_t width, uint32_t height, uint32_t quads, float d
 int vgb_morton_order(const float *matrices, uint32_t n, const float sphere[4], uint32_t *out);
 /* Checksum of a .vgeo file (serialize.ts:429-437) over the u32 words from byte `start`. */
 uint32_t vgb_vgeo_checksum(const uint8_t *bytes, uint64_t length, uint64_t start);
+
+/* meshoptimizer's vertex buffer codec (versions 0 and 1) and index buffer codec (versions 0 and 1), the two codecs of
+   the reference's compressed `.vgeo` fields (serialize.ts:244 `meshopt-vertex`, :290 `meshlet-triangles`).
+   vgb_vertex_decode: `count` vertices of `stride` bytes (a multiple of 4, <= 256) from `size` bytes; 0 = OK, -1 bad
+   header or version, -2 truncated, -3 bytes left over, -4 bad arguments. vgb_vertex_encode writes version 0 or 1 into
+   `dst` (at least vgb_vertex_encode_bound bytes) and returns its length (0 on bad arguments). vgb_index_decode:
+   `index_count` (a multiple of 3) 32-bit indices, the same codes; vgb_index_encode writes version 0 or 1 (at least
+   vgb_index_encode_bound(index_count, largest index + 1) bytes). */
+size_t vgb_vertex_encode_bound(size_t count, size_t stride);
+size_t vgb_vertex_encode(uint8_t *dst, size_t capacity, const void *vertices, size_t count, size_t stride, int version);
+int vgb_vertex_decode(void *vertices, size_t count, size_t stride, const uint8_t *src, size_t size);
+size_t vgb_index_encode_bound(size_t index_count, size_t vertex_count);
+size_t vgb_index_encode(uint8_t *dst, size_t capacity, const uint32_t *indices, size_t index_count, int version);
+int vgb_index_decode(uint32_t *indices, size_t index_count, const uint8_t *src, size_t size);
 
 const char *vgb_last_error(void);
 

@@ -1,8 +1,9 @@
 """.vgeo files (the reference's baked geometry container, serialize.ts), after tests/serialize.test.ts: exact round
 trips with and without deflate, indices dropped and rebuilt from the meshlet arrays or kept, the container's layout,
 unknown fields (a typed array, null, an object holding Infinity) surviving, and the reference's rejections (empty,
-foreign, newer version, flipped payload byte, truncation inside the payload and inside the header). meshoptimizer's
-codecs are not available here: a field that uses one is rejected by name."""
+foreign, newer version, flipped payload byte, truncation inside the payload and inside the header). Compressed files
+(meshoptimizer's codecs, the reference's default) are covered in tests/test_meshopt.py; a codec field whose stream
+is not one is rejected naming the field."""
 import json
 
 import numpy as np
@@ -87,7 +88,7 @@ def test_rejections(mesh):
         vgeo.decode(b[:40])
 
 
-def test_meshopt_fields_are_rejected_by_name(mesh):
+def test_bad_codec_stream_is_rejected_by_field(mesh):
     b = bytearray(vgeo.encode(mesh, deflate=False))
     n = int.from_bytes(b[8:12], "little")
     h = json.loads(b[16:16 + n])
@@ -101,7 +102,7 @@ def test_meshopt_fields_are_rejected_by_name(mesh):
     b[0:8] = vgeo.MAGIC.to_bytes(4, "little") + vgeo.VG_FORMAT_VERSION.to_bytes(4, "little")
     b[8:12] = len(text).to_bytes(4, "little")
     b[12:16] = vgeo.checksum(bytes(b)).to_bytes(4, "little")
-    with pytest.raises(vgeo.VirtualMeshFormatError, match="meshopt-vertex"):
+    with pytest.raises(vgeo.VirtualMeshFormatError, match='field "positions": vertex stream'):
         vgeo.decode(bytes(b))
 
 

@@ -296,6 +296,15 @@ __device__ __forceinline__ unsigned long long *queue_counter(uint32_t *ctl) {
   return reinterpret_cast<unsigned long long *>(ctl + 4);
 }
 
+// Work is handed out one warp-sized piece at a time from a counter (ctl[8]: chunks, ctl[9]: instance units), so
+// warps that drew cheap pieces take more and the persistent grid ends together; the counters empty with the queue.
+constexpr uint32_t kCtlNextChunk = 8, kCtlNextUnit = 9;
+__device__ __forceinline__ uint32_t warp_grab(uint32_t *ctl, uint32_t word) {
+  uint32_t i = 0;
+  if ((threadIdx.x & 31) == 0) i = atomicAdd(ctl + word, 1u);
+  return __shfl_sync(0xffffffffu, i, 0);
+}
+
 // End of a pass over the work queue (one thread): ctl[6] / ctl[7] keep the most spans / chunks any pass of the
 // launch sequence asked for (the host grows the queue from them for the next launch), and the queue empties.
 __device__ __forceinline__ void retire_queue(uint32_t *ctl) {
@@ -303,6 +312,8 @@ __device__ __forceinline__ void retire_queue(uint32_t *ctl) {
   ctl[6] = max(ctl[6], uint32_t(q));
   ctl[7] = max(ctl[7], uint32_t(q >> 32));
   *queue_counter(ctl) = 0;
+  ctl[kCtlNextChunk] = 0;
+  ctl[kCtlNextUnit] = 0;
 }
 
 // Band values of a view for the current round, written by k_reset and by the capacity check (dyn[1..5]).
@@ -733,8 +744,9 @@ __global__ void __launch_bounds__(128, MULTI ? 5 : 6) k_instances(Scene S0, cons
   if (round > 0 && ctl[round] == 0) return;  // no view redoes a cut in this round
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t work = ctl[0] * 4;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < work; w += nwarps) {
+  // the next unit is drawn at the top of each one, so its counter's round trip overlaps the current unit
+  for (uint32_t w = warp_grab(ctl, kCtlNextUnit), w_next; w < work; w = w_next) {
+    w_next = warp_grab(ctl, kCtlNextUnit);
     const uint2 unit = units[w >> 2];
     const ViewConst &V = views[unit.x];
     if (HIST && !(V.budget > 0.0f)) continue;
@@ -892,14 +904,14 @@ __global__ void __launch_bounds__(128, MULTI ? 5 : 6) k_instances(Scene S0, cons
       while (over) {
         const uint32_t j = __ffs(over) - 1;
         over &= over - 1;
+        const uint32_t inst = cell.first + ((w & 3u) << 5) + j;
+        // instance j's view-model matrix, recomputed (the same arithmetic as its lane's) rather than kept live
         float vmj[13];
-#pragma unroll
-        for (int i = 0; i < 13; i++) vmj[i] = __shfl_sync(0xffffffffu, VM[i], j);
+        model_view(V.V, S.inst + (size_t)inst * 4, vmj, vmj[12]);
         const bool jin0 = __shfl_sync(0xffffffffu, inside0 ? 1 : 0, j) != 0;
         const bool jin1 = __shfl_sync(0xffffffffu, inside1 ? 1 : 0, j) != 0;
         const uint32_t f0 = __shfl_sync(0xffffffffu, t0f, j), c0 = __shfl_sync(0xffffffffu, n0, j);
         const uint32_t f1 = __shfl_sync(0xffffffffu, t1f, j), c1 = __shfl_sync(0xffffffffu, n1, j);
-        const uint32_t inst = cell.first + ((w & 3u) << 5) + j;
         if (c0) warp_item<HIST>(S, V, hzbs, ws, cell.slot, 0, occl_on, jin0, vmj, inst, f0, c0);
         if (c1) warp_item<HIST>(S, V, hzbs, ws, cell.slot, 1, false, jin1, vmj, inst, f1, c1);
       }
@@ -928,9 +940,9 @@ __global__ void __launch_bounds__(128, MULTI ? 6 : 8) k_chunks(Scene S0, const S
   if (round > 0 && ctl[round] == 0) return;  // no view redoes a cut in this round
   const WorkQueue Q = work_queue(queue, capacity);
   const uint32_t n_chunks = min(uint32_t(*queue_counter(ctl) >> 32), Q.chunk_cap);
-  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t lane = threadIdx.x & 31;
-  for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < n_chunks; c += warps) {
+  for (uint32_t c = warp_grab(ctl, kCtlNextChunk), c_next; c < n_chunks; c = c_next) {
+    c_next = warp_grab(ctl, kCtlNextChunk);
     const uint4 ch = Q.chunks[c];
     const uint32_t ns = ch.z >> 8;
     if (ns == 0) continue;
@@ -1212,9 +1224,18 @@ __global__ void __launch_bounds__(256) k_expand(Scene S, const ViewConst *__rest
 // memory (tiles are aligned to 64, so every clamped neighbour lies inside the tile); mips 7+ by the tail kernel.
 constexpr uint32_t kHzbTile = 64, kHzbTileLevels = 7;
 
+__device__ __forceinline__ void hzb_store(const HzbDesc &H, float *__restrict__ out, uint32_t l, uint32_t x, uint32_t y,
+                                          float v) {
+  if (l < H.levels && x < H.w[l] && y < H.h[l]) out[H.off[l] + (size_t)y * H.w[l] + x] = v;
+}
+
+// Levels 3..6 of the tile use no clamped reads: a texel's neighbour past the level's edge holds the max over the
+// edge texels of the same rows (or columns), which the in-range texel's footprint already contains, so the max over
+// the 2x2 block equals the max over its clamped reads. Level 3 is warp-local (a warp holds two rows of level 2); one
+// barrier hands the tile's 8x8 level-3 texels to warp 0 for levels 4..6.
 __device__ __forceinline__ void hzb_tile64(const float *__restrict__ depth, const HzbDesc &H, float *__restrict__ out,
-                                           bool copy_mip0, uint32_t ox, uint32_t oy, float (*sm)[16][17]) {
-  const uint32_t t = threadIdx.x, tx = t & 15u, ty = t >> 4;
+                                           bool copy_mip0, uint32_t ox, uint32_t oy, float (*s3)[9]) {
+  const uint32_t t = threadIdx.x, tx = t & 15u, ty = t >> 4, lane = t & 31u, warp = t >> 5;
   const uint32_t W = H.w[0], Hh = H.h[0];
   const uint32_t gx = ox + 4 * tx, gy = oy + 4 * ty;
   const bool vec = (W & 3u) == 0 && (reinterpret_cast<uintptr_t>(depth) & 15u) == 0 && gx + 3 < W;
@@ -1263,46 +1284,43 @@ __device__ __forceinline__ void hzb_tile64(const float *__restrict__ depth, cons
       }
   }
   const float b = fmaxf(fmaxf(a[0][0], a[0][1]), fmaxf(a[1][0], a[1][1]));
-  if (H.levels > 2 && gx / 4 < H.w[2] && gy / 4 < H.h[2]) out[H.off[2] + (size_t)(gy / 4) * H.w[2] + gx / 4] = b;
-  sm[0][ty][tx] = b;
-  __syncthreads();
-  const uint32_t top = min(H.levels, kHzbTileLevels);
-  for (uint32_t l = 3; l < top; l++) {
-    const uint32_t n = kHzbTile >> l;                     // tile texels per side at level l
-    const uint32_t px = ox >> (l - 1), py = oy >> (l - 1);  // tile origin at level l-1
-    const uint32_t qx = ox >> l, qy = oy >> l;              // tile origin at level l
-    const float(*src)[17] = sm[(l - 1) & 1];
-    float(*dst)[17] = sm[l & 1];
-    if (t < n * n) {
-      const uint32_t lx = t % n, ly = t / n, x = qx + lx, y = qy + ly;
-      if (x < H.w[l] && y < H.h[l]) {
-        const uint32_t x0 = 2 * x, y0 = 2 * y;
-        const uint32_t x1 = min(x0 + 1, H.w[l - 1] - 1), y1 = min(y0 + 1, H.h[l - 1] - 1);
-        const float m = fmaxf(fmaxf(src[y0 - py][x0 - px], src[y0 - py][x1 - px]),
-                              fmaxf(src[y1 - py][x0 - px], src[y1 - py][x1 - px]));
-        dst[ly][lx] = m;
-        out[H.off[l] + (size_t)y * H.w[l] + x] = m;
-      }
-    }
-    __syncthreads();
+  hzb_store(H, out, 2, gx / 4, gy / 4, b);
+  // level 3: texel (tx / 2, warp) of the tile from lanes tx, tx ^ 1 of rows 2 warp, 2 warp + 1
+  float m = fmaxf(b, __shfl_xor_sync(0xffffffffu, b, 1));
+  m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 16));
+  if ((lane & 17u) == 0) {
+    hzb_store(H, out, 3, (ox >> 3) + (tx >> 1), (oy >> 3) + warp, m);
+    s3[warp][tx >> 1] = m;
   }
+  __syncthreads();
+  if (warp != 0 || H.levels <= 4) return;
+  // levels 4..6 by warp 0: lane = 4 y + x of level 4 (16 lanes), then xor 1 / 4 and xor 2 / 8 pair up the blocks
+  const uint32_t x4 = lane & 3u, y4 = (lane >> 2) & 3u;
+  float m4 = fmaxf(fmaxf(s3[2 * y4][2 * x4], s3[2 * y4][2 * x4 + 1]), fmaxf(s3[2 * y4 + 1][2 * x4], s3[2 * y4 + 1][2 * x4 + 1]));
+  if (lane < 16) hzb_store(H, out, 4, (ox >> 4) + x4, (oy >> 4) + y4, m4);
+  float m5 = fmaxf(m4, __shfl_xor_sync(0xffffffffu, m4, 1));
+  m5 = fmaxf(m5, __shfl_xor_sync(0xffffffffu, m5, 4));
+  if (lane < 16 && (lane & 5u) == 0) hzb_store(H, out, 5, (ox >> 5) + (x4 >> 1), (oy >> 5) + (y4 >> 1), m5);
+  float m6 = fmaxf(m5, __shfl_xor_sync(0xffffffffu, m5, 2));
+  m6 = fmaxf(m6, __shfl_xor_sync(0xffffffffu, m6, 8));
+  if (lane == 0) hzb_store(H, out, 6, ox >> 6, oy >> 6, m6);
 }
 
 __global__ void __launch_bounds__(256) k_hzb_tiles(const float *__restrict__ depth, HzbDesc H, float *__restrict__ out,
                                                    int copy_mip0) {
-  __shared__ float sm[2][16][17];
-  hzb_tile64(depth, H, out, copy_mip0 != 0, blockIdx.x * kHzbTile, blockIdx.y * kHzbTile, sm);
+  __shared__ float s3[8][9];
+  hzb_tile64(depth, H, out, copy_mip0 != 0, blockIdx.x * kHzbTile, blockIdx.y * kHzbTile, s3);
 }
 
 // The HZB builds of a batch: grid.z = view, views without a depth image skip.
 __global__ void __launch_bounds__(256) k_hzb_tiles_views(const ViewConst *__restrict__ views) {
-  __shared__ float sm[2][16][17];
+  __shared__ float s3[8][9];
   const ViewConst &V = views[blockIdx.z];
   if (!V.build_hzb) return;
   const HzbDesc &H = *V.hzb_desc;
   const uint32_t ox = blockIdx.x * kHzbTile, oy = blockIdx.y * kHzbTile;
   if (ox >= H.w[0] || oy >= H.h[0]) return;
-  hzb_tile64(V.depth, H, const_cast<float *>(H.data), true, ox, oy, sm);
+  hzb_tile64(V.depth, H, const_cast<float *>(H.data), true, ox, oy, s3);
 }
 
 __global__ void __launch_bounds__(1024) k_hzb_tail_views(const ViewConst *__restrict__ views) {

@@ -11,11 +11,13 @@ Layout (little-endian), as the reference writes it:
     ..  payload: one 4-byte aligned blob per typed-array field
 
 Encodings: `raw` (the array's bytes), optionally `deflate` (raw deflate) on top; `meshlet-indices` (no bytes:
-`indices` is rebuilt from meshletInfo / meshletVertices / meshletTriangles, serialize.ts:395-413). The reference's
-compressed files also use meshoptimizer's vertex and index codecs (`meshopt-vertex`, `meshlet-triangles`);
-meshoptimizer is an npm dependency that is not vendored with the reference, so this reader rejects those two
-encodings with a VirtualMeshFormatError naming them, and the writer never produces them (files written with the
-reference's `{compress: false}` read here, and files written here read in the reference).
+`indices` is rebuilt from meshletInfo / meshletVertices / meshletTriangles, serialize.ts:395-413); `meshopt-vertex`
+(meshoptimizer's vertex codec over `stride`-byte elements, serialize.ts:338-343) and `meshlet-triangles` (u32 codec
+length, meshoptimizer's index codec over the meshlet-vertex slots vertexOffset + local id, padded to 4 bytes, then
+2-bit corner rotations per triangle; serialize.ts:264-300, :369-388). The codecs are in `vgcut.meshopt`; compressed
+writing picks, per field, the smallest of raw and the codec candidates the reference tries (strides from its field
+hints), deflates the best one where that is smaller, and keeps a candidate only if it decodes to the same bytes
+(encodeField, serialize.ts:231-262).
 """
 from __future__ import annotations
 
@@ -26,6 +28,7 @@ import zlib
 import numpy as np
 
 from . import build as B
+from . import meshopt
 
 MAGIC = 0x4F454756  # 'VGEO' as a little-endian u32
 VG_FORMAT_VERSION = 1
@@ -149,9 +152,142 @@ def rebuild_indices(length: int, info: np.ndarray, mverts: np.ndarray, tris: np.
     return out
 
 
-def encode(data, deflate: bool = True, keep_indices: bool = False) -> bytes:
-    """A .vgeo file for `data` (VirtualMeshData or a record of the reference's fields): each array raw or, where
-    smaller, raw-deflated; `indices` dropped and rebuilt on decode when the meshlet arrays reproduce it."""
+# per-field element strides the vertex codec is tried with (serialize.ts:92-100 FIELD_HINTS)
+_STRIDES = {"positions": [12], "normals": [12], "colors": [12], "uvs": [8], "tangents": [16], "meshletBounds": [64],
+            "meshletInfo": [16]}
+_DEFLATE_RAW = {"meshletBounds"}
+
+
+def _deflate(blob: bytes) -> bytes:
+    z = zlib.compressobj(9, zlib.DEFLATED, -15)
+    return z.compress(blob) + z.flush()
+
+
+def encode_meshlet_triangles(tris: np.ndarray, info: np.ndarray) -> bytes | None:
+    """encodeMeshletTriangles (serialize.ts:264-300): the triangles as an index-codec stream over meshlet-vertex
+    slots plus each triangle's corner rotation; None when the meshlets do not cover every triangle exactly once or a
+    triangle uses its top byte."""
+    tris = np.asarray(tris, np.uint32).reshape(-1)
+    info = np.asarray(info, np.uint32).reshape(-1, 4)
+    slots = np.zeros(tris.size * 3, np.uint32)
+    covered = np.zeros(tris.size, np.uint8)
+    for count, first, _, voff in info.tolist():
+        t0 = first // 3
+        if t0 + count > tris.size:
+            return None
+        p = tris[t0:t0 + count]
+        if covered[t0:t0 + count].any() or (p >> 24).any():
+            return None
+        covered[t0:t0 + count] = 1
+        slots[t0 * 3:(t0 + count) * 3] = (np.stack([p & 255, (p >> 8) & 255, (p >> 16) & 255], 1) + voff).reshape(-1)
+    if not covered.all():
+        return None
+    codec = meshopt.encode_index_buffer(slots)
+    dec = meshopt.decode_index_buffer(codec, slots.size).reshape(-1, 3)
+    s = slots.reshape(-1, 3)
+    rot = np.full(tris.size, 3, np.uint8)
+    rot[(s == dec).all(1)] = 0
+    rot[(s[:, 0] == dec[:, 1]) & (s[:, 1] == dec[:, 2]) & (s[:, 2] == dec[:, 0]) & (rot == 3)] = 1
+    rot[(s[:, 0] == dec[:, 2]) & (s[:, 1] == dec[:, 0]) & (s[:, 2] == dec[:, 1]) & (rot == 3)] = 2
+    if (rot == 3).any():
+        return None
+    packed = np.zeros((tris.size + 3) // 4, np.uint8)
+    np.bitwise_or.at(packed, np.arange(tris.size) >> 2, (rot << ((np.arange(tris.size) & 3) * 2)).astype(np.uint8))
+    out = bytearray(4 + _align4(len(codec)))
+    out[0:4] = len(codec).to_bytes(4, "little")
+    out[4:4 + len(codec)] = codec
+    return bytes(out) + packed.tobytes()
+
+
+def decode_meshlet_triangles(length: int, blob: bytes, info: np.ndarray) -> np.ndarray:
+    """decodeMeshletTriangles (serialize.ts:369-388)."""
+    if len(blob) < 4:
+        raise VirtualMeshFormatError("truncated triangle data")
+    codec_len = int.from_bytes(blob[0:4], "little")
+    rot_at = 4 + _align4(codec_len)
+    if rot_at + (length + 3) // 4 > len(blob):
+        raise VirtualMeshFormatError("truncated triangle data")
+    slots = meshopt.decode_index_buffer(blob[4:4 + codec_len], length * 3).reshape(-1, 3)
+    rot = np.frombuffer(blob[rot_at:rot_at + (length + 3) // 4], np.uint8)
+    out = np.zeros(length, np.uint32)
+    for count, first, _, voff in np.asarray(info, np.uint32).reshape(-1, 4).tolist():
+        t0 = first // 3
+        if t0 + count > length:
+            raise VirtualMeshFormatError("meshlet range out of bounds")
+        t = np.arange(t0, t0 + count)
+        r = (rot[t >> 2] >> ((t & 3) * 2)) & 3
+        xyz = slots[t0:t0 + count].astype(np.int64) - int(voff)
+        a = np.where(r == 0, xyz[:, 0], np.where(r == 1, xyz[:, 1], xyz[:, 2]))
+        b = np.where(r == 0, xyz[:, 1], np.where(r == 1, xyz[:, 2], xyz[:, 0]))
+        c = np.where(r == 0, xyz[:, 2], np.where(r == 1, xyz[:, 0], xyz[:, 1]))
+        if ((a | b | c) >> 8).any() or (np.minimum(np.minimum(a, b), c) < 0).any():
+            raise VirtualMeshFormatError("meshlet-local vertex id out of range")
+        out[t0:t0 + count] = (a | (b << 8) | (c << 16)).astype(np.uint32)
+    return out
+
+
+def _decode_field(f: dict, blob: bytes, dt: np.dtype, arrays: dict) -> np.ndarray:
+    """decodeField (serialize.ts:328-361) after any inflate."""
+    enc, nbytes = f["encoding"], f["length"] * dt.itemsize
+    if enc == "raw":
+        if len(blob) != nbytes:
+            raise VirtualMeshFormatError(f'geometry file is corrupt (field "{f["name"]}" has the wrong size)')
+        return np.frombuffer(blob, dt).astype(dt.newbyteorder("="))
+    if enc == "meshopt-vertex":
+        stride = f.get("stride") or 0
+        if stride <= 0 or stride % 4 or nbytes % stride:
+            raise VirtualMeshFormatError(f'geometry file is corrupt (field "{f["name"]}" stride)')
+        raw = meshopt.decode_vertex_buffer(blob, nbytes // stride, stride) if nbytes else b""
+        return np.frombuffer(raw, dt).astype(dt.newbyteorder("="))
+    if enc == "meshlet-triangles":
+        info = arrays.get("meshletInfo")
+        if info is None:
+            raise VirtualMeshFormatError(f'geometry file is corrupt ("{f["name"]}" needs "meshletInfo")')
+        return decode_meshlet_triangles(f["length"], blob, info)
+    if enc == "meshlet-indices":
+        need = [arrays.get(k) for k in ("meshletInfo", "meshletVertices", "meshletTriangles")]
+        if any(a is None for a in need):
+            raise VirtualMeshFormatError(f'geometry file is corrupt ("{f["name"]}" needs the meshlet arrays)')
+        return rebuild_indices(f["length"], *need)
+    raise VirtualMeshFormatError(f'unknown encoding "{enc}" for field "{f["name"]}"')
+
+
+def _encode_field(name: str, arr: np.ndarray, rec: dict, deflate: bool) -> tuple:
+    """encodeField (serialize.ts:231-262): the smallest candidate that decodes back to the same bytes."""
+    raw = arr.astype(arr.dtype.newbyteorder("<"), copy=False).tobytes()
+    base = {"name": name, "type": _NAME_OF[arr.dtype], "length": int(arr.size)}
+    raw_c = (dict(base, encoding="raw"), raw)
+    cands = [raw_c]
+    tri = encode_meshlet_triangles(arr, rec["meshletInfo"]) \
+        if name == "meshletTriangles" and arr.dtype == np.uint32 and "meshletInfo" in rec else None
+    if tri is not None:
+        cands.append((dict(base, encoding="meshlet-triangles"), tri))
+    elif len(raw) % 4 == 0 and len(raw) > 0:
+        for stride in [s for s in _STRIDES.get(name, [max(4, arr.dtype.itemsize)])
+                       if s % 4 == 0 and s <= 256 and len(raw) % s == 0]:
+            cands.append((dict(base, encoding="meshopt-vertex", stride=stride),
+                          meshopt.encode_vertex_buffer(raw, stride)))
+    cands.sort(key=lambda c: len(c[1]))
+    if deflate and len(raw) >= 64:
+        todo = [cands[0], raw_c] if name in _DEFLATE_RAW and cands[0] is not raw_c else [cands[0]]
+        cands += [(dict(e, deflate=True), _deflate(b)) for e, b in todo]
+        cands.sort(key=lambda c: len(c[1]))
+    dt = np.dtype(_TYPES[base["type"]]).newbyteorder("<")
+    for entry, blob in cands:
+        try:
+            src = zlib.decompressobj(-15).decompress(blob) if entry.get("deflate") else blob
+            if _decode_field(entry, src, dt, {"meshletInfo": rec.get("meshletInfo")}).astype(dt).tobytes() == raw:
+                return entry, blob
+        except (VirtualMeshFormatError, meshopt.CodecError):
+            continue
+    return raw_c
+
+
+def encode(data, deflate: bool = True, keep_indices: bool = False, compress: bool = False) -> bytes:
+    """A .vgeo file for `data` (VirtualMeshData or a record of the reference's fields); `indices` dropped and rebuilt
+    on decode when the meshlet arrays reproduce it. compress=False: each array raw or, where smaller, raw-deflated.
+    compress=True (the reference's default, encodeVirtualMesh): per array the smallest round-tripping candidate
+    among raw, the meshoptimizer codecs and deflate over the best of them."""
     rec = to_record(data) if isinstance(data, B.VirtualMeshData) else dict(data)
     fields, blobs, values, offset = [], [], {}, 0
     keys = [k for k, v in rec.items()]
@@ -167,6 +303,8 @@ def encode(data, deflate: bool = True, keep_indices: bool = False) -> bytes:
         blob = b""
         if name == "indices" and not keep_indices and _indices_match(rec):
             entry["encoding"] = "meshlet-indices"
+        elif compress:
+            entry, blob = _encode_field(name, arr, rec, deflate)
         else:
             raw = arr.astype(arr.dtype.newbyteorder("<"), copy=False).tobytes()
             entry["encoding"], blob = "raw", raw
@@ -242,21 +380,10 @@ def decode_record(data: bytes) -> dict:
                 blob = zlib.decompressobj(-15).decompress(blob)
         except zlib.error as e:
             raise VirtualMeshFormatError(f'geometry file is corrupt (field "{f["name"]}": {e})') from None
-        enc = f["encoding"]
-        if enc == "raw":
-            if len(blob) != f["length"] * dt.itemsize:
-                raise VirtualMeshFormatError(f'geometry file is corrupt (field "{f["name"]}" has the wrong size)')
-            arrays[f["name"]] = np.frombuffer(blob, dt).astype(dt.newbyteorder("="))
-        elif enc == "meshlet-indices":
-            need = [arrays.get(k) for k in ("meshletInfo", "meshletVertices", "meshletTriangles")]
-            if any(a is None for a in need):
-                raise VirtualMeshFormatError(f'geometry file is corrupt ("{f["name"]}" needs the meshlet arrays)')
-            arrays[f["name"]] = rebuild_indices(f["length"], *need)
-        elif enc in ("meshopt-vertex", "meshlet-triangles"):
-            raise VirtualMeshFormatError(f'field "{f["name"]}" uses the meshoptimizer codec "{enc}", which this reader '
-                                         f"does not have (bake the file with compress: false)")
-        else:
-            raise VirtualMeshFormatError(f'unknown encoding "{enc}" for field "{f["name"]}"')
+        try:
+            arrays[f["name"]] = _decode_field(f, blob, dt, arrays)
+        except meshopt.CodecError as e:
+            raise VirtualMeshFormatError(f'geometry file is corrupt (field "{f["name"]}": {e})') from None
     return {k: (arrays[k] if k in arrays else header["values"].get(k)) for k in header["keys"]}
 
 
