@@ -688,9 +688,11 @@ def run_occluders(ruins, args, flush, stream):
                   for k, c in enumerate(cams)]
     vg.cut(prev, first_slot=0, stream=sp, graph=True)  # the previous frame's cuts in slots 0..P-1
 
+    # the 32 images in one call (vgc_occluder_depth_batch), its arguments packed once
+    first_frame = engine.OccluderBatch(vg, list(range(P)), cams, [d.data_ptr() for d in depth])
+
     def occluder_pass():
-        for k in range(P):
-            vg.occluder_depth(k, cams[k], depth[k].data_ptr(), W, H, stream=sp)
+        first_frame.run(W, H, stream=sp)
 
     def timed(fn):
         for _ in range(max(3, args.warmup)):
@@ -716,12 +718,88 @@ def run_occluders(ruins, args, flush, stream):
     torch.cuda.synchronize()
     drawn_open = [vg.read_stats(P + k)["drawn"][0] for k in range(P)]
     covered = statistics.mean(float((d < 1).float().mean()) for d in depth)
+
+    # End to end, the loop as a renderer runs it through the C ABI: each step uploads the views (host structs), draws
+    # every view's previous cut as occluders with its camera, cuts with the HZB built from those images, and reads
+    # the counters and draw lists back into pinned host memory; cuts alternate between two slot sets, so each step's
+    # occluders are the previous step's cuts. No depth image crosses PCIe.
+    rt = ctypes.CDLL("libcudart.so.12")
+    rt.cudaMemcpyAsync.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_void_p]
+    cw = engine.COUNTER_HEADER + vg.output(0).mesh_slots * 8
+    cap = 1 << 18
+    h_counters = torch.empty(2 * P * cw, dtype=torch.int32).pin_memory()
+    h_lists = torch.empty((P, cap, 4), dtype=torch.int32).pin_memory()
+    loop_views = [[engine.make_view(c, engine.ViewParams(error_threshold=1.0, hzb=k, state_slot=s * P + k),
+                                    depth=(depth[k].data_ptr(), W, H)) for k, c in enumerate(cams)] for s in (0, 1)]
+    d2h = [0]
+    outs = [vg.output(k) for k in range(2 * P)]
+
+    occl = [engine.OccluderBatch(vg, [src * P + k for k in range(P)], cams, [d.data_ptr() for d in depth])
+            for src in (0, 1)]
+
+    def loop_device(i):
+        src, dst = (i + 1) % 2, i % 2
+        occl[src].run(W, H, stream=sp)
+        vg.cut(loop_views[dst], first_slot=dst * P, stream=sp, graph=True)
+        return dst
+
+    def loop_step(i):
+        dst = loop_device(i)
+        rt.cudaMemcpyAsync(h_counters.data_ptr(), outs[dst * P].counters, P * cw * 4, 2, sp)
+        stream.synchronize()
+        c = h_counters.numpy()[:P * cw].reshape(P, cw)
+        nbytes = P * cw * 4
+        for k in range(P):
+            n = min(int(c[k, 2]), cap)
+            if n:
+                rt.cudaMemcpyAsync(h_lists[k].data_ptr(), outs[dst * P + k].draw_list[0], n * 16, 2, sp)
+                nbytes += n * 16
+        d2h[0] = nbytes
+
+    vg.cut(prev, first_slot=P, stream=sp, graph=True)  # slot set 1 holds "the previous frame" for step 0
+    for i in range(max(3, args.warmup)):
+        loop_step(i)
+    torch.cuda.synchronize()
+    a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for i in range(args.steps):
+        loop_step(i)
+    z.record(stream)
+    z.synchronize()
+    loop_ms = a.elapsed_time(z)
+    # the same loop on the device alone (L2 flushed before each step), and its occluder pass alone: the steady state,
+    # where each view's occluders are its previous occlusion-culled cut
+    steady_ms, steady_occ = [], []
+    for i in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        a, m, z = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        a.record(stream)
+        src, dst = (i + 1) % 2, i % 2
+        occl[src].run(W, H, stream=sp)
+        m.record(stream)
+        vg.cut(loop_views[dst], first_slot=dst * P, stream=sp, graph=True)
+        z.record(stream)
+        z.synchronize()
+        steady_ms.append(a.elapsed_time(z))
+        steady_occ.append(a.elapsed_time(m))
+    steady_drawn = statistics.mean(vg.read_stats(((args.steps - 1) % 2) * P + k)["drawn"][0] for k in range(P))
     vg.dispose()
     return dict(workload=f"two-pass occlusion, ruins-like scene, {P} poses: previous camera cut drawn depth-only with "
                          f"the next pose at {W}x{H}, HZB built in the batched cut's launch sequence",
                 occluder_pass_ms_per_view=occ_ms / P, two_pass_ms_per_step=both_ms, views_per_sec=P / (both_ms / 1e3),
                 occluder_coverage=covered, occluded_instances_mean=statistics.mean(occluded),
-                drawn_meshlets_with_hzb=statistics.mean(drawn_hzb), drawn_meshlets_without=statistics.mean(drawn_open))
+                drawn_meshlets_with_hzb=statistics.mean(drawn_hzb), drawn_meshlets_without=statistics.mean(drawn_open),
+                steady=dict(occluder_pass_ms_per_view=statistics.mean(steady_occ) / P,
+                            ms_per_step=statistics.mean(steady_ms), views_per_sec=P / (statistics.mean(steady_ms) / 1e3),
+                            occluder_meshlets_mean=steady_drawn,
+                            note="each view's occluders are its previous occlusion-culled cut (a renderer's steady "
+                                 "state); the figures above draw an unculled previous cut"),
+                e2e=dict(value=P * args.steps / (loop_ms / 1e3), unit="views/s",
+                         h2d_bytes_per_step=P * ctypes.sizeof(engine.View), d2h_bytes_per_step=int(d2h[0]),
+                         note="two-pass loop through the C ABI: views up, occluder pass from the previous step's cuts, "
+                              "cut with the HZB built from them, counters and draw lists back to pinned host memory; "
+                              "no depth upload; one event pair around all steps"))
 
 
 def run_visibility(ruins, args, flush, stream):
@@ -906,7 +984,6 @@ class ServeDriver:
     def run(self, items, paced: bool):
         base = self.server.stats()
         tickets = [0] * len(items)
-        results = [None] * len(items)
         ready = threading.Semaphore(0)
 
         def submitter():
@@ -916,18 +993,22 @@ class ServeDriver:
                     dt = t0 + at - time.perf_counter()
                     if dt <= 0:
                         break
-                    if dt > 3e-4:
-                        time.sleep(dt - 2e-4)
+                    # a sleep, even of 0, lets the waiting thread take the interpreter lock: a spin without one
+                    # keeps it for the interpreter's whole switch interval and starves the releases
+                    time.sleep(dt - 2e-4 if dt > 3e-4 else 0)
                 tickets[j] = self.server.submit(self.scene_of[i], self.views[i])
                 ready.release()
 
         th = threading.Thread(target=submitter)
         th.start()
+        from vgcut import engine
+        raw = [engine.ServeResult() for _ in items]  # filled as results come, read after the run
         for j in range(len(items)):
             ready.acquire()
-            results[j] = self.server.wait(tickets[j])
+            self.server.wait_into(tickets[j], raw[j])
             self.server.release(tickets[j])
         th.join()
+        results = [self.server.result_dict(r) for r in raw]
         st = self.server.stats()
         delta = {k: st[k] - base[k] for k in ("batches", "views_launched", "multi_scene_batches")}
         return results, delta, st
@@ -943,19 +1024,26 @@ class ServeDriver:
                     rounds_mean=statistics.mean(r["stats"]["rounds"] for r in results),
                     overflow_share=statistics.mean(1.0 if r["stats"]["overflow"] else 0.0 for r in results))
 
-    def poisson(self, rate: float, n: int, n_requests: int, seed: int = 17):
+    def poisson(self, rate: float, n: int, n_requests: int, seed: int = 17, warmup: int = 200):
+        """Poisson arrivals at `rate`: `warmup` requests at the same rate first (not summarised), then `n`."""
         import numpy as np
-        arrivals = np.cumsum(np.random.default_rng(seed).exponential(1.0 / rate, n))
+        rng = np.random.default_rng(seed)
+        if warmup:
+            w = np.cumsum(rng.exponential(1.0 / rate, warmup))
+            self.run([(float(w[j]), (n + j) % n_requests) for j in range(warmup)], True)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
         res, delta, st = self.run([(float(arrivals[j]), j % n_requests) for j in range(n)], True)
         out = self.summary(res, delta)
-        out.update(offered_per_sec=n / float(arrivals[-1]), requests=n)
+        slow = sorted(range(n), key=lambda j: res[j]["done_us"] - res[j]["submit_us"])[-max(1, n // 100):]
+        out.update(offered_per_sec=n / float(arrivals[-1]), requests=n, warmup_requests=warmup,
+                   slowest_percent_at=[round(float(arrivals[j]) / float(arrivals[-1]), 3) for j in sorted(slow)][:20])
         return out, st
 
 
 # Serving on one scene: output slots enough that admission does not cut batches short while results wait to be read
 # and released, and a linger that lets a short batch fill while another one runs (none when the GPU is idle).
 SERVE_SLOTS = 1024
-SERVE_LINGER_US = 300
+SERVE_LINGER_US = 800
 
 
 def run_serve_ruins(ruins, args, plain_vps: float):

@@ -322,6 +322,12 @@ int vgc_server_destroy(vgc_server *server);
    `stream`. */
 int vgc_occluder_depth(vgc_context *ctx, uint32_t src_slot, const vgc_view *view, float *depth, uint32_t width,
                        uint32_t height, vgc_stream stream);
+/* vgc_occluder_depth for `count` images of one size in one call, in order on `stream`: image i draws output slot
+   src_slots[i] with views[i] into depth[i] (an array of `count` device pointers, in host memory). The same images as
+   count single calls; for a renderer with many views (split screen, probes, a serving batch) it saves the per-call
+   host work. */
+int vgc_occluder_depth_batch(vgc_context *ctx, uint32_t count, const uint32_t *src_slots, const vgc_view *views,
+                             float *const *depth, uint32_t width, uint32_t height, vgc_stream stream);
 
 /* Visibility buffer: a headless consumer of a cut's output, after vgc_expand. Draws the index buffer `indices`
    (device, `capacity` indices) that vgc_expand wrote for output slot `slot` and cut `cut`, region by region as the

@@ -134,3 +134,19 @@ def test_near_plane_clipping_matches_the_oracle(occluding):
     want = oracle_depth(h, 0, near)
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), f"{int((got != want).sum())} pixels differ"
     assert (got < 1e-3).sum() > 20, "clipped triangles reach the near plane"
+
+
+def test_batch_call_equals_single_calls(occluding):
+    """vgc_occluder_depth_batch draws the same images as one vgc_occluder_depth call per image."""
+    import torch
+    h = occluding
+    cams = [moved(c, 1.2, 0.02 * (k + 1)) for k, c in enumerate(h.spec.cameras)]
+    for k, cam in enumerate(h.spec.cameras):
+        h.gpu(cam, engine.ViewParams(error_threshold=1.0), slot=k)
+    single = [gpu_depth(h, k, cams[k]) for k in range(len(cams))]
+    batch = [torch.empty((H, W), dtype=torch.float32, device="cuda") for _ in cams]
+    h.vg.occluder_depth_batch(list(range(len(cams))), cams, [d.data_ptr() for d in batch], W, H)
+    torch.cuda.synchronize()
+    for k, (a, b) in enumerate(zip(single, batch)):
+        assert (a < 1).float().mean() > 0.05
+        assert torch.equal(a.view(torch.int32), b.view(torch.int32)), f"image {k} differs"

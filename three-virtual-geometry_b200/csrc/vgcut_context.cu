@@ -216,6 +216,9 @@ int ensure_state(vgc_context *ctx, uint32_t slot) {
   return VGC_OK;
 }
 
+// the unit list of `n` (view, cell) units and, after it, the overflow bits of its 4 n warp-units
+static size_t unit_bytes(size_t n) { return n * sizeof(uint2) + (n * 4 + 31) / 32 * sizeof(uint32_t); }
+
 int ensure_scratch(vgc_context *ctx, LaunchScratch &s, uint32_t views, size_t units) {
   if (!s.owner) s.owner = ctx;  // growth below is counted where the scratch was first counted
   ctx = s.owner;
@@ -235,12 +238,15 @@ int ensure_scratch(vgc_context *ctx, LaunchScratch &s, uint32_t views, size_t un
   if (units > s.unit_capacity || !s.d_units) {
     if (s.d_units) {
       cudaFree(s.d_units);
-      ctx->bytes -= s.unit_capacity * sizeof(uint2);
+      ctx->bytes -= unit_bytes(s.unit_capacity);
     }
     s.d_units = nullptr;
+    s.d_overflow = nullptr;
     size_t n = std::max<size_t>(units, 32);
-    CUDA_TRY(cudaMalloc(&s.d_units, n * sizeof(uint2)));
-    ctx->bytes += n * sizeof(uint2);
+    CUDA_TRY(cudaMalloc(&s.d_units, unit_bytes(n)));
+    s.d_overflow = reinterpret_cast<uint32_t *>(s.d_units + n);
+    CUDA_TRY(cudaMemset(s.d_overflow, 0, unit_bytes(n) - n * sizeof(uint2)));
+    ctx->bytes += unit_bytes(n);
     s.unit_capacity = n;
   }
   if (!s.d_unit_count) CUDA_TRY(cudaMalloc(&s.d_unit_count, 64));
@@ -586,12 +592,16 @@ int enqueue(vgc_context *ctx, LaunchScratch &s, uint32_t count, cudaStream_t st,
                  [&] { return launch_reset(s.d_views, count, s.d_unit_count, st); }));
   CUDA_TRY(timed(ctx, capture, VGC_KERNEL_CELLS, st,
                  [&] { return launch_cells(S, scenes, s.d_views, count, s.units_total, s.d_units, s.d_unit_count, st); }));
+  const uint32_t redo_grid = (uint32_t)ctx->sm_count * 2;
   if (s.any_budget) {  // the triangleBudget search: histogram pass, then the threshold of each budget view
     CUDA_TRY(timed(ctx, capture, VGC_KERNEL_BUDGET, st, [&] {
       cudaError_t e = launch_instances(S, scenes, s.d_views, s.d_units, s.d_unit_count, s.d_chunks, s.chunk_capacity, -1,
-                                       select_grid, st, s.chunk_shift);
+                                       select_grid, s.d_overflow, st, s.chunk_shift);
       if (e == cudaSuccess)
         e = launch_chunks(S, scenes, s.d_views, s.d_chunks, s.d_unit_count, s.chunk_capacity, -1, chunk_grid, st);
+      if (e == cudaSuccess)
+        e = launch_instances_redo(S, scenes, s.d_views, s.d_units, s.d_unit_count, s.d_chunks, s.chunk_capacity, -1,
+                                  s.d_overflow, redo_grid, st, s.chunk_shift);
       if (e == cudaSuccess) e = launch_budget(s.d_views, count, s.d_unit_count, st);
       return e;
     }));
@@ -599,10 +609,15 @@ int enqueue(vgc_context *ctx, LaunchScratch &s, uint32_t count, cudaStream_t st,
   for (int round = 0; round < 3; round++) {
     CUDA_TRY(timed(ctx, capture, round == 0 ? VGC_KERNEL_SELECT0 : VGC_KERNEL_SELECT_RETRY, st, [&] {
       return launch_instances(S, scenes, s.d_views, s.d_units, s.d_unit_count, s.d_chunks, s.chunk_capacity, round,
-                              select_grid, st, s.chunk_shift);
+                              select_grid, s.d_overflow, st, s.chunk_shift);
     }));
     CUDA_TRY(timed(ctx, capture, round == 0 ? VGC_KERNEL_CHUNKS0 : VGC_KERNEL_SELECT_RETRY, st, [&] {
       return launch_chunks(S, scenes, s.d_views, s.d_chunks, s.d_unit_count, s.chunk_capacity, round, chunk_grid, st);
+    }));
+    // units whose items did not fit the queue (returns at once when there are none)
+    CUDA_TRY(timed(ctx, capture, VGC_KERNEL_SELECT_RETRY, st, [&] {
+      return launch_instances_redo(S, scenes, s.d_views, s.d_units, s.d_unit_count, s.d_chunks, s.chunk_capacity,
+                                   round, s.d_overflow, redo_grid, st, s.chunk_shift);
     }));
     CUDA_TRY(timed(ctx, capture, VGC_KERNEL_FINISH, st, [&] {
       return launch_finish(s.d_views, count, s.d_unit_count, round, st);
@@ -1238,7 +1253,7 @@ int vgc_batch_destroy(vgc_batch *b) {
   if (b->graph) cudaGraphDestroy(b->graph);
   if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
   if (b->scratch.d_views) b->ctx->bytes -= sizeof(ViewConst) * b->scratch.view_capacity;
-  if (b->scratch.d_units) b->ctx->bytes -= b->scratch.unit_capacity * sizeof(uint2);
+  if (b->scratch.d_units) b->ctx->bytes -= unit_bytes(b->scratch.unit_capacity);
   free_scratch(b->scratch);
   delete b;
   return VGC_OK;
@@ -1424,7 +1439,8 @@ constexpr uint32_t kNoAllocMaxUnits = 65536;                        // visible (
 constexpr uint32_t kNoAllocMaxChunks = 65536;                       // meshlet work queue entries (beyond: tested in place)
 constexpr size_t kNoAllocUnits = 1024;
 constexpr size_t kNoAllocChunks = kNoAllocUnits + (size_t)kNoAllocMaxUnits * sizeof(uint2);
-constexpr size_t kNoAllocBytes = kNoAllocChunks + (size_t)kNoAllocMaxChunks * sizeof(uint4);  // 1.5 MiB
+constexpr size_t kNoAllocOverflow = kNoAllocChunks + (size_t)kNoAllocMaxChunks * sizeof(uint4);
+constexpr size_t kNoAllocBytes = kNoAllocOverflow + (size_t)kNoAllocMaxUnits * 4 / 32 * sizeof(uint32_t);  // 1.53 MiB
 static_assert(sizeof(ViewConst) <= kNoAllocUnits - kNoAllocView, "view constants must fit their scratch slot");
 static_assert(kNoAllocChunks % 256 == 0, "chunk queue must stay 256-byte aligned");
 
@@ -1506,6 +1522,8 @@ extern "C" int vgc_cut_noalloc(vgc_context *ctx, const vgc_view *view, uint32_t 
   ViewConst *d_view = (ViewConst *)(scratch + kNoAllocView);
   uint2 *units = (uint2 *)(scratch + kNoAllocUnits);
   uint4 *chunks = (uint4 *)(scratch + kNoAllocChunks);
+  uint32_t *overflow = (uint32_t *)(scratch + kNoAllocOverflow);  // zero at load; every pass leaves it zero
+  const uint32_t redo_grid = (uint32_t)ctx->sm_count * 2;
   // the constants go in by value (k_reset clears the control words)
   k_noalloc_store_view<<<1, 128, 0, st>>>(k, d_view);
   CUDA_TRY(cudaGetLastError());
@@ -1517,13 +1535,19 @@ extern "C" int vgc_cut_noalloc(vgc_context *ctx, const vgc_view *view, uint32_t 
   CUDA_TRY(launch_reset(d_view, 1, ctl, st));
   CUDA_TRY(launch_cells(S, nullptr, d_view, 1, cells, units, ctl, st));
   if (view->triangle_budget > 0) {
-    CUDA_TRY(launch_instances(S, nullptr, d_view, units, ctl, chunks, kNoAllocMaxChunks, -1, ctx->select_grid, st));
+    CUDA_TRY(launch_instances(S, nullptr, d_view, units, ctl, chunks, kNoAllocMaxChunks, -1, ctx->select_grid, overflow,
+                              st));
     CUDA_TRY(launch_chunks(S, nullptr, d_view, chunks, ctl, kNoAllocMaxChunks, -1, ctx->chunk_grid, st));
+    CUDA_TRY(launch_instances_redo(S, nullptr, d_view, units, ctl, chunks, kNoAllocMaxChunks, -1, overflow, redo_grid,
+                                   st));
     CUDA_TRY(launch_budget(d_view, 1, ctl, st));
   }
   for (int round = 0; round < 3; round++) {
-    CUDA_TRY(launch_instances(S, nullptr, d_view, units, ctl, chunks, kNoAllocMaxChunks, round, ctx->select_grid, st));
+    CUDA_TRY(launch_instances(S, nullptr, d_view, units, ctl, chunks, kNoAllocMaxChunks, round, ctx->select_grid,
+                              overflow, st));
     CUDA_TRY(launch_chunks(S, nullptr, d_view, chunks, ctl, kNoAllocMaxChunks, round, ctx->chunk_grid, st));
+    CUDA_TRY(launch_instances_redo(S, nullptr, d_view, units, ctl, chunks, kNoAllocMaxChunks, round, overflow,
+                                   redo_grid, st));
     CUDA_TRY(launch_finish(d_view, 1, ctl, round, st));
   }
   return VGC_OK;

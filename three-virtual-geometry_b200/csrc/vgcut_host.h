@@ -61,6 +61,7 @@ struct LaunchScratch {
   ViewConst *h_views = nullptr;  // pinned
   ViewConst *d_views = nullptr;
   uint2 *d_units = nullptr;
+  uint32_t *d_overflow = nullptr;   // after d_units' entries: a bit per warp-unit (launch_instances), zero between passes
   uint32_t *d_unit_count = nullptr;  // control words (see launch_reset)
   uint4 *d_chunks = nullptr;      // meshlet work queue (spans and chunks)
   uint32_t chunk_capacity = 0;    // its entries

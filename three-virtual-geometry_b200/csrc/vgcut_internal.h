@@ -117,4 +117,34 @@ struct ViewConst {
   uint32_t counter_words;   //   counter words of one output slot
 };
 
+#ifdef __CUDACC__
+// Work handed out to warps from a counter, B consecutive pieces at a time (a warp that drew cheap pieces takes more,
+// so a persistent grid finishes together). Lane 0 requests the warp's next batch a whole batch ahead, so the
+// counter's round trip overlaps the work; B > 1 keeps the counter's rate of atomics down when pieces are short.
+// All lanes of the warp call start() and next() together; `i` is the current piece.
+template <uint32_t B>
+struct WarpFeed {
+  uint32_t *ctr;
+  uint32_t ahead;  // lane 0: the batch after the current one
+  uint32_t i, end;
+  __device__ __forceinline__ void start(uint32_t *counter) {
+    ctr = counter;
+    ahead = 0;
+    if ((threadIdx.x & 31) == 0) ahead = atomicAdd(ctr, 1u);
+    take();
+  }
+  __device__ __forceinline__ void take() {
+    const uint32_t b = __shfl_sync(0xffffffffu, ahead, 0);
+    if ((threadIdx.x & 31) == 0) ahead = atomicAdd(ctr, 1u);
+    i = b * B;
+    end = i + B;
+  }
+  // moves to the next piece and returns it
+  __device__ __forceinline__ uint32_t next() {
+    if (++i == end) take();
+    return i;
+  }
+};
+#endif
+
 }  // namespace vgc

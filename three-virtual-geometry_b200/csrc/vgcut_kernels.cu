@@ -296,9 +296,11 @@ __device__ __forceinline__ unsigned long long *queue_counter(uint32_t *ctl) {
   return reinterpret_cast<unsigned long long *>(ctl + 4);
 }
 
-// Work is handed out one warp-sized piece at a time from a counter (ctl[8]: chunks, ctl[9]: instance units), so
-// warps that drew cheap pieces take more and the persistent grid ends together; the counters empty with the queue.
+// Work is handed out to warps from counters (WarpFeed; ctl[8]: chunks, ctl[9]: instance units, ctl[11]: redo words),
+// so warps that drew cheap pieces take more and the persistent grid ends together; the counters empty with the
+// queue.
 constexpr uint32_t kCtlNextChunk = 8, kCtlNextUnit = 9;
+constexpr uint32_t kCtlOverflowed = 10, kCtlNextRedo = 11;  // a unit's items did not fit the queue; k_instances_redo's counter
 __device__ __forceinline__ uint32_t warp_grab(uint32_t *ctl, uint32_t word) {
   uint32_t i = 0;
   if ((threadIdx.x & 31) == 0) i = atomicAdd(ctl + word, 1u);
@@ -314,6 +316,8 @@ __device__ __forceinline__ void retire_queue(uint32_t *ctl) {
   *queue_counter(ctl) = 0;
   ctl[kCtlNextChunk] = 0;
   ctl[kCtlNextUnit] = 0;
+  ctl[kCtlOverflowed] = 0;
+  ctl[kCtlNextRedo] = 0;
 }
 
 // Band values of a view for the current round, written by k_reset and by the capacity check (dyn[1..5]).
@@ -728,39 +732,32 @@ __device__ __forceinline__ void drain_queue(const Scene &S, const ViewConst &V, 
   }
 }
 
-// One warp per 32 instances of a visible (view, cell) unit: the instance pass of GeometryPool.ts:846-913. Fast-path
-// instances emit their meshlets; the others hand their level range to k_chunks as chunks of <= 2^chunk_shift
-// meshlets.
-// HIST: the budget search's pass (views with a triangleBudget only): the camera cut's level range over the whole
-// threshold range, no fast path, no counters.
-template <bool HIST, bool MULTI>
-__global__ void __launch_bounds__(128, MULTI ? 5 : 6) k_instances(Scene S0, const Scene *__restrict__ scenes,
-                                                   const ViewConst *__restrict__ views,
-                                                   const HzbDesc *__restrict__ hzbs0, const uint2 *__restrict__ units,
-                                                   uint32_t *__restrict__ ctl, uint4 *__restrict__ queue,
-                                                   uint32_t capacity, int round, uint32_t chunk_shift) {
-  __shared__ WarpStage stage[4];
-  WarpStage &ws = stage[threadIdx.x >> 5];
-  if (round > 0 && ctl[round] == 0) return;  // no view redoes a cut in this round
+// One warp-unit w (32 instances of a visible (view, cell) unit) of the instance pass. REDO: a unit whose items did not
+// fit the chunk queue in this pass (marked in `overflow`): its instance tests are repeated (the same arithmetic, so
+// the same items) and its items tested in place; its counters and fast-path meshlets were already emitted.
+template <bool HIST, bool MULTI, bool REDO>
+__device__ __forceinline__ void instance_unit(const Scene &S0, const Scene *__restrict__ scenes,
+                                              const ViewConst *__restrict__ views, const HzbDesc *__restrict__ hzbs0,
+                                              const uint2 *__restrict__ units, uint32_t *__restrict__ ctl,
+                                              uint4 *__restrict__ queue, uint32_t capacity, int round,
+                                              uint32_t chunk_shift, uint32_t *__restrict__ overflow, WarpStage *ws,
+                                              uint32_t w) {
   const uint32_t lane = threadIdx.x & 31;
-  const uint32_t work = ctl[0] * 4;
-  // the next unit is drawn at the top of each one, so its counter's round trip overlaps the current unit
-  for (uint32_t w = warp_grab(ctl, kCtlNextUnit), w_next; w < work; w = w_next) {
-    w_next = warp_grab(ctl, kCtlNextUnit);
+  {
     const uint2 unit = units[w >> 2];
     const ViewConst &V = views[unit.x];
-    if (HIST && !(V.budget > 0.0f)) continue;
+    if (HIST && !(V.budget > 0.0f)) return;
     bool redo0 = true, redo1 = !HIST;
     if (round > 0) {
       redo0 = V.counters[VGC_COUNTER_REDO0] != 0;
       redo1 = V.counters[VGC_COUNTER_REDO1] != 0;
-      if (!redo0 && !redo1) continue;
+      if (!redo0 && !redo1) return;
     }
     const auto &S = SceneOf<MULTI>::get(S0, scenes, V);
     const HzbDesc *__restrict__ hzbs = SceneOf<MULTI>::hzbs(hzbs0, S);
     const CellRec cell = S.cells[unit.y];
     const uint32_t il = ((w & 3u) << 5) + lane;
-    if (((w & 3u) << 5) >= cell.count) continue;
+    if (((w & 3u) << 5) >= cell.count) return;
     const MeshRec &mesh = S.meshes[cell.slot];
     const ViewBands b = bands_of(V);
     const uint32_t levels = min(mesh.level_count, kMaxLevels);
@@ -826,7 +823,7 @@ __global__ void __launch_bounds__(128, MULTI ? 5 : 6) k_instances(Scene S0, cons
     }
     const bool surv0 = r0.last > r0.first, surv1 = r1.last > r1.first;
     const bool item0 = surv0 && !fast0, item1 = surv1 && !fast1;
-    if (!HIST) {
+    if (!HIST && !REDO) {
     // warp totals for the view's counters (one atomic per counter and warp)
     const uint32_t n_occl = __popc(__ballot_sync(0xffffffffu, occluded_now));
     const uint32_t n_s0 = __popc(__ballot_sync(0xffffffffu, surv0)), n_s1 = __popc(__ballot_sync(0xffffffffu, surv1));
@@ -856,50 +853,59 @@ __global__ void __launch_bounds__(128, MULTI ? 5 : 6) k_instances(Scene S0, cons
     const uint32_t n0 = item0 ? t0l - t0f : 0u, n1 = item1 ? t1l - t1f : 0u;
     const uint32_t s0 = warp_scan_incl(n0) - n0, s1 = warp_scan_incl(n1) - n1;  // starts in the laid-out items
     const uint32_t T0 = __shfl_sync(0xffffffffu, s0 + n0, 31), T1 = __shfl_sync(0xffffffffu, s1 + n1, 31);
-    if (T0 + T1 == 0) continue;
+    if (T0 + T1 == 0) return;
     const uint32_t chunk = 1u << chunk_shift;
     const uint32_t p0 = n0 ? ((s0 + n0 - 1) >> chunk_shift) - (s0 >> chunk_shift) + 1 : 0u;  // spans of this lane's item
     const uint32_t p1 = n1 ? ((s1 + n1 - 1) >> chunk_shift) - (s1 >> chunk_shift) + 1 : 0u;
     const uint32_t q0 = warp_scan_incl(p0) - p0, q1 = warp_scan_incl(p1) - p1;
     const uint32_t P0 = __shfl_sync(0xffffffffu, q0 + p0, 31), P1 = __shfl_sync(0xffffffffu, q1 + p1, 31);
     const uint32_t N0 = (T0 + chunk - 1) >> chunk_shift, N1 = (T1 + chunk - 1) >> chunk_shift;
-    unsigned long long got = 0;
-    if (lane == 0)
-      got = atomicAdd(queue_counter(ctl), ((unsigned long long)(N0 + N1) << 32) | (unsigned long long)(P0 + P1));
-    got = __shfl_sync(0xffffffffu, got, 0);
-    const uint32_t span_at = uint32_t(got), chunk_at = uint32_t(got >> 32);
-    const WorkQueue Q = work_queue(queue, capacity);
-    if (span_at + P0 + P1 <= Q.span_cap && chunk_at + N0 + N1 <= Q.chunk_cap) {
+    if (!REDO) {
+      unsigned long long got = 0;
+      if (lane == 0)
+        got = atomicAdd(queue_counter(ctl), ((unsigned long long)(N0 + N1) << 32) | (unsigned long long)(P0 + P1));
+      got = __shfl_sync(0xffffffffu, got, 0);
+      const uint32_t span_at = uint32_t(got), chunk_at = uint32_t(got >> 32);
+      const WorkQueue Q = work_queue(queue, capacity);
+      if (span_at + P0 + P1 <= Q.span_cap && chunk_at + N0 + N1 <= Q.chunk_cap) {
 #pragma unroll
-      for (uint32_t cut = 0; cut < 2; cut++) {
-        const uint32_t n = cut ? n1 : n0, st = cut ? s1 : s0, np = cut ? p1 : p0;
-        const uint32_t first = cut ? t1f : t0f;
-        const uint32_t flags = il | ((cut ? inside1 : inside0) ? 1u << 7 : 0u);
-        uint4 *dst = Q.spans + span_at + (cut ? P0 + q1 : q0);
-        for (uint32_t k = 0; k < np; k++) {
-          const uint32_t win = (st >> chunk_shift) + k;
-          const uint32_t lo = max(st, win << chunk_shift), hi = min(st + n, (win + 1) << chunk_shift);
-          dst[k] = make_uint4(flags, first + (lo - st), hi - lo, 0u);
+        for (uint32_t cut = 0; cut < 2; cut++) {
+          const uint32_t n = cut ? n1 : n0, st = cut ? s1 : s0, np = cut ? p1 : p0;
+          const uint32_t first = cut ? t1f : t0f;
+          const uint32_t flags = il | ((cut ? inside1 : inside0) ? 1u << 7 : 0u);
+          uint4 *dst = Q.spans + span_at + (cut ? P0 + q1 : q0);
+          for (uint32_t k = 0; k < np; k++) {
+            const uint32_t win = (st >> chunk_shift) + k;
+            const uint32_t lo = max(st, win << chunk_shift), hi = min(st + n, (win + 1) << chunk_shift);
+            dst[k] = make_uint4(flags, first + (lo - st), hi - lo, 0u);
+          }
+          // chunk t starts at the span holding laid-out position t * chunk: that of the last item starting at or
+          // before it, plus the windows that item crossed before t
+          const uint32_t N = cut ? N1 : N0;
+          for (uint32_t t = 0; t < N; t++) {
+            const uint32_t X = t << chunk_shift;
+            const uint32_t owner = 31 - __clz(__ballot_sync(0xffffffffu, st <= X));
+            const uint32_t first_span = __shfl_sync(0xffffffffu, cut ? q1 : q0, owner) + t -
+                                        (__shfl_sync(0xffffffffu, st, owner) >> chunk_shift);
+            const uint32_t spans = __popc(__ballot_sync(0xffffffffu, n > 0 && st < X + chunk && st + n > X));
+            if (lane == 0)
+              Q.chunks[chunk_at + (cut ? N0 : 0u) + t] =
+                  make_uint4(unit.x, unit.y, cut | ((cut == 0 && occl_on) ? 2u : 0u) | (spans << 8),
+                             span_at + (cut ? P0 : 0u) + first_span);
+          }
         }
-        // chunk t starts at the span holding laid-out position t * chunk: that of the last item starting at or
-        // before it, plus the windows that item crossed before t
-        const uint32_t N = cut ? N1 : N0;
-        for (uint32_t t = 0; t < N; t++) {
-          const uint32_t X = t << chunk_shift;
-          const uint32_t owner = 31 - __clz(__ballot_sync(0xffffffffu, st <= X));
-          const uint32_t first_span = __shfl_sync(0xffffffffu, cut ? q1 : q0, owner) + t -
-                                      (__shfl_sync(0xffffffffu, st, owner) >> chunk_shift);
-          const uint32_t spans = __popc(__ballot_sync(0xffffffffu, n > 0 && st < X + chunk && st + n > X));
-          if (lane == 0)
-            Q.chunks[chunk_at + (cut ? N0 : 0u) + t] =
-                make_uint4(unit.x, unit.y, cut | ((cut == 0 && occl_on) ? 2u : 0u) | (spans << 8),
-                           span_at + (cut ? P0 : 0u) + first_span);
-        }
+        return;
       }
-    } else {
-      // the queue is full: chunk slots reserved below its capacity become empty records, the items are tested here
+      // the queue is full: chunk slots reserved below its capacity become empty records, and the unit is marked for
+      // k_instances_redo, which tests its items in place
       for (uint32_t t = lane; t < N0 + N1; t += 32)
         if (chunk_at + t < Q.chunk_cap) Q.chunks[chunk_at + t] = make_uint4(0u, 0u, 0u, 0u);
+      if (lane == 0) {
+        atomicOr(overflow + (w >> 5), 1u << (w & 31));
+        ctl[kCtlOverflowed] = 1;
+      }
+    }
+    if (REDO) {
       uint32_t over = __ballot_sync(0xffffffffu, n0 + n1 > 0);
       while (over) {
         const uint32_t j = __ffs(over) - 1;
@@ -912,9 +918,56 @@ __global__ void __launch_bounds__(128, MULTI ? 5 : 6) k_instances(Scene S0, cons
         const bool jin1 = __shfl_sync(0xffffffffu, inside1 ? 1 : 0, j) != 0;
         const uint32_t f0 = __shfl_sync(0xffffffffu, t0f, j), c0 = __shfl_sync(0xffffffffu, n0, j);
         const uint32_t f1 = __shfl_sync(0xffffffffu, t1f, j), c1 = __shfl_sync(0xffffffffu, n1, j);
-        if (c0) warp_item<HIST>(S, V, hzbs, ws, cell.slot, 0, occl_on, jin0, vmj, inst, f0, c0);
-        if (c1) warp_item<HIST>(S, V, hzbs, ws, cell.slot, 1, false, jin1, vmj, inst, f1, c1);
+        if (c0) warp_item<HIST>(S, V, hzbs, *ws, cell.slot, 0, occl_on, jin0, vmj, inst, f0, c0);
+        if (c1) warp_item<HIST>(S, V, hzbs, *ws, cell.slot, 1, false, jin1, vmj, inst, f1, c1);
       }
+    }
+  }
+}
+
+// The instance pass of GeometryPool.ts:846-913, one warp per 32 instances of a visible (view, cell) unit, taken from
+// a counter. Fast-path instances emit their meshlets; the others hand their level range to k_chunks as chunks of
+// <= 2^chunk_shift meshlets. HIST: the budget search's pass (views with a triangleBudget only): the camera cut's
+// level range over the whole threshold range, no fast path, no counters. Without the in-place test of a unit whose
+// items do not fit the queue (k_instances_redo does that), the kernel keeps to 64 registers at 8 blocks per SM.
+template <bool HIST, bool MULTI>
+__global__ void __launch_bounds__(128, MULTI ? 6 : 8) k_instances(Scene S0, const Scene *__restrict__ scenes,
+                                                   const ViewConst *__restrict__ views,
+                                                   const HzbDesc *__restrict__ hzbs0, const uint2 *__restrict__ units,
+                                                   uint32_t *__restrict__ ctl, uint4 *__restrict__ queue,
+                                                   uint32_t capacity, int round, uint32_t chunk_shift,
+                                                   uint32_t *__restrict__ overflow) {
+  if (round > 0 && ctl[round] == 0) return;  // no view redoes a cut in this round
+  const uint32_t work = ctl[0] * 4;
+  WarpFeed<1> feed;
+  feed.start(ctl + kCtlNextUnit);
+  for (uint32_t w = feed.i; w < work; w = feed.next())
+    instance_unit<HIST, MULTI, false>(S0, scenes, views, hzbs0, units, ctl, queue, capacity, round, chunk_shift,
+                                      overflow, nullptr, w);
+}
+
+// The units k_instances found the chunk queue full for (bits of `overflow`, cleared here), their items tested in place
+// by the whole warp. Launched after each pass's k_chunks; returns at once when no unit overflowed.
+template <bool HIST, bool MULTI>
+__global__ void __launch_bounds__(128, 4) k_instances_redo(Scene S0, const Scene *__restrict__ scenes,
+                                                            const ViewConst *__restrict__ views,
+                                                            const HzbDesc *__restrict__ hzbs0,
+                                                            const uint2 *__restrict__ units, uint32_t *__restrict__ ctl,
+                                                            uint4 *__restrict__ queue, uint32_t capacity, int round,
+                                                            uint32_t chunk_shift, uint32_t *__restrict__ overflow) {
+  __shared__ WarpStage stage[4];
+  if (round > 0 && ctl[round] == 0) return;
+  if (ctl[kCtlOverflowed] == 0) return;
+  const uint32_t words = (ctl[0] * 4 + 31) / 32;
+  for (uint32_t i = warp_grab(ctl, kCtlNextRedo); i < words; i = warp_grab(ctl, kCtlNextRedo)) {
+    uint32_t bits = overflow[i];
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0 && bits) overflow[i] = 0;
+    while (bits) {
+      const uint32_t b = __ffs(bits) - 1;
+      bits &= bits - 1;
+      instance_unit<HIST, MULTI, true>(S0, scenes, views, hzbs0, units, ctl, queue, capacity, round, chunk_shift,
+                                       overflow, &stage[threadIdx.x >> 5], i * 32 + b);
     }
   }
 }
@@ -941,8 +994,9 @@ __global__ void __launch_bounds__(128, MULTI ? 6 : 8) k_chunks(Scene S0, const S
   const WorkQueue Q = work_queue(queue, capacity);
   const uint32_t n_chunks = min(uint32_t(*queue_counter(ctl) >> 32), Q.chunk_cap);
   const uint32_t lane = threadIdx.x & 31;
-  for (uint32_t c = warp_grab(ctl, kCtlNextChunk), c_next; c < n_chunks; c = c_next) {
-    c_next = warp_grab(ctl, kCtlNextChunk);
+  WarpFeed<1> feed;
+  feed.start(ctl + kCtlNextChunk);
+  for (uint32_t c = feed.i; c < n_chunks; c = feed.next()) {
     const uint4 ch = Q.chunks[c];
     const uint32_t ns = ch.z >> 8;
     if (ns == 0) continue;
@@ -1233,13 +1287,13 @@ __device__ __forceinline__ void hzb_store(const HzbDesc &H, float *__restrict__ 
 // edge texels of the same rows (or columns), which the in-range texel's footprint already contains, so the max over
 // the 2x2 block equals the max over its clamped reads. Level 3 is warp-local (a warp holds two rows of level 2); one
 // barrier hands the tile's 8x8 level-3 texels to warp 0 for levels 4..6.
-__device__ __forceinline__ void hzb_tile64(const float *__restrict__ depth, const HzbDesc &H, float *__restrict__ out,
-                                           bool copy_mip0, uint32_t ox, uint32_t oy, float (*s3)[9]) {
-  const uint32_t t = threadIdx.x, tx = t & 15u, ty = t >> 4, lane = t & 31u, warp = t >> 5;
+// This thread's 4x4 patch of mip 0 of the tile at (ox, oy) (loads clamped to the image).
+__device__ __forceinline__ void hzb_load(const float *__restrict__ depth, const HzbDesc &H, uint32_t ox, uint32_t oy,
+                                         float v[4][4]) {
+  const uint32_t t = threadIdx.x, tx = t & 15u, ty = t >> 4;
   const uint32_t W = H.w[0], Hh = H.h[0];
   const uint32_t gx = ox + 4 * tx, gy = oy + 4 * ty;
   const bool vec = (W & 3u) == 0 && (reinterpret_cast<uintptr_t>(depth) & 15u) == 0 && gx + 3 < W;
-  float v[4][4];
 #pragma unroll
   for (int r = 0; r < 4; r++) {
     const uint32_t y = min(gy + r, Hh - 1);
@@ -1252,6 +1306,16 @@ __device__ __forceinline__ void hzb_tile64(const float *__restrict__ depth, cons
       for (int c = 0; c < 4; c++) v[r][c] = __ldg(row + min(gx + c, W - 1));
     }
   }
+}
+
+// Mips 0..6 of the tile at (ox, oy) from the patches hzb_load read (every thread of the block calls it).
+__device__ __forceinline__ void hzb_tile64(const float *__restrict__ depth, const HzbDesc &H, float *__restrict__ out,
+                                           bool copy_mip0, uint32_t ox, uint32_t oy, float (*s3)[9],
+                                           const float (&v)[4][4]) {
+  const uint32_t t = threadIdx.x, tx = t & 15u, ty = t >> 4, lane = t & 31u, warp = t >> 5;
+  const uint32_t W = H.w[0], Hh = H.h[0];
+  const uint32_t gx = ox + 4 * tx, gy = oy + 4 * ty;
+  const bool vec = (W & 3u) == 0 && (reinterpret_cast<uintptr_t>(depth) & 15u) == 0 && gx + 3 < W;
   if (copy_mip0) {
     float *o0 = out + H.off[0];
 #pragma unroll
@@ -1306,10 +1370,24 @@ __device__ __forceinline__ void hzb_tile64(const float *__restrict__ depth, cons
   if (lane == 0) hzb_store(H, out, 6, ox >> 6, oy >> 6, m6);
 }
 
+// Two vertically adjacent tiles per block: both tiles' loads are in flight before the first tile is reduced.
+__device__ __forceinline__ void hzb_tile_pair(const float *__restrict__ depth, const HzbDesc &H, float *__restrict__ out,
+                                              bool copy_mip0, uint32_t ox, uint32_t oy, float (*s3)[9]) {
+  const bool second = oy + kHzbTile < H.h[0];  // uniform over the block
+  float a[4][4], b[4][4];
+  hzb_load(depth, H, ox, oy, a);
+  if (second) hzb_load(depth, H, ox, oy + kHzbTile, b);
+  hzb_tile64(depth, H, out, copy_mip0, ox, oy, s3, a);
+  if (second) {
+    __syncthreads();  // warp 0 has read the first tile's level 3 from s3
+    hzb_tile64(depth, H, out, copy_mip0, ox, oy + kHzbTile, s3, b);
+  }
+}
+
 __global__ void __launch_bounds__(256) k_hzb_tiles(const float *__restrict__ depth, HzbDesc H, float *__restrict__ out,
                                                    int copy_mip0) {
   __shared__ float s3[8][9];
-  hzb_tile64(depth, H, out, copy_mip0 != 0, blockIdx.x * kHzbTile, blockIdx.y * kHzbTile, s3);
+  hzb_tile_pair(depth, H, out, copy_mip0 != 0, blockIdx.x * kHzbTile, blockIdx.y * 2 * kHzbTile, s3);
 }
 
 // The HZB builds of a batch: grid.z = view, views without a depth image skip.
@@ -1318,9 +1396,9 @@ __global__ void __launch_bounds__(256) k_hzb_tiles_views(const ViewConst *__rest
   const ViewConst &V = views[blockIdx.z];
   if (!V.build_hzb) return;
   const HzbDesc &H = *V.hzb_desc;
-  const uint32_t ox = blockIdx.x * kHzbTile, oy = blockIdx.y * kHzbTile;
+  const uint32_t ox = blockIdx.x * kHzbTile, oy = blockIdx.y * 2 * kHzbTile;
   if (ox >= H.w[0] || oy >= H.h[0]) return;
-  hzb_tile64(V.depth, H, const_cast<float *>(H.data), true, ox, oy, s3);
+  hzb_tile_pair(V.depth, H, const_cast<float *>(H.data), true, ox, oy, s3);
 }
 
 __global__ void __launch_bounds__(1024) k_hzb_tail_views(const ViewConst *__restrict__ views) {
@@ -1551,23 +1629,48 @@ cudaError_t configure_select(bool multi, int *instances_per_sm, int *chunks_per_
 template <bool MULTI>
 static void instances_kernel(const Scene &S, const Scene *scenes, const ViewConst *views, const uint2 *units,
                              uint32_t *ctl, uint4 *queue, uint32_t capacity, int round, uint32_t grid,
-                             uint32_t chunk_shift, cudaStream_t st) {
+                             uint32_t chunk_shift, uint32_t *overflow, cudaStream_t st) {
   if (round < 0)  // the budget search's pass
     k_instances<true, MULTI><<<grid, 128, 0, st>>>(S, scenes, views, S.hzbs, units, ctl, queue, capacity, 0,
-                                                   chunk_shift);
+                                                   chunk_shift, overflow);
   else
     k_instances<false, MULTI><<<grid, 128, 0, st>>>(S, scenes, views, S.hzbs, units, ctl, queue, capacity, round,
-                                                    chunk_shift);
+                                                    chunk_shift, overflow);
 }
 
 cudaError_t launch_instances(const Scene &S, const Scene *scenes, const ViewConst *views, const uint2 *units,
                              uint32_t *ctl, uint4 *queue, uint32_t capacity, int round, uint32_t grid,
-                             cudaStream_t st, uint32_t chunk_shift) {
-  if (chunk_shift < kChunkShiftMin || chunk_shift > kChunkShiftMax) return cudaErrorInvalidValue;
+                             uint32_t *overflow, cudaStream_t st, uint32_t chunk_shift) {
+  if (chunk_shift < kChunkShiftMin || chunk_shift > kChunkShiftMax || !overflow) return cudaErrorInvalidValue;
   if (scenes)
-    instances_kernel<true>(S, scenes, views, units, ctl, queue, capacity, round, grid, chunk_shift, st);
+    instances_kernel<true>(S, scenes, views, units, ctl, queue, capacity, round, grid, chunk_shift, overflow, st);
   else
-    instances_kernel<false>(S, nullptr, views, units, ctl, queue, capacity, round, grid, chunk_shift, st);
+    instances_kernel<false>(S, nullptr, views, units, ctl, queue, capacity, round, grid, chunk_shift, overflow, st);
+  return cudaGetLastError();
+}
+
+template <bool MULTI>
+static void instances_redo_kernel(const Scene &S, const Scene *scenes, const ViewConst *views, const uint2 *units,
+                                  uint32_t *ctl, uint4 *queue, uint32_t capacity, int round, uint32_t chunk_shift,
+                                  uint32_t *overflow, uint32_t grid, cudaStream_t st) {
+  if (round < 0)
+    k_instances_redo<true, MULTI><<<grid, 128, 0, st>>>(S, scenes, views, S.hzbs, units, ctl, queue, capacity, 0,
+                                                        chunk_shift, overflow);
+  else
+    k_instances_redo<false, MULTI><<<grid, 128, 0, st>>>(S, scenes, views, S.hzbs, units, ctl, queue, capacity,
+                                                         round, chunk_shift, overflow);
+}
+
+cudaError_t launch_instances_redo(const Scene &S, const Scene *scenes, const ViewConst *views, const uint2 *units,
+                                  uint32_t *ctl, uint4 *queue, uint32_t capacity, int round, uint32_t *overflow,
+                                  uint32_t grid, cudaStream_t st, uint32_t chunk_shift) {
+  if (chunk_shift < kChunkShiftMin || chunk_shift > kChunkShiftMax || !overflow || grid == 0)
+    return cudaErrorInvalidValue;
+  if (scenes)
+    instances_redo_kernel<true>(S, scenes, views, units, ctl, queue, capacity, round, chunk_shift, overflow, grid, st);
+  else
+    instances_redo_kernel<false>(S, nullptr, views, units, ctl, queue, capacity, round, chunk_shift, overflow, grid,
+                                 st);
   return cudaGetLastError();
 }
 
@@ -1608,7 +1711,7 @@ cudaError_t launch_expand(const Scene &S, const ViewConst *view, uint32_t cut, u
 }
 
 cudaError_t launch_hzb(const float *depth, const HzbDesc &H, float *out, int copy_mip0, cudaStream_t st) {
-  dim3 grid((H.w[0] + kHzbTile - 1) / kHzbTile, (H.h[0] + kHzbTile - 1) / kHzbTile);
+  dim3 grid((H.w[0] + kHzbTile - 1) / kHzbTile, (H.h[0] + 2 * kHzbTile - 1) / (2 * kHzbTile));
   k_hzb_tiles<<<grid, 256, 0, st>>>(depth, H, out, copy_mip0);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || H.levels <= kHzbTileLevels) return e;
@@ -1618,7 +1721,7 @@ cudaError_t launch_hzb(const float *depth, const HzbDesc &H, float *out, int cop
 
 cudaError_t launch_hzb_views(const ViewConst *views, uint32_t nviews, uint32_t max_w,
                              uint32_t max_h, bool tail, cudaStream_t st) {
-  dim3 grid((max_w + kHzbTile - 1) / kHzbTile, (max_h + kHzbTile - 1) / kHzbTile, nviews);
+  dim3 grid((max_w + kHzbTile - 1) / kHzbTile, (max_h + 2 * kHzbTile - 1) / (2 * kHzbTile), nviews);
   k_hzb_tiles_views<<<grid, 256, 0, st>>>(views);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || !tail) return e;

@@ -20,9 +20,15 @@ cudaError_t launch_cells(const Scene &S, const Scene *scenes, const ViewConst *v
 // threshold of each budget view.
 cudaError_t launch_budget(const ViewConst *views, uint32_t nviews, uint32_t *ctl, cudaStream_t st);
 // chunk_shift: windows of 2^chunk_shift meshlets per chunk (kChunkShiftMin..Max; the default 9 = 512 meshlets).
+// overflow: a bit per warp-unit (4 per unit of `units`), zero between passes: k_instances marks the units whose
+// items did not fit the queue, and launch_instances_redo (after launch_chunks of the same pass) tests their items
+// in place and clears the bits.
 cudaError_t launch_instances(const Scene &S, const Scene *scenes, const ViewConst *views, const uint2 *units,
                              uint32_t *ctl, uint4 *queue, uint32_t capacity, int round, uint32_t grid,
-                             cudaStream_t st, uint32_t chunk_shift = kChunkShiftDefault);
+                             uint32_t *overflow, cudaStream_t st, uint32_t chunk_shift = kChunkShiftDefault);
+cudaError_t launch_instances_redo(const Scene &S, const Scene *scenes, const ViewConst *views, const uint2 *units,
+                                  uint32_t *ctl, uint4 *queue, uint32_t capacity, int round, uint32_t *overflow,
+                                  uint32_t grid, cudaStream_t st, uint32_t chunk_shift = kChunkShiftDefault);
 // The meshlet work queue (spans and chunks) lives in `queue`, `capacity` uint4 entries; ctl[4..5] counts it.
 cudaError_t launch_chunks(const Scene &S, const Scene *scenes, const ViewConst *views, uint4 *queue,
                           uint32_t *ctl, uint32_t capacity, int round, uint32_t grid, cudaStream_t st);

@@ -675,16 +675,10 @@ static int raster_queues(vgc_context *ctx, RasterArgs &R) {
   return VGC_OK;
 }
 
-extern "C" int vgc_occluder_depth(vgc_context *ctx, uint32_t src_slot, const vgc_view *view, float *depth,
-                                  uint32_t width, uint32_t height, vgc_stream stream) {
-  if (!ctx || !view || !depth) return fail(VGC_INVALID_ARG, "null argument");
-  if (width == 0 || height == 0 || width > 16384 || height > 16384)
-    return fail(VGC_INVALID_ARG, "occluder depth size must be 1..16384 per side");
-  if (src_slot >= ctx->out_slots) return fail(VGC_NOT_FOUND, "output slot not allocated");
-  cudaSetDevice(ctx->device);
-  int rc = sync_scene(ctx);
-  if (rc) return rc;
-  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+// One image of the occluder pass, its arguments checked (the launches only).
+static int occluder_depth_one(vgc_context *ctx, uint32_t src_slot, const vgc_view *view, float *depth, uint32_t width,
+                              uint32_t height, cudaStream_t st) {
+  int rc;
   OccluderArgs O{};
   for (int r = 0; r < 4; r++)
     for (int c = 0; c < 4; c++) {
@@ -718,6 +712,40 @@ extern "C" int vgc_occluder_depth(vgc_context *ctx, uint32_t src_slot, const vgc
   CUDA_TRY(cudaGetLastError());
   k_raster_queued<false><<<ctx->sm_count * std::max(1, per_sm[1]), 128, 0, st>>>(R);
   CUDA_TRY(cudaGetLastError());
+  return VGC_OK;
+}
+
+static int occluder_checks(vgc_context *ctx, uint32_t src_slot, const vgc_view *view, const float *depth,
+                           uint32_t width, uint32_t height) {
+  if (!ctx || !view || !depth) return fail(VGC_INVALID_ARG, "null argument");
+  if (width == 0 || height == 0 || width > 16384 || height > 16384)
+    return fail(VGC_INVALID_ARG, "occluder depth size must be 1..16384 per side");
+  if (src_slot >= ctx->out_slots) return fail(VGC_NOT_FOUND, "output slot not allocated");
+  return VGC_OK;
+}
+
+extern "C" int vgc_occluder_depth(vgc_context *ctx, uint32_t src_slot, const vgc_view *view, float *depth,
+                                  uint32_t width, uint32_t height, vgc_stream stream) {
+  int rc = occluder_checks(ctx, src_slot, view, depth, width, height);
+  if (rc) return rc;
+  cudaSetDevice(ctx->device);
+  if ((rc = sync_scene(ctx))) return rc;
+  return occluder_depth_one(ctx, src_slot, view, depth, width, height,
+                            stream ? (cudaStream_t)stream : ctx->stream);
+}
+
+extern "C" int vgc_occluder_depth_batch(vgc_context *ctx, uint32_t count, const uint32_t *src_slots,
+                                        const vgc_view *views, float *const *depth, uint32_t width, uint32_t height,
+                                        vgc_stream stream) {
+  if (!ctx || (count && (!src_slots || !views || !depth))) return fail(VGC_INVALID_ARG, "null argument");
+  int rc;
+  for (uint32_t i = 0; i < count; i++)
+    if ((rc = occluder_checks(ctx, src_slots[i], &views[i], depth[i], width, height))) return rc;
+  cudaSetDevice(ctx->device);
+  if ((rc = sync_scene(ctx))) return rc;
+  const cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  for (uint32_t i = 0; i < count; i++)
+    if ((rc = occluder_depth_one(ctx, src_slots[i], &views[i], depth[i], width, height, st))) return rc;
   return VGC_OK;
 }
 

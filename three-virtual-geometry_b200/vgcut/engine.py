@@ -154,6 +154,8 @@ def lib() -> C.CDLL:
         "vgc_debug_scene": ([vp, P(C.c_float), C.c_uint32, P(C.c_float), C.c_uint32, P(C.c_uint32), P(C.c_uint32)], C.c_int),
         "vgc_debug_cells_device": ([vp, P(C.c_float), C.c_uint32, P(C.c_uint32)], C.c_int),
         "vgc_occluder_depth": ([vp, C.c_uint32, P(View), vp, C.c_uint32, C.c_uint32, vp], C.c_int),
+        "vgc_occluder_depth_batch": ([vp, C.c_uint32, P(C.c_uint32), P(View), P(vp), C.c_uint32, C.c_uint32, vp],
+                                     C.c_int),
         "vgc_instances_resort": ([vp, C.c_uint32, P(C.c_uint32)], C.c_int),
         "vgc_visibility": ([vp, C.c_uint32, C.c_uint32, P(View), P(View), vp, C.c_uint64, vp, C.c_uint32, C.c_uint32,
                             C.c_uint32, vp], C.c_int),
@@ -533,6 +535,10 @@ class VirtualGeometry:
         v = make_view(camera, self.params)
         check(lib().vgc_occluder_depth(self.handle, src_slot, C.byref(v), C.c_void_p(depth_ptr), width, height, stream))
 
+    def occluder_depth_batch(self, src_slots, cameras, depth_ptrs, width: int, height: int, stream=None) -> None:
+        """vgc_occluder_depth_batch: image i draws slot src_slots[i] with cameras[i] into depth_ptrs[i]."""
+        OccluderBatch(self, src_slots, cameras, depth_ptrs).run(width, height, stream)
+
     def expand(self, slot: int, cut: int, index_ptr: int, capacity: int, stream=None) -> None:
         """Index expansion (vgc_expand) of output slot `slot`'s cut `cut` into the device buffer at `index_ptr`."""
         check(lib().vgc_expand(self.handle, slot, cut, C.c_void_p(index_ptr), capacity, stream))
@@ -587,6 +593,21 @@ class VirtualGeometry:
             pass
 
 
+class OccluderBatch:
+    """The arguments of one vgc_occluder_depth_batch call, packed once for a caller that repeats it every frame."""
+
+    def __init__(self, vg: "VirtualGeometry", src_slots, cameras, depth_ptrs):
+        n = len(src_slots)
+        self.vg, self.n = vg, n
+        self.slots = (C.c_uint32 * n)(*src_slots)
+        self.views = (View * n)(*[make_view(c, vg.params) for c in cameras])
+        self.ptrs = (C.c_void_p * n)(*depth_ptrs)
+
+    def run(self, width: int, height: int, stream=None) -> None:
+        check(lib().vgc_occluder_depth_batch(self.vg.handle, self.n, self.slots, self.views, self.ptrs, width, height,
+                                             stream))
+
+
 class Server:
     """The serving loop over several resident scenes (vgc_server_* in include/vgcut.h): requests (scene index, view)
     are submitted from any thread, admitted by free output slots and HBM budget, batched oldest first (across scenes
@@ -615,7 +636,16 @@ class Server:
 
     def wait(self, ticket: int, timeout_ms: int = 60_000) -> dict:
         r = ServeResult()
-        check(lib().vgc_server_wait(self.handle, ticket, timeout_ms, C.byref(r)))
+        self.wait_into(ticket, r, timeout_ms)
+        return self.result_dict(r)
+
+    def wait_into(self, ticket: int, out: "ServeResult", timeout_ms: int = 60_000) -> None:
+        """wait() into a caller's result struct, without building a dict (for callers that keep up with a fast
+        server: read the struct later with result_dict)."""
+        check(lib().vgc_server_wait(self.handle, ticket, timeout_ms, C.byref(out)))
+
+    @staticmethod
+    def result_dict(r: "ServeResult") -> dict:
         out = {k: getattr(r, k) for k, _ in ServeResult._fields_ if k != "stats"}
         out["stats"] = r.stats.as_dict()
         return out
