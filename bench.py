@@ -1077,7 +1077,7 @@ def run_serve_ruins(ruins, args, plain_vps: float):
         for rate in (2_000.0, 5_000.0, 10_000.0, 20_000.0):
             if rate > 0.9 * saturated["views_per_sec"]:
                 continue
-            rates[f"{int(rate)}"], _ = drv.poisson(rate, int(min(20_000, rate * 1.0)), n_req)
+            rates[f"{int(rate)}"], _ = drv.poisson(rate, int(min(40_000, rate * 2.0)), n_req)
     finally:
         server.close()
         vg.dispose()
@@ -1089,7 +1089,7 @@ def run_serve_ruins(ruins, args, plain_vps: float):
                 capacity=dict(max_meshlets=cap_meshlets, max_triangles=cap_triangles, slots=SERVE_SLOTS),
                 linger_us=SERVE_LINGER_US,
                 latency_note="submit -> completion seen by the server (host steady clock); Poisson arrivals, about "
-                             "1 s of requests per rate")
+                             "2 s of requests per rate, after 200 warm-up requests at the same rate")
 
 
 def serve_capacity(instances: int) -> tuple:

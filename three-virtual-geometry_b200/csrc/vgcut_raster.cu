@@ -46,11 +46,12 @@ constexpr uint32_t kQueuedLarge = 1u << 16;   // large triangles,
 constexpr uint32_t kTileUnits = 1u << 20;     // and their tiles
 constexpr uint32_t kNoTri = 0xffffffffu;      // an empty tile record
 constexpr uint32_t kRecord = 5;               // float4 per queued triangle
+constexpr uint32_t kMaxImages = 64;           // occluder images per launch set (vgc_occluder_depth_batch)
 
 // Where the fragments go, and the queues of the second kernel.
 struct RasterArgs {
   uint32_t width, height;
-  uint32_t *depth;               // occluder pass: float bits per pixel
+  uint32_t *depth[kMaxImages];   // occluder pass: float bits per pixel of image i (a fragment's TriTag::id)
   unsigned long long *vis;       // visibility pass: (depth bits << 32 | id) per pixel
   uint32_t frame;                // visibility pass: lodBlendFrame
   // queues: ctl[1] = large triangles, ctl[2..3] = tiles (64-bit), ctl[4 + q] = medium triangles of sub-queue q;
@@ -63,12 +64,15 @@ struct RasterArgs {
   uint2 *clip;  // occluder pass: crossing triangles (ctl[kClipCtl] of them)
 };
 
-// The occluder pass's inputs.
-struct OccluderArgs {
+// The occluder pass's inputs: per image, the camera and the cut it draws.
+struct OccluderImage {
   float vp[16];  // P * V, row-major 4x4 (float of the double product)
   const uint4 *draw_list;      // cut 0 entries of the source slot
   const uint32_t *counters;    // its counter header
-  uint32_t max_drawn;
+};
+struct OccluderArgs {
+  OccluderImage img[kMaxImages];
+  uint32_t count, max_drawn;
 };
 
 struct ScreenTri {
@@ -76,7 +80,8 @@ struct ScreenTri {
   int x0, x1, y0, y1;  // pixel bounding box, inclusive
 };
 
-// What a visibility fragment carries besides its depth: the entry's blend range and the triangle's id.
+// What a fragment carries besides its depth: for the visibility pass the entry's blend range and the triangle's id,
+// for the occluder pass (lo = hi = 0) the image it belongs to in `id`.
 struct TriTag {
   uint32_t lo, hi, id;
 };
@@ -182,7 +187,7 @@ __device__ __forceinline__ void shade_pixel(const RasterArgs &R, const ScreenTri
     if (VIS)
       atomicMin(R.vis + at, ((unsigned long long)__float_as_uint(z) << 32) | g.id);
     else
-      atomicMin(R.depth + at, __float_as_uint(z));
+      atomicMin(R.depth[g.id] + at, __float_as_uint(z));
   }
 }
 
@@ -346,6 +351,16 @@ __device__ __forceinline__ void draw_left(const RasterArgs &R, uint32_t lane, bo
   }
 }
 
+// Clears the occluder images (1.0f) and the queues' control words.
+__global__ void __launch_bounds__(256) k_occluder_clear(const __grid_constant__ RasterArgs R, uint32_t count,
+                                                        size_t pixels) {
+  if (blockIdx.x == 0)
+    for (uint32_t i = threadIdx.x; i < kCtlWords; i += blockDim.x) R.ctl[i] = 0;
+  const size_t n = pixels * count;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    R.depth[i / pixels][i % pixels] = 0x3f800000u;
+}
+
 // Clears the image and the queues' control words.
 template <typename T>
 __global__ void __launch_bounds__(256) k_target_clear(T *image, size_t n, T value, uint32_t *ctl) {
@@ -355,26 +370,62 @@ __global__ void __launch_bounds__(256) k_target_clear(T *image, size_t n, T valu
     image[i] = value;
 }
 
-__global__ void __launch_bounds__(128, 6) k_raster_occluders(Scene S, OccluderArgs O, RasterArgs R) {
+// The images' entries laid end to end: first[v] = entries of images before v, first[count] = all (block-shared).
+__device__ __forceinline__ void image_starts(const OccluderArgs &O, uint32_t *first) {
+  if (threadIdx.x < 32) {
+    uint32_t carry = 0;
+    for (uint32_t v0 = 0; v0 < O.count; v0 += 32) {
+      const uint32_t v = v0 + threadIdx.x;
+      const uint32_t c = v < O.count ? min(O.img[v].counters[VGC_COUNTER_CUT0 + VGC_CUT_SELECTED], O.max_drawn) : 0u;
+      const uint32_t incl = warp_scan_incl(c);
+      if (v < O.count) first[v] = carry + incl - c;
+      carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (threadIdx.x == 0) first[O.count] = carry;
+  }
+  __syncthreads();
+}
+
+// The image of laid-out entry e < first[count]: the last v with first[v] <= e.
+__device__ __forceinline__ uint32_t image_of(const uint32_t *first, uint32_t count, uint32_t e) {
+  uint32_t v = 0;
+  for (uint32_t span = count; span > 1;) {
+    const uint32_t half = span >> 1;
+    if (first[v + half] <= e) v += half;
+    span -= half;
+  }
+  return v;
+}
+
+__global__ void __launch_bounds__(128, 5) k_raster_occluders(Scene S, const __grid_constant__ OccluderArgs O,
+                                                              const __grid_constant__ RasterArgs R) {
   __shared__ float4 verts[4][256];     // per warp: the current meshlet's vertices in screen space (local ids < 256)
   __shared__ uint32_t packed[4][128];  // ... and its packed triangles
   __shared__ SmallStage stage[4];
+  __shared__ uint32_t first[kMaxImages + 1];
   SmallStage &sm = stage[threadIdx.x >> 5];
   float4 *sv = verts[threadIdx.x >> 5];
   uint32_t *st = packed[threadIdx.x >> 5];
   const uint32_t lane = threadIdx.x & 31;
-  const uint32_t n = min(O.counters[VGC_COUNTER_CUT0 + VGC_CUT_SELECTED], O.max_drawn);
+  image_starts(O, first);
+  const uint32_t n = first[O.count];
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
   const float W = float(R.width), H = float(R.height);
   const uint32_t sub = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) % kSubQueues;  // this warp's medium sub-queue
-  const TriTag none{0u, 0u, 0u};
   // Each step waits on memory several times (entry, instance and meshlet, vertices, triangles): the loads of a step
-  // are issued together, and the next entry is fetched while this one is drawn.
+  // are issued together, and the next entry is fetched while this one is drawn. Entries of all images are laid end
+  // to end; a warp's entry belongs to one image.
   uint32_t e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  uint4 next = e < n ? O.draw_list[e] : make_uint4(0u, 0u, 0u, 0u);
+  uint32_t v_next = e < n ? image_of(first, O.count, e) : 0u;
+  uint4 next = e < n ? O.img[v_next].draw_list[e - first[v_next]] : make_uint4(0u, 0u, 0u, 0u);
   for (; e < n; e += warps) {
     const uint4 d = next;
-    if (e + warps < n) next = O.draw_list[e + warps];
+    const uint32_t v = v_next;
+    if (e + warps < n) {
+      v_next = image_of(first, O.count, e + warps);
+      next = O.img[v_next].draw_list[e + warps - first[v_next]];
+    }
+    const TriTag none{0u, 0u, v};  // the fragments' image
     if ((d.w & 0xffff00u) != (255u << 16)) continue;  // part 1 (blended): not an occluder
     const uint32_t slot = S.inst_slot[d.x];
     const float4 *col = S.inst + (size_t)d.x * 4;
@@ -388,13 +439,13 @@ __global__ void __launch_bounds__(128, 6) k_raster_occluders(Scene S, OccluderAr
     // M's rows from the instance's columns, then clip = (P V) M p
     const float m[4][4] = {{c0.x, c1.x, c2.x, c3.x}, {c0.y, c1.y, c2.y, c3.y}, {c0.z, c1.z, c2.z, c3.z},
                            {c0.w, c1.w, c2.w, c3.w}};
+    const float *vp = O.img[v].vp;
     float mvp[4][4];
 #pragma unroll
     for (int r = 0; r < 4; r++)
 #pragma unroll
       for (int k = 0; k < 4; k++)
-        mvp[r][k] = ((O.vp[r * 4] * m[0][k] + O.vp[r * 4 + 1] * m[1][k]) + O.vp[r * 4 + 2] * m[2][k]) +
-                    O.vp[r * 4 + 3] * m[3][k];
+        mvp[r][k] = ((vp[r * 4] * m[0][k] + vp[r * 4 + 1] * m[1][k]) + vp[r * 4 + 2] * m[2][k]) + vp[r * 4 + 3] * m[3][k];
     // the meshlet's vertices (local ids 0 .. the largest its triangles use), each transformed once, 128 at a time
     uint32_t top = 0;
 #pragma unroll
@@ -432,7 +483,7 @@ __global__ void __launch_bounds__(128, 6) k_raster_occluders(Scene S, OccluderAr
         uint32_t at = 0;
         if (lane == __ffs(cm) - 1) at = atomicAdd(R.ctl + kClipCtl, __popc(cm));
         at = __shfl_sync(0xffffffffu, at, __ffs(cm) - 1) + __popc(cm & ((1u << lane) - 1u));
-        if (crossing && at < kClipQueue) R.clip[at] = make_uint2(e, ti);
+        if (crossing && at < kClipQueue) R.clip[at] = make_uint2(e - first[v], ti | (v << 8));
       }
       if (queue_triangles<false>(R, sm, sub, lane, ok, t, none)) left |= 1u << round;
     }
@@ -450,7 +501,8 @@ __global__ void __launch_bounds__(128, 6) k_raster_occluders(Scene S, OccluderAr
 // The occluder pass's triangles that cross the near plane, a lane each: the draw-list entry's (P V M), the triangle's
 // corners in clip space, clipped (setup_clipped), and its one or two screen triangles through the same size classes
 // and queues (k_raster_queued runs after this kernel).
-__global__ void __launch_bounds__(128) k_raster_clipped(Scene S, OccluderArgs O, RasterArgs R) {
+__global__ void __launch_bounds__(128) k_raster_clipped(Scene S, const __grid_constant__ OccluderArgs O,
+                                                          const __grid_constant__ RasterArgs R) {
   __shared__ SmallStage stage[4];
   SmallStage &sm = stage[threadIdx.x >> 5];
   const uint32_t lane = threadIdx.x & 31;
@@ -458,14 +510,17 @@ __global__ void __launch_bounds__(128) k_raster_clipped(Scene S, OccluderArgs O,
   const uint32_t stride = gridDim.x * blockDim.x;
   const uint32_t sub = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) % kSubQueues;
   const float W = float(R.width), H = float(R.height);
-  const TriTag none{0u, 0u, 0u};
   for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
     const uint32_t i = base + lane;
     ScreenTri t, t2;
     int k = 0;
+    TriTag none{0u, 0u, 0u};  // the fragments' image
     if (i < n) {
       const uint2 rec = R.clip[i];
-      const uint4 d = O.draw_list[rec.x];
+      const uint32_t v = rec.y >> 8;
+      none.id = v;
+      const float *vp = O.img[v].vp;
+      const uint4 d = O.img[v].draw_list[rec.x];
       const float4 *col = S.inst + (size_t)d.x * 4;
       const float4 c0 = col[0], c1 = col[1], c2 = col[2], c3 = col[3];
       const float m[4][4] = {{c0.x, c1.x, c2.x, c3.x}, {c0.y, c1.y, c2.y, c3.y}, {c0.z, c1.z, c2.z, c3.z},
@@ -475,10 +530,10 @@ __global__ void __launch_bounds__(128) k_raster_clipped(Scene S, OccluderArgs O,
       for (int r = 0; r < 4; r++)
 #pragma unroll
         for (int kk = 0; kk < 4; kk++)
-          mvp[r][kk] = ((O.vp[r * 4] * m[0][kk] + O.vp[r * 4 + 1] * m[1][kk]) + O.vp[r * 4 + 2] * m[2][kk]) +
-                       O.vp[r * 4 + 3] * m[3][kk];
+          mvp[r][kk] = ((vp[r * 4] * m[0][kk] + vp[r * 4 + 1] * m[1][kk]) + vp[r * 4 + 2] * m[2][kk]) +
+                       vp[r * 4 + 3] * m[3][kk];
       const uint4 info = S.m_info[d.y];
-      const uint32_t p = S.m_tris[info.y / 3 + rec.y], voff = info.w;
+      const uint32_t p = S.m_tris[info.y / 3 + (rec.y & 255u)], voff = info.w;
       const float4 va = clip_vertex(mvp, S.positions[S.m_verts[voff + (p & 255u)]]);
       const float4 vb = clip_vertex(mvp, S.positions[S.m_verts[voff + ((p >> 8) & 255u)]]);
       const float4 vc = clip_vertex(mvp, S.positions[S.m_verts[voff + ((p >> 16) & 255u)]]);
@@ -496,7 +551,7 @@ __global__ void __launch_bounds__(128) k_raster_clipped(Scene S, OccluderArgs O,
 // The queued triangles, spread over the whole grid: a warp per medium triangle, then a warp per tile of a large one
 // (a lane per column of the tile).
 template <bool VIS>
-__global__ void __launch_bounds__(128) k_raster_queued(RasterArgs R) {
+__global__ void __launch_bounds__(128) k_raster_queued(const __grid_constant__ RasterArgs R) {
   __shared__ uint32_t counts[kSubQueues];  // medium triangles per sub-queue
   __shared__ uint32_t most;
   if (threadIdx.x == 0) most = 0;
@@ -597,7 +652,7 @@ __device__ __forceinline__ float4 pulled_clip(const Scene &S, const VisArgs &A, 
 }
 
 // One lane per triangle of the cut, in region order (mesh slot, then part), as the draw args give them.
-__global__ void __launch_bounds__(256) k_visibility(Scene S, VisArgs A, RasterArgs R) {
+__global__ void __launch_bounds__(256) k_visibility(Scene S, VisArgs A, const __grid_constant__ RasterArgs R) {
   extern __shared__ uint32_t tri_start[];  // per region: first triangle in the laid-out order; [regions] = total
   __shared__ SmallStage stage[8];
   SmallStage &sm = stage[threadIdx.x >> 5];
@@ -675,28 +730,33 @@ static int raster_queues(vgc_context *ctx, RasterArgs &R) {
   return VGC_OK;
 }
 
-// One image of the occluder pass, its arguments checked (the launches only).
-static int occluder_depth_one(vgc_context *ctx, uint32_t src_slot, const vgc_view *view, float *depth, uint32_t width,
-                              uint32_t height, cudaStream_t st) {
+// Up to kMaxImages images of the occluder pass in one launch set (arguments checked): image i draws output slot
+// slots[i] with views[i] into depth[i].
+static int occluder_depth_images(vgc_context *ctx, uint32_t count, const uint32_t *slots, const vgc_view *views,
+                                 float *const *depth, uint32_t width, uint32_t height, cudaStream_t st) {
   int rc;
   OccluderArgs O{};
-  for (int r = 0; r < 4; r++)
-    for (int c = 0; c < 4; c++) {
-      double s = 0;
-      for (int i = 0; i < 4; i++) s += view->proj[i * 4 + r] * view->view[c * 4 + i];
-      O.vp[r * 4 + c] = (float)s;
-    }
-  O.draw_list = (const uint4 *)ctx->d_draw.ptr + (size_t)src_slot * 2 * ctx->opts.max_meshlets;
-  O.counters = (const uint32_t *)ctx->d_counters.ptr + (size_t)src_slot * ctx->counter_words;
-  O.max_drawn = ctx->opts.max_meshlets;
   RasterArgs R{};
+  O.count = count;
+  O.max_drawn = ctx->opts.max_meshlets;
+  for (uint32_t v = 0; v < count; v++) {
+    OccluderImage &I = O.img[v];
+    for (int r = 0; r < 4; r++)
+      for (int c = 0; c < 4; c++) {
+        double s = 0;
+        for (int i = 0; i < 4; i++) s += views[v].proj[i * 4 + r] * views[v].view[c * 4 + i];
+        I.vp[r * 4 + c] = (float)s;
+      }
+    I.draw_list = (const uint4 *)ctx->d_draw.ptr + (size_t)slots[v] * 2 * ctx->opts.max_meshlets;
+    I.counters = (const uint32_t *)ctx->d_counters.ptr + (size_t)slots[v] * ctx->counter_words;
+    R.depth[v] = reinterpret_cast<uint32_t *>(depth[v]);
+  }
   R.width = width;
   R.height = height;
-  R.depth = reinterpret_cast<uint32_t *>(depth);
   if ((rc = raster_queues(ctx, R))) return rc;
   const size_t pixels = (size_t)width * height;
-  k_target_clear<uint32_t><<<(unsigned)std::min<size_t>((pixels + 255) / 256, (size_t)ctx->sm_count * 16), 256, 0,
-                             st>>>(R.depth, pixels, 0x3f800000u, R.ctl);  // 1.0f
+  k_occluder_clear<<<(unsigned)std::min<size_t>((pixels * count + 255) / 256, (size_t)ctx->sm_count * 16), 256, 0,
+                     st>>>(R, count, pixels);
   CUDA_TRY(cudaGetLastError());
   if (ctx->positions.empty()) return VGC_OK;  // no mesh carries vertex data: nothing is an occluder
   // persistent grids of exactly the resident blocks: a grid-stride loop over a grid larger than one wave leaves the
@@ -730,8 +790,8 @@ extern "C" int vgc_occluder_depth(vgc_context *ctx, uint32_t src_slot, const vgc
   if (rc) return rc;
   cudaSetDevice(ctx->device);
   if ((rc = sync_scene(ctx))) return rc;
-  return occluder_depth_one(ctx, src_slot, view, depth, width, height,
-                            stream ? (cudaStream_t)stream : ctx->stream);
+  return occluder_depth_images(ctx, 1, &src_slot, view, &depth, width, height,
+                               stream ? (cudaStream_t)stream : ctx->stream);
 }
 
 extern "C" int vgc_occluder_depth_batch(vgc_context *ctx, uint32_t count, const uint32_t *src_slots,
@@ -744,8 +804,10 @@ extern "C" int vgc_occluder_depth_batch(vgc_context *ctx, uint32_t count, const 
   cudaSetDevice(ctx->device);
   if ((rc = sync_scene(ctx))) return rc;
   const cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
-  for (uint32_t i = 0; i < count; i++)
-    if ((rc = occluder_depth_one(ctx, src_slots[i], &views[i], depth[i], width, height, st))) return rc;
+  for (uint32_t i = 0; i < count; i += kMaxImages)
+    if ((rc = occluder_depth_images(ctx, std::min(kMaxImages, count - i), src_slots + i, views + i, depth + i, width,
+                                    height, st)))
+      return rc;
   return VGC_OK;
 }
 
