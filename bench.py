@@ -564,6 +564,7 @@ def run_ours(args, world, rank, local):
         gpu_launches=args.steps * ((2 if occl else 0) + 11),
         clocks=clk,
     )
+    line["autotune"] = autotune_report(vg, views, sp, stream, flush, args.steps)
     captured = parity_capture(vg, spec, views, occl, local) if rank == 0 else None
     vg.dispose()
     if world == 1 and args.config == "ruins" and not args.no_extras:
@@ -594,6 +595,36 @@ def run_ours(args, world, rank, local):
         line["cpu_baseline"] = dict(value=vps, unit="views/s", cores=cores, kind="port", sample=sample)
         line["parity"] = parity_check(runner, captured)
         print(json.dumps(tail_order(line)), flush=True)
+
+
+def autotune_report(vg, views, sp, stream, flush, steps: int) -> dict:
+    """vgc_batch_autotune on a batched launch, after the figures that use the default shapes: the shapes it picks
+    (meshlets per chunk, blocks per SM of the instance and meshlet kernels) and the device time per step before and
+    after (L2 flushed before each step)."""
+    import torch
+
+    def step_ms():
+        for _ in range(3):
+            vg.cut(views, first_slot=0, stream=sp, graph=True)
+        ms = []
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            vg.cut(views, first_slot=0, stream=sp, graph=True)
+            b.record(stream)
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        return statistics.mean(ms)
+
+    default_ms = step_ms()
+    tuned = vg.autotune(views, stream=sp, reps=3)
+    tuned_ms = step_ms()
+    return dict(chunk_meshlets=tuned["chunk_meshlets"], instances_blocks_per_sm=tuned["instances_blocks_per_sm"],
+                chunks_blocks_per_sm=tuned["chunks_blocks_per_sm"], default_ms_per_step=default_ms,
+                tuned_ms_per_step=tuned_ms, gain=default_ms / tuned_ms - 1.0,
+                note="default shapes: 512 meshlets per chunk, the kernels' occupancy limits; `value` uses the defaults")
 
 
 TAIL_KEYS = ("cpu_baseline", "parity", "roofline", "e2e", "plain_views_per_sec", "batched_over_plain", "p50_ms",
@@ -957,6 +988,7 @@ def run_large_world(ruins, args, flush, stream):
         b.synchronize()
         ms.append(a.elapsed_time(b))
     st = [vg.read_stats(k) for k in range(len(views))]
+    tune = autotune_report(vg, views, sp, stream, flush, args.steps)
     drawn = [s["requested_indices"][0] // 3 for s in st]
     pred = [s["predicted_triangles"] for s in st]
     out = dict(workload=f"large world: {spec.instance_count} instances of {len(spec.meshes)} meshes over 6x6 km "
@@ -967,6 +999,7 @@ def run_large_world(ruins, args, flush, stream):
                camera_cut_triangles_mean=statistics.mean(drawn),
                threshold_range=list(trange),
                thresholds=[min(s["effective_threshold"] for s in st), max(s["effective_threshold"] for s in st)],
+               autotune=tune,
                note="predicted = the histogram's plain-cut triangles at the chosen threshold; the drawn camera cut adds "
                     "the LOD-blend band's overlap")
     vg.dispose()
