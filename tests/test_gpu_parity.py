@@ -123,9 +123,12 @@ def test_hzb_mips_bit_exact(ruins_small):
     assert np.array_equal(d2h(info["data"], len(mips), np.float32), mips)
 
 
-@pytest.mark.parametrize("shape", [(611, 997), (1, 7), (9, 1), (130, 64), (1080, 1920), (67, 129)])
+@pytest.mark.parametrize("shape", [(611, 997), (1, 7), (9, 1), (130, 64), (1080, 1920), (67, 129), (300, 1004),
+                                   (77, 100), (1, 4)])
 def test_hzb_mips_odd_sizes(ruins_small, shape):
-    """Edge clamping at every level: odd and tiny sizes through the host-copy, device and in-sequence builds."""
+    """Edge clamping at every level: odd and tiny sizes through the host-copy, device and in-sequence builds (float4
+    rows where the width is a multiple of 4 and the pointer aligned, with a partial tile at the right edge for 1004
+    and 100; scalar loads otherwise)."""
     import torch
     h = ruins_small
     rng = np.random.default_rng(shape[0] * 7919 + shape[1])
