@@ -90,7 +90,13 @@ enum {
                                shadow cut keeps the casters inside the camera frustum swept along shadowSweep): no
                                camera cut; the shadow cut keeps its reference semantics (LOD from the camera: view,
                                projection, threshold x shadowErrorScale; no occlusion) but culls against the clip
-                               volume of `cascade_clip`; shadowSweep is not used; triangle_budget must be 0 */
+                               volume of `cascade_clip`; shadowSweep is not used; triangle_budget must be 0 */,
+  VGC_VIEW_DEPTH_AS_MIP0 = 4 /* with `depth` and hzb >= 0 (no counterpart in the reference, which copies the depth
+                               texture into the HZB's first level every frame): the cut reads the HZB's mip 0 from
+                               `depth` itself instead of copying the image into the slot; mips 1 and up are built as
+                               usual, and the results are the same. The slot's mip 0 keeps its previous contents, so
+                               a later cut that uses the slot without a new `depth` must follow a build without this
+                               flag. Saves writing 4 bytes per depth pixel when the HZB is rebuilt every frame. */
 };
 
 /* One cut request: the uniforms VirtualGeometry.update() writes (VirtualGeometry.ts:414-442) and the levers

@@ -307,3 +307,34 @@ def test_hzb_built_in_cut_sequence(ruins_small):
             info = h.vg.hzb_info(20 + k)
             mips = O.hzb_build(img)[0]
             assert np.array_equal(d2h(info["data"], len(mips), np.float32), mips)
+
+
+def test_depth_as_mip0(ruins_small):
+    """VGC_VIEW_DEPTH_AS_MIP0: the cut reads mip 0 from the view's depth image instead of a copy in the slot. Same
+    draw sets and counters as the copying build (and as the oracle with the full HZB); the slot's mip 0 keeps what an
+    earlier build left there while mips 1 and up are the new image's."""
+    import torch
+    h = ruins_small
+    slot = 27
+    first = h.spec.depth_images[0]
+    for graph in (False, True):
+        for k, cam in enumerate(h.spec.cameras[1:4], start=1):
+            img = h.spec.depth_images[k]
+            d = torch.from_numpy(img).cuda()
+            got = {}
+            for flag in (False, True):
+                h.vg.build_hzb(slot, first)  # an earlier frame's HZB in the slot
+                p = engine.ViewParams(error_threshold=1.0, hzb=slot, depth_as_mip0=flag)
+                v = engine.make_view(cam, p, depth=(d.data_ptr(), img.shape[1], img.shape[0]))
+                h.vg.cut([v], first_slot=0, graph=graph)
+                got[flag] = (key_set(h.vg.draw_list(0, 0), (0, 1, 3)), h.vg.read_stats(0))
+            assert got[True][0] == got[False][0], "the draw set differs with mip 0 read from the depth image"
+            assert got[True][1] == got[False][1]
+            res, _ = h.oracle(cam, engine.ViewParams(error_threshold=1.0, hzb=slot), hzb=O.hzb_build(img))
+            assert got[True][0] == key_set(res["entries"][0], (0, 1, 2))
+            info = h.vg.hzb_info(slot)
+            mips, levels, off, w, hh = O.hzb_build(img)
+            old = O.hzb_build(first)[0]
+            data = d2h(info["data"], len(mips), np.float32)
+            assert np.array_equal(data[:off[1]], old[:off[1]]), "mip 0 of the slot is not written"
+            assert np.array_equal(data[off[1]:], mips[off[1]:]), "mips 1 and up are the new image's"

@@ -433,6 +433,7 @@ int view_constants(vgc_context *ctx, const vgc_view &in, uint32_t out_slot, uint
   k.build_hzb = (in.hzb >= 0 && in.depth) ? 1u : 0u;
   k.fresh_state = (in.flags & VGC_VIEW_FRESH_STATE) ? 1u : 0u;
   k.depth = in.depth;
+  k.hzb_mip0 = (k.build_hzb && (in.flags & VGC_VIEW_DEPTH_AS_MIP0)) ? in.depth : nullptr;
   k.unit_offset = unit_offset;
   k.max_drawn = ctx->opts.max_meshlets;
   k.index_capacity[0] = ctx->opts.max_triangles * 3;

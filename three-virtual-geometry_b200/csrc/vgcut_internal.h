@@ -102,6 +102,7 @@ struct ViewConst {
   uint32_t fresh_state; // 1: k_reset puts the controller state back to its initial words first
   uint32_t cascade;     // 1: shadow cascade (no camera cut; plane[] are the cascade's planes, sweep[] zero)
   const float *depth;   // occluder depth of this frame (build_hzb)
+  const float *hzb_mip0;  // VGC_VIEW_DEPTH_AS_MIP0: the HZB's mip 0 is `depth` (not copied into the slot); else null
   uint32_t *counters;   // VGC_COUNTER_* header, then per (cut, slot, part): count, start
   uint32_t *state;      // kStateWords, carried between frames
   uint4 *draw_list;     // 2 * max_drawn

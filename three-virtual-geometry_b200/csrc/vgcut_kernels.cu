@@ -155,7 +155,8 @@ __device__ bool hzb_occluded(const ViewConst &V, const HzbDesc &H, const float c
   uint32_t level = ceil_log2((dx > dy ? dx : dy) + 1u);
   if (level > H.levels - 1) level = H.levels - 1;
   uint32_t lw = H.w[level], lh = H.h[level];
-  const float *mip = H.data + H.off[level];
+  // mip 0 from the view's depth image when the build left it there (VGC_VIEW_DEPTH_AS_MIP0; same size and values)
+  const float *mip = (level == 0 && V.hzb_mip0) ? V.hzb_mip0 : H.data + H.off[level];
   uint32_t tx0 = min(x0 >> level, lw - 1), tx1 = min(x1 >> level, lw - 1);
   uint32_t ty0 = min(y0 >> level, lh - 1), ty1 = min(y1 >> level, lh - 1);
   float s00 = __ldg(mip + ty0 * lw + tx0), s10 = __ldg(mip + ty0 * lw + tx1);
@@ -1398,7 +1399,7 @@ __global__ void __launch_bounds__(256) k_hzb_tiles_views(const ViewConst *__rest
   const HzbDesc &H = *V.hzb_desc;
   const uint32_t ox = blockIdx.x * kHzbTile, oy = blockIdx.y * 2 * kHzbTile;
   if (ox >= H.w[0] || oy >= H.h[0]) return;
-  hzb_tile_pair(V.depth, H, const_cast<float *>(H.data), true, ox, oy, s3);
+  hzb_tile_pair(V.depth, H, const_cast<float *>(H.data), V.hzb_mip0 == nullptr, ox, oy, s3);
 }
 
 __global__ void __launch_bounds__(1024) k_hzb_tail_views(const ViewConst *__restrict__ views) {

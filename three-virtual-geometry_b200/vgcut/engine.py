@@ -235,10 +235,12 @@ class ViewParams:
     state_slot: int = 0
     fresh_state: bool = False  # VGC_VIEW_FRESH_STATE: the capacity controller starts from its initial state
     cascade_clip: object = None  # VGC_VIEW_CASCADE: 16 floats, the cascade's world -> clip matrix (column-major)
+    depth_as_mip0: bool = False  # VGC_VIEW_DEPTH_AS_MIP0: an HZB built from `depth` reads its mip 0 from it (no copy)
 
 
 VGC_VIEW_FRESH_STATE = 1
 VGC_VIEW_CASCADE = 2
+VGC_VIEW_DEPTH_AS_MIP0 = 4
 
 
 def make_view(camera: Camera, p: ViewParams | None = None, depth=None) -> View:
@@ -263,7 +265,8 @@ def make_view(camera: Camera, p: ViewParams | None = None, depth=None) -> View:
     v.frustum_culling = 1 if p.frustum_culling else 0
     v.hzb = p.hzb
     v.state_slot = p.state_slot
-    v.flags = (VGC_VIEW_FRESH_STATE if p.fresh_state else 0) | (VGC_VIEW_CASCADE if p.cascade_clip is not None else 0)
+    v.flags = (VGC_VIEW_FRESH_STATE if p.fresh_state else 0) | (VGC_VIEW_CASCADE if p.cascade_clip is not None else 0) | \
+        (VGC_VIEW_DEPTH_AS_MIP0 if p.depth_as_mip0 else 0)
     if p.cascade_clip is not None:
         for k in range(16):
             v.cascade_clip[k] = float(p.cascade_clip[k])
