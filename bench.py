@@ -720,7 +720,8 @@ def run_occluders(ruins, args, flush, stream):
     # this frame's poses: the next pose of the spline (the last one repeats)
     cams = [ruins.cameras[min(k + 1, P - 1)] for k in range(P)]
     depth = [torch.empty((H, W), dtype=torch.float32, device="cuda") for _ in range(P)]
-    views = [engine.make_view(c, engine.ViewParams(error_threshold=1.0, hzb=k, state_slot=P + k, fresh_state=True),
+    views = [engine.make_view(c, engine.ViewParams(error_threshold=1.0, hzb=k, state_slot=P + k, fresh_state=True,
+                                                   depth_as_mip0=True),
                               depth=(depth[k].data_ptr(), W, H)) for k, c in enumerate(cams)]
     open_views = [engine.make_view(c, engine.ViewParams(error_threshold=1.0, state_slot=P + k, fresh_state=True))
                   for k, c in enumerate(cams)]
@@ -767,7 +768,8 @@ def run_occluders(ruins, args, flush, stream):
     cap = 1 << 18
     h_counters = torch.empty(2 * P * cw, dtype=torch.int32).pin_memory()
     h_lists = torch.empty((P, cap, 4), dtype=torch.int32).pin_memory()
-    loop_views = [[engine.make_view(c, engine.ViewParams(error_threshold=1.0, hzb=k, state_slot=s * P + k),
+    loop_views = [[engine.make_view(c, engine.ViewParams(error_threshold=1.0, hzb=k, state_slot=s * P + k,
+                                                         depth_as_mip0=True),
                                     depth=(depth[k].data_ptr(), W, H)) for k, c in enumerate(cams)] for s in (0, 1)]
     d2h = [0]
     outs = [vg.output(k) for k in range(2 * P)]
