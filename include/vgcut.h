@@ -146,7 +146,7 @@ enum {
   VGC_COUNTER_REDO0 = 12,
   VGC_COUNTER_REDO1 = 13,
   VGC_COUNTER_ROUNDS = 14,
-  VGC_COUNTER_ERROR = 15,
+  VGC_COUNTER_ERROR = 15,           /* VGC_FAULT_* bits of this view's launch sequence */
   VGC_COUNTER_INSTANCES_TESTED = 16, /* instances of visible cells (all rounds) */
   VGC_COUNTER_MESHLETS_TESTED = 17,  /* meshlets run through the per-meshlet test (all rounds) */
   VGC_COUNTER_FAST_EMITTED = 18,     /* meshlets emitted by the instance fast path (all rounds) */
@@ -158,6 +158,10 @@ enum {
                                         certain (tested in the meshlet pass; MESHLETS_TESTED counts the full ranges) */
   VGC_COUNTER_HEADER = 24,
 };
+/* Device-side failures a kernel reports instead of waiting on: VGC_FAULT_HZB_WAIT = a tile copy of the HZB
+ * build did not arrive within about a second (the launch's HZBs are incomplete; its cuts may keep occluded geometry
+ * or drop visible geometry). */
+enum { VGC_FAULT_HZB_WAIT = 1 };
 enum { VGC_CUT_SELECTED = 0, VGC_CUT_DRAWN = 1, VGC_CUT_SURVIVED = 2, VGC_CUT_WORK = 3, VGC_CUT_REQUESTED = 4 };
 
 /* Stats of one output slot: VirtualGeometryStats (VirtualGeometry.ts:24-47) per view. */
@@ -173,6 +177,7 @@ typedef struct vgc_stats {
   uint32_t instances_tested, meshlets_tested, fast_emitted, levels_read; /* work done, all rounds */
   uint64_t predicted_triangles; /* triangleBudget search: predicted plain camera-cut triangles */
   uint32_t meshlets_queued;     /* meshlets the meshlet pass tested after item trimming (all rounds) */
+  uint32_t faults;              /* VGC_FAULT_* bits (0: none) */
 } vgc_stats;
 
 const char *vgc_last_error(void);

@@ -121,6 +121,7 @@ class Harness:
         self.last_state = state
         stats, lists = self.gpu(cam, params, slot, graph)
         c = res["counters"]
+        assert stats["faults"] == 0, "a kernel gave up waiting"
         assert stats["visible_cells"] == c[0]
         if any(m > self.max_meshlets for m in res["max_selected"]):
             # A round selected more meshlets than the draw list holds: the GPU kept the subset its atomics reached

@@ -145,9 +145,44 @@ def test_hzb_mips_odd_sizes(ruins_small, shape):
         engine.check(engine.lib().vgc_hzb_build(h.vg.handle, 10, ptr, img.shape[1], img.shape[0], 1, None))
         assert np.array_equal(d2h(h.vg.hzb_info(10)["data"], len(mips), np.float32), mips)
     cam = h.spec.cameras[0]
-    v = engine.make_view(cam, engine.ViewParams(error_threshold=1.0, hzb=11), depth=(d.data_ptr(), img.shape[1], img.shape[0]))
-    h.vg.cut([v], first_slot=0)
-    assert np.array_equal(d2h(h.vg.hzb_info(11)["data"], len(mips), np.float32), mips)
+    for ptr in (d.data_ptr(), dd.data_ptr() + 4):  # in the cut's tile stream: a tensor map, or plain loads
+        v = engine.make_view(cam, engine.ViewParams(error_threshold=1.0, hzb=11), depth=(ptr, img.shape[1], img.shape[0]))
+        h.vg.cut([v], first_slot=0)
+        assert np.array_equal(d2h(h.vg.hzb_info(11)["data"], len(mips), np.float32), mips)
+        assert h.vg.read_stats(0)["faults"] == 0
+
+
+def test_hzb_stream_mixed_jobs(ruins_small):
+    """One launch whose HZB builds differ in size and kind: 128 x 32 strips through tensor maps (widths a multiple of
+    4, with partial strips at the right and bottom edges) and through plain loads (odd width, unaligned pointer,
+    narrower than a strip) in one stream; every slot equals the oracle's max reduction, through the plain call and
+    the captured graph."""
+    import torch
+    h = ruins_small
+    shapes = [(1080, 1920), (77, 132), (611, 997), (130, 256), (40, 36), (300, 1004), (2160, 3840)]
+    rng = np.random.default_rng(11)
+    imgs = [rng.random(s, dtype=np.float32) for s in shapes]
+    keep = []
+    views = []
+    for k, img in enumerate(imgs):
+        d = torch.zeros(img.size + 4, dtype=torch.float32, device="cuda")
+        off = 1 if k == 3 else 0  # job 3: a 4-byte offset pointer (no tensor map)
+        d[off:off + img.size] = torch.from_numpy(img).flatten().cuda()
+        keep.append(d)
+        ptr = d.data_ptr() + 4 * off
+        views.append(engine.make_view(h.spec.cameras[k % len(h.spec.cameras)],
+                                      engine.ViewParams(error_threshold=1.0, hzb=40 + k, depth_as_mip0=(k % 2 == 1)),
+                                      depth=(ptr, img.shape[1], img.shape[0])))
+    for graph in (False, True):
+        for k in range(len(shapes)):
+            h.vg.build_hzb(40 + k, np.zeros((8, 8), np.float32))  # stale contents of another size
+        h.vg.cut(views, first_slot=0, graph=graph)
+        for k, img in enumerate(imgs):
+            mips, levels, off, w, hh = O.hzb_build(img)
+            data = d2h(h.vg.hzb_info(40 + k)["data"], len(mips), np.float32)
+            lo = off[1] if k % 2 == 1 else 0  # mip 0 is not written when it is read from the depth image
+            assert np.array_equal(data[lo:], mips[lo:]), (graph, shapes[k])
+            assert h.vg.read_stats(k)["faults"] == 0
 
 
 def test_capacity_retry_rounds():

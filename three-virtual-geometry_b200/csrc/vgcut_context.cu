@@ -6,6 +6,7 @@
 // growth re-uploads the host mirror into a larger allocation. Output slots (one per view of a batch) hold the
 // per-view results: counters, draw list, draw args.
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -49,6 +50,7 @@ void decode_stats(const vgc_context *ctx, const uint32_t *c, float threshold, vg
   s->levels_read = c[VGC_COUNTER_LEVELS_READ];
   s->predicted_triangles = (uint64_t)c[VGC_COUNTER_PREDICTED_LO] | ((uint64_t)c[VGC_COUNTER_PREDICTED_HI] << 32);
   s->meshlets_queued = c[VGC_COUNTER_MESHLETS_QUEUED];
+  s->faults = c[VGC_COUNTER_ERROR];
   s->effective_threshold = threshold;
 }
 
@@ -228,11 +230,22 @@ int ensure_scratch(vgc_context *ctx, LaunchScratch &s, uint32_t views, size_t un
       cudaFree(s.d_views);
       ctx->bytes -= sizeof(ViewConst) * s.view_capacity;
     }
+    if (s.h_plan) cudaFreeHost(s.h_plan);
+    if (s.d_plan) {
+      cudaFree(s.d_plan);
+      ctx->bytes -= hzb_plan_bytes(s.view_capacity);
+    }
     s.h_views = nullptr;
     s.d_views = nullptr;
+    s.h_plan = s.d_plan = nullptr;
+    s.view_capacity = 0;
     CUDA_TRY(cudaMallocHost(&s.h_views, sizeof(ViewConst) * views));
     CUDA_TRY(cudaMalloc(&s.d_views, sizeof(ViewConst) * views));
-    ctx->bytes += sizeof(ViewConst) * views;
+    CUDA_TRY(cudaMallocHost(&s.h_plan, hzb_plan_bytes(views)));
+    CUDA_TRY(cudaMalloc(&s.d_plan, hzb_plan_bytes(views)));
+    ctx->bytes += sizeof(ViewConst) * views + hzb_plan_bytes(views);
+    s.plan_keys.assign(views, LaunchScratch::PlanKey{});
+    s.plan_maps = 0;
     s.view_capacity = views;
   }
   if (units > s.unit_capacity || !s.d_units) {
@@ -278,6 +291,8 @@ void free_scratch(LaunchScratch &s) {
   if (s.d_scenes) cudaFree(s.d_scenes);
   if (s.h_views) cudaFreeHost(s.h_views);
   if (s.d_views) cudaFree(s.d_views);
+  if (s.h_plan) cudaFreeHost(s.h_plan);
+  if (s.d_plan) cudaFree(s.d_plan);
   if (s.d_units) cudaFree(s.d_units);
   if (s.d_unit_count) cudaFree(s.d_unit_count);
   if (s.d_chunks) cudaFree(s.d_chunks);
@@ -348,6 +363,74 @@ HzbDesc hzb_layout(uint32_t width, uint32_t height, size_t *total_floats) {
 
 // Allocates / lays out HZB slot `hzb` for a width x height mip 0 and publishes its descriptor; returns whether the
 // device descriptor array changed (the caller uploads it).
+// cuTensorMapEncodeTiled of the driver, found once through the runtime (the library does not link libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+    }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// The tensor map k_hzb_stream reads a float depth image through: 128 x 32 boxes, zeros past the image's edge. False
+// (the plain loads then read the image) when the image breaks a bulk-tensor copy rule - base 16-byte aligned, row
+// pitch a multiple of 16 bytes - or is smaller than a box.
+bool depth_tensor_map(const float *depth, uint32_t w, uint32_t h, void *out) {
+  const PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+  if (!encode || (w & 3u) || (reinterpret_cast<uintptr_t>(depth) & 15u) || w < kHzbStripW || h < kHzbStripH)
+    return false;
+  const cuuint64_t dims[2] = {w, h}, pitch[1] = {(cuuint64_t)w * 4};
+  const cuuint32_t box[2] = {kHzbStripW, kHzbStripH}, step[2] = {1, 1};
+  return encode(static_cast<CUtensorMap *>(out), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(depth), dims,
+                pitch, box, step, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The HZB plan of the prepared views in `s.h_plan`: one job per view that brings a depth image, strips in view order.
+// A tensor map is encoded again only when its job's image changed since the last launch of this scratch.
+void build_hzb_plan(vgc_context *ctx, LaunchScratch &s, const vgc_view *views, uint32_t count) {
+  HzbPlanHead &P = *reinterpret_cast<HzbPlanHead *>(s.h_plan);
+  HzbJob *jobs = reinterpret_cast<HzbJob *>(s.h_plan + sizeof(HzbPlanHead));
+  const size_t maps = hzb_plan_maps(count);
+  if (s.plan_maps != maps) {
+    s.plan_keys.assign(s.view_capacity, LaunchScratch::PlanKey{});
+    s.plan_maps = maps;
+  }
+  uint32_t n = 0, tiles = 0;
+  for (uint32_t i = 0; i < count; i++) {
+    const vgc_view &v = views[i];
+    if (v.hzb < 0 || !v.depth) continue;
+    const uint32_t w = v.depth_width, h = v.depth_height;
+    const uint32_t tx = (w + kHzbStripW - 1) / kHzbStripW, ty = (h + kHzbStripH - 1) / kHzbStripH;
+    LaunchScratch::PlanKey &key = s.plan_keys[n];
+    if (key.depth != v.depth || key.w != w || key.h != h) {
+      key.depth = v.depth;
+      key.w = w;
+      key.h = h;
+      key.tma = depth_tensor_map(v.depth, w, h, s.h_plan + maps + (size_t)n * kTensorMapBytes) ? 1u : 0u;
+    }
+    HzbJob &J = jobs[n++];
+    J.depth = v.depth;
+    J.desc = (const HzbDesc *)ctx->d_hzb_desc.ptr + v.hzb;
+    J.error = s.h_views[i].counters + VGC_COUNTER_ERROR;
+    J.tile0 = tiles;
+    J.tiles_x = (uint16_t)tx;
+    J.tma = (uint8_t)key.tma;
+    J.copy_mip0 = s.h_views[i].hzb_mip0 == nullptr ? 1 : 0;
+    tiles += tx * ty;
+  }
+  std::memset(&P, 0, sizeof P);
+  P.jobs = n;
+  P.tiles = tiles;
+  P.maps = (uint32_t)maps;
+}
+
 int hzb_prepare(vgc_context *ctx, int32_t hzb, uint32_t width, uint32_t height, bool *changed) {
   if (width == 0 || height == 0 || width > 32768 || height > 32768) return fail(VGC_INVALID_ARG, "HZB size out of range");
   size_t total = 0;
@@ -484,7 +567,8 @@ int prepare(vgc_context *ctx, LaunchScratch &s, const vgc_view *views, uint32_t 
       changed = changed || c;
       s.hzb_w = std::max(s.hzb_w, v.depth_width);
       s.hzb_h = std::max(s.hzb_h, v.depth_height);
-      s.hzb_tail = s.hzb_tail || ctx->hzb[v.hzb].desc.levels > 7;  // levels 7+ by the tail kernel
+      // the tail kernel builds levels 5+ after the strip stream (7+ after the per-view tile kernel)
+      s.hzb_tail = s.hzb_tail || ctx->hzb[v.hzb].desc.levels > (ctx->hzb_grid ? 5u : 7u);
     }
   }
   if (changed) {
@@ -494,6 +578,7 @@ int prepare(vgc_context *ctx, LaunchScratch &s, const vgc_view *views, uint32_t 
   }
   for (uint32_t i = 0; i < count; i++)
     if ((rc = view_constants(ctx, views[i], slots ? slots[i] : first_slot + i, i * cells, s.h_views[i]))) return rc;
+  if (s.hzb_w) build_hzb_plan(ctx, s, views, count);
   return VGC_OK;
 }
 
@@ -585,12 +670,15 @@ int enqueue(vgc_context *ctx, LaunchScratch &s, uint32_t count, cudaStream_t st,
   const uint32_t chunk_grid = s.grid_chunks ? s.grid_chunks : ctx->chunk_grid;
   CUDA_TRY(cudaMemcpyAsync(s.d_views, s.h_views, sizeof(ViewConst) * count, cudaMemcpyHostToDevice, st));
   if (s.multi) CUDA_TRY(cudaMemcpyAsync(s.d_scenes, s.h_scenes, sizeof(Scene) * s.scene_count, cudaMemcpyHostToDevice, st));
-  if (s.hzb_w)
-    CUDA_TRY(timed(ctx, capture, VGC_KERNEL_HZB, st, [&] {
-      return launch_hzb_views(s.d_views, count, s.hzb_w, s.hzb_h, s.hzb_tail, st);
-    }));
+  if (s.hzb_w && ctx->hzb_grid)
+    CUDA_TRY(cudaMemcpyAsync(s.d_plan, s.h_plan, hzb_plan_bytes(count), cudaMemcpyHostToDevice, st));
   CUDA_TRY(timed(ctx, capture, VGC_KERNEL_RESET, st,
                  [&] { return launch_reset(s.d_views, count, s.d_unit_count, st); }));
+  if (s.hzb_w)  // after the reset, which clears the counter word a failed wait of the build reports in
+    CUDA_TRY(timed(ctx, capture, VGC_KERNEL_HZB, st, [&] {
+      return ctx->hzb_grid ? launch_hzb_stream(s.d_plan, ctx->hzb_grid, s.d_views, count, s.hzb_tail, st)
+                           : launch_hzb_views(s.d_views, count, s.hzb_w, s.hzb_h, s.hzb_tail, st);
+    }));
   CUDA_TRY(timed(ctx, capture, VGC_KERNEL_CELLS, st,
                  [&] { return launch_cells(S, scenes, s.d_views, count, s.units_total, s.d_units, s.d_unit_count, st); }));
   const uint32_t redo_grid = (uint32_t)ctx->sm_count * 2;
@@ -781,6 +869,8 @@ int vgc_context_create(const vgc_options *opts, vgc_context **out) {
   }
   ctx->select_grid = (uint32_t)std::max(1, per_sm) * ctx->sm_count;
   ctx->chunk_grid = (uint32_t)std::max(1, chunks_per_sm) * ctx->sm_count;
+  ctx->hzb_grid = hzb_stream_blocks_per_sm() * ctx->sm_count;
+  cudaGetLastError();
   ctx->meshes.resize(ctx->slot_capacity);
   ctx->mesh_host.resize(ctx->slot_capacity);
   ctx->hzb.resize(vgc_context::kHzbSlots);
@@ -1253,7 +1343,8 @@ int vgc_batch_destroy(vgc_batch *b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
-  if (b->scratch.d_views) b->ctx->bytes -= sizeof(ViewConst) * b->scratch.view_capacity;
+  if (b->scratch.d_views)
+    b->ctx->bytes -= sizeof(ViewConst) * b->scratch.view_capacity + hzb_plan_bytes(b->scratch.view_capacity);
   if (b->scratch.d_units) b->ctx->bytes -= unit_bytes(b->scratch.unit_capacity);
   free_scratch(b->scratch);
   delete b;

@@ -77,6 +77,14 @@ struct LaunchScratch {
   Scene *h_scenes = nullptr;      // pinned: the multi-scene launch's scene table (ViewConst::scene indexes it)
   Scene *d_scenes = nullptr;
   uint32_t scene_count = 0, scene_capacity = 0;
+  unsigned char *h_plan = nullptr;  // pinned: the HZB plan (HzbPlanHead) of the prepared launch, view_capacity jobs
+  unsigned char *d_plan = nullptr;
+  struct PlanKey {                  // per job: the depth image the tensor map at `maps` + 128 j describes
+    const float *depth = nullptr;
+    uint32_t w = 0, h = 0, tma = 0;
+  };
+  std::vector<PlanKey> plan_keys;
+  size_t plan_maps = 0;             // byte offset of the tensor maps the keys were made for
   cudaEvent_t done = nullptr;
   bool pending = false;
 };
@@ -88,6 +96,7 @@ struct vgc_context {
   int sm_count = 0;
   uint32_t select_grid = 0;  // persistent grid of k_instances
   uint32_t chunk_grid = 0;   // persistent grid of k_chunks
+  uint32_t hzb_grid = 0;     // persistent grid of k_hzb_stream (0: the per-view tile kernel instead)
   uint64_t bytes = 0;
   std::mutex mu;
   // host mirrors of the resident scene

@@ -84,6 +84,33 @@ struct HzbDesc {
   uint32_t off[kMaxHzbLevels], w[kMaxHzbLevels], h[kMaxHzbLevels];
 };
 
+// The HZB builds of one launch sequence as one stream of 128 x 32 mip-0 strips (k_hzb_stream): a header, one job per
+// view that brings a depth image, then one tensor map per job. Written on the host into pinned memory and copied
+// with the view constants.
+struct HzbPlanHead {
+  uint32_t jobs, tiles;  // jobs; strips of all jobs
+  uint32_t maps;         // byte offset of the tensor maps (kTensorMapBytes each, in job order)
+  uint32_t pad[13];
+};
+struct HzbJob {
+  const float *depth;    // the view's depth image: mip 0
+  const HzbDesc *desc;   // the HZB slot's descriptor (device)
+  uint32_t *error;       // the view's VGC_COUNTER_ERROR word
+  uint32_t tile0;        // the job's first strip in the stream; strip tile0 + y * tiles_x + x is at (128 x, 32 y)
+  uint16_t tiles_x;
+  uint8_t tma;           // 1: the job's tensor map describes the depth image (else plain loads)
+  uint8_t copy_mip0;     // 1: mip 0 is copied into the slot (0: the cut reads it from the depth image)
+};
+constexpr uint32_t kTensorMapBytes = 128;  // CUtensorMap, 64-byte aligned
+constexpr uint32_t kHzbStripW = 128, kHzbStripH = 32;  // strip of the stream (and box of its tensor maps)
+__host__ __device__ constexpr size_t hzb_plan_maps(uint32_t jobs) {  // byte offset of the tensor maps
+  return sizeof(HzbPlanHead) + (((size_t)jobs * sizeof(HzbJob) + 63) & ~size_t(63));
+}
+__host__ __device__ constexpr size_t hzb_plan_bytes(uint32_t jobs) {
+  return hzb_plan_maps(jobs) + (size_t)jobs * kTensorMapBytes;
+}
+static_assert(sizeof(HzbJob) == 32 && sizeof(HzbPlanHead) == 64, "plan layout");
+
 // Per-view constants derived on the host in double precision (VirtualGeometry.ts:414-442) and stored as float.
 struct ViewConst {
   float V[12];        // rows 0..2 of world->view, row-major 3x4

@@ -1402,12 +1402,13 @@ __global__ void __launch_bounds__(256) k_hzb_tiles_views(const ViewConst *__rest
   hzb_tile_pair(V.depth, H, const_cast<float *>(H.data), V.hzb_mip0 == nullptr, ox, oy, s3);
 }
 
-__global__ void __launch_bounds__(1024) k_hzb_tail_views(const ViewConst *__restrict__ views) {
+// Levels `first` and up of each building view's HZB, one block per view (the tile kernels wrote the levels below).
+__global__ void __launch_bounds__(1024) k_hzb_tail_views(const ViewConst *__restrict__ views, uint32_t first) {
   const ViewConst &V = views[blockIdx.x];
   if (!V.build_hzb) return;
   const HzbDesc &H = *V.hzb_desc;
   float *out = const_cast<float *>(H.data);
-  for (uint32_t l = kHzbTileLevels; l < H.levels; l++) {
+  for (uint32_t l = first; l < H.levels; l++) {
     const float *src = out + H.off[l - 1];
     const uint32_t sw = H.w[l - 1], sh = H.h[l - 1];
     for (uint32_t i = threadIdx.x; i < H.w[l] * H.h[l]; i += blockDim.x) {
@@ -1434,6 +1435,269 @@ __global__ void __launch_bounds__(1024) k_hzb_tail(HzbDesc H, float *__restrict_
       out[H.off[l] + i] = fmaxf(a, b);
     }
     __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------------------------------------ HZB strip stream
+// The HZB builds of a launch sequence as one persistent pass over 128 x 32 strips of mip 0 of all its jobs (the
+// views that bring a depth image; HzbPlanHead / HzbJob), levels 1..4; levels 5 and up by k_hzb_tail_views. Block b
+// takes the contiguous strips [b T / grid, (b + 1) T / grid) of the stream's T strips.
+//
+// Warp 8 streams the strips in: lane 0 waits until the consumers released a stage (an `empty` mbarrier, one arrival
+// per consumer warp), looks up the strip's job and issues a 2D bulk-tensor copy (TMA, one CTA, no multicast) of the
+// strip from the depth image into the stage, completing on the stage's `full` mbarrier; kHzbStages strips are in
+// flight. The TMA unit fills texels past the image's edge with zeros; the consumers' reads clamp to the image, so the
+// values are those of clamped loads. A job whose image no tensor map describes (width not a multiple of 4, pointer not
+// 16-byte aligned, or smaller than a strip) has its strips loaded by the consumers themselves, in the same pass.
+//
+// Warps 0..7 reduce: warp w takes the 32 x 16 pixels at column 32 (w & 3), row 16 (w >> 2) of the strip, lane l the
+// 4 x 4 patch at (4 (l & 7), 4 (l >> 3)) of those; levels 1 and 2 of the patch in registers, level 3 (2 x 2 patches:
+// lanes l ^ 1, l ^ 8) and level 4 (4 x 4 patches: lanes l ^ 2, l ^ 16) by shuffles, so no warp waits for another.
+// Every wait gives up after about a second (or when another warp gave up): the block then sets VGC_FAULT_HZB_WAIT in
+// every job's view and leaves, the streaming lane after its copies still in flight have landed.
+#ifndef VGC_HZB_STAGES
+#define VGC_HZB_STAGES 4  // strips in flight per block
+#endif
+#ifndef VGC_HZB_BLOCKS_PER_SM
+#define VGC_HZB_BLOCKS_PER_SM 3
+#endif
+constexpr uint32_t kHzbStages = VGC_HZB_STAGES;
+constexpr uint32_t kStripW = kHzbStripW, kStripH = kHzbStripH, kStripFloats = kStripW * kStripH;
+constexpr uint32_t kStripBytes = kStripFloats * 4;
+constexpr uint32_t kHzbStripLevels = 5;  // levels 1..4 per strip; k_hzb_tail_views from level 5
+constexpr size_t kHzbStreamSmem = (size_t)kHzbStages * kStripBytes + 128;  // + slack to align the stages to 128
+constexpr uint64_t kWaitLimitNs = 1000000000ull;
+constexpr uint32_t kHzbConsumerWarps = 8, kHzbStreamThreads = 32 * (kHzbConsumerWarps + 1);
+static_assert(kStripW == 128 && kStripH == 32, "the consumer layout covers 128 x 32 strips with 8 warps");
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(done)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Phase `parity` of `bar` completed: false once about a second (or 2^30 polls) passed without it, or once `*abort`
+// (when given) is set.
+__device__ __noinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile uint32_t *abort) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (uint32_t i = 0; i < (1u << 30); i++) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 63u) == 0 && (global_ns() - t0 > kWaitLimitNs || (abort && *abort))) return false;
+  }
+  return false;
+}
+
+// The tensor map was written to global memory by a copy before this launch: order that write before its use by
+// the tensor-map proxy.
+__device__ __forceinline__ void tensormap_acquire(const void *map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
+}
+
+// The strip (128 x 32 floats) at element (x, y) of the map's image into `dst`, completing on `bar`. x is a multiple
+// of 128 (512 bytes), so the copy starts on a 16-byte boundary.
+__device__ __forceinline__ void tma_strip(float *dst, const void *map, uint32_t x, uint32_t y, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+          "r"(smem_addr(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// Sizes and offsets of levels 0..4 of a job's HZB slot, held in registers while a warp works on the job.
+struct StripDesc {
+  float *out;
+  uint32_t levels;
+  uint32_t off[5], w[5], h[5];
+};
+
+__device__ __forceinline__ void strip_desc(const HzbDesc &H, StripDesc &D) {
+  D.out = const_cast<float *>(H.data);
+  D.levels = H.levels;
+#pragma unroll
+  for (int l = 0; l < 5; l++) D.off[l] = H.off[l], D.w[l] = H.w[l], D.h[l] = H.h[l];
+}
+
+__device__ __forceinline__ void strip_store(const StripDesc &D, uint32_t l, uint32_t x, uint32_t y, float v) {
+  if (l < D.levels && x < D.w[l] && y < D.h[l]) D.out[D.off[l] + (size_t)y * D.w[l] + x] = v;
+}
+
+__global__ void __launch_bounds__(kHzbStreamThreads, VGC_HZB_BLOCKS_PER_SM) k_hzb_stream(
+    const unsigned char *__restrict__ plan) {
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  // kHzbStages strips from the first 128-byte boundary of the dynamic shared memory (a bulk-tensor destination)
+  float *stage = reinterpret_cast<float *>(dyn_smem + ((128u - (smem_addr(dyn_smem) & 127u)) & 127u));
+  __shared__ __align__(8) uint64_t full[kHzbStages], empty[kHzbStages];
+  __shared__ uint4 meta[kHzbStages];  // job, ox, oy, tma of the strip in each stage
+  __shared__ uint32_t abort;
+  const HzbPlanHead &P = *reinterpret_cast<const HzbPlanHead *>(plan);
+  const HzbJob *jobs = reinterpret_cast<const HzbJob *>(plan + sizeof(HzbPlanHead));
+  const uint32_t njobs = P.jobs;
+  const uint32_t first = (uint32_t)((uint64_t)P.tiles * blockIdx.x / gridDim.x);
+  const uint32_t last = (uint32_t)((uint64_t)P.tiles * (blockIdx.x + 1) / gridDim.x);
+  if (first >= last) return;
+  const uint32_t t = threadIdx.x, warp = t >> 5, lane = t & 31u;
+  if (t == 0) {
+    for (uint32_t s = 0; s < kHzbStages; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kHzbConsumerWarps);
+    }
+    abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  volatile uint32_t *flag = &abort;
+  auto give_up = [&] {  // a wait gave up: stop the other warps and report it in every job's view
+    *flag = 1;
+    for (uint32_t j = 0; j < njobs; j++)
+      if (jobs[j].error) atomicOr(jobs[j].error, (uint32_t)VGC_FAULT_HZB_WAIT);
+  };
+  if (warp == kHzbConsumerWarps) {  // the streaming warp: lane 0 issues every copy of the block
+    if (lane != 0) return;
+    const unsigned char *maps = plan + P.maps;
+    uint32_t acquired = ~0u, k = 0;
+    for (;; k++) {
+      const uint32_t item = first + k;
+      if (item >= last) return;  // the consumers wait for the copies issued so far
+      const uint32_t s = k % kHzbStages;
+      if (k >= kHzbStages && !mbar_wait(&empty[s], (k / kHzbStages - 1) & 1u, flag)) break;
+      uint32_t lo = 0, hi = njobs;  // the last job whose first strip is <= item
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (jobs[mid].tile0 <= item) lo = mid;
+        else hi = mid;
+      }
+      const uint32_t r = item - jobs[lo].tile0, sx = jobs[lo].tiles_x, tma = jobs[lo].tma;
+      const uint32_t ox = (r % sx) * kStripW, oy = (r / sx) * kStripH;
+      meta[s] = make_uint4(lo, ox, oy, tma);
+      if (tma) {
+        const void *map = maps + (size_t)lo * kTensorMapBytes;
+        if (lo != acquired) {
+          tensormap_acquire(map);
+          acquired = lo;
+        }
+        mbar_arrive_tx(&full[s], kStripBytes);
+        tma_strip(stage + s * kStripFloats, map, ox, oy, &full[s]);
+      } else {
+        mbar_arrive(&full[s]);  // the consumers load this strip themselves
+      }
+    }
+    give_up();  // then let the copies in flight land before this lane exits
+    for (uint32_t q = k > kHzbStages ? k - kHzbStages : 0; q < k; q++)
+      mbar_wait(&full[q % kHzbStages], (q / kHzbStages) & 1u, nullptr);
+    return;
+  }
+  const uint32_t px = 32u * (warp & 3u) + 4u * (lane & 7u), py = 16u * (warp >> 2) + 4u * (lane >> 3);  // in the strip
+  StripDesc D;
+  uint32_t job = ~0u, W = 0, Hh = 0;
+  bool copy_mip0 = false;
+  const float *depth = nullptr;
+  for (uint32_t k = 0;; k++) {
+    if (first + k >= last) return;  // every strip of this block reduced
+    const uint32_t s = k % kHzbStages;
+    if (!__all_sync(0xffffffffu, mbar_wait(&full[s], (k / kHzbStages) & 1u, flag))) {
+      if (lane == 0) give_up();
+      return;
+    }
+    const uint4 m = meta[s];
+    if (m.x != job) {
+      job = m.x;
+      const HzbJob &J = jobs[job];
+      strip_desc(*J.desc, D);
+      W = D.w[0], Hh = D.h[0], copy_mip0 = J.copy_mip0 != 0, depth = J.depth;
+    }
+    const uint32_t gx = m.y + px, gy = m.z + py;  // this lane's patch in the image
+    float v[4][4];
+    const bool inside = m.y + kStripW <= W && m.z + kStripH <= Hh;
+    if (m.w) {
+      const float *st = stage + s * kStripFloats;
+      if (inside) {
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+          const float4 q = *reinterpret_cast<const float4 *>(st + (py + r) * kStripW + px);
+          v[r][0] = q.x, v[r][1] = q.y, v[r][2] = q.z, v[r][3] = q.w;
+        }
+      } else {  // clamped to the image (every index stays inside the strip: m.y < W, m.z < Hh)
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+          const uint32_t y = min(gy + r, Hh - 1) - m.z;
+#pragma unroll
+          for (int c = 0; c < 4; c++) v[r][c] = st[y * kStripW + (min(gx + c, W - 1) - m.y)];
+        }
+      }
+    } else {
+      const bool vec = (W & 3u) == 0 && (reinterpret_cast<uintptr_t>(depth) & 15u) == 0 && gx + 3 < W;
+#pragma unroll
+      for (int r = 0; r < 4; r++) {
+        const float *row = depth + (size_t)min(gy + r, Hh - 1) * W;
+        if (vec) {
+          const float4 q = __ldg(reinterpret_cast<const float4 *>(row + gx));
+          v[r][0] = q.x, v[r][1] = q.y, v[r][2] = q.z, v[r][3] = q.w;
+        } else {
+#pragma unroll
+          for (int c = 0; c < 4; c++) v[r][c] = __ldg(row + min(gx + c, W - 1));
+        }
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);  // this warp is done with stage s
+    if (copy_mip0) {
+      float *o0 = D.out + D.off[0];
+      const bool vec = (W & 3u) == 0 && (reinterpret_cast<uintptr_t>(o0) & 15u) == 0 && gx + 3 < W;
+#pragma unroll
+      for (int r = 0; r < 4; r++) {
+        if (gy + r >= Hh) continue;
+        float *row = o0 + (size_t)(gy + r) * W;
+        if (vec) {
+          *reinterpret_cast<float4 *>(row + gx) = make_float4(v[r][0], v[r][1], v[r][2], v[r][3]);
+        } else {
+#pragma unroll
+          for (int c = 0; c < 4; c++)
+            if (gx + c < W) row[gx + c] = v[r][c];
+        }
+      }
+    }
+    float a[2][2];
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        a[i][j] = fmaxf(fmaxf(v[2 * i][2 * j], v[2 * i][2 * j + 1]), fmaxf(v[2 * i + 1][2 * j], v[2 * i + 1][2 * j + 1]));
+        strip_store(D, 1, gx / 2 + j, gy / 2 + i, a[i][j]);
+      }
+    const float b = fmaxf(fmaxf(a[0][0], a[0][1]), fmaxf(a[1][0], a[1][1]));
+    strip_store(D, 2, gx / 4, gy / 4, b);
+    float m3 = fmaxf(b, __shfl_xor_sync(0xffffffffu, b, 1));
+    m3 = fmaxf(m3, __shfl_xor_sync(0xffffffffu, m3, 8));
+    if ((lane & 9u) == 0) strip_store(D, 3, gx / 8, gy / 8, m3);
+    float m4 = fmaxf(m3, __shfl_xor_sync(0xffffffffu, m3, 2));
+    m4 = fmaxf(m4, __shfl_xor_sync(0xffffffffu, m4, 16));
+    if ((lane & 27u) == 0) strip_store(D, 4, gx / 16, gy / 16, m4);
+    if (*flag) return;  // another warp gave up
   }
 }
 
@@ -1726,7 +1990,27 @@ cudaError_t launch_hzb_views(const ViewConst *views, uint32_t nviews, uint32_t m
   k_hzb_tiles_views<<<grid, 256, 0, st>>>(views);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || !tail) return e;
-  k_hzb_tail_views<<<nviews, 1024, 0, st>>>(views);
+  k_hzb_tail_views<<<nviews, 1024, 0, st>>>(views, kHzbTileLevels);
+  return cudaGetLastError();
+}
+
+uint32_t hzb_stream_blocks_per_sm() {
+  if (cudaFuncSetAttribute(k_hzb_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHzbStreamSmem) !=
+      cudaSuccess)
+    return 0;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_hzb_stream, kHzbStreamThreads, kHzbStreamSmem) !=
+      cudaSuccess)
+    return 0;
+  return (uint32_t)n;
+}
+
+cudaError_t launch_hzb_stream(const unsigned char *plan, uint32_t grid, const ViewConst *views, uint32_t nviews,
+                              bool tail, cudaStream_t st) {
+  k_hzb_stream<<<grid, kHzbStreamThreads, kHzbStreamSmem, st>>>(plan);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !tail) return e;
+  k_hzb_tail_views<<<nviews, 1024, 0, st>>>(views, kHzbStripLevels);
   return cudaGetLastError();
 }
 

@@ -45,6 +45,12 @@ cudaError_t launch_hzb(const float *depth, const HzbDesc &H, float *out, int cop
 // HZB builds of the views whose constants carry build_hzb (grid covers the largest depth image).
 cudaError_t launch_hzb_views(const ViewConst *views, uint32_t nviews, uint32_t max_w,
                              uint32_t max_h, bool tail, cudaStream_t st);
+// The same builds as one stream of strips (k_hzb_stream, levels 0..4) from the launch's HZB plan in device memory;
+// `grid` blocks (hzb_stream_blocks_per_sm() per SM), then the tail kernel for levels 5+ when `tail`.
+cudaError_t launch_hzb_stream(const unsigned char *plan, uint32_t grid, const ViewConst *views, uint32_t nviews,
+                              bool tail, cudaStream_t st);
+// Blocks of k_hzb_stream resident per SM (sets its shared-memory limit on the first call for the current device).
+uint32_t hzb_stream_blocks_per_sm();
 cudaError_t launch_select_cut(const Scene &S, uint32_t slot, uint32_t mcount, uint32_t count, const float *vm16,
                               const float *params, float threshold, float blend, uint8_t *lo, uint8_t *hi, uint32_t grid,
                               cudaStream_t st);

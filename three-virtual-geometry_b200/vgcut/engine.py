@@ -95,7 +95,7 @@ class Stats(C.Structure):
                 ("threshold_scale", C.c_float * 2), ("fill", C.c_float * 2), ("effective_threshold", C.c_float),
                 ("instances_tested", C.c_uint32), ("meshlets_tested", C.c_uint32), ("fast_emitted", C.c_uint32),
                 ("levels_read", C.c_uint32), ("predicted_triangles", C.c_uint64),
-                ("meshlets_queued", C.c_uint32)]
+                ("meshlets_queued", C.c_uint32), ("faults", C.c_uint32)]
 
     def as_dict(self) -> dict:
         out = {}
