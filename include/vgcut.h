@@ -400,6 +400,10 @@ int vgc_debug_scene(const vgc_context *ctx, float *cells, uint32_t cell_capacity
 /* The device's cell records in the same 8-float form (after the pending upload, if any): instance updates recompute
    them on the device, and they must equal the host's. */
 int vgc_debug_cells_device(vgc_context *ctx, float *cells, uint32_t capacity, uint32_t *count);
+/* Runs the device's bounded mbarrier wait (the one the HZB strip stream waits with) on a barrier that nothing
+   completes, with a limit of `limit_us` microseconds: *completed = 0 and *waited_ns = the time it waited before it
+   gave up; the context stays usable. */
+int vgc_debug_wait_probe(vgc_context *ctx, uint32_t limit_us, uint32_t *completed, uint64_t *waited_ns);
 
 #ifdef __cplusplus
 }

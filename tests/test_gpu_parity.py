@@ -373,3 +373,23 @@ def test_depth_as_mip0(ruins_small):
             data = d2h(info["data"], len(mips), np.float32)
             assert np.array_equal(data[:off[1]], old[:off[1]]), "mip 0 of the slot is not written"
             assert np.array_equal(data[off[1]:], mips[off[1]:]), "mips 1 and up are the new image's"
+
+
+def test_bounded_wait_gives_up_and_context_stays_usable(ruins_small):
+    """The mbarrier wait the HZB strip stream uses, on a barrier nothing completes: it gives up after its limit (not
+    later than a few milliseconds past it) and reports that it did not complete; a cut with an HZB build afterwards
+    is still exact and reports no fault."""
+    import torch
+    h = ruins_small
+    for limit_us in (2000, 20000):
+        done, ns = h.vg.wait_probe(limit_us)
+        assert done == 0
+        assert limit_us * 1000 <= ns < limit_us * 1000 + 50_000_000, ns
+    img = h.spec.depth_images[0]
+    d = torch.from_numpy(img).cuda()
+    cam = h.spec.cameras[0]
+    v = engine.make_view(cam, engine.ViewParams(error_threshold=1.0, hzb=12), depth=(d.data_ptr(), img.shape[1], img.shape[0]))
+    h.vg.cut([v], first_slot=0)
+    assert h.vg.read_stats(0)["faults"] == 0
+    mips = O.hzb_build(img)[0]
+    assert np.array_equal(d2h(h.vg.hzb_info(12)["data"], len(mips), np.float32), mips)

@@ -1122,6 +1122,22 @@ int vgc_mesh_remove(vgc_context *ctx, uint32_t slot) {
   return publish_mesh_record(ctx, slot);
 }
 
+int vgc_debug_wait_probe(vgc_context *ctx, uint32_t limit_us, uint32_t *completed, uint64_t *waited_ns) {
+  if (!ctx || !completed || !waited_ns || limit_us == 0 || limit_us > 2000000)
+    return fail(VGC_INVALID_ARG, "vgc_debug_wait_probe: bad arguments (limit 1 us .. 2 s)");
+  cudaSetDevice(ctx->device);
+  unsigned long long *d = nullptr, h[2] = {0, 0};
+  CUDA_TRY(cudaMalloc(&d, sizeof h));
+  cudaError_t e = launch_wait_probe((uint64_t)limit_us * 1000u, d, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h, d, sizeof h, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(VGC_DEVICE_ERROR, std::string("vgc_debug_wait_probe: ") + cudaGetErrorString(e));
+  *completed = (uint32_t)h[0];
+  *waited_ns = h[1];
+  return VGC_OK;
+}
+
 int vgc_debug_cells_device(vgc_context *ctx, float *cells, uint32_t capacity, uint32_t *count) {
   if (!ctx || !count) return fail(VGC_INVALID_ARG, "null argument");
   int rc = sync_scene(ctx);

@@ -1500,16 +1500,33 @@ __device__ __forceinline__ uint64_t global_ns() {
   return t;
 }
 
-// Phase `parity` of `bar` completed: false once about a second (or 2^30 polls) passed without it, or once `*abort`
+// Phase `parity` of `bar` completed: false once `limit_ns` (or 2^30 polls) passed without it, or once `*abort`
 // (when given) is set.
-__device__ __noinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile uint32_t *abort) {
+__device__ __noinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile uint32_t *abort,
+                                       uint64_t limit_ns = kWaitLimitNs) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_ns();
   for (uint32_t i = 0; i < (1u << 30); i++) {
     if (mbar_try_wait(bar, parity)) return true;
-    if ((i & 63u) == 0 && (global_ns() - t0 > kWaitLimitNs || (abort && *abort))) return false;
+    if ((i & 63u) == 0 && (global_ns() - t0 > limit_ns || (abort && *abort))) return false;
   }
   return false;
+}
+
+// mbar_wait on a barrier that nothing arrives at: out[0] = 1 if it completed (never), out[1] = nanoseconds waited.
+__global__ void k_wait_probe(uint64_t limit_ns, unsigned long long *out) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const uint64_t t0 = global_ns();
+    const bool done = mbar_wait(&bar, 0, nullptr, limit_ns);
+    out[1] = global_ns() - t0;
+    out[0] = done ? 1ull : 0ull;
+  }
 }
 
 // The tensor map was written to global memory by a copy before this launch: order that write before its use by
@@ -1991,6 +2008,11 @@ cudaError_t launch_hzb_views(const ViewConst *views, uint32_t nviews, uint32_t m
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || !tail) return e;
   k_hzb_tail_views<<<nviews, 1024, 0, st>>>(views, kHzbTileLevels);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wait_probe(uint64_t limit_ns, unsigned long long *out, cudaStream_t st) {
+  k_wait_probe<<<1, 32, 0, st>>>(limit_ns, out);
   return cudaGetLastError();
 }
 

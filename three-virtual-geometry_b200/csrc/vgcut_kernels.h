@@ -49,6 +49,8 @@ cudaError_t launch_hzb_views(const ViewConst *views, uint32_t nviews, uint32_t m
 // `grid` blocks (hzb_stream_blocks_per_sm() per SM), then the tail kernel for levels 5+ when `tail`.
 cudaError_t launch_hzb_stream(const unsigned char *plan, uint32_t grid, const ViewConst *views, uint32_t nviews,
                               bool tail, cudaStream_t st);
+// The bounded mbarrier wait of the strip stream on a barrier nothing completes (out[0]: completed, out[1]: ns waited).
+cudaError_t launch_wait_probe(uint64_t limit_ns, unsigned long long *out, cudaStream_t st);
 // Blocks of k_hzb_stream resident per SM (sets its shared-memory limit on the first call for the current device).
 uint32_t hzb_stream_blocks_per_sm();
 cudaError_t launch_select_cut(const Scene &S, uint32_t slot, uint32_t mcount, uint32_t count, const float *vm16,

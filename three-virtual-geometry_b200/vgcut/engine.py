@@ -153,6 +153,7 @@ def lib() -> C.CDLL:
         "vgc_kernel_times": ([vp, P(C.c_double), P(C.c_uint32), C.c_int], C.c_int),
         "vgc_debug_scene": ([vp, P(C.c_float), C.c_uint32, P(C.c_float), C.c_uint32, P(C.c_uint32), P(C.c_uint32)], C.c_int),
         "vgc_debug_cells_device": ([vp, P(C.c_float), C.c_uint32, P(C.c_uint32)], C.c_int),
+        "vgc_debug_wait_probe": ([vp, C.c_uint32, P(C.c_uint32), P(C.c_uint64)], C.c_int),
         "vgc_occluder_depth": ([vp, C.c_uint32, P(View), vp, C.c_uint32, C.c_uint32, vp], C.c_int),
         "vgc_occluder_depth_batch": ([vp, C.c_uint32, P(C.c_uint32), P(View), P(vp), C.c_uint32, C.c_uint32, vp],
                                      C.c_int),
@@ -562,6 +563,12 @@ class VirtualGeometry:
         cells = np.zeros((n.value, 8), np.float32)
         check(lib().vgc_debug_cells_device(self.handle, _fp(cells), n.value, C.byref(n)))
         return cells
+
+    def wait_probe(self, limit_us: int) -> tuple[int, int]:
+        """The device's bounded mbarrier wait run out on purpose: (completed, nanoseconds waited)."""
+        done, ns = C.c_uint32(), C.c_uint64()
+        check(lib().vgc_debug_wait_probe(self.handle, limit_us, C.byref(done), C.byref(ns)))
+        return done.value, ns.value
 
     def select_cut(self, slot: int, viewmodels: np.ndarray, proj_scale, near, scale, threshold: float,
                    blend: float = 1.0) -> tuple[np.ndarray, np.ndarray]:
