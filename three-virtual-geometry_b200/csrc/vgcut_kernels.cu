@@ -733,51 +733,63 @@ __device__ __forceinline__ void drain_queue(const Scene &S, const ViewConst &V, 
   }
 }
 
-// One warp-unit w (32 instances of a visible (view, cell) unit) of the instance pass. REDO: a unit whose items did not
-// fit the chunk queue in this pass (marked in `overflow`): its instance tests are repeated (the same arithmetic, so
-// the same items) and its items tested in place; its counters and fast-path meshlets were already emitted.
+// Survivors of a half-unit's instance tests, compacted per warp: instance index in the cell (7 bits) and flags, the
+// LOD sphere's pixel scales at its near and far distances.
+struct Survivor {
+  uint32_t bits;  // il | camera << 7 | shadow << 8 | inside0 << 9 | inside1 << 10
+  float px_min, px_max;
+};
+constexpr uint32_t kHalfUnit = 64;  // instances of one (view, cell) unit a warp tests at a time
+
+// One half-unit w (instances 64 (w & 1) .. + 63 of the visible (view, cell) unit w >> 1) of the instance pass. The
+// warp first runs the instance tests (frustum, minimum pixel size, draw distance, occlusion) over the half-unit, 32
+// instances at a time, and compacts the survivors in order into `list`; the level ranges, item trimming, fast path,
+// counters and span / chunk emission then run on full warps of survivors (pass p: survivors 32 p .. 32 p + 31).
+// Overflow bit 2 w + p marks a pass whose items did not fit the chunk queue. REDO: pass `redo_pass` of such a
+// half-unit; its tests are repeated (the same arithmetic and order, so the same survivors and items) and its items
+// tested in place; its counters and fast-path meshlets were already emitted.
 template <bool HIST, bool MULTI, bool REDO>
 __device__ __forceinline__ void instance_unit(const Scene &S0, const Scene *__restrict__ scenes,
                                               const ViewConst *__restrict__ views, const HzbDesc *__restrict__ hzbs0,
                                               const uint2 *__restrict__ units, uint32_t *__restrict__ ctl,
                                               uint4 *__restrict__ queue, uint32_t capacity, int round,
                                               uint32_t chunk_shift, uint32_t *__restrict__ overflow, WarpStage *ws,
-                                              uint32_t w) {
+                                              Survivor *__restrict__ list, uint32_t w, uint32_t redo_pass) {
   const uint32_t lane = threadIdx.x & 31;
-  {
-    const uint2 unit = units[w >> 2];
-    const ViewConst &V = views[unit.x];
-    if (HIST && !(V.budget > 0.0f)) return;
-    bool redo0 = true, redo1 = !HIST;
-    if (round > 0) {
-      redo0 = V.counters[VGC_COUNTER_REDO0] != 0;
-      redo1 = V.counters[VGC_COUNTER_REDO1] != 0;
-      if (!redo0 && !redo1) return;
-    }
-    const auto &S = SceneOf<MULTI>::get(S0, scenes, V);
-    const HzbDesc *__restrict__ hzbs = SceneOf<MULTI>::hzbs(hzbs0, S);
-    const CellRec cell = S.cells[unit.y];
-    const uint32_t il = ((w & 3u) << 5) + lane;
-    if (((w & 3u) << 5) >= cell.count) return;
-    const MeshRec &mesh = S.meshes[cell.slot];
-    const ViewBands b = bands_of(V);
-    const uint32_t levels = min(mesh.level_count, kMaxLevels);
-    const LevelRec *L = S.levels + mesh.level_base;
-    const uint32_t instance = cell.first + il;
-    const bool valid = il < cell.count;
-    const bool occl_on = mesh.occlusion != 0;
-    float VM[13];
+  const uint2 unit = units[w >> 1];
+  const ViewConst &V = views[unit.x];
+  if (HIST && !(V.budget > 0.0f)) return;
+  bool redo0 = true, redo1 = !HIST;
+  if (round > 0) {
+    redo0 = V.counters[VGC_COUNTER_REDO0] != 0;
+    redo1 = V.counters[VGC_COUNTER_REDO1] != 0;
+    if (!redo0 && !redo1) return;
+  }
+  const auto &S = SceneOf<MULTI>::get(S0, scenes, V);
+  const HzbDesc *__restrict__ hzbs = SceneOf<MULTI>::hzbs(hzbs0, S);
+  const CellRec cell = S.cells[unit.y];
+  const uint32_t base = (w & 1u) * kHalfUnit;
+  if (base >= cell.count) return;
+  const MeshRec &mesh = S.meshes[cell.slot];
+  const ViewBands b = bands_of(V);
+  const uint32_t levels = min(mesh.level_count, kMaxLevels);
+  const LevelRec *L = S.levels + mesh.level_base;
+  const bool occl_on = mesh.occlusion != 0;
+  const bool no_frustum = !V.frustum;
+  // ---- instance tests, compacted
+  uint32_t n_surv = 0, n_occl = 0;  // warp-uniform
+  for (uint32_t q = 0; q < kHalfUnit && base + q < cell.count; q += 32) {
+    const uint32_t il = base + q + lane;
+    bool camera = false, shadow = false, inside0 = true, inside1 = true;
+    float px_min = 0.0f, px_max = 0.0f;
     bool occluded_now = false;
-    LevelRange r0{0xffffffffu, 0, 0, 0, 0, 0}, r1{0xffffffffu, 0, 0, 0, 0, 0};
-    uint32_t t0f = 0, t0l = 0, t1f = 0, t1l = 0;  // the items' trimmed meshlet ranges
-    bool fast0 = false, fast1 = false, inside0 = true, inside1 = true;
-    if (valid) {
-      model_view(V.V, S.inst + (size_t)instance * 4, VM, VM[12]);
+    if (il < cell.count) {
+      float VM[13];
+      model_view(V.V, S.inst + (size_t)(cell.first + il) * 4, VM, VM[12]);
       const float scale = VM[12];
       float c[3];
       xform(VM, mesh.sphere.x, mesh.sphere.y, mesh.sphere.z, c);
       const float radius = mesh.sphere.w * scale;
-      const bool no_frustum = !V.frustum;
       bool in_camera = !V.cascade && (no_frustum || frustum(V, c, false) >= -radius);
       bool in_shadow = mesh.shadow != 0 && (no_frustum || frustum(V, c, true) >= -radius);
       in_camera = in_camera && redo0;
@@ -791,70 +803,99 @@ __device__ __forceinline__ void instance_unit(const Scene &S0, const Scene *__re
           in_camera = false;
           occluded_now = true;
         }
-        float lc[3];
-        xform(VM, mesh.lod.x, mesh.lod.y, mesh.lod.z, lc);
-        const float d = len3(lc), r = mesh.lod.w * scale;
-        const float px_min = (scale * V.proj_scale) / fmx(d - r, V.near_);
-        const float px_max = (scale * V.proj_scale) / fmx(d + r, V.near_);
-        float cc[3];
-        xform(VM, mesh.cull.x, mesh.cull.y, mesh.cull.z, cc);
-        const float cr = mesh.cull.w * scale;
-        // inside: the cullBoundsSphere lies in the frustum, so every meshlet passes its frustum test
-        if (HIST && in_camera) {
-          const float sc = get_state(V.state, 0);
-          const float e0 = budget_e(V, sc, 0), h255 = budget_high(V, sc, 255);
-          r0 = level_range(L, levels, e0, h255, px_min, px_max);
-          inside0 = no_frustum || frustum(V, cc, false) >= cr;
-          trim_item(S, mesh, L, r0, e0, h255, px_min, px_max, t0f, t0l);
-        } else if (in_camera) {
-          r0 = level_range(L, levels, b.low0, b.high0, px_min, px_max);
-          inside0 = no_frustum || frustum(V, cc, false) >= cr;
-          fast0 = r0.last > r0.first && r0.possible == r0.last - r0.first && r0.guaranteed == r0.possible &&
-                  r0.possible <= kFastPathMax && inside0;
-          trim_item(S, mesh, L, r0, b.low0, b.high0, px_min, px_max, t0f, t0l);
-        }
-        if (in_shadow) {
-          r1 = level_range(L, levels, b.low1, b.high1, px_min, px_max);
-          inside1 = no_frustum || frustum(V, cc, true) >= cr;
-          fast1 = r1.last > r1.first && r1.possible == r1.last - r1.first && r1.guaranteed == r1.possible &&
-                  r1.possible <= kFastPathMax && inside1;
-          trim_item(S, mesh, L, r1, b.low1, b.high1, px_min, px_max, t1f, t1l);
+        if (in_camera || in_shadow) {
+          float lc[3];
+          xform(VM, mesh.lod.x, mesh.lod.y, mesh.lod.z, lc);
+          const float d = len3(lc), r = mesh.lod.w * scale;
+          px_min = (scale * V.proj_scale) / fmx(d - r, V.near_);
+          px_max = (scale * V.proj_scale) / fmx(d + r, V.near_);
+          float cc[3];
+          xform(VM, mesh.cull.x, mesh.cull.y, mesh.cull.z, cc);
+          const float cr = mesh.cull.w * scale;
+          // inside: the cullBoundsSphere lies in the frustum, so every meshlet passes its frustum test
+          if (in_camera) inside0 = no_frustum || frustum(V, cc, false) >= cr;
+          if (in_shadow) inside1 = no_frustum || frustum(V, cc, true) >= cr;
+          camera = in_camera;
+          shadow = in_shadow;
         }
       }
+    }
+    const bool alive = camera || shadow;
+    const uint32_t mask = __ballot_sync(0xffffffffu, alive);
+    if (alive)
+      list[n_surv + __popc(mask & ((1u << lane) - 1u))] =
+          Survivor{il | (camera ? 1u << 7 : 0u) | (shadow ? 1u << 8 : 0u) | (inside0 ? 1u << 9 : 0u) |
+                       (inside1 ? 1u << 10 : 0u),
+                   px_min, px_max};
+    n_surv += __popc(mask);
+    n_occl += __popc(__ballot_sync(0xffffffffu, occluded_now));
+  }
+  __syncwarp();
+  if (!HIST && !REDO && lane == 0) {
+    uint32_t *ctr = V.counters;
+    if (n_occl) atomicAdd(ctr + VGC_COUNTER_OCCLUDED, n_occl);
+    atomicAdd(ctr + VGC_COUNTER_INSTANCES_TESTED, min(kHalfUnit, cell.count - base));
+    if (base == 0) atomicAdd(ctr + VGC_COUNTER_LEVELS_READ, levels);
+  }
+  // ---- level ranges, items and their spans / chunks, on full warps of survivors
+  for (uint32_t pass = 0; pass * 32 < n_surv; pass++) {
+    if (REDO && pass != redo_pass) continue;
+    const bool valid = pass * 32 + lane < n_surv;
+    Survivor sv{0u, 0.0f, 0.0f};
+    if (valid) sv = list[pass * 32 + lane];
+    const uint32_t il = sv.bits & 127u, instance = cell.first + il;
+    const bool in_camera = (sv.bits >> 7) & 1u, in_shadow = (sv.bits >> 8) & 1u;
+    const bool inside0 = (sv.bits >> 9) & 1u, inside1 = (sv.bits >> 10) & 1u;
+    const float px_min = sv.px_min, px_max = sv.px_max;
+    LevelRange r0{0xffffffffu, 0, 0, 0, 0, 0}, r1{0xffffffffu, 0, 0, 0, 0, 0};
+    uint32_t t0f = 0, t0l = 0, t1f = 0, t1l = 0;  // the items' trimmed meshlet ranges
+    bool fast0 = false, fast1 = false;
+    if (HIST && in_camera) {
+      const float sc = get_state(V.state, 0);
+      const float e0 = budget_e(V, sc, 0), h255 = budget_high(V, sc, 255);
+      r0 = level_range(L, levels, e0, h255, px_min, px_max);
+      trim_item(S, mesh, L, r0, e0, h255, px_min, px_max, t0f, t0l);
+    } else if (in_camera) {
+      r0 = level_range(L, levels, b.low0, b.high0, px_min, px_max);
+      fast0 = r0.last > r0.first && r0.possible == r0.last - r0.first && r0.guaranteed == r0.possible &&
+              r0.possible <= kFastPathMax && inside0;
+      trim_item(S, mesh, L, r0, b.low0, b.high0, px_min, px_max, t0f, t0l);
+    }
+    if (in_shadow) {
+      r1 = level_range(L, levels, b.low1, b.high1, px_min, px_max);
+      fast1 = r1.last > r1.first && r1.possible == r1.last - r1.first && r1.guaranteed == r1.possible &&
+              r1.possible <= kFastPathMax && inside1;
+      trim_item(S, mesh, L, r1, b.low1, b.high1, px_min, px_max, t1f, t1l);
     }
     const bool surv0 = r0.last > r0.first, surv1 = r1.last > r1.first;
     const bool item0 = surv0 && !fast0, item1 = surv1 && !fast1;
     if (!HIST && !REDO) {
-    // warp totals for the view's counters (one atomic per counter and warp)
-    const uint32_t n_occl = __popc(__ballot_sync(0xffffffffu, occluded_now));
-    const uint32_t n_s0 = __popc(__ballot_sync(0xffffffffu, surv0)), n_s1 = __popc(__ballot_sync(0xffffffffu, surv1));
-    const uint32_t n_i0 = __popc(__ballot_sync(0xffffffffu, item0)), n_i1 = __popc(__ballot_sync(0xffffffffu, item1));
-    const uint32_t fast_m = __reduce_add_sync(0xffffffffu, (fast0 ? r0.possible : 0u) + (fast1 ? r1.possible : 0u));
-    const uint32_t tested = __reduce_add_sync(0xffffffffu, (item0 ? r0.last - r0.first : 0u) + (item1 ? r1.last - r1.first : 0u));
-    const uint32_t queued = __reduce_add_sync(0xffffffffu, (item0 ? t0l - t0f : 0u) + (item1 ? t1l - t1f : 0u));
-    if (lane == 0) {
-      uint32_t *ctr = V.counters;
-      if (n_occl) atomicAdd(ctr + VGC_COUNTER_OCCLUDED, n_occl);
-      if (n_s0) atomicAdd(ctr + C_CUT(0) + VGC_CUT_SURVIVED, n_s0);
-      if (n_s1) atomicAdd(ctr + C_CUT(1) + VGC_CUT_SURVIVED, n_s1);
-      if (n_i0) atomicAdd(ctr + C_CUT(0) + VGC_CUT_WORK, n_i0);
-      if (n_i1) atomicAdd(ctr + C_CUT(1) + VGC_CUT_WORK, n_i1);
-      if (fast_m) atomicAdd(ctr + VGC_COUNTER_FAST_EMITTED, fast_m);
-      if (tested) atomicAdd(ctr + VGC_COUNTER_MESHLETS_TESTED, tested);
-      if (queued) atomicAdd(ctr + VGC_COUNTER_MESHLETS_QUEUED, queued);
-      atomicAdd(ctr + VGC_COUNTER_INSTANCES_TESTED, min(32u, cell.count - ((w & 3u) << 5)));
-      if ((w & 3u) == 0) atomicAdd(ctr + VGC_COUNTER_LEVELS_READ, levels);
-    }
-    emit_fast(S, V, cell.slot, 0, fast0 ? r0.possible : 0u, r0.first, instance);
-    emit_fast(S, V, cell.slot, 1, fast1 ? r1.possible : 0u, r1.first, instance);
+      // warp totals for the view's counters (one atomic per counter and warp)
+      const uint32_t n_s0 = __popc(__ballot_sync(0xffffffffu, surv0)), n_s1 = __popc(__ballot_sync(0xffffffffu, surv1));
+      const uint32_t n_i0 = __popc(__ballot_sync(0xffffffffu, item0)), n_i1 = __popc(__ballot_sync(0xffffffffu, item1));
+      const uint32_t fast_m = __reduce_add_sync(0xffffffffu, (fast0 ? r0.possible : 0u) + (fast1 ? r1.possible : 0u));
+      const uint32_t tested =
+          __reduce_add_sync(0xffffffffu, (item0 ? r0.last - r0.first : 0u) + (item1 ? r1.last - r1.first : 0u));
+      const uint32_t queued = __reduce_add_sync(0xffffffffu, (item0 ? t0l - t0f : 0u) + (item1 ? t1l - t1f : 0u));
+      if (lane == 0) {
+        uint32_t *ctr = V.counters;
+        if (n_s0) atomicAdd(ctr + C_CUT(0) + VGC_CUT_SURVIVED, n_s0);
+        if (n_s1) atomicAdd(ctr + C_CUT(1) + VGC_CUT_SURVIVED, n_s1);
+        if (n_i0) atomicAdd(ctr + C_CUT(0) + VGC_CUT_WORK, n_i0);
+        if (n_i1) atomicAdd(ctr + C_CUT(1) + VGC_CUT_WORK, n_i1);
+        if (fast_m) atomicAdd(ctr + VGC_COUNTER_FAST_EMITTED, fast_m);
+        if (tested) atomicAdd(ctr + VGC_COUNTER_MESHLETS_TESTED, tested);
+        if (queued) atomicAdd(ctr + VGC_COUNTER_MESHLETS_QUEUED, queued);
+      }
+      emit_fast(S, V, cell.slot, 0, fast0 ? r0.possible : 0u, r0.first, instance);
+      emit_fast(S, V, cell.slot, 1, fast1 ? r1.possible : 0u, r1.first, instance);
     }
     // items -> spans -> chunks: per cut, the warp's items laid end to end in lane order and cut into windows of
-    // 2^chunk_shift meshlets;
-    // a window's spans (<= 32, one per item) form one chunk of one (view, cell, cut)
+    // 2^chunk_shift meshlets; a window's spans (<= 32, one per item) form one chunk of one (view, cell, cut)
     const uint32_t n0 = item0 ? t0l - t0f : 0u, n1 = item1 ? t1l - t1f : 0u;
     const uint32_t s0 = warp_scan_incl(n0) - n0, s1 = warp_scan_incl(n1) - n1;  // starts in the laid-out items
     const uint32_t T0 = __shfl_sync(0xffffffffu, s0 + n0, 31), T1 = __shfl_sync(0xffffffffu, s1 + n1, 31);
-    if (T0 + T1 == 0) return;
+    if (T0 + T1 == 0) continue;
     const uint32_t chunk = 1u << chunk_shift;
     const uint32_t p0 = n0 ? ((s0 + n0 - 1) >> chunk_shift) - (s0 >> chunk_shift) + 1 : 0u;  // spans of this lane's item
     const uint32_t p1 = n1 ? ((s1 + n1 - 1) >> chunk_shift) - (s1 >> chunk_shift) + 1 : 0u;
@@ -895,14 +936,15 @@ __device__ __forceinline__ void instance_unit(const Scene &S0, const Scene *__re
                              span_at + (cut ? P0 : 0u) + first_span);
           }
         }
-        return;
+        continue;
       }
-      // the queue is full: chunk slots reserved below its capacity become empty records, and the unit is marked for
+      // the queue is full: chunk slots reserved below its capacity become empty records, and the pass is marked for
       // k_instances_redo, which tests its items in place
       for (uint32_t t = lane; t < N0 + N1; t += 32)
         if (chunk_at + t < Q.chunk_cap) Q.chunks[chunk_at + t] = make_uint4(0u, 0u, 0u, 0u);
+      const uint32_t bit = 2u * w + pass;
       if (lane == 0) {
-        atomicOr(overflow + (w >> 5), 1u << (w & 31));
+        atomicOr(overflow + (bit >> 5), 1u << (bit & 31));
         ctl[kCtlOverflowed] = 1;
       }
     }
@@ -911,8 +953,8 @@ __device__ __forceinline__ void instance_unit(const Scene &S0, const Scene *__re
       while (over) {
         const uint32_t j = __ffs(over) - 1;
         over &= over - 1;
-        const uint32_t inst = cell.first + ((w & 3u) << 5) + j;
-        // instance j's view-model matrix, recomputed (the same arithmetic as its lane's) rather than kept live
+        const uint32_t inst = cell.first + __shfl_sync(0xffffffffu, il, j);
+        // instance j's view-model matrix, recomputed (the same arithmetic as in the tests) rather than kept live
         float vmj[13];
         model_view(V.V, S.inst + (size_t)inst * 4, vmj, vmj[12]);
         const bool jin0 = __shfl_sync(0xffffffffu, inside0 ? 1 : 0, j) != 0;
@@ -926,11 +968,12 @@ __device__ __forceinline__ void instance_unit(const Scene &S0, const Scene *__re
   }
 }
 
-// The instance pass of GeometryPool.ts:846-913, one warp per 32 instances of a visible (view, cell) unit, taken from
-// a counter. Fast-path instances emit their meshlets; the others hand their level range to k_chunks as chunks of
-// <= 2^chunk_shift meshlets. HIST: the budget search's pass (views with a triangleBudget only): the camera cut's
-// level range over the whole threshold range, no fast path, no counters. Without the in-place test of a unit whose
-// items do not fit the queue (k_instances_redo does that), the kernel keeps to 64 registers at 8 blocks per SM.
+// The instance pass of GeometryPool.ts:846-913, one warp per 64 instances of a visible (view, cell) unit (a
+// half-unit), taken from a counter. Fast-path instances emit their meshlets; the others hand their level range to
+// k_chunks as chunks of <= 2^chunk_shift meshlets. HIST: the budget search's pass (views with a triangleBudget only):
+// the camera cut's level range over the whole threshold range, no fast path, no counters. Without the in-place test
+// of a pass whose items do not fit the queue (k_instances_redo does that), the kernel keeps to 64 registers at 8
+// blocks per SM.
 template <bool HIST, bool MULTI>
 __global__ void __launch_bounds__(128, MULTI ? 6 : 8) k_instances(Scene S0, const Scene *__restrict__ scenes,
                                                    const ViewConst *__restrict__ views,
@@ -938,17 +981,21 @@ __global__ void __launch_bounds__(128, MULTI ? 6 : 8) k_instances(Scene S0, cons
                                                    uint32_t *__restrict__ ctl, uint4 *__restrict__ queue,
                                                    uint32_t capacity, int round, uint32_t chunk_shift,
                                                    uint32_t *__restrict__ overflow) {
+  __shared__ Survivor lists[4][kHalfUnit];
   if (round > 0 && ctl[round] == 0) return;  // no view redoes a cut in this round
-  const uint32_t work = ctl[0] * 4;
+  const uint32_t work = ctl[0] * 2;
   WarpFeed<1> feed;
   feed.start(ctl + kCtlNextUnit);
-  for (uint32_t w = feed.i; w < work; w = feed.next())
+  for (uint32_t w = feed.i; w < work; w = feed.next()) {
     instance_unit<HIST, MULTI, false>(S0, scenes, views, hzbs0, units, ctl, queue, capacity, round, chunk_shift,
-                                      overflow, nullptr, w);
+                                      overflow, nullptr, lists[threadIdx.x >> 5], w, 0);
+    __syncwarp();  // the survivor list is rewritten by the next half-unit
+  }
 }
 
-// The units k_instances found the chunk queue full for (bits of `overflow`, cleared here), their items tested in place
-// by the whole warp. Launched after each pass's k_chunks; returns at once when no unit overflowed.
+// The survivor passes k_instances found the chunk queue full for (bits of `overflow`: bit 2 w + p for pass p of
+// half-unit w, cleared here), their items tested in place by the whole warp. Launched after each pass's k_chunks;
+// returns at once when nothing overflowed.
 template <bool HIST, bool MULTI>
 __global__ void __launch_bounds__(128, 4) k_instances_redo(Scene S0, const Scene *__restrict__ scenes,
                                                             const ViewConst *__restrict__ views,
@@ -957,6 +1004,7 @@ __global__ void __launch_bounds__(128, 4) k_instances_redo(Scene S0, const Scene
                                                             uint4 *__restrict__ queue, uint32_t capacity, int round,
                                                             uint32_t chunk_shift, uint32_t *__restrict__ overflow) {
   __shared__ WarpStage stage[4];
+  __shared__ Survivor lists[4][kHalfUnit];
   if (round > 0 && ctl[round] == 0) return;
   if (ctl[kCtlOverflowed] == 0) return;
   const uint32_t words = (ctl[0] * 4 + 31) / 32;
@@ -967,8 +1015,10 @@ __global__ void __launch_bounds__(128, 4) k_instances_redo(Scene S0, const Scene
     while (bits) {
       const uint32_t b = __ffs(bits) - 1;
       bits &= bits - 1;
+      const uint32_t bit = i * 32 + b;
       instance_unit<HIST, MULTI, true>(S0, scenes, views, hzbs0, units, ctl, queue, capacity, round, chunk_shift,
-                                       overflow, &stage[threadIdx.x >> 5], i * 32 + b);
+                                       overflow, &stage[threadIdx.x >> 5], lists[threadIdx.x >> 5], bit >> 1, bit & 1u);
+      __syncwarp();
     }
   }
 }
