@@ -696,9 +696,10 @@ int enqueue(vgc_context *ctx, LaunchScratch &s, uint32_t count, cudaStream_t st,
     }));
   }
   for (int round = 0; round < 3; round++) {
+    const uint32_t shift = round > 0 && kChunkShiftRetry ? kChunkShiftRetry : s.chunk_shift;
     CUDA_TRY(timed(ctx, capture, round == 0 ? VGC_KERNEL_SELECT0 : VGC_KERNEL_SELECT_RETRY, st, [&] {
       return launch_instances(S, scenes, s.d_views, s.d_units, s.d_unit_count, s.d_chunks, s.chunk_capacity, round,
-                              select_grid, s.d_overflow, st, s.chunk_shift);
+                              select_grid, s.d_overflow, st, shift);
     }));
     CUDA_TRY(timed(ctx, capture, round == 0 ? VGC_KERNEL_CHUNKS0 : VGC_KERNEL_SELECT_RETRY, st, [&] {
       return launch_chunks(S, scenes, s.d_views, s.d_chunks, s.d_unit_count, s.chunk_capacity, round, chunk_grid, st);
@@ -706,7 +707,7 @@ int enqueue(vgc_context *ctx, LaunchScratch &s, uint32_t count, cudaStream_t st,
     // units whose items did not fit the queue (returns at once when there are none)
     CUDA_TRY(timed(ctx, capture, VGC_KERNEL_SELECT_RETRY, st, [&] {
       return launch_instances_redo(S, scenes, s.d_views, s.d_units, s.d_unit_count, s.d_chunks, s.chunk_capacity,
-                                   round, s.d_overflow, redo_grid, st, s.chunk_shift);
+                                   round, s.d_overflow, redo_grid, st, shift);
     }));
     CUDA_TRY(timed(ctx, capture, VGC_KERNEL_FINISH, st, [&] {
       return launch_finish(s.d_views, count, s.d_unit_count, round, st);

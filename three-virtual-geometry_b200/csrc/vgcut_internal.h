@@ -35,6 +35,13 @@ constexpr uint32_t kMaxHzbLevels = 16;
 constexpr uint32_t kStateWords = 8;        // S_SCALE 0..1, S_FILL 2..3, S_RETRY 4..5
 constexpr uint32_t kBudgetBins = 256;
 constexpr uint32_t kChunkShiftMin = 8, kChunkShiftDefault = 9, kChunkShiftMax = 10;  // meshlets per chunk: 256..1024
+#ifndef VGC_RETRY_CHUNK_SHIFT
+// meshlets per chunk in the retry rounds: 2^shift (0: as in round 0). The few views a retry round usually redoes
+// spread over more warps with 256-meshlet chunks (a view's retry: 0.51 -> 0.49 ms per 32-view step; 64-meshlet chunks:
+// 0.48 ms, but 7% slower when most views redo)
+#define VGC_RETRY_CHUNK_SHIFT 8
+#endif
+constexpr uint32_t kChunkShiftRetry = VGC_RETRY_CHUNK_SHIFT, kChunkShiftFloor = 6;
 constexpr uint32_t kLevelSamples = 64;     // per level: samples of the meshlets in test order (item trimming)
 
 struct MeshRec {  // 96 bytes

@@ -921,19 +921,29 @@ __device__ __forceinline__ void instance_unit(const Scene &S0, const Scene *__re
             const uint32_t lo = max(st, win << chunk_shift), hi = min(st + n, (win + 1) << chunk_shift);
             dst[k] = make_uint4(flags, first + (lo - st), hi - lo, 0u);
           }
-          // chunk t starts at the span holding laid-out position t * chunk: that of the last item starting at or
-          // before it, plus the windows that item crossed before t
-          const uint32_t N = cut ? N1 : N0;
-          for (uint32_t t = 0; t < N; t++) {
-            const uint32_t X = t << chunk_shift;
-            const uint32_t owner = 31 - __clz(__ballot_sync(0xffffffffu, st <= X));
-            const uint32_t first_span = __shfl_sync(0xffffffffu, cut ? q1 : q0, owner) + t -
-                                        (__shfl_sync(0xffffffffu, st, owner) >> chunk_shift);
-            const uint32_t spans = __popc(__ballot_sync(0xffffffffu, n > 0 && st < X + chunk && st + n > X));
-            if (lane == 0)
+          // chunk t (lane t % 32) starts at the span holding laid-out position X = t * chunk: that of the last item
+          // starting at or before X, plus the windows that item crossed before t; its spans are the non-empty items
+          // meeting [X, X + chunk). The lanes' starts `st` and ends `st + n` do not decrease with the lane, so each is
+          // a search over the lanes (by shuffles).
+          const uint32_t N = cut ? N1 : N0, q = cut ? q1 : q0, e = st + n;
+          const uint32_t nonempty = __ballot_sync(0xffffffffu, n > 0);
+          for (uint32_t t0 = 0; t0 < N; t0 += 32) {
+            const uint32_t t = t0 + lane, X = t << chunk_shift;
+            uint32_t owner = 0, a = 0, b = 0;  // last lane with st <= X; with st < X + chunk; with st + n <= X
+#pragma unroll
+            for (uint32_t step = 16; step > 0; step >>= 1) {
+              if (__shfl_sync(0xffffffffu, st, owner + step) <= X) owner += step;
+              if (__shfl_sync(0xffffffffu, st, a + step) < X + chunk) a += step;
+              if (__shfl_sync(0xffffffffu, e, b + step) <= X) b += step;
+            }
+            const uint32_t o_q = __shfl_sync(0xffffffffu, q, owner), o_st = __shfl_sync(0xffffffffu, st, owner);
+            const uint32_t e0 = __shfl_sync(0xffffffffu, e, 0);
+            const uint32_t before = e0 <= X ? __popc(nonempty & ((2u << b) - 1u)) : 0u;  // items ending by X
+            const uint32_t spans = __popc(nonempty & ((2u << a) - 1u)) - before;
+            if (t < N)
               Q.chunks[chunk_at + (cut ? N0 : 0u) + t] =
                   make_uint4(unit.x, unit.y, cut | ((cut == 0 && occl_on) ? 2u : 0u) | (spans << 8),
-                             span_at + (cut ? P0 : 0u) + first_span);
+                             span_at + (cut ? P0 : 0u) + o_q + t - (o_st >> chunk_shift));
           }
         }
         continue;
@@ -1973,7 +1983,7 @@ static void instances_kernel(const Scene &S, const Scene *scenes, const ViewCons
 cudaError_t launch_instances(const Scene &S, const Scene *scenes, const ViewConst *views, const uint2 *units,
                              uint32_t *ctl, uint4 *queue, uint32_t capacity, int round, uint32_t grid,
                              uint32_t *overflow, cudaStream_t st, uint32_t chunk_shift) {
-  if (chunk_shift < kChunkShiftMin || chunk_shift > kChunkShiftMax || !overflow) return cudaErrorInvalidValue;
+  if (chunk_shift < kChunkShiftFloor || chunk_shift > kChunkShiftMax || !overflow) return cudaErrorInvalidValue;
   if (scenes)
     instances_kernel<true>(S, scenes, views, units, ctl, queue, capacity, round, grid, chunk_shift, overflow, st);
   else
@@ -1996,7 +2006,7 @@ static void instances_redo_kernel(const Scene &S, const Scene *scenes, const Vie
 cudaError_t launch_instances_redo(const Scene &S, const Scene *scenes, const ViewConst *views, const uint2 *units,
                                   uint32_t *ctl, uint4 *queue, uint32_t capacity, int round, uint32_t *overflow,
                                   uint32_t grid, cudaStream_t st, uint32_t chunk_shift) {
-  if (chunk_shift < kChunkShiftMin || chunk_shift > kChunkShiftMax || !overflow || grid == 0)
+  if (chunk_shift < kChunkShiftFloor || chunk_shift > kChunkShiftMax || !overflow || grid == 0)
     return cudaErrorInvalidValue;
   if (scenes)
     instances_redo_kernel<true>(S, scenes, views, units, ctl, queue, capacity, round, chunk_shift, overflow, grid, st);
