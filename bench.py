@@ -592,7 +592,9 @@ def run_ours(args, world, rank, local):
         hzb_mode=("each view's HZB is built from its depth image in the cut's launch sequence with mip 0 read from the "
                   "image (VGC_VIEW_DEPTH_AS_MIP0; the reference copies the depth texture into the HZB's first level: "
                   "about 30 us more per 32-view step here); draw lists identical (tested)") if occl else None,
-        gpu_launches=args.steps * ((2 if occl else 0) + 11),
+        # per step: HZB strip stream + tail (with occlusion), reset, cells, and per capacity round k_instances,
+        # k_chunks, k_instances_redo, k_finish (rounds 1-2 return at once when no view redoes)
+        gpu_launches=args.steps * ((2 if occl else 0) + 2 + 3 * 4),
         clocks=clk,
     )
     line["autotune"] = autotune_report(vg, views, sp, stream, flush, args.steps)

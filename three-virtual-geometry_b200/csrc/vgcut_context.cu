@@ -278,6 +278,9 @@ int ensure_scratch(vgc_context *ctx, LaunchScratch &s, uint32_t views, size_t un
     s.chunk_capacity = want_chunks;
   }
   if (!s.done) CUDA_TRY(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
+  if (!s.side) CUDA_TRY(cudaStreamCreateWithFlags(&s.side, cudaStreamNonBlocking));
+  if (!s.fork) CUDA_TRY(cudaEventCreateWithFlags(&s.fork, cudaEventDisableTiming));
+  if (!s.join) CUDA_TRY(cudaEventCreateWithFlags(&s.join, cudaEventDisableTiming));
   if (!s.h_ctl) {
     CUDA_TRY(cudaMallocHost(&s.h_ctl, 64));
     std::memset(s.h_ctl, 0, 64);
@@ -298,6 +301,9 @@ void free_scratch(LaunchScratch &s) {
   if (s.d_chunks) cudaFree(s.d_chunks);
   if (s.h_ctl) cudaFreeHost(s.h_ctl);
   if (s.done) cudaEventDestroy(s.done);
+  if (s.fork) cudaEventDestroy(s.fork);
+  if (s.join) cudaEventDestroy(s.join);
+  if (s.side) cudaStreamDestroy(s.side);
   s = LaunchScratch();
 }
 
@@ -674,13 +680,26 @@ int enqueue(vgc_context *ctx, LaunchScratch &s, uint32_t count, cudaStream_t st,
     CUDA_TRY(cudaMemcpyAsync(s.d_plan, s.h_plan, hzb_plan_bytes(count), cudaMemcpyHostToDevice, st));
   CUDA_TRY(timed(ctx, capture, VGC_KERNEL_RESET, st,
                  [&] { return launch_reset(s.d_views, count, s.d_unit_count, st); }));
-  if (s.hzb_w)  // after the reset, which clears the counter word a failed wait of the build reports in
+  // the HZB build (after the reset, which clears the counter word a failed wait of the build reports in) and the
+  // cell pass do not depend on each other: the cell pass runs on a second stream beside the build (a parallel branch
+  // of the captured graph), submitted after it so that the build's persistent blocks are resident first, and joins
+  // before the instance pass
+  if (s.hzb_w) {
+    CUDA_TRY(cudaEventRecord(s.fork, st));
+    CUDA_TRY(cudaStreamWaitEvent(s.side, s.fork, 0));
     CUDA_TRY(timed(ctx, capture, VGC_KERNEL_HZB, st, [&] {
       return ctx->hzb_grid ? launch_hzb_stream(s.d_plan, ctx->hzb_grid, s.d_views, count, s.hzb_tail, st)
                            : launch_hzb_views(s.d_views, count, s.hzb_w, s.hzb_h, s.hzb_tail, st);
     }));
-  CUDA_TRY(timed(ctx, capture, VGC_KERNEL_CELLS, st,
-                 [&] { return launch_cells(S, scenes, s.d_views, count, s.units_total, s.d_units, s.d_unit_count, st); }));
+  }
+  const cudaStream_t cells_st = s.hzb_w ? s.side : st;
+  CUDA_TRY(timed(ctx, capture, VGC_KERNEL_CELLS, cells_st, [&] {
+    return launch_cells(S, scenes, s.d_views, count, s.units_total, s.d_units, s.d_unit_count, cells_st);
+  }));
+  if (s.hzb_w) {
+    CUDA_TRY(cudaEventRecord(s.join, s.side));
+    CUDA_TRY(cudaStreamWaitEvent(st, s.join, 0));
+  }
   const uint32_t redo_grid = (uint32_t)ctx->sm_count * 2;
   if (s.any_budget) {  // the triangleBudget search: histogram pass, then the threshold of each budget view
     CUDA_TRY(timed(ctx, capture, VGC_KERNEL_BUDGET, st, [&] {

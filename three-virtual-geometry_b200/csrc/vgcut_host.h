@@ -85,6 +85,8 @@ struct LaunchScratch {
   };
   std::vector<PlanKey> plan_keys;
   size_t plan_maps = 0;             // byte offset of the tensor maps the keys were made for
+  cudaStream_t side = nullptr;      // the cell pass beside the HZB build (forked from and joined to the launch stream)
+  cudaEvent_t fork = nullptr, join = nullptr;
   cudaEvent_t done = nullptr;
   bool pending = false;
 };
