@@ -120,7 +120,9 @@ typedef struct vgc_view {
   uint32_t flags;               /* VGC_VIEW_* bits */
   /* Optional occluder depth of this frame (device memory, NDC depth, row 0 at the top): when set with hzb >= 0,
      the cut first builds HZB slot `hzb` from it in the same launch sequence, as the reference prepends its HZB
-     kernels to the frame's compute submission (VirtualGeometry.ts:482-484). NULL: use the slot as built. */
+     kernels to the frame's compute submission (VirtualGeometry.ts:482-484). NULL: use the slot as built. An image
+     whose width is a multiple of 4, at least 128 x 32, with a 16-byte aligned pointer is streamed in with bulk-tensor
+     copies; any other is read with plain loads (same result). */
   const float *depth;
   uint32_t depth_width, depth_height;
   /* VGC_VIEW_CASCADE: the cascade's clip matrix (light projection x light view, column-major, [0, 1] depth),
