@@ -1118,9 +1118,8 @@ SERVE_LINGER_US = 800
 
 @contextlib.contextmanager
 def driver_without_gc():
-    """Python's garbage collector paused while the serving driver paces requests and reads results: a collection
-    pass stalls the driver thread (not the native server) for milliseconds, which at thousands of requests per second
-    shows up as tail latency of the server."""
+    """Python's garbage collector paused while the serving driver paces requests and reads results, so that no
+    collection pass delays a submission or a read-out (the server itself is native)."""
     gc.collect()
     gc.disable()
     try:
