@@ -300,7 +300,7 @@ def hzb_build(depth: np.ndarray):
 def make_view(camera, params, max_drawn=1 << 20, index_capacity=(30_000_000, 12_000_000), hzb=None, state=None,
               pin_state: bool = False) -> _View:
     """The oracle's view of a camera and levers. `pin_state`: one round at `state` (no capacity check, retry or
-    steer), to judge a cut's decisions at the controller state another run's final round used."""
+    steer), to assess a cut's decisions at the controller state another run's final round used."""
     v = _View()
     v.pin_state = 1 if pin_state else 0
     for i in range(16):

@@ -119,7 +119,7 @@ typedef struct vgo_view {
   uint32_t cut_state[2][2];   /* out: per cut, the controller scales (state words 0, 1) its final computation ran
                                  with (a retry round redoes only the cuts that overflowed; the steer after the last
                                  round moves state[0..1] on for the next frame) */
-  uint32_t pin_state;         /* 1: one round at `state` as given, no capacity check, retry or steer (to judge the
+  uint32_t pin_state;         /* 1: one round at `state` as given, no capacity check, retry or steer (to assess the
                                  cut's decisions at the controller state another run ended with) */
 } vgo_view;
 

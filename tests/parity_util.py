@@ -98,7 +98,7 @@ class Harness:
         checked bit for bit against the float mirror; pinning keeps one margin decision in an early round from
         moving a retried cut's scale, which would shift every decision of the view. Returns (entries per cut,
         oracle view per cut)."""
-        if getattr(params, "triangle_budget", 0.0) > 0:  # judge the cut at the threshold the search picked
+        if getattr(params, "triangle_budget", 0.0) > 0:  # assess the cut at the threshold the search picked
             import dataclasses
             params = dataclasses.replace(params, triangle_budget=0.0,
                                          error_threshold=float(self.last_view.chosen_threshold))

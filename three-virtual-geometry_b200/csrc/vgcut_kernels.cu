@@ -1504,9 +1504,8 @@ __global__ void __launch_bounds__(1024) k_hzb_tail(HzbDesc H, float *__restrict_
 // takes the contiguous strips [b T / grid, (b + 1) T / grid) of the stream's T strips.
 //
 // Warp 8 streams the strips in: lane 0 waits until the consumers released a stage (an `empty` mbarrier, one arrival
-// per consumer warp), looks up the strip's job and issues a 2D bulk-tensor copy (TMA, one CTA, no multicast) of the
-// strip from the depth image into the stage, completing on the stage's `full` mbarrier; kHzbStages strips are in
-// flight. The TMA unit fills texels past the image's edge with zeros; the consumers' reads clamp to the image, so the
+// per consumer warp), looks up the strip's job and issues a 2D bulk-tensor copy (TMA) of the strip from the depth
+// image into the block's own stage, completing on the stage's `full` mbarrier; kHzbStages strips are in flight. The TMA unit fills texels past the image's edge with zeros; the consumers' reads clamp to the image, so the
 // values are those of clamped loads. A job whose image no tensor map describes (width not a multiple of 4, pointer not
 // 16-byte aligned, or smaller than a strip) has its strips loaded by the consumers themselves, in the same pass.
 //
