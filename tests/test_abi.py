@@ -41,3 +41,39 @@ def test_engine_reports_no_device_loudly():
 def test_version_string():
     from vgcut import engine
     assert b"sm_100a" in engine.lib().vgc_version()
+
+
+STRUCTS = [("Options", "vgc_options"), ("MeshData", "vgc_mesh_data"), ("MeshOpts", "vgc_mesh_opts"), ("View", "vgc_view"),
+           ("TuneResult", "vgc_tune_result"), ("ServerOptions", "vgc_server_options"),
+           ("ServerStats", "vgc_server_stats"), ("Output", "vgc_output"), ("Stats", "vgc_stats"),
+           ("ServeResult", "vgc_serve_result")]
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """The ctypes mirrors in vgcut/engine.py have the C structs' sizes and field offsets (a C program compiled
+    against include/vgcut.h prints them)."""
+    import shutil
+    import subprocess
+    from vgcut import engine
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "vgcut.h"', "int main(void) {"]
+    want = {}
+    for py, c in STRUCTS:
+        cls = getattr(engine, py)
+        lines.append(f'  printf("{py} size %zu\\n", sizeof({c}));')
+        want[(py, "size")] = ctypes.sizeof(cls)
+        for name, _ in cls._fields_:
+            lines.append(f'  printf("{py} {name} %zu\\n", offsetof({c}, {name}));')
+            want[(py, name)] = getattr(cls, name).offset
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        py, name, value = line.split()
+        got[(py, name)] = int(value)
+    assert got == want
