@@ -43,25 +43,26 @@ def test_version_string():
     assert b"sm_100a" in engine.lib().vgc_version()
 
 
-STRUCTS = [("Options", "vgc_options"), ("MeshData", "vgc_mesh_data"), ("MeshOpts", "vgc_mesh_opts"), ("View", "vgc_view"),
-           ("TuneResult", "vgc_tune_result"), ("ServerOptions", "vgc_server_options"),
-           ("ServerStats", "vgc_server_stats"), ("Output", "vgc_output"), ("Stats", "vgc_stats"),
-           ("ServeResult", "vgc_serve_result")]
+STRUCTS = [("engine", "Options", "vgc_options"), ("engine", "MeshData", "vgc_mesh_data"),
+           ("engine", "MeshOpts", "vgc_mesh_opts"), ("engine", "View", "vgc_view"), ("engine", "TuneResult", "vgc_tune_result"),
+           ("engine", "ServerOptions", "vgc_server_options"), ("engine", "ServerStats", "vgc_server_stats"),
+           ("engine", "Output", "vgc_output"), ("engine", "Stats", "vgc_stats"), ("engine", "ServeResult", "vgc_serve_result"),
+           ("build", "_Mesh", "vgb_mesh"), ("build", "_Options", "vgb_options"), ("build", "_Raw", "vgb_raw")]
 
 
 def test_struct_layouts_match_the_header(tmp_path):
-    """The ctypes mirrors in vgcut/engine.py have the C structs' sizes and field offsets (a C program compiled
-    against include/vgcut.h prints them)."""
+    """The ctypes mirrors in vgcut/engine.py and vgcut/build.py have the C structs' sizes and field offsets (a C
+    program compiled against include/vgcut.h and include/vgbuild.h prints them)."""
+    import importlib
     import shutil
     import subprocess
-    from vgcut import engine
     cc = shutil.which("gcc") or shutil.which("cc")
     if cc is None:
         pytest.skip("no C compiler")
-    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "vgcut.h"', "int main(void) {"]
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "vgcut.h"', '#include "vgbuild.h"', "int main(void) {"]
     want = {}
-    for py, c in STRUCTS:
-        cls = getattr(engine, py)
+    for mod, py, c in STRUCTS:
+        cls = getattr(importlib.import_module("vgcut." + mod), py)
         lines.append(f'  printf("{py} size %zu\\n", sizeof({c}));')
         want[(py, "size")] = ctypes.sizeof(cls)
         for name, _ in cls._fields_:
