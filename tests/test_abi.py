@@ -44,9 +44,10 @@ def test_version_string():
 
 
 STRUCTS = [("engine", "Options", "vgc_options"), ("engine", "MeshData", "vgc_mesh_data"),
-           ("engine", "MeshOpts", "vgc_mesh_opts"), ("engine", "View", "vgc_view"), ("engine", "TuneResult", "vgc_tune_result"),
-           ("engine", "ServerOptions", "vgc_server_options"), ("engine", "ServerStats", "vgc_server_stats"),
-           ("engine", "Output", "vgc_output"), ("engine", "Stats", "vgc_stats"), ("engine", "ServeResult", "vgc_serve_result"),
+           ("engine", "MeshOpts", "vgc_mesh_opts"), ("engine", "View", "vgc_view"),
+           ("engine", "TuneResult", "vgc_tune_result"), ("engine", "ServerOptions", "vgc_server_options"),
+           ("engine", "ServerStats", "vgc_server_stats"), ("engine", "Output", "vgc_output"),
+           ("engine", "Stats", "vgc_stats"), ("engine", "ServeResult", "vgc_serve_result"),
            ("build", "_Mesh", "vgb_mesh"), ("build", "_Options", "vgb_options"), ("build", "_Raw", "vgb_raw")]
 
 
@@ -59,7 +60,8 @@ def test_struct_layouts_match_the_header(tmp_path):
     cc = shutil.which("gcc") or shutil.which("cc")
     if cc is None:
         pytest.skip("no C compiler")
-    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "vgcut.h"', '#include "vgbuild.h"', "int main(void) {"]
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "vgcut.h"', '#include "vgbuild.h"',
+             "int main(void) {"]
     want = {}
     for mod, py, c in STRUCTS:
         cls = getattr(importlib.import_module("vgcut." + mod), py)
