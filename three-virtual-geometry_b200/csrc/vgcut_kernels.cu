@@ -707,23 +707,28 @@ __device__ __forceinline__ void drain_queue(const Scene &S, const ViewConst &V, 
     bool inside;
     frame_vm(F, q.span[lane], VM, instance, inside);
     const float4 er = __ldg(S.m_err + pos);
+    const float4 cs = __ldg(S.m_cull + pos);
+    float c[3];
+    xform(VM, cs.x, cs.y, cs.z, c);
+    const float r = cs.w * VM[12];
+    // visible: the culling sphere against the frustum and, for the camera cut, the HZB; a meshlet is drawn when it
+    // is visible and its fade range [lo, hi) is not empty, so the fade steps (a division and a log each) are taken
+    // only for the visible ones
+    const bool visible = !(V.frustum && !inside && !(frustum(V, c, cut == 1) >= -r)) &&
+                         !(cut == 0 && occluded(V, hzbs, high0, occl_on, c, r));
     if (HIST) {
       lo = __float_as_uint(q.own[lane]);
       hi = __float_as_uint(q.parent[lane]);
-    } else if (fs > 0.0f) {
-      lo = fade_step(err_value((er.x * VM[12]) * V.proj_scale, q.own[lane], er.x), inv_low, fs);
-      hi = fade_step(err_value((er.y * VM[12]) * V.proj_scale, q.parent[lane], er.y), inv_low, fs);
+      drawn = visible;
+    } else if (visible) {
+      if (fs > 0.0f) {
+        lo = fade_step(err_value((er.x * VM[12]) * V.proj_scale, q.own[lane], er.x), inv_low, fs);
+        hi = fade_step(err_value((er.y * VM[12]) * V.proj_scale, q.parent[lane], er.y), inv_low, fs);
+      }
+      drawn = hi > lo;
     }
-    if (HIST || hi > lo) {
-      const float4 cs = __ldg(S.m_cull + pos);
-      id = __float_as_uint(er.w);
-      packed = HIST ? __float_as_uint(er.z) : (__float_as_uint(er.z) | (lo << 8) | (hi << 16));
-      float c[3];
-      xform(VM, cs.x, cs.y, cs.z, c);
-      const float r = cs.w * VM[12];
-      drawn = !(V.frustum && !inside && !(frustum(V, c, cut == 1) >= -r)) &&
-              !(cut == 0 && occluded(V, hzbs, high0, occl_on, c, r));
-    }
+    id = __float_as_uint(er.w);
+    packed = HIST ? __float_as_uint(er.z) : (__float_as_uint(er.z) | (lo << 8) | (hi << 16));
   }
   if (HIST) {
     warp_hist_add(V.hist, drawn, lo, packed);
